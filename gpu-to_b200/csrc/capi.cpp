@@ -1,0 +1,402 @@
+// The C ABI of include/gputo.h.
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "solver.h"
+
+using gputo::Grid;
+using gputo::Solver;
+
+struct gputo_solver {
+    Solver s;
+};
+
+namespace gputo {
+
+static thread_local std::string g_last_error;
+static std::atomic<long long> g_launches{0};
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+int cuda_status(cudaError_t e, const char *what)
+{
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? GPUTO_ERR_OOM : GPUTO_ERR_CUDA;
+}
+
+void count_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+long long launches_issued() { return g_launches.load(std::memory_order_relaxed); }
+
+// The kernels are built for sm_100a only; refuse other devices up front
+// instead of failing on the first launch.
+static int check_device()
+{
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        set_error("no CUDA device is visible");
+        return GPUTO_ERR_NO_DEVICE;
+    }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int major = 0, minor = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
+    if (major != 10 || minor != 0) {
+        set_error("gputo is built for sm_100a (B200); device " + std::to_string(dev) +
+                  " is sm_" + std::to_string(major) + std::to_string(minor));
+        return GPUTO_ERR_NO_DEVICE;
+    }
+    return GPUTO_OK;
+}
+
+}  // namespace gputo
+
+extern "C" {
+
+const char *gputo_status_string(int status)
+{
+    switch (status) {
+    case GPUTO_OK: return "ok";
+    case GPUTO_ERR_ARG: return "invalid argument";
+    case GPUTO_ERR_CUDA: return "CUDA error";
+    case GPUTO_ERR_OOM: return "out of device memory";
+    case GPUTO_ERR_NOT_SPD: return "coarsest-grid matrix not positive definite";
+    case GPUTO_ERR_BREAKDOWN: return "PCG breakdown";
+    case GPUTO_ERR_NO_DEVICE: return "no usable CUDA device";
+    case GPUTO_ERR_TIMEOUT: return "device wait timed out";
+    default: return "unknown status";
+    }
+}
+
+const char *gputo_last_error(void) { return gputo::g_last_error.c_str(); }
+
+const char *gputo_version(void) { return "gputo-b200 0.1 (sm_100a)"; }
+
+void gputo_default_options(gputo_options *o)
+{
+    if (!o) return;
+    o->precision = GPUTO_PREC_FP64;
+    o->nswp = 3;
+    o->omega = 0.48;
+    o->prerelax = 0.7;
+    o->nu = 0.3;
+    o->check_every = 1;
+    o->use_graph = 1;
+    o->max_coarse_dofs = 12000;
+}
+
+int gputo_solver_create(gputo_solver **out, int nelx, int nely, int nelz, int nl,
+                        const gputo_options *opt)
+{
+    if (!out) return GPUTO_ERR_ARG;
+    *out = nullptr;
+    int st = gputo::check_device();
+    if (st) return st;
+    auto *h = new gputo_solver();
+    st = h->s.create(nelx, nely, nelz, nl, opt);
+    if (st) {
+        delete h;
+        return st;
+    }
+    *out = h;
+    return GPUTO_OK;
+}
+
+void gputo_solver_destroy(gputo_solver *s) { delete s; }
+
+size_t gputo_solver_device_bytes(const gputo_solver *s) { return s ? s->s.bytes : 0; }
+
+int gputo_solver_set_problem(gputo_solver *s, const double *Ke0, const double *fixed1b, int nfd)
+{
+    if (!s) return GPUTO_ERR_ARG;
+    return s->s.set_problem(Ke0, fixed1b, nfd, s->s.own_stream);
+}
+
+int gputo_solver_setup_dev(gputo_solver *s, const double *CX, void *stream)
+{
+    if (!s || !CX) return GPUTO_ERR_ARG;
+    return s->s.setup(CX, s->s.stream(stream));
+}
+
+int gputo_solver_solve_dev(gputo_solver *s, const double *F, double *U, double tol, int maxit,
+                           double *relres, int *nit, void *stream)
+{
+    if (!s || !F || !U || !relres || !nit) return GPUTO_ERR_ARG;
+    return s->s.solve(F, U, tol, maxit, relres, nit, s->s.stream(stream), nullptr);
+}
+
+int gputo_solver_vcycle_dev(gputo_solver *s, const double *r, double *z, void *stream)
+{
+    if (!s || !r || !z) return GPUTO_ERR_ARG;
+    if (!s->s.ready) return GPUTO_ERR_ARG;
+    cudaStream_t st = s->s.stream(stream);
+    s->s.vcycle(r, z, nullptr, st);
+    GPUTO_CUDA(cudaStreamSynchronize(st));
+    GPUTO_CUDA(cudaGetLastError());
+    return GPUTO_OK;
+}
+
+int gputo_solver_apply_dev(gputo_solver *s, const double *u, double *r, void *stream)
+{
+    if (!s || !u || !r) return GPUTO_ERR_ARG;
+    if (!s->s.ready) return GPUTO_ERR_ARG;
+    cudaStream_t st = s->s.stream(stream);
+    s->s.apply(u, r, st);
+    GPUTO_CUDA(cudaStreamSynchronize(st));
+    GPUTO_CUDA(cudaGetLastError());
+    return GPUTO_OK;
+}
+
+long long gputo_solver_launch_count(const gputo_solver *) { return gputo::launches_issued(); }
+
+// ---------------------------------------------------------------------------
+// drop-in MEX entry point with a per-shape solver cache
+// ---------------------------------------------------------------------------
+
+namespace {
+using Key = std::tuple<int, int, int, int, int, int, int, double, double, double, int, int>;
+std::mutex g_cache_mu;
+std::map<Key, std::unique_ptr<gputo_solver>> g_cache;
+std::vector<Key> g_cache_order;
+
+gputo_solver *cached_solver(int nelx, int nely, int nelz, int nl, const gputo_options &o, int *st)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    Key k{dev, nelx, nely, nelz, nl, o.precision, o.nswp, o.omega, o.prerelax, o.nu,
+          o.check_every, o.use_graph};
+    auto it = g_cache.find(k);
+    if (it != g_cache.end()) return it->second.get();
+    // keep at most two shapes resident
+    while (g_cache.size() >= 2) {
+        g_cache.erase(g_cache_order.front());
+        g_cache_order.erase(g_cache_order.begin());
+    }
+    gputo_solver *s = nullptr;
+    *st = gputo_solver_create(&s, nelx, nely, nelz, nl, &o);
+    if (*st == GPUTO_ERR_OOM) {
+        // release everything cached and try once more
+        g_cache.clear();
+        g_cache_order.clear();
+        cudaDeviceSynchronize();
+        *st = gputo_solver_create(&s, nelx, nely, nelz, nl, &o);
+    }
+    if (*st) return nullptr;
+    g_cache[k].reset(s);
+    g_cache_order.push_back(k);
+    return s;
+}
+}  // namespace
+
+int gputo_mgcg1_ex(const double *Ke0, const double *F, double *U, const double *CX,
+                   const double *fixed1b, int nfd, int nelx, int nely, int nelz, int nl,
+                   double tol, int maxit, int printLev, const gputo_options *opt, double *relres,
+                   int *nit)
+{
+    if (relres) *relres = 0.0;
+    if (nit) *nit = -1;
+    if (!Ke0 || !F || !U || !CX || (nfd > 0 && !fixed1b) || !relres || !nit || nfd < 0) {
+        gputo::set_error("null argument");
+        return GPUTO_ERR_ARG;
+    }
+    gputo_options o;
+    if (opt) o = *opt;
+    else gputo_default_options(&o);
+    auto t0 = std::chrono::steady_clock::now();
+    std::lock_guard<std::mutex> lock(g_cache_mu);
+    int st = gputo::check_device();
+    if (st) return st;
+    gputo_solver *h = cached_solver(nelx, nely, nelz, nl, o, &st);
+    if (!h) return st;
+    Solver &s = h->s;
+    cudaStream_t strm = s.own_stream;
+    FILE *log = nullptr;
+    if (printLev >= 1) log = std::fopen("mgcg1.log", "w");
+    st = s.set_problem(Ke0, fixed1b, nfd, strm);
+    if (st) {
+        if (log) std::fclose(log);
+        return st;
+    }
+    const long long nd = s.g[0].ndof(), ne = s.g[0].nel();
+    GPUTO_CUDA(cudaMemcpyAsync(s.Fw, F, sizeof(double) * nd, cudaMemcpyHostToDevice, strm));
+    GPUTO_CUDA(cudaMemcpyAsync(s.CX, CX, sizeof(double) * ne, cudaMemcpyHostToDevice, strm));
+    st = s.setup(s.CX, strm);
+    if (!st) st = s.solve(s.Fw, s.Uw, tol, maxit, relres, nit, strm, printLev >= 2 ? log : nullptr);
+    if (!st || st == GPUTO_ERR_BREAKDOWN) {
+        gputo::launch_flip_y(s.g[0].nnod(), s.Uw, strm);
+        GPUTO_CUDA(cudaMemcpyAsync(U, s.Uw, sizeof(double) * nd, cudaMemcpyDeviceToHost, strm));
+        GPUTO_CUDA(cudaStreamSynchronize(strm));
+    }
+    if (log) {
+        const double secs =
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        std::fprintf(log, "MGCG Initial residual=%12.6g\n", s.last_res0);
+        std::fprintf(log, "MGCG Nit=%d  Time %8.3g  Final residual=%12.6g\n", *nit, secs, *relres);
+        std::fclose(log);
+    }
+    return st;
+}
+
+int gputo_mgcg1(const double *Ke0, const double *F, double *U, const double *CX,
+                const double *fixed1b, int nfd, int nelx, int nely, int nelz, int nl,
+                double tol, int maxit, int printLev, double *relres, int *nit)
+{
+    return gputo_mgcg1_ex(Ke0, F, U, CX, fixed1b, nfd, nelx, nely, nelz, nl, tol, maxit, printLev,
+                          nullptr, relres, nit);
+}
+
+// ---------------------------------------------------------------------------
+// design-loop steps
+// ---------------------------------------------------------------------------
+
+namespace {
+struct Scratch {
+    double *partial = nullptr;
+    unsigned *ticket = nullptr;
+    double *scalar = nullptr;
+    cudaStream_t st = nullptr;
+    int init()
+    {
+        if (partial) return GPUTO_OK;
+        GPUTO_CUDA(cudaMalloc(&partial, sizeof(double) * 2048));
+        GPUTO_CUDA(cudaMalloc(&ticket, 16));
+        GPUTO_CUDA(cudaMalloc(&scalar, sizeof(double)));
+        GPUTO_CUDA(cudaMemset(ticket, 0, 16));
+        GPUTO_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        return GPUTO_OK;
+    }
+};
+std::mutex g_scratch_mu;
+Scratch g_scratch;
+
+bool grid_ok(int nelx, int nely, int nelz)
+{
+    return nelx > 0 && nely > 0 && nelz > 0;
+}
+}  // namespace
+
+int gputo_compliance_sens_dev(const double *Ke0, const double *U, const double *CX,
+                              const double *dsK, int nelx, int nely, int nelz, double *ce,
+                              double *dc, double *compliance, void *stream)
+{
+    if (!Ke0 || !U || !grid_ok(nelx, nely, nelz) || (dc && !dsK) || (compliance && !CX))
+        return GPUTO_ERR_ARG;
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    int st = gputo::check_device();
+    if (st) return st;
+    st = g_scratch.init();
+    if (st) return st;
+    cudaStream_t s = stream ? (cudaStream_t)stream : g_scratch.st;
+    st = gputo::upload_fine_ke(Ke0, s);
+    if (st) return st;
+    Grid g{nelx, nely, nelz};
+    gputo::launch_element_energy(g, U, CX, dsK, ce, dc, g_scratch.partial, g_scratch.ticket,
+                                 compliance ? g_scratch.scalar : nullptr, s);
+    if (compliance)
+        GPUTO_CUDA(cudaMemcpyAsync(compliance, g_scratch.scalar, sizeof(double),
+                                   cudaMemcpyDeviceToHost, s));
+    GPUTO_CUDA(cudaStreamSynchronize(s));
+    GPUTO_CUDA(cudaGetLastError());
+    return GPUTO_OK;
+}
+
+int gputo_compliance_sens(const double *Ke0, const double *U, const double *CX,
+                          const double *dsK, int nelx, int nely, int nelz, double *ce,
+                          double *dc, double *compliance)
+{
+    if (!Ke0 || !U || !grid_ok(nelx, nely, nelz) || (dc && !dsK) || (compliance && !CX))
+        return GPUTO_ERR_ARG;
+    int st = gputo::check_device();
+    if (st) return st;
+    Grid g{nelx, nely, nelz};
+    const size_t nd = (size_t)g.ndof(), ne = (size_t)g.nel();
+    double *dU = nullptr, *dCX = nullptr, *dS = nullptr, *dce = nullptr, *ddc = nullptr;
+    auto cleanup = [&]() {
+        cudaFree(dU);
+        cudaFree(dCX);
+        cudaFree(dS);
+        cudaFree(dce);
+        cudaFree(ddc);
+    };
+    if (cudaMalloc(&dU, nd * 8) || (CX && cudaMalloc(&dCX, ne * 8)) ||
+        (dsK && cudaMalloc(&dS, ne * 8)) || (ce && cudaMalloc(&dce, ne * 8)) ||
+        (dc && cudaMalloc(&ddc, ne * 8))) {
+        cudaGetLastError();
+        cleanup();
+        gputo::set_error("cudaMalloc failed in gputo_compliance_sens");
+        return GPUTO_ERR_OOM;
+    }
+    cudaMemcpy(dU, U, nd * 8, cudaMemcpyHostToDevice);
+    gputo::launch_flip_y(g.nnod(), dU, 0);  // MATLAB frame -> solver frame
+    if (CX) cudaMemcpy(dCX, CX, ne * 8, cudaMemcpyHostToDevice);
+    if (dsK) cudaMemcpy(dS, dsK, ne * 8, cudaMemcpyHostToDevice);
+    cudaDeviceSynchronize();
+    st = gputo_compliance_sens_dev(Ke0, dU, dCX, dS, nelx, nely, nelz, dce, ddc, compliance,
+                                   nullptr);
+    if (!st && ce) cudaMemcpy(ce, dce, ne * 8, cudaMemcpyDeviceToHost);
+    if (!st && dc) cudaMemcpy(dc, ddc, ne * 8, cudaMemcpyDeviceToHost);
+    cleanup();
+    return st;
+}
+
+int gputo_density_filter_dev(const double *in, const double *divisor, double *out, int nelx,
+                             int nely, int nelz, double rmin, int normalize, void *stream)
+{
+    if (!in || !out || !grid_ok(nelx, nely, nelz) || !(rmin > 0)) return GPUTO_ERR_ARG;
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    int st = gputo::check_device();
+    if (st) return st;
+    st = g_scratch.init();
+    if (st) return st;
+    cudaStream_t s = stream ? (cudaStream_t)stream : g_scratch.st;
+    const int R = (int)std::ceil(rmin) - 1;
+    if (nelx <= R || nely <= R || nelz <= R) {
+        gputo::set_error("filter radius exceeds the grid");
+        return GPUTO_ERR_ARG;
+    }
+    st = gputo::launch_filter(Grid{nelx, nely, nelz}, in, divisor, out, rmin, normalize, s);
+    if (st) return st;
+    GPUTO_CUDA(cudaStreamSynchronize(s));
+    GPUTO_CUDA(cudaGetLastError());
+    return GPUTO_OK;
+}
+
+int gputo_density_filter(const double *in, const double *divisor, double *out, int nelx,
+                         int nely, int nelz, double rmin, int normalize)
+{
+    if (!in || !out || !grid_ok(nelx, nely, nelz)) return GPUTO_ERR_ARG;
+    int st = gputo::check_device();
+    if (st) return st;
+    const size_t ne = (size_t)nelx * nely * nelz;
+    double *din = nullptr, *ddiv = nullptr, *dout = nullptr;
+    if (cudaMalloc(&din, ne * 8) || (divisor && cudaMalloc(&ddiv, ne * 8)) ||
+        cudaMalloc(&dout, ne * 8)) {
+        cudaGetLastError();
+        cudaFree(din);
+        cudaFree(ddiv);
+        cudaFree(dout);
+        gputo::set_error("cudaMalloc failed in gputo_density_filter");
+        return GPUTO_ERR_OOM;
+    }
+    cudaMemcpy(din, in, ne * 8, cudaMemcpyHostToDevice);
+    if (divisor) cudaMemcpy(ddiv, divisor, ne * 8, cudaMemcpyHostToDevice);
+    st = gputo_density_filter_dev(din, ddiv, dout, nelx, nely, nelz, rmin, normalize, nullptr);
+    if (!st) cudaMemcpy(out, dout, ne * 8, cudaMemcpyDeviceToHost);
+    cudaFree(din);
+    cudaFree(ddiv);
+    cudaFree(dout);
+    return st;
+}
+
+}  // extern "C"

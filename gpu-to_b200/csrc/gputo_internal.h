@@ -1,0 +1,163 @@
+// Internal declarations shared by the gputo kernels and the host solver.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+#include <string>
+
+#include "gputo.h"
+
+namespace gputo {
+
+constexpr int kMaxLevels = 12;
+
+// Structured hex grid of nx*ny*nz elements (the reference's nelx, nely, nelz).
+struct Grid {
+    int nx, ny, nz;
+    __host__ __device__ long long nnod() const { return (long long)(nx + 1) * (ny + 1) * (nz + 1); }
+    __host__ __device__ long long ndof() const { return 3 * nnod(); }
+    __host__ __device__ long long nel() const { return (long long)nx * ny * nz; }
+    // node n = (nz+1)(ny+1) i + (ny+1) k + j   (mgcg1.cu:966)
+    __host__ __device__ long long node(int i, int j, int k) const {
+        return ((long long)(nz + 1) * (ny + 1)) * i + (long long)(ny + 1) * k + j;
+    }
+    // element e = nz ny i + ny k + j   (mgcg1.cu:980)
+    __host__ __device__ long long elem(int i, int j, int k) const {
+        return ((long long)nz * ny) * i + (long long)ny * k + j;
+    }
+};
+
+// Element-local node a -> (x,y,z) offset, reference order (mgcg1.c:621-624):
+// 0:(0,0,0) 1:(1,0,0) 2:(1,1,0) 3:(0,1,0) 4:(0,0,1) 5:(1,0,1) 6:(1,1,1) 7:(0,1,1)
+__host__ __device__ constexpr int local_x(int a) { return (a == 1 || a == 2 || a == 5 || a == 6) ? 1 : 0; }
+__host__ __device__ constexpr int local_y(int a) { return (a == 2 || a == 3 || a == 6 || a == 7) ? 1 : 0; }
+__host__ __device__ constexpr int local_z(int a) { return a >= 4 ? 1 : 0; }
+__host__ __device__ constexpr int local_index(int x, int y, int z) { return 4 * z + (y == 0 ? x : 3 - x); }
+// Packed lower-triangular index of the symmetric 24x24 element matrix
+// (the 300-entry layout of mgcg1.cu:1302-1306).
+__host__ __device__ constexpr int packed_index(int m, int n) {
+    return m >= n ? (m * (m + 1)) / 2 + n : (n * (n + 1)) / 2 + m;
+}
+
+// Device-resident PCG scalars: the host never needs them inside an iteration.
+struct PcgScalars {
+    double res0;     // ||F||
+    double rho_p;    // r'z of the previous iteration
+    double pq;       // p'q
+    double alpha;
+    double rr;       // r'r after the update
+    double rz;       // r'z after the preconditioner
+    double rz_old;   // r'z_old, flexible (Polak-Ribiere) variant
+    double beta;
+    double relres;
+    double tol;
+    int iter;        // iterations completed
+    int maxit;
+    int done;        // 1 once converged or maxit reached
+    int nit;         // reference's return value
+    int status;      // gputo_status raised on the device (breakdown)
+    int flexible;
+};
+
+// Per-level storage of the multigrid hierarchy.
+template <typename T>
+struct LevelBuf {
+    Grid g;
+    T *u0 = nullptr, *u1 = nullptr;  // smoother iterates (ping-pong)
+    T *f = nullptr;                  // right-hand side of this level
+    T *r = nullptr;                  // defect after pre-smoothing (restriction input)
+    T *diag = nullptr;               // operator diagonal
+    T *Apk = nullptr;                // packed element matrices, [300][nel] (levels >= 1)
+    uint8_t *mask = nullptr;         // fixed-dof bits per node (bit d = dof d fixed)
+};
+
+// ---- error plumbing ------------------------------------------------------
+void set_error(const std::string &msg);
+int cuda_status(cudaError_t e, const char *what);
+#define GPUTO_CUDA(call)                                                     \
+    do {                                                                     \
+        cudaError_t _e = (call);                                             \
+        if (_e != cudaSuccess) return ::gputo::cuda_status(_e, #call);       \
+    } while (0)
+
+// ---- kernel launchers (kernels_*.cu) --------------------------------------
+// Level-0 element matrix in constant memory (FP64 and FP32 copies).
+int upload_fine_ke(const double *Ke_host, cudaStream_t st);
+int upload_design_ke(const double *Ke_host, cudaStream_t st);
+// Level-1 quadrature parts Kg[g] (packed 300 each) for nu, h = 2.
+int upload_quadrature_parts(double nu, cudaStream_t st);
+
+enum SweepMode { MODE_APPLY = 0, MODE_DEFECT = 1, MODE_JACOBI = 2, MODE_JACOBI_PRE = 3 };
+
+// Fine level (K = sum CX_e Ke), FP64 and FP32 instantiations.
+template <typename T>
+void launch_fine_sweep(int mode, const Grid &g, const T *CX, const T *u, const T *f,
+                       const T *diag, const uint8_t *mask, T *out, T omega, T prerelax,
+                       double *dot_partial, const int *done, cudaStream_t st);
+int fine_sweep_blocks(const Grid &g);
+// Coarse level (packed element matrices).
+template <typename T>
+void launch_packed_sweep(int mode, const Grid &g, const T *Apk, const T *u, const T *f,
+                         const T *diag, const uint8_t *mask, T *out, T omega, T prerelax,
+                         const int *done, cudaStream_t st);
+
+template <typename T>
+void launch_restrict(const Grid &gc, const T *rf, const uint8_t *maskc, T *fc, const int *done,
+                     cudaStream_t st);
+template <typename T>
+void launch_prolong_add(const Grid &gf, const T *uc, const uint8_t *maskf, T *uf, const int *done,
+                        cudaStream_t st);
+
+void launch_diag_fine(const Grid &g, const double *CX, double *diag, cudaStream_t st);
+template <typename T>
+void launch_diag_packed(const Grid &g, const T *Apk, T *diag, cudaStream_t st);
+void launch_build_level1(const Grid &gc, const double *CXfine, double *Apk, cudaStream_t st);
+void launch_build_galerkin(const Grid &gc, const double *Afine, double *Apk, cudaStream_t st);
+void launch_coarsest_penalty(const Grid &g, const uint8_t *mask, double *Apk, cudaStream_t st);
+void launch_assemble_dense(const Grid &g, const double *Apk, double *AQ, cudaStream_t st);
+void launch_dense_fine(const Grid &g, const double *CX, double *Apk_tmp, cudaStream_t st);
+// Cholesky + explicit inverse of the lower factor; info[0] = 0 or bad pivot (1-based).
+void launch_cholesky(int n, double *A, int *info, cudaStream_t st);
+void launch_tri_inverse(int n, const double *L, double *Linv, double *LinvT, cudaStream_t st);
+template <typename T>
+void launch_coarse_solve(int n, const double *Linv, const double *LinvT, const T *b, T *x,
+                         double *tmp, const uint8_t *mask, const int *done, cudaStream_t st);
+
+void launch_mask_from_list(long long nnod, const double *fixed1b, int nfd, uint8_t *mask,
+                           cudaStream_t st);
+void launch_mask_restrict(const Grid &gc, const uint8_t *maskf, uint8_t *maskc, cudaStream_t st);
+template <typename Tin, typename Tout>
+void launch_convert(long long n, const Tin *in, Tout *out, const int *done, cudaStream_t st);
+void launch_cast_f32(long long n, const double *in, float *out, cudaStream_t st);
+
+// PCG vector kernels (kernels_blas.cu).
+int reduce_partials_capacity();
+void launch_dot(long long n, const double *a, const double *b, double *partial, unsigned *ticket,
+                PcgScalars *sc, int which, const int *done, cudaStream_t st);
+void launch_pcg_update(long long n, double *U, double *R, const double *P, const double *Q,
+                       double *partial, unsigned *ticket, PcgScalars *sc, cudaStream_t st);
+void launch_p_update(long long n, const double *Z, double *P, double *Zold, const PcgScalars *sc,
+                     cudaStream_t st);
+void launch_dot2(long long n, const double *r, const double *z, const double *zold, double *partial,
+                 unsigned *ticket, PcgScalars *sc, const int *done, cudaStream_t st);
+void launch_pcg_init(long long n, const double *F, double *U, double *R, double *partial,
+                     unsigned *ticket, PcgScalars *sc, double tol, int maxit, int flexible,
+                     cudaStream_t st);
+void launch_finish_apply_dot(int nblocks, double *partial, unsigned *ticket, PcgScalars *sc,
+                             cudaStream_t st);
+void launch_copy(long long n, const double *a, double *b, const int *done, cudaStream_t st);
+void launch_flip_y(long long nnod, double *U, cudaStream_t st);
+
+// Design steps (kernels_design.cu).
+void launch_element_energy(const Grid &g, const double *U, const double *CX, const double *dsK,
+                           double *ce, double *dc, double *partial, unsigned *ticket,
+                           double *compliance, cudaStream_t st);
+int launch_filter(const Grid &g, const double *in, const double *div, double *out, double rmin,
+                  int normalize, cudaStream_t st);
+
+// Counter of kernel launches issued by this library (per process).
+void count_launches(long long n);
+long long launches_issued();
+
+}  // namespace gputo

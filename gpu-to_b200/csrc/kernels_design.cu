@@ -1,0 +1,182 @@
+// Design-loop steps that the MATLAB driver runs around the solve
+// (Cantilever/TOP3D125MGCGCUDA/top3D125modCuda.m:95-96,109,139-141,163).
+#include "gputo_internal.h"
+
+#include <cmath>
+#include <vector>
+
+namespace gputo {
+
+// Element matrix for the energy kernel.  Constant memory is per translation
+// unit without relocatable device code, so this file keeps its own copy,
+// written by upload_fine_ke() together with the solver's.
+__constant__ double cKeD[576];
+
+int upload_design_ke(const double *Ke_host, cudaStream_t st)
+{
+    GPUTO_CUDA(cudaMemcpyToSymbolAsync(cKeD, Ke_host, sizeof(double) * 576, 0,
+                                       cudaMemcpyHostToDevice, st));
+    return GPUTO_OK;
+}
+
+constexpr int kMaxFilterRadius = 6;           // stencil up to 13^3
+constexpr int kFilterW = 2 * kMaxFilterRadius + 1;
+__constant__ double cFilterH[kFilterW * kFilterW * kFilterW];
+
+// ce_e = u_e^T Ke u_e, dc_e = dsK_e ce_e, and sum_e CX_e ce_e.  Thread per
+// element; Ke from constant memory.  U is in the solver frame: the driver's
+// U(cMat) gather (top3D125modCuda.m:39-41,139) lists element nodes in an order
+// mirrored in y, which matches the y-negated U the MEX hands back, so both
+// give the same ce.
+__global__ void __launch_bounds__(256)
+element_energy_kernel(Grid g, const double *__restrict__ U, const double *__restrict__ CX,
+                      const double *__restrict__ dsK, double *__restrict__ ce,
+                      double *__restrict__ dc, double *__restrict__ partial, unsigned *ticket,
+                      double *compliance)
+{
+    __shared__ double red[8];
+    __shared__ bool is_last;
+    const long long nel = g.nel();
+    double csum = 0.0;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nel;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long t = e / g.ny;
+        const int j = (int)(e - t * g.ny);
+        const int i = (int)(t / g.nz);
+        const int k = (int)(t - (long long)i * g.nz);
+        double ue[24];
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+            const long long n = g.node(i + local_x(a), j + local_y(a), k + local_z(a));
+#pragma unroll
+            for (int d = 0; d < 3; ++d) ue[3 * a + d] = U[3 * n + d];
+        }
+        double s = 0.0;
+#pragma unroll 4
+        for (int m = 0; m < 24; ++m) {
+            double tm = 0.0;
+#pragma unroll
+            for (int q = 0; q < 24; ++q) tm = fma(cKeD[m * 24 + q], ue[q], tm);
+            s = fma(ue[m], tm, s);
+        }
+        if (ce) ce[e] = s;
+        if (dc) dc[e] = dsK[e] * s;
+        if (CX) csum = fma(CX[e], s, csum);
+    }
+    if (!compliance) return;
+    for (int o = 16; o > 0; o >>= 1) csum += __shfl_xor_sync(0xffffffffu, csum, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = csum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[w];
+        partial[blockIdx.x] = v;
+        __threadfence();
+        is_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (is_last && threadIdx.x == 0) {
+        __threadfence();
+        double v = 0.0;
+        for (unsigned b = 0; b < gridDim.x; ++b) v += partial[b];
+        *compliance = v;
+        *ticket = 0;
+    }
+}
+
+void launch_element_energy(const Grid &g, const double *U, const double *CX, const double *dsK,
+                           double *ce, double *dc, double *partial, unsigned *ticket,
+                           double *compliance, cudaStream_t st)
+{
+    long long nb = (g.nel() + 255) / 256;
+    if (nb > 1184) nb = 1184;
+    if (nb < 1) nb = 1;
+    element_energy_kernel<<<(unsigned)nb, 256, 0, st>>>(g, U, CX, dsK, ce, dc, partial, ticket,
+                                                         compliance);
+    count_launches(1);
+}
+
+// MATLAB 'symmetric' padding: mirror including the edge sample.
+__device__ __forceinline__ int mirror_index(int i, int n)
+{
+    while (i < 0 || i >= n) {
+        if (i < 0) i = -1 - i;
+        if (i >= n) i = 2 * n - 1 - i;
+    }
+    return i;
+}
+
+// out = correlate(in ./ div, h) [/ sum h], elements in (y fastest) order.
+// Thread per element; the stencil weights live in constant memory.
+template <int R>
+__global__ void __launch_bounds__(256)
+filter_kernel(Grid g, const double *__restrict__ in, const double *__restrict__ div,
+              double *__restrict__ out, double scale)
+{
+    const long long nel = g.nel();
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nel) return;
+    const long long t = e / g.ny;
+    const int j = (int)(e - t * g.ny);
+    const int i = (int)(t / g.nz);
+    const int k = (int)(t - (long long)i * g.nz);
+    constexpr int W = 2 * R + 1;
+    double acc = 0.0;
+#pragma unroll
+    for (int a = -R; a <= R; ++a) {
+        const int ii = mirror_index(i + a, g.nx);
+#pragma unroll
+        for (int c = -R; c <= R; ++c) {
+            const int kk = mirror_index(k + c, g.nz);
+#pragma unroll
+            for (int b = -R; b <= R; ++b) {
+                const int jj = mirror_index(j + b, g.ny);
+                const long long s = g.elem(ii, jj, kk);
+                const double v = div ? in[s] / div[s] : in[s];
+                acc = fma(cFilterH[((a + R) * W + (b + R)) * W + (c + R)], v, acc);
+            }
+        }
+    }
+    out[e] = acc * scale;
+}
+
+int launch_filter(const Grid &g, const double *in, const double *div, double *out, double rmin,
+                  int normalize, cudaStream_t st)
+{
+    const int R = (int)std::ceil(rmin) - 1;
+    if (R < 0 || R > kMaxFilterRadius) return GPUTO_ERR_ARG;
+    const int W = 2 * R + 1;
+    std::vector<double> h((size_t)W * W * W);
+    double hs = 0.0;
+    for (int a = -R; a <= R; ++a)
+        for (int b = -R; b <= R; ++b)
+            for (int c = -R; c <= R; ++c) {
+                const double v = rmin - std::sqrt((double)(a * a + b * b + c * c));
+                const double w = v > 0 ? v : 0.0;
+                h[((a + R) * W + (b + R)) * W + (c + R)] = w;
+                hs += w;
+            }
+    static double last_rmin = -1.0;
+    if (rmin != last_rmin) {
+        GPUTO_CUDA(cudaMemcpyToSymbolAsync(cFilterH, h.data(), sizeof(double) * h.size(), 0,
+                                           cudaMemcpyHostToDevice, st));
+        GPUTO_CUDA(cudaStreamSynchronize(st));
+        last_rmin = rmin;
+    }
+    const double scale = normalize ? 1.0 / hs : 1.0;
+    const int bs = 256;
+    const unsigned nb = (unsigned)((g.nel() + bs - 1) / bs);
+    switch (R) {
+    case 0: filter_kernel<0><<<nb, bs, 0, st>>>(g, in, div, out, scale); break;
+    case 1: filter_kernel<1><<<nb, bs, 0, st>>>(g, in, div, out, scale); break;
+    case 2: filter_kernel<2><<<nb, bs, 0, st>>>(g, in, div, out, scale); break;
+    case 3: filter_kernel<3><<<nb, bs, 0, st>>>(g, in, div, out, scale); break;
+    case 4: filter_kernel<4><<<nb, bs, 0, st>>>(g, in, div, out, scale); break;
+    case 5: filter_kernel<5><<<nb, bs, 0, st>>>(g, in, div, out, scale); break;
+    default: filter_kernel<6><<<nb, bs, 0, st>>>(g, in, div, out, scale); break;
+    }
+    count_launches(1);
+    return GPUTO_OK;
+}
+
+}  // namespace gputo

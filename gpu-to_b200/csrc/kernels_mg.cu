@@ -1,0 +1,879 @@
+// Multigrid kernels: operator sweeps, grid transfers and hierarchy setup.
+//
+// Every operator kernel is a node-centred gather over the (up to) 8 elements
+// around a node, as the reference's multAV0c/defect0c/defectc
+// (Cantilever/TOP3D125MGCGCUDA/mgcg1.cu:941-997,1208-1324): one thread owns a
+// node's three rows, so no atomics are needed.  Unlike the reference (one
+// thread per dof, Ke read with a divergent row index), a thread computes all
+// three rows of its node, the element-local row block is warp-uniform and Ke
+// is read from constant memory as an instruction operand, and the damped
+// Jacobi update (mgcg1.cu:1199-1206) and Dirichlet zeroing (ZeroBCc,
+// :1326-1331) are fused into the sweep's epilogue.
+#include "gputo_internal.h"
+
+namespace gputo {
+
+__constant__ double cKe64[576];
+__constant__ float cKe32[576];
+// Level-1 quadrature parts: Kg[g] packed (300), g = 4 ix + 2 iz + iy.
+__constant__ double cKg[8 * 300];
+// Prolongation weights of a coarse element onto its 8 children:
+// cPc[c][b][a] = weight of coarse local node a at child c's local node b.
+__constant__ double cPc[8 * 8 * 8];
+
+template <typename T> __device__ __forceinline__ T ke(int idx);
+template <> __device__ __forceinline__ double ke<double>(int idx) { return cKe64[idx]; }
+template <> __device__ __forceinline__ float ke<float>(int idx) { return cKe32[idx]; }
+
+int upload_fine_ke(const double *Ke_host, cudaStream_t st)
+{
+    static double last[576];
+    static bool have = false;
+    // Ke0 is an argument of every MEX call; skip the copy when it repeats.
+    bool same = have;
+    for (int m = 0; same && m < 576; ++m) same = (last[m] == Ke_host[m]);
+    if (same) return GPUTO_OK;
+    float kf[576];
+    for (int m = 0; m < 576; ++m) {
+        last[m] = Ke_host[m];
+        kf[m] = (float)Ke_host[m];
+    }
+    have = true;
+    GPUTO_CUDA(cudaMemcpyToSymbolAsync(cKe64, last, sizeof(last), 0, cudaMemcpyHostToDevice, st));
+    GPUTO_CUDA(cudaMemcpyToSymbolAsync(cKe32, kf, sizeof(kf), 0, cudaMemcpyHostToDevice, st));
+    const int s2 = upload_design_ke(last, st);
+    if (s2) return s2;
+    GPUTO_CUDA(cudaStreamSynchronize(st));
+    return GPUTO_OK;
+}
+
+// ---------------------------------------------------------------------------
+// host-side element algebra for the constant tables
+// ---------------------------------------------------------------------------
+
+// B^T D B at one Gauss point of an h*h*h hex, E=1 (the integrand of
+// mgcg1.c:1370-1418 Kem3 and mgcg1.cu:2000-2040 prepAelm).
+static void gauss_part(double nu, double h, int ix, int iy, int iz, double K[24][24])
+{
+    const double gp[2] = {-0.5773502691896257645, 0.5773502691896257645};
+    const double s = gp[ix], e = gp[iy], t = gp[iz];
+    double B[6][24] = {};
+    for (int a = 0; a < 8; ++a) {
+        const double xa = 2 * local_x(a) - 1, ya = 2 * local_y(a) - 1, za = 2 * local_z(a) - 1;
+        const double fx = 1 + xa * s, fy = 1 + ya * e, fz = 1 + za * t;
+        const double dx = 0.25 * xa * fy * fz / h, dy = 0.25 * ya * fx * fz / h,
+                     dz = 0.25 * za * fx * fy / h;
+        B[0][3 * a] = dx;
+        B[1][3 * a + 1] = dy;
+        B[2][3 * a + 2] = dz;
+        B[3][3 * a] = dy;
+        B[3][3 * a + 1] = dx;
+        B[4][3 * a + 1] = dz;
+        B[4][3 * a + 2] = dy;
+        B[5][3 * a] = dz;
+        B[5][3 * a + 2] = dx;
+    }
+    const double c = 1.0 / ((1.0 + nu) * (1.0 - 2.0 * nu));
+    double D[6][6] = {};
+    for (int p = 0; p < 3; ++p)
+        for (int q = 0; q < 3; ++q) D[p][q] = c * (p == q ? 1.0 - nu : nu);
+    for (int p = 3; p < 6; ++p) D[p][p] = c * (1.0 - 2.0 * nu) / 2.0;
+    const double w = h * h * h / 8.0;
+    for (int m = 0; m < 24; ++m)
+        for (int n = 0; n <= m; ++n) {
+            double acc = 0.0;
+            for (int p = 0; p < 6; ++p) {
+                double db = 0.0;
+                for (int q = 0; q < 6; ++q) db += D[p][q] * B[q][n];
+                acc += B[p][m] * db;
+            }
+            K[m][n] = K[n][m] = w * acc;
+        }
+}
+
+int upload_quadrature_parts(double nu, cudaStream_t st)
+{
+    static double last_nu = -1.0;
+    if (nu == last_nu) return GPUTO_OK;
+    static double kg[8 * 300];
+    for (int ix = 0; ix < 2; ++ix)
+        for (int iz = 0; iz < 2; ++iz)
+            for (int iy = 0; iy < 2; ++iy) {
+                double K[24][24];
+                gauss_part(nu, 2.0, ix, iy, iz, K);
+                const int g = 4 * ix + 2 * iz + iy;
+                for (int m = 0; m < 24; ++m)
+                    for (int n = 0; n <= m; ++n) kg[g * 300 + packed_index(m, n)] = K[m][n];
+            }
+    static double pc[512];
+    for (int c = 0; c < 8; ++c)
+        for (int b = 0; b < 8; ++b)
+            for (int a = 0; a < 8; ++a) {
+                const int px = local_x(c) + local_x(b), py = local_y(c) + local_y(b),
+                          pz = local_z(c) + local_z(b);
+                const double wx = 1.0 - 0.5 * abs(px - 2 * local_x(a));
+                const double wy = 1.0 - 0.5 * abs(py - 2 * local_y(a));
+                const double wz = 1.0 - 0.5 * abs(pz - 2 * local_z(a));
+                pc[(c * 8 + b) * 8 + a] = (wx > 0 && wy > 0 && wz > 0) ? wx * wy * wz : 0.0;
+            }
+    GPUTO_CUDA(cudaMemcpyToSymbolAsync(cKg, kg, sizeof(kg), 0, cudaMemcpyHostToDevice, st));
+    GPUTO_CUDA(cudaMemcpyToSymbolAsync(cPc, pc, sizeof(pc), 0, cudaMemcpyHostToDevice, st));
+    GPUTO_CUDA(cudaStreamSynchronize(st));
+    last_nu = nu;
+    return GPUTO_OK;
+}
+
+// ---------------------------------------------------------------------------
+// fine-level sweep: K = sum_e CX_e Ke
+// ---------------------------------------------------------------------------
+
+// CTA tile of nodes: 32 (y) x 4 (z) x 2 (x); halo of one node / element.
+constexpr int TY = 32, TZ = 4, TX = 2;
+constexpr int HY = TY + 2, HZ = TZ + 2, HX = TX + 2;
+constexpr int EY = TY + 1, EZ = TZ + 1, EX = TX + 1;
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(TY *TZ *TX)
+fine_sweep_kernel(Grid g, const T *__restrict__ CX, const T *__restrict__ u,
+                  const T *__restrict__ f, const T *__restrict__ diag,
+                  const uint8_t *__restrict__ mask, T *__restrict__ out, T omega, T prerelax,
+                  double *__restrict__ dot_partial, const int *__restrict__ done)
+{
+    if (done && *done) return;
+    __shared__ T su[HX][HZ][HY * 3];
+    __shared__ T sc[EX][EZ][EY];
+
+    const int j0 = blockIdx.x * TY, k0 = blockIdx.y * TZ, i0 = blockIdx.z * TX;
+    const int tid = threadIdx.x + TY * (threadIdx.y + TZ * threadIdx.z);
+    constexpr int NT = TY * TZ * TX;
+
+    // halo of u: rows of HY consecutive nodes (3*HY consecutive values in memory)
+    for (int idx = tid; idx < HX * HZ * HY * 3; idx += NT) {
+        const int row = idx / (HY * 3), col = idx - row * (HY * 3);
+        const int hx = row / HZ, hz = row - hx * HZ;
+        const int hy = col / 3, d = col - 3 * hy;
+        const int i = i0 - 1 + hx, k = k0 - 1 + hz, j = j0 - 1 + hy;
+        T v = T(0);
+        if (i >= 0 && i <= g.nx && k >= 0 && k <= g.nz && j >= 0 && j <= g.ny) {
+            const long long dof = 3 * g.node(i, j, k) + d;
+            if (MODE == MODE_JACOBI_PRE)
+                v = prerelax * f[dof] / diag[dof];
+            else
+                v = u[dof];
+        }
+        su[hx][hz][col] = v;
+    }
+    for (int idx = tid; idx < EX * EZ * EY; idx += NT) {
+        const int row = idx / EY, ey = idx - row * EY;
+        const int ex = row / EZ, ez = row - ex * EZ;
+        const int i = i0 - 1 + ex, k = k0 - 1 + ez, j = j0 - 1 + ey;
+        T v = T(0);
+        if (i >= 0 && i < g.nx && k >= 0 && k < g.nz && j >= 0 && j < g.ny) v = CX[g.elem(i, j, k)];
+        sc[ex][ez][ey] = v;
+    }
+    __syncthreads();
+
+    const int ty = threadIdx.x, tz = threadIdx.y, tx = threadIdx.z;
+    const int j = j0 + ty, k = k0 + tz, i = i0 + tx;
+    const bool active = (j <= g.ny) && (k <= g.nz) && (i <= g.nx);
+
+    T acc0 = T(0), acc1 = T(0), acc2 = T(0);
+#pragma unroll
+    for (int ex = 0; ex < 2; ++ex)
+#pragma unroll
+        for (int ez = 0; ez < 2; ++ez)
+#pragma unroll
+            for (int ey = 0; ey < 2; ++ey) {
+                const T c = sc[tx + ex][tz + ez][ty + ey];
+                const int a = local_index(1 - ex, 1 - ey, 1 - ez);
+                T t0 = T(0), t1 = T(0), t2 = T(0);
+#pragma unroll
+                for (int b = 0; b < 8; ++b) {
+                    const T *up = &su[tx + ex + local_x(b)][tz + ez + local_z(b)][(ty + ey + local_y(b)) * 3];
+                    const T u0 = up[0], u1 = up[1], u2 = up[2];
+                    const int r0 = (3 * a) * 24 + 3 * b, r1 = r0 + 24, r2 = r0 + 48;
+                    t0 = fma(ke<T>(r0), u0, fma(ke<T>(r0 + 1), u1, fma(ke<T>(r0 + 2), u2, t0)));
+                    t1 = fma(ke<T>(r1), u0, fma(ke<T>(r1 + 1), u1, fma(ke<T>(r1 + 2), u2, t1)));
+                    t2 = fma(ke<T>(r2), u0, fma(ke<T>(r2 + 1), u1, fma(ke<T>(r2 + 2), u2, t2)));
+                }
+                acc0 = fma(c, t0, acc0);
+                acc1 = fma(c, t1, acc1);
+                acc2 = fma(c, t2, acc2);
+            }
+
+    double dsum = 0.0;
+    if (active) {
+        const long long n = g.node(i, j, k);
+        const unsigned m = mask[n];
+        const T acc[3] = {acc0, acc1, acc2};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const long long dof = 3 * n + d;
+            const bool fixed = (m >> d) & 1u;
+            if (MODE == MODE_APPLY) {
+                const T q = fixed ? T(0) : acc[d];
+                out[dof] = q;
+                if (dot_partial) dsum += (double)su[tx + 1][tz + 1][(ty + 1) * 3 + d] * (double)q;
+            } else if (MODE == MODE_DEFECT) {
+                out[dof] = fixed ? T(0) : f[dof] - acc[d];
+            } else {
+                const T r = fixed ? T(0) : f[dof] - acc[d];
+                const T us = su[tx + 1][tz + 1][(ty + 1) * 3 + d];
+                out[dof] = us + omega * r / diag[dof];
+            }
+        }
+    }
+    if (MODE == MODE_APPLY && dot_partial) {
+        // block reduction of p'q in FP64, fixed order
+        __shared__ double red[NT / 32];
+        for (int o = 16; o > 0; o >>= 1) dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
+        if ((tid & 31) == 0) red[tid >> 5] = dsum;
+        __syncthreads();
+        if (tid < 32) {
+            double v = tid < NT / 32 ? red[tid] : 0.0;
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (tid == 0)
+                dot_partial[blockIdx.x + gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z)] = v;
+        }
+    }
+}
+
+template <typename T>
+void launch_fine_sweep(int mode, const Grid &g, const T *CX, const T *u, const T *f, const T *diag,
+                       const uint8_t *mask, T *out, T omega, T prerelax, double *dot_partial,
+                       const int *done, cudaStream_t st)
+{
+    dim3 block(TY, TZ, TX);
+    dim3 grid((g.ny + 1 + TY - 1) / TY, (g.nz + 1 + TZ - 1) / TZ, (g.nx + 1 + TX - 1) / TX);
+    switch (mode) {
+    case MODE_APPLY:
+        fine_sweep_kernel<T, MODE_APPLY><<<grid, block, 0, st>>>(g, CX, u, f, diag, mask, out, omega,
+                                                                 prerelax, dot_partial, done);
+        break;
+    case MODE_DEFECT:
+        fine_sweep_kernel<T, MODE_DEFECT><<<grid, block, 0, st>>>(g, CX, u, f, diag, mask, out, omega,
+                                                                  prerelax, dot_partial, done);
+        break;
+    case MODE_JACOBI:
+        fine_sweep_kernel<T, MODE_JACOBI><<<grid, block, 0, st>>>(g, CX, u, f, diag, mask, out, omega,
+                                                                  prerelax, dot_partial, done);
+        break;
+    default:
+        fine_sweep_kernel<T, MODE_JACOBI_PRE><<<grid, block, 0, st>>>(g, CX, u, f, diag, mask, out,
+                                                                      omega, prerelax, dot_partial, done);
+    }
+    count_launches(1);
+}
+
+int fine_sweep_blocks(const Grid &g)
+{
+    return ((g.ny + 1 + TY - 1) / TY) * ((g.nz + 1 + TZ - 1) / TZ) * ((g.nx + 1 + TX - 1) / TX);
+}
+
+template void launch_fine_sweep<double>(int, const Grid &, const double *, const double *,
+                                        const double *, const double *, const uint8_t *, double *,
+                                        double, double, double *, const int *, cudaStream_t);
+template void launch_fine_sweep<float>(int, const Grid &, const float *, const float *, const float *,
+                                       const float *, const uint8_t *, float *, float, float,
+                                       double *, const int *, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// coarse-level sweep: packed element matrices [300][nel]
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ void node_ijk(const Grid &g, long long n, int &i, int &j, int &k)
+{
+    const long long t = n / (g.ny + 1);
+    j = (int)(n - t * (g.ny + 1));
+    i = (int)(t / (g.nz + 1));
+    k = (int)(t - (long long)i * (g.nz + 1));
+}
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(128)
+packed_sweep_kernel(Grid g, const T *__restrict__ A, const T *__restrict__ u,
+                    const T *__restrict__ f, const T *__restrict__ diag,
+                    const uint8_t *__restrict__ mask, T *__restrict__ out, T omega, T prerelax,
+                    const int *__restrict__ done)
+{
+    if (done && *done) return;
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= g.nnod()) return;
+    int i, j, k;
+    node_ijk(g, n, i, j, k);
+    const long long nel = g.nel();
+    T acc[3] = {T(0), T(0), T(0)};
+#pragma unroll
+    for (int ex = 0; ex < 2; ++ex) {
+        const int ei = i - 1 + ex;
+        if (ei < 0 || ei >= g.nx) continue;
+#pragma unroll
+        for (int ez = 0; ez < 2; ++ez) {
+            const int ek = k - 1 + ez;
+            if (ek < 0 || ek >= g.nz) continue;
+#pragma unroll
+            for (int ey = 0; ey < 2; ++ey) {
+                const int ej = j - 1 + ey;
+                if (ej < 0 || ej >= g.ny) continue;
+                const long long e = g.elem(ei, ej, ek);
+                const int a = local_index(1 - ex, 1 - ey, 1 - ez);
+#pragma unroll
+                for (int b = 0; b < 8; ++b) {
+                    const long long nb = g.node(ei + local_x(b), ej + local_y(b), ek + local_z(b));
+                    T ub[3];
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) {
+                        const long long dof = 3 * nb + q;
+                        ub[q] = (MODE == MODE_JACOBI_PRE) ? prerelax * f[dof] / diag[dof] : u[dof];
+                    }
+#pragma unroll
+                    for (int d = 0; d < 3; ++d)
+#pragma unroll
+                        for (int q = 0; q < 3; ++q)
+                            acc[d] = fma(A[(long long)packed_index(3 * a + d, 3 * b + q) * nel + e], ub[q], acc[d]);
+                }
+            }
+        }
+    }
+    const unsigned m = mask[n];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const long long dof = 3 * n + d;
+        const bool fixed = (m >> d) & 1u;
+        if (MODE == MODE_APPLY) {
+            out[dof] = fixed ? T(0) : acc[d];
+        } else if (MODE == MODE_DEFECT) {
+            out[dof] = fixed ? T(0) : f[dof] - acc[d];
+        } else {
+            const T r = fixed ? T(0) : f[dof] - acc[d];
+            const T us = (MODE == MODE_JACOBI_PRE) ? prerelax * f[dof] / diag[dof] : u[dof];
+            out[dof] = us + omega * r / diag[dof];
+        }
+    }
+}
+
+template <typename T>
+void launch_packed_sweep(int mode, const Grid &g, const T *Apk, const T *u, const T *f,
+                         const T *diag, const uint8_t *mask, T *out, T omega, T prerelax,
+                         const int *done, cudaStream_t st)
+{
+    const int bs = 128;
+    const unsigned nb = (unsigned)((g.nnod() + bs - 1) / bs);
+    switch (mode) {
+    case MODE_APPLY:
+        packed_sweep_kernel<T, MODE_APPLY><<<nb, bs, 0, st>>>(g, Apk, u, f, diag, mask, out, omega, prerelax, done);
+        break;
+    case MODE_DEFECT:
+        packed_sweep_kernel<T, MODE_DEFECT><<<nb, bs, 0, st>>>(g, Apk, u, f, diag, mask, out, omega, prerelax, done);
+        break;
+    case MODE_JACOBI:
+        packed_sweep_kernel<T, MODE_JACOBI><<<nb, bs, 0, st>>>(g, Apk, u, f, diag, mask, out, omega, prerelax, done);
+        break;
+    default:
+        packed_sweep_kernel<T, MODE_JACOBI_PRE><<<nb, bs, 0, st>>>(g, Apk, u, f, diag, mask, out, omega, prerelax, done);
+    }
+    count_launches(1);
+}
+
+template void launch_packed_sweep<double>(int, const Grid &, const double *, const double *,
+                                          const double *, const double *, const uint8_t *, double *,
+                                          double, double, const int *, cudaStream_t);
+template void launch_packed_sweep<float>(int, const Grid &, const float *, const float *,
+                                         const float *, const float *, const uint8_t *, float *,
+                                         float, float, const int *, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// grid transfers
+// ---------------------------------------------------------------------------
+
+// F_c = P^T R_f with the full-weighting weights 2^-(|di|+|dj|+|dk|) over the 27
+// fine neighbours of each coarse node (mgcg1.cu:792-831 rstrFc), then the
+// coarse Dirichlet rows are zeroed (ZeroBCc after rstrFc, mgcg1.cu:537).
+template <typename T>
+__global__ void restrict_kernel(Grid gc, const T *__restrict__ rf, const uint8_t *__restrict__ maskc,
+                                T *__restrict__ fc, const int *__restrict__ done)
+{
+    if (done && *done) return;
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= gc.nnod()) return;
+    int i, j, k;
+    node_ijk(gc, n, i, j, k);
+    const Grid gf{2 * gc.nx, 2 * gc.ny, 2 * gc.nz};
+    T acc[3] = {T(0), T(0), T(0)};
+    for (int di = -1; di <= 1; ++di) {
+        const int fi = 2 * i + di;
+        if (fi < 0 || fi > gf.nx) continue;
+        for (int dk = -1; dk <= 1; ++dk) {
+            const int fk = 2 * k + dk;
+            if (fk < 0 || fk > gf.nz) continue;
+            for (int dj = -1; dj <= 1; ++dj) {
+                const int fj = 2 * j + dj;
+                if (fj < 0 || fj > gf.ny) continue;
+                const T w = T(1) / T(1 << (abs(di) + abs(dj) + abs(dk)));
+                const long long nf = gf.node(fi, fj, fk);
+#pragma unroll
+                for (int d = 0; d < 3; ++d) acc[d] = fma(w, rf[3 * nf + d], acc[d]);
+            }
+        }
+    }
+    const unsigned m = maskc[n];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) fc[3 * n + d] = ((m >> d) & 1u) ? T(0) : acc[d];
+}
+
+template <typename T>
+void launch_restrict(const Grid &gc, const T *rf, const uint8_t *maskc, T *fc, const int *done,
+                     cudaStream_t st)
+{
+    const int bs = 128;
+    restrict_kernel<T><<<(unsigned)((gc.nnod() + bs - 1) / bs), bs, 0, st>>>(gc, rf, maskc, fc, done);
+    count_launches(1);
+}
+template void launch_restrict<double>(const Grid &, const double *, const uint8_t *, double *,
+                                      const int *, cudaStream_t);
+template void launch_restrict<float>(const Grid &, const float *, const uint8_t *, float *,
+                                     const int *, cudaStream_t);
+
+// u_f += P u_c, trilinear (mgcg1.cu:1587-1641 interpc), then the fine
+// Dirichlet dofs are zeroed (ZeroBCc after interpc, mgcg1.cu:631).
+template <typename T>
+__global__ void prolong_kernel(Grid gf, const T *__restrict__ uc, const uint8_t *__restrict__ maskf,
+                               T *__restrict__ uf, const int *__restrict__ done)
+{
+    if (done && *done) return;
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= gf.nnod()) return;
+    int i, j, k;
+    node_ijk(gf, n, i, j, k);
+    const Grid gc{gf.nx / 2, gf.ny / 2, gf.nz / 2};
+    const int ni = (i & 1) + 1, nj = (j & 1) + 1, nk = (k & 1) + 1;
+    T acc[3] = {T(0), T(0), T(0)};
+    for (int a = 0; a < ni; ++a)
+        for (int c = 0; c < nk; ++c)
+            for (int b = 0; b < nj; ++b) {
+                const long long nc = gc.node((i >> 1) + a, (j >> 1) + b, (k >> 1) + c);
+#pragma unroll
+                for (int d = 0; d < 3; ++d) acc[d] += uc[3 * nc + d];
+            }
+    const T w = T(1) / T(ni * nj * nk);
+    const unsigned m = maskf[n];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const long long dof = 3 * n + d;
+        uf[dof] = ((m >> d) & 1u) ? T(0) : fma(w, acc[d], uf[dof]);
+    }
+}
+
+template <typename T>
+void launch_prolong_add(const Grid &gf, const T *uc, const uint8_t *maskf, T *uf, const int *done,
+                        cudaStream_t st)
+{
+    const int bs = 128;
+    prolong_kernel<T><<<(unsigned)((gf.nnod() + bs - 1) / bs), bs, 0, st>>>(gf, uc, maskf, uf, done);
+    count_launches(1);
+}
+template void launch_prolong_add<double>(const Grid &, const double *, const uint8_t *, double *,
+                                         const int *, cudaStream_t);
+template void launch_prolong_add<float>(const Grid &, const float *, const uint8_t *, float *,
+                                        const int *, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// hierarchy setup
+// ---------------------------------------------------------------------------
+
+// diag(K) on the fine level: sum over adjacent elements of CX_e Ke[m][m]
+// (mgcg1.cu:1447-1487 prepAD0c).
+__global__ void diag_fine_kernel(Grid g, const double *__restrict__ CX, double *__restrict__ diag)
+{
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= g.nnod()) return;
+    int i, j, k;
+    node_ijk(g, n, i, j, k);
+    double acc[3] = {0, 0, 0};
+    for (int ex = 0; ex < 2; ++ex)
+        for (int ez = 0; ez < 2; ++ez)
+            for (int ey = 0; ey < 2; ++ey) {
+                const int ei = i - 1 + ex, ej = j - 1 + ey, ek = k - 1 + ez;
+                if (ei < 0 || ei >= g.nx || ej < 0 || ej >= g.ny || ek < 0 || ek >= g.nz) continue;
+                const double c = CX[g.elem(ei, ej, ek)];
+                const int a = local_index(1 - ex, 1 - ey, 1 - ez);
+                for (int d = 0; d < 3; ++d) acc[d] += c * cKe64[(3 * a + d) * 25];
+            }
+    for (int d = 0; d < 3; ++d) diag[3 * n + d] = acc[d];
+}
+
+void launch_diag_fine(const Grid &g, const double *CX, double *diag, cudaStream_t st)
+{
+    const int bs = 128;
+    diag_fine_kernel<<<(unsigned)((g.nnod() + bs - 1) / bs), bs, 0, st>>>(g, CX, diag);
+    count_launches(1);
+}
+
+// diag of a packed coarse level (mgcg1.cu:1404-1445 prepADc).
+template <typename T>
+__global__ void diag_packed_kernel(Grid g, const T *__restrict__ A, T *__restrict__ diag)
+{
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= g.nnod()) return;
+    int i, j, k;
+    node_ijk(g, n, i, j, k);
+    const long long nel = g.nel();
+    T acc[3] = {0, 0, 0};
+    for (int ex = 0; ex < 2; ++ex)
+        for (int ez = 0; ez < 2; ++ez)
+            for (int ey = 0; ey < 2; ++ey) {
+                const int ei = i - 1 + ex, ej = j - 1 + ey, ek = k - 1 + ez;
+                if (ei < 0 || ei >= g.nx || ej < 0 || ej >= g.ny || ek < 0 || ek >= g.nz) continue;
+                const long long e = g.elem(ei, ej, ek);
+                const int a = local_index(1 - ex, 1 - ey, 1 - ez);
+                for (int d = 0; d < 3; ++d) acc[d] += A[(long long)packed_index(3 * a + d, 3 * a + d) * nel + e];
+            }
+    for (int d = 0; d < 3; ++d) diag[3 * n + d] = acc[d];
+}
+
+template <typename T>
+void launch_diag_packed(const Grid &g, const T *Apk, T *diag, cudaStream_t st)
+{
+    const int bs = 128;
+    diag_packed_kernel<T><<<(unsigned)((g.nnod() + bs - 1) / bs), bs, 0, st>>>(g, Apk, diag);
+    count_launches(1);
+}
+template void launch_diag_packed<double>(const Grid &, const double *, double *, cudaStream_t);
+template void launch_diag_packed<float>(const Grid &, const float *, float *, cudaStream_t);
+
+// Level 1: A_E = sum_g CX(child containing Gauss point g) Kg[g]
+// (mgcg1.cu:2042-2070 coarseAe2c).  One thread per (element, packed entry).
+__global__ void build_level1_kernel(Grid gc, const double *__restrict__ CXf, double *__restrict__ A)
+{
+    const long long nel = gc.nel();
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nel) return;
+    const long long t = e / gc.ny;
+    const int j = (int)(e - t * gc.ny);
+    const int i = (int)(t / gc.nz);
+    const int k = (int)(t - (long long)i * gc.nz);
+    const Grid gf{2 * gc.nx, 2 * gc.ny, 2 * gc.nz};
+    double cx[8];
+    for (int ix = 0; ix < 2; ++ix)
+        for (int iz = 0; iz < 2; ++iz)
+            for (int iy = 0; iy < 2; ++iy) cx[4 * ix + 2 * iz + iy] = CXf[gf.elem(2 * i + ix, 2 * j + iy, 2 * k + iz)];
+    for (int p = 0; p < 300; ++p) {
+        double acc = 0.0;
+#pragma unroll
+        for (int gq = 0; gq < 8; ++gq) acc = fma(cx[gq], cKg[gq * 300 + p], acc);
+        A[(long long)p * nel + e] = acc;
+    }
+}
+
+void launch_build_level1(const Grid &gc, const double *CXfine, double *Apk, cudaStream_t st)
+{
+    const int bs = 128;
+    build_level1_kernel<<<(unsigned)((gc.nel() + bs - 1) / bs), bs, 0, st>>>(gc, CXfine, Apk);
+    count_launches(1);
+}
+
+// Levels >= 2: Galerkin P^T A P over the 8 children of each coarse element
+// (mgcg1.cu:1678-1743 coarseAe3c), computed child by child as
+// A_E = sum_c Pc^T A_c Pc with the 8x8 node weights Pc.  One CTA of 576
+// threads per coarse element; thread t owns entry (t/24, t%24).
+__global__ void __launch_bounds__(576) build_galerkin_kernel(Grid gc, const double *__restrict__ Af,
+                                                             double *__restrict__ A)
+{
+    const long long E = blockIdx.x;
+    const long long nel = gc.nel();
+    const long long t = E / gc.ny;
+    const int j = (int)(E - t * gc.ny);
+    const int i = (int)(t / gc.nz);
+    const int k = (int)(t - (long long)i * gc.nz);
+    const Grid gf{2 * gc.nx, 2 * gc.ny, 2 * gc.nz};
+    const long long nelf = gf.nel();
+    __shared__ double S[576];
+    __shared__ double Tm[576];
+    const int tid = threadIdx.x;
+    const int m = tid / 24, n = tid - 24 * (tid / 24);
+    const int am = m / 3, p = m - 3 * am;   // row: coarse local node, component
+    const int an = n / 3, q = n - 3 * an;   // column
+    double acc = 0.0;
+    for (int c = 0; c < 8; ++c) {
+        const long long ec = gf.elem(2 * i + local_x(c), 2 * j + local_y(c), 2 * k + local_z(c));
+        S[tid] = Af[(long long)packed_index(m, n) * nelf + ec];
+        __syncthreads();
+        // Tm[(b,p)][(an,q)] = sum_b' S[(b,p)][(b',q)] Pc[b'][an]   (here m = (b,p))
+        double tv = 0.0;
+#pragma unroll
+        for (int b2 = 0; b2 < 8; ++b2) tv = fma(S[m * 24 + 3 * b2 + q], cPc[(c * 8 + b2) * 8 + an], tv);
+        Tm[tid] = tv;
+        __syncthreads();
+        // acc[(am,p)][n] += sum_b Pc[b][am] Tm[(b,p)][n]
+#pragma unroll
+        for (int b = 0; b < 8; ++b) acc = fma(cPc[(c * 8 + b) * 8 + am], Tm[(3 * b + p) * 24 + n], acc);
+        __syncthreads();
+    }
+    if (n <= m) A[(long long)packed_index(m, n) * nel + E] = acc;
+}
+
+void launch_build_galerkin(const Grid &gc, const double *Afine, double *Apk, cudaStream_t st)
+{
+    build_galerkin_kernel<<<(unsigned)gc.nel(), 576, 0, st>>>(gc, Afine, Apk);
+    count_launches(1);
+}
+
+// Fine level as packed matrices (only for a single-level hierarchy).
+__global__ void dense_fine_kernel(Grid g, const double *__restrict__ CX, double *__restrict__ A)
+{
+    const long long nel = g.nel();
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nel) return;
+    const double c = CX[e];
+    for (int m = 0; m < 24; ++m)
+        for (int n = 0; n <= m; ++n) A[(long long)packed_index(m, n) * nel + e] = c * cKe64[m * 24 + n];
+}
+
+void launch_dense_fine(const Grid &g, const double *CX, double *Apk, cudaStream_t st)
+{
+    const int bs = 128;
+    dense_fine_kernel<<<(unsigned)((g.nel() + bs - 1) / bs), bs, 0, st>>>(g, CX, Apk);
+    count_launches(1);
+}
+
+// Dirichlet penalty on the coarsest element matrices (mgcg1.cu:1368-1402
+// CorrCsAc).  For a fixed dof of node (i,j,k) and each adjacent element
+// (i+di, j+dj, k+dk), the reference writes 1e10 on the diagonal of the
+// element-local node with offset (-di, 1+dj, -dk) -- its lookup table is the
+// true local index mirrored in y -- and this kernel penalises the same
+// entries.  Concurrent writers store the same value.
+__global__ void penalty_kernel(Grid g, const uint8_t *__restrict__ mask, double *__restrict__ A)
+{
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= g.nnod()) return;
+    const unsigned mk = mask[n];
+    if (!mk) return;
+    int i, j, k;
+    node_ijk(g, n, i, j, k);
+    const long long nel = g.nel();
+    for (int d = 0; d < 3; ++d) {
+        if (!((mk >> d) & 1u)) continue;
+        for (int di = -1; di <= 0; ++di)
+            for (int dk = -1; dk <= 0; ++dk)
+                for (int dj = -1; dj <= 0; ++dj) {
+                    const int ei = i + di, ej = j + dj, ek = k + dk;
+                    if (ei < 0 || ei >= g.nx || ej < 0 || ej >= g.ny || ek < 0 || ek >= g.nz) continue;
+                    const int a = local_index(-di, 1 + dj, -dk);
+                    const int mm = 3 * a + d;
+                    A[(long long)packed_index(mm, mm) * nel + g.elem(ei, ej, ek)] = 1e10;
+                }
+    }
+}
+
+void launch_coarsest_penalty(const Grid &g, const uint8_t *mask, double *Apk, cudaStream_t st)
+{
+    const int bs = 128;
+    penalty_kernel<<<(unsigned)((g.nnod() + bs - 1) / bs), bs, 0, st>>>(g, mask, Apk);
+    count_launches(1);
+}
+
+// Dense coarsest matrix, one thread per row (mgcg1.cu:1747-1806 assembAc).
+__global__ void assemble_dense_kernel(Grid g, const double *__restrict__ A, double *__restrict__ AQ)
+{
+    const long long row = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long N = g.ndof();
+    if (row >= N) return;
+    const long long n = row / 3;
+    const int d = (int)(row - 3 * n);
+    int i, j, k;
+    node_ijk(g, n, i, j, k);
+    const long long nel = g.nel();
+    double *out = AQ + row * N;
+    for (long long c = 0; c < N; ++c) out[c] = 0.0;
+    for (int ex = 0; ex < 2; ++ex)
+        for (int ez = 0; ez < 2; ++ez)
+            for (int ey = 0; ey < 2; ++ey) {
+                const int ei = i - 1 + ex, ej = j - 1 + ey, ek = k - 1 + ez;
+                if (ei < 0 || ei >= g.nx || ej < 0 || ej >= g.ny || ek < 0 || ek >= g.nz) continue;
+                const long long e = g.elem(ei, ej, ek);
+                const int a = local_index(1 - ex, 1 - ey, 1 - ez);
+                for (int b = 0; b < 8; ++b) {
+                    const long long nb = g.node(ei + local_x(b), ej + local_y(b), ek + local_z(b));
+                    for (int q = 0; q < 3; ++q)
+                        out[3 * nb + q] += A[(long long)packed_index(3 * a + d, 3 * b + q) * nel + e];
+                }
+            }
+}
+
+void launch_assemble_dense(const Grid &g, const double *Apk, double *AQ, cudaStream_t st)
+{
+    const int bs = 64;
+    assemble_dense_kernel<<<(unsigned)((g.ndof() + bs - 1) / bs), bs, 0, st>>>(g, Apk, AQ);
+    count_launches(1);
+}
+
+// Right-looking Cholesky of the dense coarsest matrix by one CTA, in place
+// (lower triangle).  Textbook algorithm: scale the pivot column, stage it in
+// shared memory, then one warp per trailing row subtracts the rank-1 update
+// with coalesced row accesses.  info = 1-based index of the first non-positive
+// pivot, 0 on success.  (The reference launches one kernel per row,
+// mgcg1.cu:2099-2142.)
+__global__ void __launch_bounds__(1024) cholesky_kernel(int n, double *__restrict__ A, int *info)
+{
+    extern __shared__ double colv[];
+    __shared__ double piv;
+    __shared__ int bad;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
+    if (tid == 0) bad = 0;
+    __syncthreads();
+    for (int c = 0; c < n; ++c) {
+        if (tid == 0) {
+            const double s = A[(long long)c * n + c];
+            if (!(s > 0.0)) {
+                bad = c + 1;
+                piv = 1.0;
+            } else {
+                piv = sqrt(s);
+            }
+            A[(long long)c * n + c] = piv;
+        }
+        __syncthreads();
+        if (bad) break;
+        const double dinv = 1.0 / piv;
+        for (int r = c + 1 + tid; r < n; r += nt) {
+            const double v = A[(long long)r * n + c] * dinv;
+            A[(long long)r * n + c] = v;
+            colv[r] = v;
+        }
+        __syncthreads();
+        for (int r = c + 1 + warp; r < n; r += nw) {
+            const double lr = colv[r];
+            double *row = A + (long long)r * n;
+            for (int col = c + 1 + lane; col <= r; col += 32) row[col] = fma(-lr, colv[col], row[col]);
+        }
+        __syncthreads();
+    }
+    if (tid == 0) *info = bad;
+}
+
+void launch_cholesky(int n, double *A, int *info, cudaStream_t st)
+{
+    const size_t smem = sizeof(double) * (size_t)n;
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(cholesky_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cholesky_kernel<<<1, 1024, smem, st>>>(n, A, info);
+    count_launches(1);
+}
+
+// Explicit inverse of the lower Cholesky factor, one warp per column
+// (forward substitution against e_c); writes Linv (row-major, lower) and its
+// transpose.  Used so that each coarse solve is two dense triangular
+// matrix-vector products instead of 2n dependent steps.
+__global__ void tri_inverse_kernel(int n, const double *__restrict__ L, double *__restrict__ Linv,
+                                   double *__restrict__ LinvT)
+{
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const int c = warp;
+    if (c >= n) return;
+    for (int r = lane; r < c; r += 32) {
+        Linv[(long long)r * n + c] = 0.0;
+        LinvT[(long long)c * n + r] = 0.0;
+    }
+    for (int r = c; r < n; ++r) {
+        // x_r = (delta_rc - sum_{c<=kk<r} L[r][kk] x_kk) / L[r][r]
+        double s = 0.0;
+        for (int kk = c + lane; kk < r; kk += 32) s += L[(long long)r * n + kk] * Linv[(long long)kk * n + c];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        const double x = ((r == c ? 1.0 : 0.0) - s) / L[(long long)r * n + r];
+        if (lane == 0) {
+            Linv[(long long)r * n + c] = x;
+            LinvT[(long long)c * n + r] = x;
+        }
+        __syncwarp();
+    }
+}
+
+void launch_tri_inverse(int n, const double *L, double *Linv, double *LinvT, cudaStream_t st)
+{
+    const int bs = 128;  // 4 columns per CTA
+    tri_inverse_kernel<<<(unsigned)((n * 32 + bs - 1) / bs), bs, 0, st>>>(n, L, Linv, LinvT);
+    count_launches(1);
+}
+
+// y = M x for a dense row-major n x n matrix, one warp per row, FP64
+// accumulation; the input and output may be FP32 or FP64.
+template <typename Tin, typename Tout>
+__global__ void gemv_warp_kernel(int n, const double *__restrict__ M, const Tin *__restrict__ x,
+                                 Tout *__restrict__ y, int lower, const int *__restrict__ done)
+{
+    if (done && *done) return;
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const int lo = lower ? 0 : row, hi = lower ? row + 1 : n;
+    const double *mr = M + (long long)row * n;
+    double s = 0.0;
+    for (int c = lo + lane; c < hi; c += 32) s = fma(mr[c], (double)x[c], s);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) y[row] = (Tout)s;
+}
+
+template <typename T>
+void launch_coarse_solve(int n, const double *Linv, const double *LinvT, const T *b, T *x,
+                         double *tmp, const uint8_t *, const int *done, cudaStream_t st)
+{
+    const int bs = 256;
+    const unsigned nb = (unsigned)((n * 32 + bs - 1) / bs);
+    gemv_warp_kernel<T, double><<<nb, bs, 0, st>>>(n, Linv, b, tmp, 1, done);
+    gemv_warp_kernel<double, T><<<nb, bs, 0, st>>>(n, LinvT, tmp, x, 0, done);
+    count_launches(2);
+}
+template void launch_coarse_solve<double>(int, const double *, const double *, const double *,
+                                          double *, double *, const uint8_t *, const int *,
+                                          cudaStream_t);
+template void launch_coarse_solve<float>(int, const double *, const double *, const float *,
+                                         float *, double *, const uint8_t *, const int *,
+                                         cudaStream_t);
+
+// Fixed-dof mask from the 1-based list (indices validated on the host).
+__global__ void mask_from_list_kernel(const double *__restrict__ fixed1b, int nfd, uint8_t *mask)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nfd) return;
+    const long long dof = (long long)fixed1b[t] - 1;
+    const long long n = dof / 3;
+    const unsigned bit = 1u << (unsigned)(dof - 3 * n);
+    // byte-wise OR through the enclosing aligned 32-bit word
+    unsigned *word = reinterpret_cast<unsigned *>(reinterpret_cast<uintptr_t>(mask + n) & ~uintptr_t(3));
+    const unsigned shift = 8u * (unsigned)(reinterpret_cast<uintptr_t>(mask + n) & 3u);
+    atomicOr(word, bit << shift);
+}
+
+void launch_mask_from_list(long long nnod_bytes, const double *fixed1b, int nfd, uint8_t *mask,
+                           cudaStream_t st)
+{
+    cudaMemsetAsync(mask, 0, (size_t)nnod_bytes, st);
+    if (nfd > 0) {
+        const int bs = 256;
+        mask_from_list_kernel<<<(nfd + bs - 1) / bs, bs, 0, st>>>(fixed1b, nfd, mask);
+        count_launches(1);
+    }
+}
+
+// Coarse fixed dofs: those of the fine nodes with even (i,j,k)
+// (mgcg1.cu:747-790 rstrFDc; a mask instead of an atomically ordered list).
+__global__ void mask_restrict_kernel(Grid gc, const uint8_t *__restrict__ mf, uint8_t *__restrict__ mc)
+{
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= gc.nnod()) return;
+    int i, j, k;
+    node_ijk(gc, n, i, j, k);
+    const Grid gf{2 * gc.nx, 2 * gc.ny, 2 * gc.nz};
+    mc[n] = mf[gf.node(2 * i, 2 * j, 2 * k)];
+}
+
+void launch_mask_restrict(const Grid &gc, const uint8_t *maskf, uint8_t *maskc, cudaStream_t st)
+{
+    const int bs = 256;
+    mask_restrict_kernel<<<(unsigned)((gc.nnod() + bs - 1) / bs), bs, 0, st>>>(gc, maskf, maskc);
+    count_launches(1);
+}
+
+}  // namespace gputo

@@ -1,0 +1,429 @@
+// Host side of the MGCG solver: hierarchy allocation and setup, the V-cycle
+// schedule and the PCG loop (Cantilever/TOP3D125MGCGCUDA/mgcg1.cu:184-651).
+//
+// Differences from the reference's host code, all behaviour-preserving:
+//  * buffers are allocated once per solver (64-bit sizes) and reused across
+//    calls instead of cudaDeviceReset + cudaMalloc on every call (:202-215);
+//  * PCG scalars never leave the device inside an iteration; the host reads a
+//    16-byte status block every opt.check_every iterations (the reference
+//    copies each dot product back, :1033-1041);
+//  * level 1 stores the quadrature operator, levels >= 2 the Galerkin
+//    operator, both packed [300][nel] (structure of arrays, coalesced);
+//  * the coarsest solve is two dense triangular products with the explicitly
+//    inverted Cholesky factor instead of 2n single-block launches (:2175-2232);
+//  * fixed dofs are a per-node bit mask on every level instead of index lists
+//    built with atomics (:747-790).
+#include "solver.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+namespace gputo {
+
+static int checked_malloc(void **p, size_t bytes, size_t &total)
+{
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        set_error(std::string("cudaMalloc of ") + std::to_string(bytes) + " bytes failed: " +
+                  cudaGetErrorString(e));
+        return e == cudaErrorMemoryAllocation ? GPUTO_ERR_OOM : GPUTO_ERR_CUDA;
+    }
+    total += bytes;
+    return GPUTO_OK;
+}
+
+#define ALLOC(ptr, count)                                                                 \
+    do {                                                                                  \
+        int _st = checked_malloc((void **)&(ptr), sizeof(*(ptr)) * (size_t)(count), bytes); \
+        if (_st) return _st;                                                              \
+    } while (0)
+
+Solver::~Solver()
+{
+    for (void *p : owned) cudaFree(p);
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (h_sc) cudaFreeHost(h_sc);
+    if (own_stream) cudaStreamDestroy(own_stream);
+}
+
+template <typename T>
+int Solver::alloc_levels(LevelBuf<T> *Lv, bool with_matrices)
+{
+    for (int l = 0; l < nl; ++l) {
+        LevelBuf<T> &b = Lv[l];
+        b.g = g[l];
+        const long long nd = g[l].ndof();
+        ALLOC(b.u0, nd);
+        owned.push_back(b.u0);
+        ALLOC(b.r, nd);
+        owned.push_back(b.r);
+        ALLOC(b.diag, nd);
+        owned.push_back(b.diag);
+        ALLOC(b.u1, nd);
+        owned.push_back(b.u1);
+        ALLOC(b.f, nd);
+        owned.push_back(b.f);
+        if (l > 0) {
+            if (with_matrices) {
+                ALLOC(b.Apk, 300 * g[l].nel());
+                owned.push_back(b.Apk);
+            }
+        }
+        b.mask = mask[l];
+    }
+    return GPUTO_OK;
+}
+
+int Solver::create(int nelx, int nely, int nelz, int nl_, const gputo_options *o)
+{
+    if (o) opt = *o;
+    else gputo_default_options(&opt);
+    if (nl_ < 1 || nl_ > kMaxLevels || nelx < 1 || nely < 1 || nelz < 1) {
+        set_error("grid sizes must be positive and 1 <= nl <= 12");
+        return GPUTO_ERR_ARG;
+    }
+    const int m = 1 << (nl_ - 1);
+    if (nelx % m || nely % m || nelz % m) {
+        set_error("nelx, nely, nelz must be divisible by 2^(nl-1)");
+        return GPUTO_ERR_ARG;
+    }
+    if (opt.nswp < 0 || opt.check_every < 1 || !(opt.omega > 0) ||
+        (opt.precision != GPUTO_PREC_FP64 && opt.precision != GPUTO_PREC_MIXED)) {
+        set_error("invalid solver options");
+        return GPUTO_ERR_ARG;
+    }
+    nl = nl_;
+    for (int l = 0; l < nl; ++l) g[l] = Grid{nelx >> l, nely >> l, nelz >> l};
+    nc = (int)g[nl - 1].ndof();
+    if (nc > opt.max_coarse_dofs) {
+        set_error("coarsest grid has " + std::to_string(nc) + " dofs, above max_coarse_dofs=" +
+                  std::to_string(opt.max_coarse_dofs) + "; use more levels");
+        return GPUTO_ERR_ARG;
+    }
+    GPUTO_CUDA(cudaGetDevice(&device));
+    GPUTO_CUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
+
+    const long long nd = g[0].ndof(), ne = g[0].nel();
+    for (int l = 0; l < nl; ++l) {
+        ALLOC(mask[l], (g[l].nnod() + 3) & ~3LL);
+        owned.push_back(mask[l]);
+    }
+    ALLOC(CX, ne);
+    owned.push_back(CX);
+    ALLOC(R, nd);
+    owned.push_back(R);
+    ALLOC(P, nd);
+    owned.push_back(P);
+    ALLOC(Q, nd);
+    owned.push_back(Q);
+    ALLOC(Z, nd);
+    owned.push_back(Z);
+    ALLOC(Uw, nd);
+    owned.push_back(Uw);
+    ALLOC(Fw, nd);
+    owned.push_back(Fw);
+    if (opt.precision == GPUTO_PREC_MIXED) {
+        ALLOC(Zold, nd);
+        owned.push_back(Zold);
+    }
+    int st = alloc_levels<double>(L, true);
+    if (st) return st;
+    if (opt.precision == GPUTO_PREC_MIXED) {
+        st = alloc_levels<float>(Lf, true);
+        if (st) return st;
+        ALLOC(CXf, ne);
+        owned.push_back(CXf);
+    }
+    ALLOC(AQ, (long long)nc * nc);
+    owned.push_back(AQ);
+    ALLOC(Linv, (long long)nc * nc);
+    owned.push_back(Linv);
+    ALLOC(LinvT, (long long)nc * nc);
+    owned.push_back(LinvT);
+    ALLOC(ctmp, nc);
+    owned.push_back(ctmp);
+    if (nl == 1) {
+        ALLOC(Apk0, 300 * g[0].nel());
+        owned.push_back(Apk0);
+    }
+    partial_cap = std::max(fine_sweep_blocks(g[0]), 1 << 12);  // dot2 needs 2 per CTA
+    ALLOC(partial, partial_cap);
+    owned.push_back(partial);
+    ALLOC(ticket, 4);
+    owned.push_back(ticket);
+    ALLOC(sc, 1);
+    owned.push_back(sc);
+    ALLOC(info, 4);
+    owned.push_back(info);
+    ALLOC(fixed_dev, 1);
+    owned.push_back(fixed_dev);
+    GPUTO_CUDA(cudaMallocHost((void **)&h_sc, sizeof(PcgScalars)));
+    GPUTO_CUDA(cudaMemsetAsync(ticket, 0, 16, own_stream));
+    GPUTO_CUDA(cudaStreamSynchronize(own_stream));
+    return GPUTO_OK;
+}
+
+int Solver::set_problem(const double *Ke0, const double *fixed1b, int nfd, cudaStream_t st)
+{
+    if (!Ke0 || (nfd > 0 && !fixed1b) || nfd < 0) {
+        set_error("Ke0 and fixed must be given");
+        return GPUTO_ERR_ARG;
+    }
+    const long long nd = g[0].ndof();
+    for (int n = 0; n < nfd; ++n) {
+        const double v = fixed1b[n];
+        if (!(v >= 1.0 && v <= (double)nd) || v != std::floor(v)) {
+            set_error("fixed dof index " + std::to_string(v) + " outside 1.." + std::to_string(nd));
+            return GPUTO_ERR_ARG;
+        }
+    }
+    for (int m = 0; m < 576; ++m) {
+        if (!std::isfinite(Ke0[m])) {
+            set_error("Ke0 has a non-finite entry");
+            return GPUTO_ERR_ARG;
+        }
+    }
+    // Ke0 may arrive in either storage order; it is symmetric in every driver,
+    // and the gateway reads it as mgcg1.cu:131-133 does (element [24*i+j]).
+    std::memcpy(Ke, Ke0, sizeof(Ke));
+    int s1 = upload_fine_ke(Ke, st);
+    if (s1) return s1;
+    s1 = upload_quadrature_parts(opt.nu, st);
+    if (s1) return s1;
+    // the fixed list: unchanged lists are not re-uploaded
+    std::vector<double> list(fixed1b, fixed1b + nfd);
+    if (list != fixed_host) {
+        if ((long long)list.size() > fixed_cap) {
+            cudaFree(fixed_dev);
+            owned.erase(std::find(owned.begin(), owned.end(), (void *)fixed_dev));
+            fixed_dev = nullptr;
+            ALLOC(fixed_dev, list.size());
+            owned.push_back(fixed_dev);
+            fixed_cap = (long long)list.size();
+        }
+        if (nfd > 0)
+            GPUTO_CUDA(cudaMemcpyAsync(fixed_dev, list.data(), sizeof(double) * nfd,
+                                       cudaMemcpyHostToDevice, st));
+        launch_mask_from_list((g[0].nnod() + 3) & ~3LL, fixed_dev, nfd, mask[0], st);
+        for (int l = 1; l < nl; ++l) launch_mask_restrict(g[l], mask[l - 1], mask[l], st);
+        GPUTO_CUDA(cudaStreamSynchronize(st));
+        fixed_host.swap(list);
+    }
+    have_problem = true;
+    return GPUTO_OK;
+}
+
+int Solver::setup(const double *CX_in, cudaStream_t st)
+{
+    if (!have_problem) {
+        set_error("gputo_solver_set_problem must come before setup");
+        return GPUTO_ERR_ARG;
+    }
+    const long long ne = g[0].nel();
+    if (CX_in != CX)
+        GPUTO_CUDA(cudaMemcpyAsync(CX, CX_in, sizeof(double) * ne, cudaMemcpyDeviceToDevice, st));
+    launch_diag_fine(g[0], CX, L[0].diag, st);
+    for (int l = 1; l < nl; ++l) {
+        if (l == 1) launch_build_level1(g[1], CX, L[1].Apk, st);
+        else launch_build_galerkin(g[l], L[l - 1].Apk, L[l].Apk, st);
+        if (l == nl - 1) launch_coarsest_penalty(g[l], mask[l], L[l].Apk, st);
+        launch_diag_packed<double>(g[l], L[l].Apk, L[l].diag, st);
+    }
+    const double *Acoarse = (nl > 1) ? L[nl - 1].Apk : Apk0;
+    if (nl == 1) {
+        launch_dense_fine(g[0], CX, Apk0, st);
+        launch_coarsest_penalty(g[0], mask[0], Apk0, st);
+    }
+    launch_assemble_dense(g[nl - 1], Acoarse, AQ, st);
+    launch_cholesky(nc, AQ, info, st);
+    launch_tri_inverse(nc, AQ, Linv, LinvT, st);
+    if (opt.precision == GPUTO_PREC_MIXED) {
+        launch_cast_f32(ne, CX, CXf, st);
+        launch_cast_f32(g[0].ndof(), L[0].diag, Lf[0].diag, st);
+        for (int l = 1; l < nl; ++l) {
+            launch_cast_f32(300 * g[l].nel(), L[l].Apk, Lf[l].Apk, st);
+            launch_cast_f32(g[l].ndof(), L[l].diag, Lf[l].diag, st);
+        }
+    }
+    int h_info = 0;
+    GPUTO_CUDA(cudaMemcpyAsync(&h_info, info, sizeof(int), cudaMemcpyDeviceToHost, st));
+    GPUTO_CUDA(cudaStreamSynchronize(st));
+    GPUTO_CUDA(cudaGetLastError());
+    if (h_info) {
+        set_error("coarsest-grid Cholesky met a non-positive pivot at row " + std::to_string(h_info));
+        ready = false;
+        return GPUTO_ERR_NOT_SPD;
+    }
+    ready = true;
+    return GPUTO_OK;
+}
+
+// V-cycle z = M r (mgcg1.cu:468-651): pre-smoothing with the initial guess
+// prerelax*F/diag, nswp damped-Jacobi sweeps, defect, restriction; coarsest
+// direct solve; prolongation, nswp sweeps.  The smoother ping-pongs between
+// two buffers; the schedule is arranged so that every level's result lands
+// in its second buffer (bufs[1]), which for level 0 is z itself.
+template <typename T>
+void Solver::vcycle_impl(LevelBuf<T> *Lv, const T *CXl, const T *r0, T *z0, const int *done,
+                         cudaStream_t st)
+{
+    const int ns = opt.nswp;
+    const T om = (T)opt.omega, pr = (T)opt.prerelax;
+    auto sweep = [&](int l, int mode, const T *u, const T *f, T *out, T w) {
+        if (l == 0)
+            launch_fine_sweep<T>(mode, g[0], CXl, u, f, Lv[0].diag, mask[0], out, w, pr, nullptr, done, st);
+        else
+            launch_packed_sweep<T>(mode, g[l], Lv[l].Apk, u, f, Lv[l].diag, mask[l], out, w, pr, done, st);
+    };
+    auto bufs = [&](int l, int which) -> T * {
+        if (l == 0) return which ? z0 : Lv[0].u0;
+        return which ? Lv[l].u1 : Lv[l].u0;
+    };
+    for (int l = 0; l < nl; ++l) {
+        const T *f = (l == 0) ? r0 : Lv[l].f;
+        if (l > 0) launch_restrict<T>(g[l], Lv[l - 1].r, mask[l], Lv[l].f, done, st);
+        if (l < nl - 1) {
+            if (ns == 0) {
+                sweep(l, MODE_JACOBI_PRE, nullptr, f, bufs(l, 1), T(0));  // U = prerelax F / diag
+            } else {
+                for (int s = 0; s < ns; ++s)
+                    sweep(l, s == 0 ? MODE_JACOBI_PRE : MODE_JACOBI, s == 0 ? nullptr : bufs(l, (s - 1) & 1),
+                          f, bufs(l, s & 1), om);
+            }
+            const T *upre = (ns == 0) ? bufs(l, 1) : bufs(l, (ns - 1) & 1);
+            sweep(l, MODE_DEFECT, upre, f, Lv[l].r, om);
+        } else {
+            launch_coarse_solve<T>(nc, Linv, LinvT, f, bufs(l, 1), ctmp, mask[l], done, st);
+        }
+    }
+    for (int l = nl - 2; l >= 0; --l) {
+        const T *f = (l == 0) ? r0 : Lv[l].f;
+        int cur = (ns == 0) ? 1 : ((ns - 1) & 1);
+        launch_prolong_add<T>(g[l], bufs(l + 1, 1), mask[l], bufs(l, cur), done, st);
+        for (int s = 0; s < ns; ++s) {
+            sweep(l, MODE_JACOBI, bufs(l, cur), f, bufs(l, cur ^ 1), om);
+            cur ^= 1;
+        }
+    }
+}
+
+int Solver::vcycle(const double *r, double *z, const int *done, cudaStream_t st)
+{
+    if (opt.precision == GPUTO_PREC_MIXED) {
+        // FP32 V-cycle between FP64 vectors
+        launch_convert<double, float>(g[0].ndof(), r, Lf[0].f, done, st);
+        vcycle_impl<float>(Lf, CXf, Lf[0].f, Lf[0].u1, done, st);
+        launch_convert<float, double>(g[0].ndof(), Lf[0].u1, z, done, st);
+    } else {
+        vcycle_impl<double>(L, CX, r, z, done, st);
+    }
+    return GPUTO_OK;
+}
+
+int Solver::apply(const double *u, double *r, cudaStream_t st)
+{
+    launch_fine_sweep<double>(MODE_APPLY, g[0], CX, u, nullptr, L[0].diag, mask[0], r, 1.0, 0.0,
+                              nullptr, nullptr, st);
+    return GPUTO_OK;
+}
+
+// One PCG iteration (mgcg1.cu:254-275), every scalar on the device.
+void Solver::iteration(cudaStream_t st)
+{
+    const long long nd = g[0].ndof();
+    const int *done = &sc->done;
+    launch_fine_sweep<double>(MODE_APPLY, g[0], CX, P, nullptr, L[0].diag, mask[0], Q, 1.0, 0.0,
+                              partial, done, st);
+    launch_finish_apply_dot(fine_sweep_blocks(g[0]), partial, ticket, sc, st);
+    launch_pcg_update(nd, Uw, R, P, Q, partial, ticket, sc, st);
+    vcycle(R, Z, done, st);
+    if (Zold) {
+        launch_dot2(nd, R, Z, Zold, partial, ticket, sc, done, st);
+        launch_p_update(nd, Z, P, Zold, sc, st);
+    } else {
+        launch_dot(nd, R, Z, partial, ticket, sc, 2 /*DOT_RZ*/, done, st);
+        launch_p_update(nd, Z, P, nullptr, sc, st);
+    }
+}
+
+int Solver::solve(const double *F, double *U, double tol, int maxit, double *relres, int *nit,
+                  cudaStream_t st, FILE *log)
+{
+    if (!ready) {
+        set_error("solver setup has not succeeded");
+        return GPUTO_ERR_ARG;
+    }
+    if (maxit < 0 || !(tol >= 0)) {
+        set_error("maxit must be >= 0 and tol >= 0");
+        return GPUTO_ERR_ARG;
+    }
+    const long long nd = g[0].ndof();
+    const int *done = &sc->done;
+    launch_pcg_init(nd, F, Uw, R, partial, ticket, sc, tol, maxit,
+                    opt.precision == GPUTO_PREC_MIXED, st);
+    vcycle(R, P, done, st);
+    launch_dot(nd, R, P, partial, ticket, sc, 1 /*DOT_RHO0*/, done, st);
+    if (Zold) launch_copy(nd, P, Zold, done, st);
+
+    const bool graph = opt.use_graph != 0;
+    int it = 0;
+    for (;;) {
+        GPUTO_CUDA(cudaMemcpyAsync(h_sc, sc, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+        GPUTO_CUDA(cudaStreamSynchronize(st));
+        if (log && it > 0) std::fprintf(log, "CG It %d  %12.6g\n", h_sc->iter - 1, h_sc->relres);
+        if (h_sc->done || it >= maxit) break;
+        const int batch = std::min(opt.check_every, maxit - it);
+        if (graph) {
+            int gs = run_graph(batch, st);
+            if (gs) return gs;
+        } else {
+            for (int b = 0; b < batch; ++b) iteration(st);
+        }
+        it += batch;
+    }
+    GPUTO_CUDA(cudaGetLastError());
+    if (U != Uw)
+        GPUTO_CUDA(cudaMemcpyAsync(U, Uw, sizeof(double) * nd, cudaMemcpyDeviceToDevice, st));
+    GPUTO_CUDA(cudaStreamSynchronize(st));
+    *relres = h_sc->relres;
+    *nit = h_sc->nit;
+    last_res0 = h_sc->res0;
+    if (h_sc->status) {
+        set_error("PCG breakdown: p'q <= 0 or a non-finite scalar at iteration " +
+                  std::to_string(h_sc->nit));
+        return h_sc->status;
+    }
+    return GPUTO_OK;
+}
+
+// The PCG iteration captured once into a CUDA graph (all pointers are
+// solver-owned, all scalars device-resident), replayed 'batch' times.
+int Solver::run_graph(int batch, cudaStream_t st)
+{
+    if (!graph_exec || graph_stream != st) {
+        if (graph_exec) {
+            cudaGraphExecDestroy(graph_exec);
+            graph_exec = nullptr;
+        }
+        cudaGraph_t gr;
+        GPUTO_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        iteration(st);
+        GPUTO_CUDA(cudaStreamEndCapture(st, &gr));
+        cudaError_t e = cudaGraphInstantiate(&graph_exec, gr, 0);
+        cudaGraphDestroy(gr);
+        GPUTO_CUDA(e);
+        graph_stream = st;
+    }
+    for (int b = 0; b < batch; ++b) GPUTO_CUDA(cudaGraphLaunch(graph_exec, st));
+    return GPUTO_OK;
+}
+
+template int Solver::alloc_levels<double>(LevelBuf<double> *, bool);
+template int Solver::alloc_levels<float>(LevelBuf<float> *, bool);
+
+}  // namespace gputo

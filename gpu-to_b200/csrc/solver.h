@@ -1,0 +1,67 @@
+// The MGCG solver object behind the C ABI.
+#pragma once
+
+#include <cstdio>
+#include <vector>
+
+#include "gputo_internal.h"
+
+namespace gputo {
+
+struct Solver {
+    gputo_options opt{};
+    int nl = 0, device = 0, nc = 0;
+    Grid g[kMaxLevels]{};
+    cudaStream_t own_stream = nullptr;
+
+    double Ke[576]{};
+    bool have_problem = false, ready = false;
+    std::vector<double> fixed_host;
+    double *fixed_dev = nullptr;
+    long long fixed_cap = 1;
+
+    // fine-level PCG vectors (FP64) and solver-owned copies of CX, F, U
+    double *CX = nullptr, *R = nullptr, *P = nullptr, *Q = nullptr, *Z = nullptr, *Zold = nullptr;
+    double *Uw = nullptr, *Fw = nullptr;
+    uint8_t *mask[kMaxLevels]{};
+    LevelBuf<double> L[kMaxLevels];
+    // FP32 preconditioner copies (mixed precision)
+    LevelBuf<float> Lf[kMaxLevels];
+    float *CXf = nullptr;
+    // coarsest grid
+    double *AQ = nullptr, *Linv = nullptr, *LinvT = nullptr, *ctmp = nullptr, *Apk0 = nullptr;
+    int *info = nullptr;
+    // device scalars and reduction scratch
+    PcgScalars *sc = nullptr, *h_sc = nullptr;
+    double *partial = nullptr;
+    int partial_cap = 0;
+    unsigned *ticket = nullptr;
+    double last_res0 = 0.0;
+
+    cudaGraphExec_t graph_exec = nullptr;
+    cudaStream_t graph_stream = nullptr;
+
+    size_t bytes = 0;
+    std::vector<void *> owned;
+
+    ~Solver();
+    int create(int nelx, int nely, int nelz, int nl, const gputo_options *o);
+    int set_problem(const double *Ke0, const double *fixed1b, int nfd, cudaStream_t st);
+    int setup(const double *CX_dev, cudaStream_t st);
+    int solve(const double *F, double *U, double tol, int maxit, double *relres, int *nit,
+              cudaStream_t st, FILE *log);
+    int vcycle(const double *r, double *z, const int *done, cudaStream_t st);
+    int apply(const double *u, double *r, cudaStream_t st);
+    cudaStream_t stream(void *s) const { return s ? (cudaStream_t)s : own_stream; }
+
+  private:
+    template <typename T>
+    int alloc_levels(LevelBuf<T> *Lv, bool with_matrices);
+    template <typename T>
+    void vcycle_impl(LevelBuf<T> *Lv, const T *CXl, const T *r0, T *z0, const int *done,
+                     cudaStream_t st);
+    void iteration(cudaStream_t st);
+    int run_graph(int batch, cudaStream_t st);
+};
+
+}  // namespace gputo

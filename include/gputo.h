@@ -1,0 +1,183 @@
+/*
+ * gputo: B200 (sm_100a) implementation of GPU-TO's topology-optimization
+ * solver path, exposed as a plain C ABI.
+ *
+ * The drop-in entry point is gputo_mgcg1(), which takes exactly the arguments
+ * of the MATLAB MEX function mgcg1 that the top3D125 MGCG drivers call:
+ *
+ *   [cgres,cgiters] = mgcg1(Ke0,F1,U,CX,fixed',nfd,nelx,nely,nelz,nl,cgtol,cgmax[,printLev])
+ *   (Cantilever/TOP3D125MGCGCUDA/top3D125modCuda.m:134; 13-argument form
+ *    ArchBridge/1/top3D125modCudaBridge1.m:175; gateway mgcg1.cu:120-182)
+ *
+ * The MEX gateway in gpu-to_b200/csrc/mex_gateway.cpp calls it; so can ctypes,
+ * cgo, JNI or any other FFI.  Everything else here is the device-resident API
+ * that the design loop uses to keep its fields in HBM between steps.
+ *
+ * Grid conventions (identical to the reference):
+ *   node n = (nelz+1)(nely+1) i + (nely+1) k + j,  i=x, j=y, k=z, y fastest
+ *   element e = nelz nely i + nely k + j;  dof = 3 n + d, d in {x,y,z}
+ *
+ * All functions return a gputo_status; none of them exits the process or traps
+ * the GPU.  Functions whose names end in _dev take device pointers; the rest
+ * take host pointers.  Calls are synchronous with respect to the host unless
+ * stated otherwise.
+ */
+#ifndef GPUTO_H
+#define GPUTO_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    GPUTO_OK = 0,
+    GPUTO_ERR_ARG = 1,          /* bad size, index or option                        */
+    GPUTO_ERR_CUDA = 2,         /* a CUDA call failed (message: gputo_last_error)     */
+    GPUTO_ERR_OOM = 3,          /* not enough device memory (MEX returns cgiters=-1) */
+    GPUTO_ERR_NOT_SPD = 4,      /* coarsest-grid Cholesky met a non-positive pivot   */
+    GPUTO_ERR_BREAKDOWN = 5,    /* CG breakdown: p'q <= 0 or a non-finite scalar     */
+    GPUTO_ERR_NO_DEVICE = 6,    /* no CUDA device / no sm_100 device                 */
+    GPUTO_ERR_TIMEOUT = 7       /* a bounded device wait gave up                     */
+} gputo_status;
+
+/* Human-readable name of a status code. */
+const char *gputo_status_string(int status);
+/* Last error message recorded by this thread (empty string when none). */
+const char *gputo_last_error(void);
+/* Library version string. */
+const char *gputo_version(void);
+
+/* Precision of the preconditioner.  The outer PCG (residual update, dot
+ * products, operator apply p -> K p) is always FP64. */
+typedef enum {
+    GPUTO_PREC_FP64 = 0,   /* everything FP64: the reference's arithmetic        */
+    GPUTO_PREC_MIXED = 1   /* V-cycle in FP32 (coarsest Cholesky still FP64),
+                              flexible PCG                                       */
+} gputo_precision;
+
+/* Solver options.  gputo_default_options() gives the constants that the MEX
+ * hard-codes (mgcg1.cu:188 nswp=3, :1199-1206 omega=0.48, :1190-1197
+ * pre-relaxation 0.7, :331 nu=0.3 for the level-1 quadrature). */
+typedef struct {
+    int precision;       /* gputo_precision                                      */
+    int nswp;            /* Jacobi sweeps per pre/post smoothing step             */
+    double omega;        /* damped-Jacobi weight                                  */
+    double prerelax;     /* initial smoother guess U = prerelax * F / diag(A)     */
+    double nu;           /* Poisson ratio of the level-1 quadrature operator      */
+    int check_every;     /* PCG iterations between host convergence checks (>=1) */
+    int use_graph;       /* capture the PCG iteration in a CUDA graph (0/1)      */
+    int max_coarse_dofs; /* reject hierarchies whose coarsest grid is larger      */
+} gputo_options;
+
+void gputo_default_options(gputo_options *opt);
+
+/* ---------------------------------------------------------------------- */
+/* Drop-in MEX replacement                                                  */
+/* ---------------------------------------------------------------------- */
+
+/*
+ * Replaces the MEX mgcg1 (Cantilever/TOP3D125MGCGCUDA/mgcg1.cu:120-291).
+ *
+ * Ke0     24x24 element stiffness (symmetric; either storage order)
+ * F       ndof right-hand side, ndof = 3 (nelx+1)(nely+1)(nelz+1)
+ * U       ndof output, written in place; its input values are ignored (the
+ *         solve starts from zero, mgcg1.cu:235); y components are negated on
+ *         output (mgcg1.cu:282-283), as the MATLAB drivers expect
+ * CX      nel element stiffness scale E(x)
+ * fixed1b nfd 1-based indices of the fixed dofs (MATLAB's fixed')
+ * nl      multigrid levels; nelx, nely, nelz divisible by 2^(nl-1)
+ * tol     relative residual tolerance on ||r||/||F||
+ * maxit   PCG iteration limit
+ * printLev  0: silent; >=1: append a summary to ./mgcg1.log as the MEX does
+ * relres  output: ||r||/||F|| at exit
+ * nit     output: 0-based iteration index at which relres < tol first held,
+ *         maxit if it never did, -1 if device memory was insufficient
+ *         (mgcg1.cu:166-174)
+ * The hierarchy and buffers are cached per device and grid shape, so later
+ * calls of the same shape allocate nothing.
+ */
+int gputo_mgcg1(const double *Ke0, const double *F, double *U, const double *CX,
+                const double *fixed1b, int nfd, int nelx, int nely, int nelz, int nl,
+                double tol, int maxit, int printLev, double *relres, int *nit);
+
+/* gputo_mgcg1 with explicit options (precision, sweeps, ...). */
+int gputo_mgcg1_ex(const double *Ke0, const double *F, double *U, const double *CX,
+                   const double *fixed1b, int nfd, int nelx, int nely, int nelz, int nl,
+                   double tol, int maxit, int printLev, const gputo_options *opt,
+                   double *relres, int *nit);
+
+/* ---------------------------------------------------------------------- */
+/* Device-resident solver (the same solve without host copies)             */
+/* ---------------------------------------------------------------------- */
+
+typedef struct gputo_solver gputo_solver;
+
+/* Create a solver for one grid shape on the current CUDA device.  Replaces the
+ * allocation half of mgcg1.cu:184-232 and estWorkSpace (mgcg1.cu:293-322),
+ * with 64-bit sizes throughout. */
+int gputo_solver_create(gputo_solver **out, int nelx, int nely, int nelz, int nl,
+                        const gputo_options *opt);
+void gputo_solver_destroy(gputo_solver *s);
+/* Bytes of device memory the solver holds. */
+size_t gputo_solver_device_bytes(const gputo_solver *s);
+
+/* Element matrix (host, 24x24) and Dirichlet dofs (host, 1-based doubles, as
+ * the MEX receives them).  Must be called before setup. */
+int gputo_solver_set_problem(gputo_solver *s, const double *Ke0, const double *fixed1b, int nfd);
+
+/* Build the multigrid hierarchy for the element scales CX (device, nel
+ * doubles): diagonal, level-1 quadrature operator, Galerkin levels, coarsest
+ * Cholesky (initVcycle, mgcg1.cu:326-466).  Stream-ordered on 'stream'
+ * (a cudaStream_t, NULL = the solver's own stream); returns after the
+ * coarsest factorisation has been checked. */
+int gputo_solver_setup_dev(gputo_solver *s, const double *CX, void *stream);
+
+/* PCG solve K u = f (mgcg1.cu:233-286) on device vectors of ndof doubles.
+ * U is in the solver's frame (no y negation).  relres/nit as gputo_mgcg1. */
+int gputo_solver_solve_dev(gputo_solver *s, const double *F, double *U, double tol, int maxit,
+                           double *relres, int *nit, void *stream);
+
+/* One V-cycle z = M r on device vectors (the preconditioner alone). */
+int gputo_solver_vcycle_dev(gputo_solver *s, const double *r, double *z, void *stream);
+
+/* r = K(CX) u with fixed rows zeroed, on device vectors (multAV0c + ZeroBCc,
+ * mgcg1.cu:941-997,1326-1331). */
+int gputo_solver_apply_dev(gputo_solver *s, const double *u, double *r, void *stream);
+
+/* Kernel launches the solver has issued since creation (for accounting). */
+long long gputo_solver_launch_count(const gputo_solver *s);
+
+/* ---------------------------------------------------------------------- */
+/* Design-loop steps that the MATLAB drivers run around the solve          */
+/* ---------------------------------------------------------------------- */
+
+/* Compliance sensitivity (top3D125modCuda.m:139,163) on device data:
+ *   ce_e = u_e^T Ke u_e,  dc_e = dsK_e ce_e  (dc may be NULL),
+ *   *compliance = sum_e CX_e ce_e (= F'U at equilibrium) when non-NULL.
+ * U in the solver's frame. */
+int gputo_compliance_sens_dev(const double *Ke0, const double *U, const double *CX,
+                              const double *dsK, int nelx, int nely, int nelz, double *ce,
+                              double *dc, double *compliance, void *stream);
+/* Same with host buffers; U in the MATLAB frame (as gputo_mgcg1 returns it). */
+int gputo_compliance_sens(const double *Ke0, const double *U, const double *CX,
+                          const double *dsK, int nelx, int nely, int nelz, double *ce,
+                          double *dc, double *compliance);
+
+/* Density filter, the three imfilter calls of the driver
+ * (top3D125modCuda.m:95-96,109,140-141):
+ *   out = imfilter(reshape(in ./ divisor, nely,nelz,nelx), h, 'symmetric')   [./ Hs]
+ * with h = max(0, rmin - |d|) on the (2 ceil(rmin)-1)^3 stencil.  divisor may
+ * be NULL (no division).  normalize != 0 divides the result by Hs, which under
+ * 'symmetric' padding is sum(h) everywhere (the xTilde form, :109);
+ * normalize == 0 with divisor = dHs is the dc / dV0 form (:140-141). */
+int gputo_density_filter_dev(const double *in, const double *divisor, double *out, int nelx,
+                             int nely, int nelz, double rmin, int normalize, void *stream);
+int gputo_density_filter(const double *in, const double *divisor, double *out, int nelx,
+                         int nely, int nelz, double rmin, int normalize);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

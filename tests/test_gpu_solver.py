@@ -1,0 +1,235 @@
+"""Parity of the CUDA solver path with the oracle and the reference's golden
+solves, through the C ABI.  Needs a B200.
+
+Tolerances: FP64 operator / preconditioner applies agree with the oracle to
+1e-12 relative (only summation order differs); FP64 solves at the same
+tolerance agree to 1e-9 relative in U with the same iteration count;
+mixed-precision solves agree with the FP64 oracle to 1e-6 in compliance and
+relative displacement L2 at the tolerance the north-star metric uses.
+"""
+import numpy as np
+import pytest
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as T
+    assert T.cuda.is_available(), "GPU tests need a CUDA device"
+    return T
+
+
+def _problem(O, d):
+    return O.Problem(int(d["nelx"]), int(d["nely"]), int(d["nelz"]), d["F"], d["fixed"])
+
+
+def _dev(torch, a):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")
+
+
+def _solver(gputo, p, nl, CX_dev, **opt):
+    s = gputo.Solver(p.nelx, p.nely, p.nelz, nl, gputo.default_options(**opt))
+    s.set_problem(p.Ke0, p.fixed)
+    s.setup(CX_dev)
+    return s
+
+
+@pytest.mark.parametrize("shape,nl", [((16, 8, 8), 3), ((34, 18, 10), 2), ((64, 32, 32), 4),
+                                      ((8, 40, 6), 2)])
+def test_apply_matches_oracle(oracle, gputo, torch, shape, nl):
+    p = oracle.cantilever(*shape)
+    rng = np.random.default_rng(1)
+    CX = oracle.simp(rng.uniform(0.01, 1.0, p.nel))[0]
+    u = rng.standard_normal(p.ndof)
+    s = _solver(gputo, p, nl, _dev(torch, CX))
+    r = torch.zeros(p.ndof, dtype=torch.float64, device="cuda")
+    s.apply(_dev(torch, u), r)
+    ref = oracle.apply_fine(p, CX, u)
+    ref[p.fixed.astype(np.int64) - 1] = 0.0
+    got = r.cpu().numpy()
+    assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("shape,nl", [((16, 8, 8), 3), ((32, 16, 16), 4), ((24, 8, 16), 4)])
+def test_vcycle_matches_oracle(oracle, gputo, torch, shape, nl):
+    p = oracle.cantilever(*shape)
+    rng = np.random.default_rng(2)
+    CX = oracle.simp(oracle.random_density(*shape, seed=4))[0]
+    r = rng.standard_normal(p.ndof)
+    r[p.fixed.astype(np.int64) - 1] = 0.0
+    s = _solver(gputo, p, nl, _dev(torch, CX))
+    z = torch.zeros(p.ndof, dtype=torch.float64, device="cuda")
+    s.vcycle(_dev(torch, r), z)
+    ref = oracle.vcycle(p, CX, nl, r)
+    got = z.cpu().numpy()
+    assert np.abs(got - ref).max() <= 1e-10 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("name", ["solve_16x8x8_rand_nl3", "solve_32x16x16_unif_nl4",
+                                  "solve_16x8x8_maxit3_nl2"])
+def test_mex_entry_matches_reference_golden(oracle, gputo, name):
+    """gputo.mgcg1 (the MEX call layout, host buffers) vs the compiled reference."""
+    d = load_golden(name)
+    p = _problem(oracle, d)
+    U = np.full(p.ndof, 7.0)  # input values must be ignored
+    rr, nit = gputo.mgcg1(p.Ke0, p.F, U, d["CX"], p.fixed, len(p.fixed), p.nelx, p.nely, p.nelz,
+                          int(d["nl"]), float(d["tol"]), int(d["maxit"]), printLev=0)
+    assert nit == int(d["nit"])
+    assert abs(rr - float(d["relres"])) <= 1e-6 * float(d["relres"])
+    assert np.linalg.norm(U - d["U"]) <= 1e-9 * np.linalg.norm(d["U"])
+
+
+def test_corner_supports_converged_solution(oracle, gputo):
+    d = load_golden("solve_16x8x8_corner_nl3")
+    p = _problem(oracle, d)
+    U = np.zeros(p.ndof)
+    rr, nit = gputo.mgcg1(p.Ke0, p.F, U, d["CX"], p.fixed, len(p.fixed), 16, 8, 8, 3, 1e-8, 200,
+                          printLev=0)
+    Uo, rro, nito = oracle.mgcg1(p, d["CX"], 3, 1e-8, 200)
+    assert nit == nito and rr < 1e-8
+    assert np.linalg.norm(U - Uo) <= 1e-9 * np.linalg.norm(Uo)
+    assert np.linalg.norm(U - d["U"]) <= 1e-6 * np.linalg.norm(d["U"])
+
+
+def test_cantilever_64x32x32_first_solve(oracle, gputo):
+    d = load_golden("solve_c1_first")
+    p = oracle.cantilever(64, 32, 32)
+    CX = oracle.simp(np.full(p.nel, 0.12))[0]
+    U = np.zeros(p.ndof)
+    rr, nit = gputo.mgcg1(p.Ke0, p.F, U, CX, p.fixed, len(p.fixed), 64, 32, 32, 4, 1e-8, 200,
+                          printLev=0)
+    assert nit == int(d["nit"])
+    assert abs(p.F @ U - float(d["compliance"])) <= 1e-9 * float(d["compliance"])
+    s = d["sample"]
+    assert np.linalg.norm(U[s] - d["U_sample"]) <= 1e-9 * np.linalg.norm(d["U_sample"])
+
+
+def test_mex_gateway_through_mexfunction(oracle, gputo):
+    from test_capi import _load_mex, call_mex
+    mex, _ = _load_mex()
+    d = load_golden("solve_16x8x8_rand_nl3")
+    p = _problem(oracle, d)
+    U = np.zeros(p.ndof)
+    # 12-argument cantilever form (printLev absent)
+    res, it = call_mex(mex, [p.Ke0.reshape(-1).copy(), p.F, U, d["CX"], p.fixed, len(p.fixed),
+                             16, 8, 8, 3, 1e-8, 200])
+    assert it == int(d["nit"])
+    assert np.linalg.norm(U - d["U"]) <= 1e-9 * np.linalg.norm(d["U"])
+    # 13-argument form, printLev = 0
+    U2 = np.zeros(p.ndof)
+    res2, it2 = call_mex(mex, [p.Ke0.reshape(-1).copy(), p.F, U2, d["CX"], p.fixed, len(p.fixed),
+                               16, 8, 8, 3, 1e-8, 200, 0])
+    assert it2 == it and np.array_equal(U, U2)
+
+
+def test_repeated_calls_are_deterministic(oracle, gputo):
+    d = load_golden("solve_32x16x16_unif_nl4")
+    p = _problem(oracle, d)
+    outs = []
+    for _ in range(3):
+        U = np.zeros(p.ndof)
+        gputo.mgcg1(p.Ke0, p.F, U, d["CX"], p.fixed, len(p.fixed), 32, 16, 16, 4, 1e-8, 200,
+                    printLev=0)
+        outs.append(U)
+    assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[1], outs[2])
+
+
+def test_graph_and_eager_agree(oracle, gputo):
+    d = load_golden("solve_16x8x8_rand_nl3")
+    p = _problem(oracle, d)
+    res = []
+    for g in (0, 1):
+        U = np.zeros(p.ndof)
+        rr, nit = gputo.mgcg1(p.Ke0, p.F, U, d["CX"], p.fixed, len(p.fixed), 16, 8, 8, 3, 1e-8, 200,
+                              printLev=0, options=gputo.default_options(use_graph=g, check_every=3))
+        res.append((U, nit))
+    assert res[0][1] == res[1][1] == int(d["nit"])
+    assert np.array_equal(res[0][0], res[1][0])
+
+
+def test_mixed_precision_matches_fp64_oracle(oracle, gputo):
+    """FP32 V-cycle + flexible FP64 outer PCG, tol 1e-6: compliance and
+    displacement within 1e-6 of the FP64 oracle solved to 1e-10."""
+    p = oracle.cantilever(32, 16, 16)
+    CX = oracle.simp(oracle.random_density(32, 16, 16, seed=9))[0]
+    Uo, _, _ = oracle.mgcg1(p, CX, 4, 1e-10, 400)
+    U = np.zeros(p.ndof)
+    rr, nit = gputo.mgcg1(p.Ke0, p.F, U, CX, p.fixed, len(p.fixed), 32, 16, 16, 4, 1e-8, 400,
+                          printLev=0, options=gputo.default_options(precision=gputo.PREC_MIXED))
+    assert rr < 1e-8 and nit > 0
+    assert abs(p.F @ U - p.F @ Uo) <= 1e-6 * abs(p.F @ Uo)
+    assert np.linalg.norm(U - Uo) <= 1e-6 * np.linalg.norm(Uo)
+
+
+def test_compliance_sensitivity_matches_oracle(oracle, gputo):
+    d = load_golden("solve_32x16x16_unif_nl4")
+    p = _problem(oracle, d)
+    U = d["U"]  # MATLAB frame, as the MEX returns it
+    xphys = np.random.default_rng(4).uniform(0.05, 1.0, p.nel)
+    CX, dsK = oracle.simp(xphys)
+    ce, dc, c = gputo.compliance_sens(p.Ke0, U, CX, dsK, 32, 16, 16)
+    Uc = U.copy()
+    Uc[1::3] *= -1  # back to the solver frame
+    ce_ref = oracle.element_energy(p, Uc)
+    assert np.abs(ce - ce_ref).max() <= 1e-12 * np.abs(ce_ref).max()
+    assert np.abs(dc - dsK * ce_ref).max() <= 1e-12 * np.abs(dsK * ce_ref).max()
+    assert abs(c - CX @ ce_ref) <= 1e-12 * abs(CX @ ce_ref)
+
+
+@pytest.mark.parametrize("rmin", [3 ** 0.5, 2 * 3 ** 0.5, 1.2])
+def test_density_filter_matches_oracle(oracle, gputo, rmin):
+    nelx, nely, nelz = 20, 12, 10
+    rng = np.random.default_rng(5)
+    x = rng.random(nelx * nely * nelz)
+    dv = rng.uniform(0.5, 2.0, x.size)
+    out, hs = oracle.filter3d(x, nelx, nely, nelz, rmin)
+    got = gputo.density_filter(x, nelx, nely, nelz, rmin, normalize=True)
+    assert np.abs(got - out / hs).max() <= 1e-14
+    out2, _ = oracle.filter3d(x / dv, nelx, nely, nelz, rmin)
+    got2 = gputo.density_filter(x, nelx, nely, nelz, rmin, divisor=dv, normalize=False)
+    assert np.abs(got2 - out2).max() <= 1e-13 * np.abs(out2).max()
+
+
+def test_bad_arguments_return_status(oracle, gputo):
+    p = oracle.cantilever(16, 8, 8)
+    CX = np.ones(p.nel)
+    U = np.zeros(p.ndof)
+    with pytest.raises(gputo.GputoError) as e:  # nl does not divide the grid
+        gputo.mgcg1(p.Ke0, p.F, U, CX, p.fixed, len(p.fixed), 16, 8, 8, 5, 1e-8, 10, printLev=0)
+    assert e.value.status == gputo.GPUTO_ERR_ARG
+    bad = p.fixed.copy()
+    bad[3] = p.ndof + 1.0  # out-of-range fixed dof
+    with pytest.raises(gputo.GputoError) as e:
+        gputo.mgcg1(p.Ke0, p.F, U, CX, bad, len(bad), 16, 8, 8, 3, 1e-8, 10, printLev=0)
+    assert e.value.status == gputo.GPUTO_ERR_ARG
+    # the context stays usable after errors
+    rr, nit = gputo.mgcg1(p.Ke0, p.F, U, CX, p.fixed, len(p.fixed), 16, 8, 8, 3, 1e-8, 200, printLev=0)
+    assert rr < 1e-8
+
+
+def test_nonpositive_coarse_matrix_reports_not_spd(oracle, gputo):
+    p = oracle.cantilever(8, 4, 4)
+    CX = -np.ones(p.nel)  # negative stiffness: the coarsest Cholesky must refuse it
+    U = np.zeros(p.ndof)
+    with pytest.raises(gputo.GputoError) as e:
+        gputo.mgcg1(p.Ke0, p.F, U, CX, p.fixed, len(p.fixed), 8, 4, 4, 2, 1e-8, 10, printLev=0)
+    assert e.value.status == gputo.GPUTO_ERR_NOT_SPD
+
+
+def test_zero_load_returns_zero(oracle, gputo):
+    p = oracle.cantilever(8, 4, 4)
+    U = np.ones(p.ndof)
+    rr, nit = gputo.mgcg1(p.Ke0, np.zeros(p.ndof), U, np.ones(p.nel), p.fixed, len(p.fixed), 8, 4,
+                          4, 2, 1e-8, 10, printLev=0)
+    assert nit == 0 and np.all(U == 0)
+
+
+def test_log_file_written_like_the_mex(oracle, gputo, tmp_path):
+    p = oracle.cantilever(8, 4, 4)
+    U = np.zeros(p.ndof)
+    gputo.mgcg1(p.Ke0, p.F, U, np.ones(p.nel), p.fixed, len(p.fixed), 8, 4, 4, 2, 1e-8, 50,
+                printLev=1)
+    text = (tmp_path / "mgcg1.log").read_text()
+    assert "MGCG Initial residual" in text and "Final residual" in text
