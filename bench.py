@@ -1,0 +1,464 @@
+"""Benchmark: seconds per design iteration of the GPU-TO topology-optimisation
+loop on the 256x128x128 cantilever (4.19M hex8 elements, 12.83M DOF), MGCG
+tolerance 1e-6, 6 multigrid levels, on one B200.
+
+A step is one design iteration of the top3D125 loop: density filter, SIMP,
+MGCG solve (hierarchy setup + PCG to relres < 1e-6), compliance sensitivity,
+filtered sensitivities and the OC update, every field resident in HBM.  Every
+step starts from the same design, so every step does the same work.  The
+design is a mid-optimisation one: the 64x32x32 cantilever design after 50 OC
+iterations (tests/golden/design_c1.npz, produced with the reference's solver),
+upsampled 4x to 256x128x128 -- synthetic, deterministic, with the void/solid
+contrast of a real run.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gputo|reference]
+
+The headline ``value`` is the mixed-precision path (FP32 V-cycle, flexible
+FP64 PCG); ``fp64`` carries the plain FP64 MGCG on the same design.  ``e2e`` is
+the same design iteration through the host-buffer C ABI a MATLAB caller uses
+(gputo_density_filter, mgcg1, gputo_compliance_sens, gputo_oc_update), with all
+host<->device copies inside the timed region.  ``--impl reference`` times the
+reference's own OpenMP MEX (Cantilever/omp/mgcg1.c, compiled into oracle/_ref)
+on the host cores on the same design.
+
+With N > 1 (torchrun) every rank runs an independent replica ("replicas
+only": the path has no exchange step); value = max-over-ranks time / (N K).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "gpu-to_b200"))
+
+NELX, NELY, NELZ, NL = 256, 128, 128, 6
+TOL, MAXIT = 1e-6, 500
+VOLFRAC, PENAL, RMIN, MOVE = 0.12, 3.0, 3 ** 0.5, 0.2
+METRIC = "s/design-iter @12.7M DOF, tol 1e-6: mixed+learned vs FP64 MGCG, same B200"
+# PCG iterations the FP64 MGCG needs on the bench design at tol 1e-6, as the
+# FP64 arm of this benchmark measures them on a B200 (the reference's MGCG
+# runs the same algorithm and takes the same count; the tests check that
+# iteration for iteration on smaller grids).  The CPU arm extrapolates its
+# bounded sample to this count.
+FP64_NIT_ON_BENCH_DESIGN = 71
+
+
+def bench_design(nelx=NELX, nely=NELY, nelz=NELZ):
+    d = np.load(os.path.join(ROOT, "tests", "golden", "design_c1.npz"))
+    x = d["x"].astype(np.float64).reshape(64, 32, 32)  # (x, z, y) element order
+    fx, fz, fy = nelx // 64, nelz // 32, nely // 32
+    if fx * 64 != nelx or fz * 32 != nelz or fy * 32 != nely:
+        return np.full(nelx * nely * nelz, VOLFRAC)
+    xb = np.repeat(np.repeat(np.repeat(x, fx, 0), fz, 1), fy, 2)
+    return np.ascontiguousarray(xb.reshape(-1))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index=0):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [t.strip() for t in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def max_over_ranks(v, ws):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def time_design_loop(gputo, torch, precision, x0, F, fixed, Ke0, steps, warmup, ws, stream,
+                     clocks=None):
+    opts = gputo.default_options(precision=precision)
+    dl = gputo.DesignLoop(NELX, NELY, NELZ, NL, F, fixed, Ke0, volfrac=VOLFRAC, penal=PENAL,
+                          rmin=RMIN, move=MOVE, tol=TOL, maxit=MAXIT, options=opts, x0=x0,
+                          stream=stream)
+    x0_dev = dl.x.clone()
+    infos = []
+
+    def one():
+        dl.x.copy_(x0_dev)
+        return dl.step()
+
+    for _ in range(warmup):
+        one()
+    torch.cuda.synchronize()
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = gputo.launch_count()
+    ctx = clocks if clocks is not None else _Null()
+    with ctx:
+        e0.record(stream)
+        for _ in range(steps):
+            infos.append(one())
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier(ws)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = gputo.launch_count() - launches0
+    return dl, ms / 1000.0, infos, launches
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
+def e2e_design_iteration(gputo, x, F, fixed, Ke0, opts):
+    """One design iteration through the host-buffer C ABI, as a MATLAB caller
+    would run it with these drop-ins.  Returns (xnew, info, h2d, d2h)."""
+    nel = x.size
+    nd = F.size
+    xPhys = gputo.density_filter(x, NELX, NELY, NELZ, RMIN)
+    xp = xPhys * xPhys
+    CX = 1e-9 + xp * xPhys * (1.0 - 1e-9)
+    dsK = -PENAL * (1.0 - 1e-9) * xp
+    U = np.zeros(nd)
+    rr, nit = gputo.mgcg1(Ke0, F, U, CX, fixed, fixed.size, NELX, NELY, NELZ, NL, TOL, MAXIT,
+                          printLev=0, options=opts)
+    ce, dc, c = gputo.compliance_sens(Ke0, U, CX, dsK, NELX, NELY, NELZ)
+    dcf = gputo.density_filter(dc, NELX, NELY, NELZ, RMIN)
+    dV0 = gputo.density_filter(np.full(nel, 1.0 / nel / VOLFRAC), NELX, NELY, NELZ, RMIN)
+    xnew, lmid = gputo.oc_update(x, dcf, dV0, VOLFRAC, MOVE)
+    # bytes crossing PCIe, counted from the arrays each call copies
+    h2d = 8 * (nel                       # filter(x)
+               + nd + nel + fixed.size   # mgcg1: F, CX, fixed
+               + nd + 2 * nel            # compliance_sens: U, CX, dsK
+               + nel + nel               # the two sensitivity filters
+               + 3 * nel)                # oc_update: x, dc, dV0
+    d2h = 8 * (nel + nd + 2 * nel + 2 * nel + nel)
+    return xnew, {"c": c, "nit": nit, "relres": rr}, h2d, d2h
+
+
+def run_ours(args):
+    import torch
+
+    import gputo
+    ws, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    Ke0 = gputo.hex8_stiffness(0.3)
+    F, fixed = gputo.cantilever(NELX, NELY, NELZ)
+    x0 = bench_design()
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "of measured" if "hbm_gbs" in peaks else "of fallback"
+
+    with torch.cuda.stream(stream):
+        clocks = ClockSampler(local)
+        dl_m, t_m, inf_m, launches = time_design_loop(gputo, torch, gputo.PREC_MIXED, x0, F, fixed,
+                                                      Ke0, args.steps, args.warmup, ws, stream,
+                                                      clocks)
+        # per-kernel timing on the mixed hierarchy, for the roofline
+        ms_apply64 = dl_m.solver.time_kernel(0, 20, stream)
+        ms_jac32 = dl_m.solver.time_kernel(1, 20, stream)
+        ms_lvl1_32 = dl_m.solver.time_kernel(2, 20, stream)
+        del dl_m
+        torch.cuda.empty_cache()
+        dl_d, t_d, inf_d, _ = time_design_loop(gputo, torch, gputo.PREC_FP64, x0, F, fixed, Ke0,
+                                               max(1, args.steps // 2), args.warmup, ws, stream)
+        ms_lvl1_64 = dl_d.solver.time_kernel(3, 20, stream)
+        del dl_d
+        torch.cuda.empty_cache()
+
+    t_m = max_over_ranks(t_m, ws)
+    t_d = max_over_ranks(t_d, ws)
+    K = args.steps
+    s_mixed = t_m / K
+    s_fp64 = t_d / max(1, args.steps // 2)
+
+    # e2e: host buffers through the drop-in C ABI
+    opts = gputo.default_options(precision=gputo.PREC_MIXED)
+    xhost = x0.copy()
+    for _ in range(1):
+        e2e_design_iteration(gputo, xhost, F, fixed, Ke0, opts)  # warm caches
+    barrier(ws)
+    t0 = time.perf_counter()
+    ke2e = max(1, min(args.steps, 3))
+    for _ in range(ke2e):
+        _, inf_e, h2d, d2h = e2e_design_iteration(gputo, xhost, F, fixed, Ke0, opts)
+    t_e2e = max_over_ranks((time.perf_counter() - t0) / ke2e, ws)
+
+    ndof = 3 * (NELX + 1) * (NELY + 1) * (NELZ + 1)
+    nel = NELX * NELY * NELZ
+    nel1 = nel // 8
+    ndof1 = 3 * (NELX // 2 + 1) * (NELY // 2 + 1) * (NELZ // 2 + 1)
+    kernels = {
+        "fine_apply_fp64": {"ms": ms_apply64, "bytes": 16 * ndof + 8 * nel,
+                            "flops": 1152 * nel},
+        "fine_jacobi_fp32": {"ms": ms_jac32, "bytes": 16 * ndof + 4 * nel, "flops": 1152 * nel},
+        "level1_jacobi_fp32": {"ms": ms_lvl1_32, "bytes": 1200 * nel1 + 16 * ndof1},
+        "level1_jacobi_fp64": {"ms": ms_lvl1_64, "bytes": 2400 * nel1 + 32 * ndof1},
+    }
+    for k in kernels.values():
+        k["gbs"] = k["bytes"] / (k["ms"] * 1e-3) / 1e9
+        if "flops" in k:
+            k["tflops"] = k["flops"] / (k["ms"] * 1e-3) / 1e12
+    dom = kernels["fine_apply_fp64"]
+    roofline = {"bound": "hbm", "kernel": "fine_sweep_kernel<double, MODE_APPLY> (K p, FP64)",
+                "achieved": round(dom["gbs"], 1), "peak": hbm_peak, "unit": "GB/s",
+                "frac": round(dom["gbs"] / hbm_peak, 4), "peak_source": peak_src,
+                "traffic": None,
+                "note": "FP64 apply is FP64-pipe bound (1152 FLOP/element): also see "
+                        "kernels.fine_apply_fp64.tflops"}
+
+    result = {
+        "metric": METRIC, "value": round(s_mixed, 5), "unit": "s/design-iter",
+        "n_gpus": ws, "steps": K, "warmup": args.warmup,
+        "ms_per_step": round(1000 * s_mixed, 3), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 outer PCG / f32 V-cycle",
+        "data": "synthetic: 256x128x128 cantilever, mid-optimisation design (64x32x32 design "
+                "after 50 OC iterations, upsampled 4x); working set > L2",
+        "config": {"workload": "one top3D125 design iteration (filter, SIMP, MGCG solve to "
+                               "1e-6, sensitivity, filters, OC) on the 256x128x128 cantilever",
+                   "nelx": NELX, "nely": NELY, "nelz": NELZ, "ndof": ndof, "nl": NL,
+                   "tol": TOL, "rmin": RMIN, "volfrac": VOLFRAC,
+                   "l2": "inputs larger than L2 (12.8M-DOF FP64 vectors of 103 MB; ~4 GB per step)",
+                   "parallelism": f"replicas x{ws}"},
+        "fp64": {"value": round(s_fp64, 5), "unit": "s/design-iter",
+                 "nit": [i["nit"] for i in inf_d], "speedup_mixed_vs_fp64": round(s_fp64 / s_mixed, 3)},
+        "nit": [i["nit"] for i in inf_m],
+        "relres": [i["relres"] for i in inf_m],
+        "compliance": inf_m[-1]["c"] if inf_m else None,
+        "dof_iters_per_s": round(ndof * np.mean([i["nit"] for i in inf_m]) / s_mixed, 1),
+        "e2e": {"value": round(t_e2e, 5), "unit": "s/design-iter", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "timing": "host wall clock around synchronous "
+                                                          "host-buffer C-ABI calls"},
+        "gpu_launches": int(launches),
+        "roofline": roofline,
+        "kernels": {k: {kk: (round(vv, 4) if isinstance(vv, float) else vv) for kk, vv in v.items()}
+                    for k, v in kernels.items()},
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline_sample(x0, inf_d)
+    if rank == 0:
+        print(json.dumps(result))
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# the reference's CPU implementation (oracle/_ref: Cantilever/omp/mgcg1.c)
+# ---------------------------------------------------------------------------
+
+def _ref_module():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if not O.ref_available():
+        return None, "compiled reference oracle/_ref/libmgcg1_omp_ref.so is absent"
+    return O, None
+
+
+def _ref_call(O, p, CX, maxit):
+    t = time.perf_counter()
+    U, rr, nit = O.ref_mgcg1(p, CX, NL, TOL, maxit)
+    return time.perf_counter() - t, U
+
+
+def _design_rest_cpu(O, p, xPhys, U):
+    """The MATLAB-side steps (filter, sensitivity, OC) on the host, timed once."""
+    t = time.perf_counter()
+    nel = p.nel
+    CX, dsK = O.simp(xPhys)
+    Uc = U.copy()
+    Uc[1::3] *= -1
+    ce = O.element_energy(p, Uc)
+    dcf, hs = O.filter3d(dsK * ce, NELX, NELY, NELZ, RMIN)
+    dv0, _ = O.filter3d(np.full(nel, 1.0 / nel / VOLFRAC), NELX, NELY, NELZ, RMIN)
+    O.oc_update(xPhys, dcf / hs, dv0 / hs, VOLFRAC, MOVE)
+    return time.perf_counter() - t
+
+
+def _cores():
+    lim = os.environ.get("OMP_THREAD_LIMIT")
+    n = os.cpu_count() or 1
+    # mgcg1.c:120-121 hard-codes 16 OpenMP threads
+    return min(16, n, int(lim) if lim else n)
+
+
+def cpu_baseline_sample(x0, inf_d=None):
+    O, why = _ref_module()
+    if O is None:
+        return {"value": None, "unit": "s/design-iter", "cores": 0, "kind": "reference",
+                "sample": why}
+    os.environ.setdefault("OMP_THREAD_LIMIT", str(os.cpu_count()))
+    p = O.cantilever(NELX, NELY, NELZ)
+    xf, hs = O.filter3d(x0, NELX, NELY, NELZ, RMIN)
+    xPhys = xf / hs
+    CX, _ = O.simp(xPhys)
+    t1, U = _ref_call(O, p, CX, 1)
+    t2, _ = _ref_call(O, p, CX, 2)
+    t_iter = max(t2 - t1, 0.0)
+    nit = FP64_NIT_ON_BENCH_DESIGN
+    if inf_d:
+        nit = int(np.median([i["nit"] for i in inf_d]))
+    t_rest = _design_rest_cpu(O, p, xPhys, U)
+    est = t1 + (nit - 1) * t_iter + t_rest
+    return {"value": round(est, 2), "unit": "s/design-iter", "cores": _cores(), "kind": "reference",
+            "sample": f"reference OpenMP MEX (Cantilever/omp/mgcg1.c) on the bench design: "
+                      f"setup+1 PCG iteration {t1:.1f}s, one more iteration {t_iter:.1f}s, "
+                      f"extrapolated to {nit} iterations (the FP64 count) plus {t_rest:.1f}s for "
+                      f"filter/sensitivity/OC (oracle restatement)"}
+
+
+def run_reference(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    O, why = _ref_module()
+    if O is None:
+        print(json.dumps({"impl": "reference", "unavailable": why}))
+        return
+    os.environ.setdefault("OMP_THREAD_LIMIT", str(os.cpu_count()))
+    p = O.cantilever(NELX, NELY, NELZ)
+    x0 = bench_design()
+    xf, hs = O.filter3d(x0, NELX, NELY, NELZ, RMIN)
+    xPhys = xf / hs
+    CX, _ = O.simp(xPhys)
+    # one extra PCG iteration in the first warm-up call gives the per-iteration cost
+    t2, U = _ref_call(O, p, CX, 2)
+    t1s = []
+    for _ in range(max(0, args.warmup - 1)):
+        t1s.append(_ref_call(O, p, CX, 1)[0])
+    timed = []
+    for _ in range(args.steps):
+        timed.append(_ref_call(O, p, CX, 1)[0])
+    t1 = float(np.mean(timed))
+    t_iter = max(t2 - t1, 0.0)
+    t_rest = _design_rest_cpu(O, p, xPhys, U)
+    nit = FP64_NIT_ON_BENCH_DESIGN
+    value = t1 + (nit - 1) * t_iter + t_rest
+    cores = _cores()
+    sample = (f"each step: the reference OpenMP MEX (Cantilever/omp/mgcg1.c, unmodified) on the "
+              f"bench design with cgmax=1 (hierarchy setup + first V-cycle + 1 PCG iteration, "
+              f"mean {t1:.2f}s); per further iteration {t_iter:.2f}s (cgmax=2 call); value "
+              f"extrapolated to {nit} PCG iterations (FP64 MGCG count on this design) plus "
+              f"{t_rest:.2f}s for filter/sensitivity/OC (oracle restatement of the MATLAB steps)")
+    out = {"metric": METRIC, "value": round(value, 3), "unit": "s/design-iter", "n_gpus": ws,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * value, 1),
+           "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64", "data": "synthetic: same design as the gputo arm",
+           "config": {"workload": "one top3D125 design iteration on the 256x128x128 cantilever",
+                      "nelx": NELX, "nely": NELY, "nelz": NELZ, "nl": NL, "tol": TOL},
+           "impl": "reference",
+           "cpu_baseline": {"value": round(value, 3), "unit": "s/design-iter", "cores": cores,
+                            "kind": "reference", "sample": sample},
+           "e2e": {"value": round(value, 3), "unit": "s/design-iter", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gputo", choices=["gputo", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

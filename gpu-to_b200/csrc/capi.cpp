@@ -83,6 +83,21 @@ const char *gputo_last_error(void) { return gputo::g_last_error.c_str(); }
 
 const char *gputo_version(void) { return "gputo-b200 0.1 (sm_100a)"; }
 
+int gputo_hex8_stiffness(double nu, double h, double *Ke)
+{
+    if (!Ke || !(h > 0) || !(nu > -1.0 && nu < 0.5)) return GPUTO_ERR_ARG;
+    for (int m = 0; m < 576; ++m) Ke[m] = 0.0;
+    for (int ix = 0; ix < 2; ++ix)
+        for (int iy = 0; iy < 2; ++iy)
+            for (int iz = 0; iz < 2; ++iz) {
+                double K[24][24];
+                gputo::gauss_part(nu, h, ix, iy, iz, K);
+                for (int m = 0; m < 24; ++m)
+                    for (int n = 0; n < 24; ++n) Ke[m * 24 + n] += K[m][n];
+            }
+    return GPUTO_OK;
+}
+
 void gputo_default_options(gputo_options *o)
 {
     if (!o) return;
@@ -159,6 +174,53 @@ int gputo_solver_apply_dev(gputo_solver *s, const double *u, double *r, void *st
 }
 
 long long gputo_solver_launch_count(const gputo_solver *) { return gputo::launches_issued(); }
+
+int gputo_solver_time_kernel(gputo_solver *h, int which, int reps, double *ms, void *stream)
+{
+    if (!h || !ms || reps < 1 || which < 0 || which > 3) return GPUTO_ERR_ARG;
+    Solver &s = h->s;
+    if (!s.ready) return GPUTO_ERR_ARG;
+    if ((which == 1 || which == 2) && s.opt.precision != GPUTO_PREC_MIXED) return GPUTO_ERR_ARG;
+    if ((which == 2 || which == 3) && s.nl < 2) return GPUTO_ERR_ARG;
+    cudaStream_t st = s.stream(stream);
+    cudaEvent_t e0, e1;
+    GPUTO_CUDA(cudaEventCreate(&e0));
+    GPUTO_CUDA(cudaEventCreate(&e1));
+    auto launch = [&]() {
+        switch (which) {
+        case 0:
+            gputo::launch_fine_sweep<double>(gputo::MODE_APPLY, s.g[0], s.CX, s.P, nullptr, s.L[0].diag,
+                                             s.mask[0], s.Q, 1.0, 0.0, nullptr, nullptr, st);
+            break;
+        case 1:
+            gputo::launch_fine_sweep<float>(gputo::MODE_JACOBI, s.g[0], s.CXf, s.Lf[0].u0, s.Lf[0].f,
+                                            s.Lf[0].diag, s.mask[0], s.Lf[0].u1, 0.48f, 0.7f, nullptr,
+                                            nullptr, st);
+            break;
+        case 2:
+            gputo::launch_packed_sweep<float>(gputo::MODE_JACOBI, s.g[1], s.Lf[1].Apk, s.Lf[1].u0,
+                                              s.Lf[1].f, s.Lf[1].diag, s.mask[1], s.Lf[1].u1, 0.48f,
+                                              0.7f, nullptr, st);
+            break;
+        default:
+            gputo::launch_packed_sweep<double>(gputo::MODE_JACOBI, s.g[1], s.L[1].Apk, s.L[1].u0,
+                                               s.L[1].f, s.L[1].diag, s.mask[1], s.L[1].u1, 0.48,
+                                               0.7, nullptr, st);
+        }
+    };
+    launch();  // warm-up
+    GPUTO_CUDA(cudaEventRecord(e0, st));
+    for (int r = 0; r < reps; ++r) launch();
+    GPUTO_CUDA(cudaEventRecord(e1, st));
+    GPUTO_CUDA(cudaEventSynchronize(e1));
+    float t = 0.f;
+    GPUTO_CUDA(cudaEventElapsedTime(&t, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    GPUTO_CUDA(cudaGetLastError());
+    *ms = (double)t / reps;
+    return GPUTO_OK;
+}
 
 // ---------------------------------------------------------------------------
 // drop-in MEX entry point with a per-shape solver cache
@@ -396,6 +458,90 @@ int gputo_density_filter(const double *in, const double *divisor, double *out, i
     cudaFree(din);
     cudaFree(ddiv);
     cudaFree(dout);
+    return st;
+}
+
+int gputo_simp_dev(const double *xPhys, long long n, double penal, double E0, double Emin,
+                   double *CX, double *dsK, void *stream)
+{
+    if (!xPhys || !CX || n <= 0) return GPUTO_ERR_ARG;
+    int st = gputo::check_device();
+    if (st) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    gputo::launch_simp(n, xPhys, penal, E0, Emin, CX, dsK, s);
+    GPUTO_CUDA(cudaStreamSynchronize(s));
+    GPUTO_CUDA(cudaGetLastError());
+    return GPUTO_OK;
+}
+
+namespace {
+// Scratch of the OC update, grown on demand and kept for later calls.
+struct OcScratch {
+    double *ocp = nullptr, *partial = nullptr, *lmid_dev = nullptr;
+    unsigned *ticket = nullptr;
+    void *state = nullptr;
+    long long cap = 0;
+    int reserve(long long n)
+    {
+        if (!partial) {
+            GPUTO_CUDA(cudaMalloc(&partial, sizeof(double) * 2048));
+            GPUTO_CUDA(cudaMalloc(&ticket, 16));
+            GPUTO_CUDA(cudaMemset(ticket, 0, 16));
+            GPUTO_CUDA(cudaMalloc(&state, 64));
+        }
+        if (n > cap) {
+            cudaFree(ocp);
+            ocp = nullptr;
+            cap = 0;
+            GPUTO_CUDA(cudaMalloc(&ocp, sizeof(double) * (size_t)n));
+            cap = n;
+        }
+        return GPUTO_OK;
+    }
+};
+std::mutex g_oc_mu;
+OcScratch g_oc;
+}  // namespace
+
+int gputo_oc_update_dev(const double *x, const double *dc, const double *dV0, long long n,
+                        double volfrac, double move, double *xnew, double *lmid, void *stream)
+{
+    if (!x || !dc || !dV0 || !xnew || n <= 0 || x == xnew || !(volfrac > 0) || !(move >= 0))
+        return GPUTO_ERR_ARG;
+    std::lock_guard<std::mutex> lock(g_oc_mu);
+    int st = gputo::check_device();
+    if (st) return st;
+    st = g_oc.reserve(n);
+    if (st) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    gputo::launch_oc_update(n, x, dc, dV0, volfrac, move, g_oc.ocp, xnew, g_oc.partial,
+                            g_oc.ticket, g_oc.state, 64, s);
+    double hst[3] = {0, 0, 0};
+    GPUTO_CUDA(cudaMemcpyAsync(hst, g_oc.state, sizeof(hst), cudaMemcpyDeviceToHost, s));
+    GPUTO_CUDA(cudaStreamSynchronize(s));
+    GPUTO_CUDA(cudaGetLastError());
+    if (lmid) *lmid = hst[2];
+    return GPUTO_OK;
+}
+
+int gputo_oc_update(const double *x, const double *dc, const double *dV0, long long n,
+                    double volfrac, double move, double *xnew, double *lmid)
+{
+    if (!x || !dc || !dV0 || !xnew || n <= 0) return GPUTO_ERR_ARG;
+    int st = gputo::check_device();
+    if (st) return st;
+    double *d = nullptr;
+    if (cudaMalloc(&d, sizeof(double) * 4 * (size_t)n) != cudaSuccess) {
+        cudaGetLastError();
+        gputo::set_error("cudaMalloc failed in gputo_oc_update");
+        return GPUTO_ERR_OOM;
+    }
+    cudaMemcpy(d, x, sizeof(double) * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(d + n, dc, sizeof(double) * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(d + 2 * n, dV0, sizeof(double) * n, cudaMemcpyHostToDevice);
+    st = gputo_oc_update_dev(d, d + n, d + 2 * n, n, volfrac, move, d + 3 * n, lmid, nullptr);
+    if (!st) cudaMemcpy(xnew, d + 3 * n, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    cudaFree(d);
     return st;
 }
 

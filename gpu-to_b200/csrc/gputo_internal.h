@@ -85,6 +85,8 @@ int cuda_status(cudaError_t e, const char *what);
 // Level-0 element matrix in constant memory (FP64 and FP32 copies).
 int upload_fine_ke(const double *Ke_host, cudaStream_t st);
 int upload_design_ke(const double *Ke_host, cudaStream_t st);
+// B^T D B w at one Gauss point (ix,iy,iz) of an h-cube, E = 1 (host).
+void gauss_part(double nu, double h, int ix, int iy, int iz, double K[24][24]);
 // Level-1 quadrature parts Kg[g] (packed 300 each) for nu, h = 2.
 int upload_quadrature_parts(double nu, cudaStream_t st);
 
@@ -155,6 +157,12 @@ void launch_element_energy(const Grid &g, const double *U, const double *CX, con
                            double *compliance, cudaStream_t st);
 int launch_filter(const Grid &g, const double *in, const double *div, double *out, double rmin,
                   int normalize, cudaStream_t st);
+void launch_simp(long long n, const double *x, double penal, double E0, double Emin, double *CX,
+                 double *dsK, cudaStream_t st);
+int oc_state_bytes();
+void launch_oc_update(long long n, const double *x, const double *dc, const double *dv0,
+                      double volfrac, double move, double *ocp, double *xnew, double *partial,
+                      unsigned *ticket, void *state, int max_steps, cudaStream_t st);
 
 // Counter of kernel launches issued by this library (per process).
 void count_launches(long long n);

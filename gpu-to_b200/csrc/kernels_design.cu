@@ -180,3 +180,166 @@ int launch_filter(const Grid &g, const double *in, const double *div, double *ou
 }
 
 }  // namespace gputo
+
+namespace gputo {
+
+// SIMP stiffness and its derivative (top3D125modCuda.m:124,130):
+//   CX = Emin + x^p (E0 - Emin),   dsK = -p (E0 - Emin) x^(p-1)
+__global__ void simp_kernel(long long n, const double *__restrict__ x, double penal, double E0,
+                            double Emin, double *__restrict__ CX, double *__restrict__ dsK)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double xi = x[i];
+        const double xp1 = pow(xi, penal - 1.0);
+        CX[i] = Emin + xp1 * xi * (E0 - Emin);
+        if (dsK) dsK[i] = -penal * (E0 - Emin) * xp1;
+    }
+}
+
+void launch_simp(long long n, const double *x, double penal, double E0, double Emin, double *CX,
+                 double *dsK, cudaStream_t st)
+{
+    long long nb = (n + 255) / 256;
+    if (nb > 4736) nb = 4736;
+    simp_kernel<<<(unsigned)nb, 256, 0, st>>>(n, x, penal, E0, Emin, CX, dsK);
+    count_launches(1);
+}
+
+// OC update with bisection on the Lagrange multiplier
+// (top3D125modCuda.m:143-151).  The multiplier bracket lives on the device;
+// each bisection step is one pass that evaluates the candidate design at
+// lmid, sums it in a fixed order and moves the bracket, so the whole loop
+// needs no host round trip.  A step whose bracket is already tight returns
+// at once, leaving the design of the last evaluated lmid, as the MATLAB loop
+// does.
+struct OcState {
+    double l1, l2, lmid;
+    int steps, done;
+};
+
+constexpr int kOcThreads = 256;
+constexpr int kOcBlocks = 1184;
+
+__device__ __forceinline__ double oc_candidate(double x, double ocp, double lmid, double move)
+{
+    // max(max(min(min(ocP/lmid, xU), 1), xL), 0)
+    const double xU = x + move, xL = x - move;
+    double v = ocp / lmid;
+    v = fmin(v, xU);
+    v = fmin(v, 1.0);
+    v = fmax(v, xL);
+    return fmax(v, 0.0);
+}
+
+__global__ void __launch_bounds__(kOcThreads)
+oc_prepare_kernel(long long n, const double *__restrict__ x, const double *__restrict__ dc,
+                  const double *__restrict__ dv0, double *__restrict__ ocp, double volfrac,
+                  double *__restrict__ partial, unsigned *ticket, OcState *state)
+{
+    __shared__ double red[kOcThreads / 32];
+    __shared__ bool is_last;
+    double s = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double v = x[i] * sqrt(-dc[i] / dv0[i]);
+        ocp[i] = v;
+        s += v;
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = 0.0;
+        for (int w = 0; w < kOcThreads / 32; ++w) b += red[w];
+        partial[blockIdx.x] = b;
+        __threadfence();
+        is_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (is_last && threadIdx.x == 0) {
+        __threadfence();
+        double t = 0.0;
+        for (unsigned b = 0; b < gridDim.x; ++b) t += partial[b];
+        OcState z;
+        z.l1 = 0.0;
+        z.l2 = (t / (double)n) / volfrac;
+        z.lmid = 0.5 * (z.l1 + z.l2);
+        z.steps = 0;
+        z.done = !((z.l2 - z.l1) / (z.l2 + z.l1) > 1e-4);
+        *state = z;
+        *ticket = 0;
+    }
+}
+
+__global__ void __launch_bounds__(kOcThreads)
+oc_bisect_kernel(long long n, const double *__restrict__ x, const double *__restrict__ ocp,
+                 double move, double volfrac, double *__restrict__ xnew,
+                 double *__restrict__ partial, unsigned *ticket, OcState *state)
+{
+    if (state->done) return;
+    __shared__ double red[kOcThreads / 32];
+    __shared__ bool is_last;
+    const double lmid = 0.5 * (state->l1 + state->l2);
+    double s = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double v = oc_candidate(x[i], ocp[i], lmid, move);
+        xnew[i] = v;
+        s += v;
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = 0.0;
+        for (int w = 0; w < kOcThreads / 32; ++w) b += red[w];
+        partial[blockIdx.x] = b;
+        __threadfence();
+        is_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (is_last && threadIdx.x == 0) {
+        __threadfence();
+        double t = 0.0;
+        for (unsigned b = 0; b < gridDim.x; ++b) t += partial[b];
+        OcState z = *state;
+        z.lmid = lmid;
+        if (t / (double)n > volfrac) z.l1 = lmid;
+        else z.l2 = lmid;
+        z.steps += 1;
+        z.done = !((z.l2 - z.l1) / (z.l2 + z.l1) > 1e-4);
+        *state = z;
+        *ticket = 0;
+    }
+}
+
+// x_new = x when the loop body never runs (bracket already tight).
+__global__ void copy_if_untouched_kernel(long long n, const double *__restrict__ x,
+                                         double *__restrict__ xnew, const OcState *state)
+{
+    if (state->steps > 0) return;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        xnew[i] = x[i];
+}
+
+int oc_state_bytes() { return (int)sizeof(OcState); }
+
+void launch_oc_update(long long n, const double *x, const double *dc, const double *dv0,
+                      double volfrac, double move, double *ocp, double *xnew, double *partial,
+                      unsigned *ticket, void *state, int max_steps, cudaStream_t st)
+{
+    long long nb = (n + kOcThreads - 1) / kOcThreads;
+    if (nb > kOcBlocks) nb = kOcBlocks;
+    OcState *s = (OcState *)state;
+    oc_prepare_kernel<<<(unsigned)nb, kOcThreads, 0, st>>>(n, x, dc, dv0, ocp, volfrac, partial,
+                                                           ticket, s);
+    for (int k = 0; k < max_steps; ++k)
+        oc_bisect_kernel<<<(unsigned)nb, kOcThreads, 0, st>>>(n, x, ocp, move, volfrac, xnew,
+                                                              partial, ticket, s);
+    copy_if_untouched_kernel<<<(unsigned)nb, kOcThreads, 0, st>>>(n, x, xnew, s);
+    count_launches(2 + max_steps);
+}
+
+}  // namespace gputo

@@ -53,7 +53,7 @@ int upload_fine_ke(const double *Ke_host, cudaStream_t st)
 
 // B^T D B at one Gauss point of an h*h*h hex, E=1 (the integrand of
 // mgcg1.c:1370-1418 Kem3 and mgcg1.cu:2000-2040 prepAelm).
-static void gauss_part(double nu, double h, int ix, int iy, int iz, double K[24][24])
+void gauss_part(double nu, double h, int ix, int iy, int iz, double K[24][24])
 {
     const double gp[2] = {-0.5773502691896257645, 0.5773502691896257645};
     const double s = gp[ix], e = gp[iy], t = gp[iz];

@@ -58,6 +58,7 @@ SIGNATURES = {
     "gputo_last_error": (ctypes.c_char_p, []),
     "gputo_version": (ctypes.c_char_p, []),
     "gputo_default_options": (None, [ctypes.POINTER(Options)]),
+    "gputo_hex8_stiffness": (_i, [_d, _d, _dp]),
     "gputo_mgcg1": (_i, [_dp, _dp, _dp, _dp, _dp, _i, _i, _i, _i, _i, _d, _i, _i, _dp, _ip]),
     "gputo_mgcg1_ex": (_i, [_dp, _dp, _dp, _dp, _dp, _i, _i, _i, _i, _i, _d, _i, _i,
                             ctypes.POINTER(Options), _dp, _ip]),
@@ -70,10 +71,14 @@ SIGNATURES = {
     "gputo_solver_vcycle_dev": (_i, [_vp, _vp, _vp, _vp]),
     "gputo_solver_apply_dev": (_i, [_vp, _vp, _vp, _vp]),
     "gputo_solver_launch_count": (ctypes.c_longlong, [_vp]),
+    "gputo_solver_time_kernel": (_i, [_vp, _i, _i, _dp, _vp]),
     "gputo_compliance_sens_dev": (_i, [_dp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _dp, _vp]),
     "gputo_compliance_sens": (_i, [_dp, _dp, _dp, _dp, _i, _i, _i, _dp, _dp, _dp]),
     "gputo_density_filter_dev": (_i, [_vp, _vp, _vp, _i, _i, _i, _d, _i, _vp]),
     "gputo_density_filter": (_i, [_dp, _dp, _dp, _i, _i, _i, _d, _i]),
+    "gputo_simp_dev": (_i, [_vp, ctypes.c_longlong, _d, _d, _d, _vp, _vp, _vp]),
+    "gputo_oc_update_dev": (_i, [_vp, _vp, _vp, ctypes.c_longlong, _d, _d, _vp, _dp, _vp]),
+    "gputo_oc_update": (_i, [_dp, _dp, _dp, ctypes.c_longlong, _d, _d, _dp, _dp]),
 }
 
 
@@ -122,6 +127,27 @@ def default_options(**kw) -> Options:
             raise AttributeError(k)
         setattr(o, k, v)
     return o
+
+
+def hex8_stiffness(nu=0.3, h=1.0) -> np.ndarray:
+    """The drivers' Ke0 (24x24) computed by the library (host only)."""
+    Ke = np.zeros(576)
+    _check(_lib.gputo_hex8_stiffness(float(nu), float(h), _p(Ke)), "gputo_hex8_stiffness")
+    return Ke.reshape(24, 24)
+
+
+def cantilever(nelx, nely, nelz):
+    """Load and supports of the benchmark cantilever: x = 0 face clamped
+    (fixed = 1:3(nely+1)(nelz+1), top3D125modCuda.m:80) and a unit total -z
+    load spread over the bottom edge (k = 0) of the free end x = nelx.
+    Returns (F, fixed) in the MEX's layout."""
+    nd = 3 * (nelx + 1) * (nely + 1) * (nelz + 1)
+    F = np.zeros(nd)
+    js = np.arange(nely + 1)
+    nodes = (nelz + 1) * (nely + 1) * nelx + js
+    F[3 * nodes + 2] = -1.0 / (nely + 1)
+    fixed = np.arange(1, 3 * (nely + 1) * (nelz + 1) + 1, dtype=np.float64)
+    return F, fixed
 
 
 def version() -> str:
@@ -218,6 +244,12 @@ class Solver:
         _check(_lib.gputo_solver_vcycle_dev(self._h, _ptr(r), _ptr(z), _ptr_stream(stream)),
                "gputo_solver_vcycle_dev")
 
+    def time_kernel(self, which, reps=20, stream=None):
+        ms = ctypes.c_double(0.0)
+        _check(_lib.gputo_solver_time_kernel(self._h, int(which), int(reps), ctypes.byref(ms),
+                                             _ptr_stream(stream)), "gputo_solver_time_kernel")
+        return ms.value
+
     def apply(self, u, r, stream=None):
         _check(_lib.gputo_solver_apply_dev(self._h, _ptr(u), _ptr(r), _ptr_stream(stream)),
                "gputo_solver_apply_dev")
@@ -274,3 +306,92 @@ def density_filter_dev(x, out, nelx, nely, nelz, rmin, divisor=None, normalize=T
     _check(_lib.gputo_density_filter_dev(_ptr(x), _ptr(divisor), _ptr(out), nelx, nely, nelz,
                                          float(rmin), int(bool(normalize)), _ptr_stream(stream)),
            "gputo_density_filter_dev")
+
+
+def simp_dev(xphys, CX, dsK=None, penal=3.0, E0=1.0, Emin=1e-9, stream=None):
+    _check(_lib.gputo_simp_dev(_ptr(xphys), xphys.numel(), float(penal), float(E0), float(Emin),
+                               _ptr(CX), _ptr(dsK), _ptr_stream(stream)), "gputo_simp_dev")
+
+
+def oc_update_dev(x, dc, dv0, xnew, volfrac, move, stream=None):
+    lm = ctypes.c_double(0.0)
+    _check(_lib.gputo_oc_update_dev(_ptr(x), _ptr(dc), _ptr(dv0), x.numel(), float(volfrac),
+                                    float(move), _ptr(xnew), ctypes.byref(lm), _ptr_stream(stream)),
+           "gputo_oc_update_dev")
+    return lm.value
+
+
+def oc_update(x, dc, dv0, volfrac, move):
+    """Host-buffer form: returns (xnew, lmid)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    dc = np.ascontiguousarray(dc, dtype=np.float64)
+    dv0 = np.ascontiguousarray(dv0, dtype=np.float64)
+    xn = np.zeros_like(x)
+    lm = ctypes.c_double(0.0)
+    _check(_lib.gputo_oc_update(_p(x), _p(dc), _p(dv0), x.size, float(volfrac), float(move),
+                                _p(xn), ctypes.byref(lm)), "gputo_oc_update")
+    return xn, lm.value
+
+
+class DesignLoop:
+    """The top3D125 optimisation loop with every field resident on the GPU
+    (Cantilever/TOP3D125MGCGCUDA/top3D125modCuda.m:105-166, density filter ft=1):
+
+        xPhys = imfilter(x, h, 'symmetric') ./ Hs          density filter
+        CX, dsK = SIMP(xPhys)                               stiffness
+        [cgres, cgiters] = mgcg1(...)                       MGCG solve
+        dc = dsK .* ce;  c = sum(CX .* ce)                  sensitivity, compliance
+        dc = imfilter(dc ./ Hs); dV0 = imfilter(dV ./ Hs)   filtered sensitivities
+        x = OC(x, dc, dV0)                                  bisection update
+
+    Every step is a C-ABI call on device buffers; the host sees only scalars.
+    Under 'symmetric' padding Hs is the constant sum(h), so dividing by it
+    before or after the filter is the same; the normalised filter is used.
+    ``torch`` tensors provide the device memory.
+    """
+
+    def __init__(self, nelx, nely, nelz, nl, F, fixed, Ke0, volfrac=0.12, penal=3.0,
+                 rmin=3 ** 0.5, move=0.2, tol=1e-6, maxit=200, E0=1.0, Emin=1e-9,
+                 options: Options | None = None, x0=None, stream=None):
+        import torch
+        self.torch = torch
+        self.shape = (nelx, nely, nelz)
+        self.nel = nelx * nely * nelz
+        self.ndof = 3 * (nelx + 1) * (nely + 1) * (nelz + 1)
+        self.volfrac, self.penal, self.rmin, self.move = volfrac, penal, rmin, move
+        self.tol, self.maxit, self.E0, self.Emin = tol, maxit, E0, Emin
+        self.Ke0 = np.ascontiguousarray(Ke0, dtype=np.float64).reshape(-1)
+        self.stream = stream
+        dev = torch.device("cuda")
+        f64 = dict(dtype=torch.float64, device=dev)
+        self.F = torch.as_tensor(np.ascontiguousarray(F, dtype=np.float64), **f64)
+        self.x = torch.full((self.nel,), float(volfrac), **f64) if x0 is None else \
+            torch.as_tensor(np.ascontiguousarray(x0, dtype=np.float64), **f64).clone()
+        self.xnew = torch.empty_like(self.x)
+        self.xPhys = torch.empty_like(self.x)
+        self.CX = torch.empty_like(self.x)
+        self.dsK = torch.empty_like(self.x)
+        self.ce = torch.empty_like(self.x)
+        self.dc = torch.empty_like(self.x)
+        self.dcf = torch.empty_like(self.x)
+        self.dV = torch.full((self.nel,), 1.0 / self.nel / volfrac, **f64)
+        self.dV0 = torch.empty_like(self.x)
+        self.U = torch.zeros(self.ndof, **f64)
+        self.solver = Solver(nelx, nely, nelz, nl, options)
+        self.solver.set_problem(self.Ke0, fixed)
+
+    def step(self):
+        nelx, nely, nelz = self.shape
+        s = self.stream
+        density_filter_dev(self.x, self.xPhys, nelx, nely, nelz, self.rmin, stream=s)
+        simp_dev(self.xPhys, self.CX, self.dsK, self.penal, self.E0, self.Emin, stream=s)
+        self.solver.setup(self.CX, stream=s)
+        relres, nit = self.solver.solve(self.F, self.U, self.tol, self.maxit, stream=s)
+        c = compliance_sens_dev(self.Ke0, self.U, self.CX, self.dsK, nelx, nely, nelz,
+                                ce=self.ce, dc=self.dc, stream=s)
+        density_filter_dev(self.dc, self.dcf, nelx, nely, nelz, self.rmin, stream=s)
+        density_filter_dev(self.dV, self.dV0, nelx, nely, nelz, self.rmin, stream=s)
+        lmid = oc_update_dev(self.x, self.dcf, self.dV0, self.xnew, self.volfrac, self.move,
+                             stream=s)
+        self.x, self.xnew = self.xnew, self.x
+        return {"c": c, "nit": nit, "relres": relres, "lmid": lmid}

@@ -73,6 +73,13 @@ typedef struct {
 
 void gputo_default_options(gputo_options *opt);
 
+/* Element stiffness of a unit-modulus hex8 cube of edge h with Poisson ratio
+ * nu, 2x2x2 Gauss quadrature, in the reference's element node order; Ke is
+ * 576 doubles, row-major and symmetric.  Equals the Ke0 the drivers build
+ * (top3D125modCuda.m:50-77) and Kem3 (Cantilever/omp/mgcg1.c:1370).  Host
+ * only; needs no GPU. */
+int gputo_hex8_stiffness(double nu, double h, double *Ke);
+
 /* ---------------------------------------------------------------------- */
 /* Drop-in MEX replacement                                                  */
 /* ---------------------------------------------------------------------- */
@@ -146,8 +153,16 @@ int gputo_solver_vcycle_dev(gputo_solver *s, const double *r, double *z, void *s
  * mgcg1.cu:941-997,1326-1331). */
 int gputo_solver_apply_dev(gputo_solver *s, const double *u, double *r, void *stream);
 
-/* Kernel launches the solver has issued since creation (for accounting). */
+/* Kernel launches this library has issued in this process (for accounting). */
 long long gputo_solver_launch_count(const gputo_solver *s);
+
+/* Time 'reps' back-to-back launches of one solver kernel on the current
+ * hierarchy with CUDA events on 'stream' and return the mean launch time in
+ * milliseconds.  which: 0 fine-level FP64 apply (p -> K p), 1 fine-level FP32
+ * Jacobi sweep, 2 level-1 FP32 sweep, 3 level-1 FP64 sweep.  Inputs are the
+ * solver's own work vectors; results are discarded.  Needs setup first. */
+int gputo_solver_time_kernel(gputo_solver *s, int which, int reps, double *ms_per_launch,
+                             void *stream);
 
 /* ---------------------------------------------------------------------- */
 /* Design-loop steps that the MATLAB drivers run around the solve          */
@@ -176,6 +191,24 @@ int gputo_density_filter_dev(const double *in, const double *divisor, double *ou
                              int nely, int nelz, double rmin, int normalize, void *stream);
 int gputo_density_filter(const double *in, const double *divisor, double *out, int nelx,
                          int nely, int nelz, double rmin, int normalize);
+
+/* SIMP interpolation (top3D125modCuda.m:124,130) on device arrays of n:
+ *   CX = Emin + xPhys^penal (E0 - Emin),  dsK = -penal (E0 - Emin) xPhys^(penal-1)
+ * dsK may be NULL. */
+int gputo_simp_dev(const double *xPhys, long long n, double penal, double E0, double Emin,
+                   double *CX, double *dsK, void *stream);
+
+/* Optimality-criteria update with bisection on the Lagrange multiplier
+ * (top3D125modCuda.m:143-151), all elements active:
+ *   ocP = x .* sqrt(-dc ./ dV0);  l = [0, mean(ocP)/volfrac]
+ *   while (l2-l1)/(l2+l1) > 1e-4: lmid = (l1+l2)/2;
+ *       xnew = max(max(min(min(ocP/lmid, x+move), 1), x-move), 0)
+ *       if mean(xnew) > volfrac: l1 = lmid else l2 = lmid
+ * xnew must not alias x.  *lmid receives the last multiplier evaluated. */
+int gputo_oc_update_dev(const double *x, const double *dc, const double *dV0, long long n,
+                        double volfrac, double move, double *xnew, double *lmid, void *stream);
+int gputo_oc_update(const double *x, const double *dc, const double *dV0, long long n,
+                    double volfrac, double move, double *xnew, double *lmid);
 
 #ifdef __cplusplus
 }
