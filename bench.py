@@ -444,6 +444,52 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+KERNELS = {"apply64": 0, "jacobi32": 1, "level1_32": 2, "level1_64": 3}
+
+
+def run_micro(args):
+    """Profiling aid: build one solver on the bench design and launch a single
+    kernel kind a few times (for ncu -k ... -c ...); prints mean times."""
+    import torch
+
+    import gputo
+    nelx, nely, nelz = (int(v) for v in args.size.split("x"))
+    nl = args.nl
+    F, fixed = gputo.cantilever(nelx, nely, nelz)
+    x0 = bench_design(nelx, nely, nelz)
+    kinds = list(KERNELS) if args.micro == "all" else [args.micro]
+    mixed = any(k in ("jacobi32", "level1_32") for k in kinds)
+    opts = gputo.default_options(precision=gputo.PREC_MIXED if mixed else gputo.PREC_FP64)
+    s = gputo.Solver(nelx, nely, nelz, nl, opts)
+    s.set_problem(gputo.hex8_stiffness(), fixed)
+    xd = torch.as_tensor(x0, dtype=torch.float64, device="cuda")
+    xp = torch.empty_like(xd)
+    gputo.density_filter_dev(xd, xp, nelx, nely, nelz, RMIN)
+    CX = torch.empty_like(xd)
+    gputo.simp_dev(xp, CX)
+    s.setup(CX)
+    out = {"micro": args.micro, "size": args.size, "nl": nl, "device_bytes": s.device_bytes}
+    for k in kinds:
+        out[k + "_ms"] = s.time_kernel(KERNELS[k], args.reps)
+    print(json.dumps(out))
+
+
+def run_one_step(args):
+    """Profiling aid: exactly one design iteration of the bench workload after
+    the solver is built (for an ncu launch list of one step)."""
+    import torch
+
+    import gputo
+    prec = gputo.PREC_MIXED if args.one_step == "mixed" else gputo.PREC_FP64
+    F, fixed = gputo.cantilever(NELX, NELY, NELZ)
+    dl = gputo.DesignLoop(NELX, NELY, NELZ, NL, F, fixed, gputo.hex8_stiffness(), volfrac=VOLFRAC,
+                          penal=PENAL, rmin=RMIN, move=MOVE, tol=TOL, maxit=MAXIT,
+                          options=gputo.default_options(precision=prec), x0=bench_design())
+    info = dl.step()
+    torch.cuda.synchronize()
+    print(json.dumps({"one_step": args.one_step, **info}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -451,10 +497,19 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gputo", choices=["gputo", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--micro", choices=list(KERNELS) + ["all"], help="profiling aid: one kernel kind")
+    ap.add_argument("--size", default=f"{NELX}x{NELY}x{NELZ}")
+    ap.add_argument("--nl", type=int, default=NL)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--one-step", choices=["mixed", "fp64"], help="profiling aid: one design iteration")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.micro:
+        run_micro(args)
+    elif args.one_step:
+        run_one_step(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

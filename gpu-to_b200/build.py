@@ -29,8 +29,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", f"-I{CSRC}",
           f"-I{os.path.join(ROOT, 'include')}"]
 
-SOURCES = ["kernels_mg.cu", "kernels_blas.cu", "kernels_design.cu", "solver.cu", "capi.cpp"]
-HEADERS = ["gputo_internal.h", "solver.h"]
+SOURCES = ["kernels_fine.cu", "kernels_mg.cu", "kernels_blas.cu", "kernels_design.cu", "solver.cu",
+           "capi.cpp"]
+HEADERS = ["gputo_internal.h", "solver.h", "tma.h"]
 
 
 def _newer(target: str, deps: list[str]) -> bool:

@@ -144,33 +144,52 @@ int gputo_solver_setup_dev(gputo_solver *s, const double *CX, void *stream)
     return s->s.setup(CX, s->s.stream(stream));
 }
 
-int gputo_solver_solve_dev(gputo_solver *s, const double *F, double *U, double tol, int maxit,
+int gputo_solver_solve_dev(gputo_solver *h, const double *F, double *U, double tol, int maxit,
                            double *relres, int *nit, void *stream)
 {
-    if (!s || !F || !U || !relres || !nit) return GPUTO_ERR_ARG;
-    return s->s.solve(F, U, tol, maxit, relres, nit, s->s.stream(stream), nullptr);
+    if (!h || !F || !U || !relres || !nit) return GPUTO_ERR_ARG;
+    Solver &s = h->s;
+    if (!s.ready) return GPUTO_ERR_ARG;
+    cudaStream_t st = s.stream(stream);
+    gputo::launch_pack(s.lay[0], F, s.Fw, 0, st);
+    int r = s.solve(s.Fw, s.Uw, tol, maxit, relres, nit, st, nullptr);
+    if (r == GPUTO_OK || r == GPUTO_ERR_BREAKDOWN) {
+        gputo::launch_unpack(s.lay[0], s.Uw, U, 0, st);
+        GPUTO_CUDA(cudaStreamSynchronize(st));
+    }
+    return r;
 }
 
-int gputo_solver_vcycle_dev(gputo_solver *s, const double *r, double *z, void *stream)
+int gputo_solver_vcycle_dev(gputo_solver *h, const double *r, double *z, void *stream)
 {
-    if (!s || !r || !z) return GPUTO_ERR_ARG;
-    if (!s->s.ready) return GPUTO_ERR_ARG;
-    cudaStream_t st = s->s.stream(stream);
-    s->s.vcycle(r, z, nullptr, st);
+    if (!h || !r || !z) return GPUTO_ERR_ARG;
+    Solver &s = h->s;
+    if (!s.ready) return GPUTO_ERR_ARG;
+    cudaStream_t st = s.stream(stream);
+    s.launch_status = GPUTO_OK;
+    gputo::launch_pack(s.lay[0], r, s.Fw, 0, st);
+    s.vcycle(s.Fw, s.Z, nullptr, st);
+    gputo::launch_unpack(s.lay[0], s.Z, z, 0, st);
     GPUTO_CUDA(cudaStreamSynchronize(st));
     GPUTO_CUDA(cudaGetLastError());
-    return GPUTO_OK;
+    if (s.launch_status) return s.launch_status;
+    return s.check_error_flags(st);
 }
 
-int gputo_solver_apply_dev(gputo_solver *s, const double *u, double *r, void *stream)
+int gputo_solver_apply_dev(gputo_solver *h, const double *u, double *r, void *stream)
 {
-    if (!s || !u || !r) return GPUTO_ERR_ARG;
-    if (!s->s.ready) return GPUTO_ERR_ARG;
-    cudaStream_t st = s->s.stream(stream);
-    s->s.apply(u, r, st);
+    if (!h || !u || !r) return GPUTO_ERR_ARG;
+    Solver &s = h->s;
+    if (!s.ready) return GPUTO_ERR_ARG;
+    cudaStream_t st = s.stream(stream);
+    s.launch_status = GPUTO_OK;
+    gputo::launch_pack(s.lay[0], u, s.P, 0, st);
+    s.apply(s.P, s.Q, nullptr, nullptr, st);
+    gputo::launch_unpack(s.lay[0], s.Q, r, 0, st);
     GPUTO_CUDA(cudaStreamSynchronize(st));
     GPUTO_CUDA(cudaGetLastError());
-    return GPUTO_OK;
+    if (s.launch_status) return s.launch_status;
+    return s.check_error_flags(st);
 }
 
 long long gputo_solver_launch_count(const gputo_solver *) { return gputo::launches_issued(); }
@@ -186,27 +205,31 @@ int gputo_solver_time_kernel(gputo_solver *h, int which, int reps, double *ms, v
     cudaEvent_t e0, e1;
     GPUTO_CUDA(cudaEventCreate(&e0));
     GPUTO_CUDA(cudaEventCreate(&e1));
+    int lst = GPUTO_OK;
     auto launch = [&]() {
+        int r = GPUTO_OK;
         switch (which) {
         case 0:
-            gputo::launch_fine_sweep<double>(gputo::MODE_APPLY, s.g[0], s.CX, s.P, nullptr, s.L[0].diag,
-                                             s.mask[0], s.Q, 1.0, 0.0, nullptr, nullptr, st);
+            r = gputo::launch_fine_sweep<double>(gputo::MODE_APPLY, s.lay[0], s.elay, s.CXp, s.P, nullptr,
+                                                 s.L[0].diag, s.mask[0], s.Q, 1.0, 0.0, nullptr, nullptr,
+                                                 s.err, st);
             break;
         case 1:
-            gputo::launch_fine_sweep<float>(gputo::MODE_JACOBI, s.g[0], s.CXf, s.Lf[0].u0, s.Lf[0].f,
-                                            s.Lf[0].diag, s.mask[0], s.Lf[0].u1, 0.48f, 0.7f, nullptr,
-                                            nullptr, st);
+            r = gputo::launch_fine_sweep<float>(gputo::MODE_JACOBI, s.lay[0], s.elay, s.CXpf, s.Lf[0].u0,
+                                                s.Lf[0].f, s.Lf[0].diag, s.mask[0], s.Lf[0].u1, 0.48f,
+                                                0.7f, nullptr, nullptr, s.err, st);
             break;
         case 2:
-            gputo::launch_packed_sweep<float>(gputo::MODE_JACOBI, s.g[1], s.Lf[1].Apk, s.Lf[1].u0,
+            gputo::launch_packed_sweep<float>(gputo::MODE_JACOBI, s.lay[1], s.Lf[1].Apk, s.Lf[1].u0,
                                               s.Lf[1].f, s.Lf[1].diag, s.mask[1], s.Lf[1].u1, 0.48f,
                                               0.7f, nullptr, st);
             break;
         default:
-            gputo::launch_packed_sweep<double>(gputo::MODE_JACOBI, s.g[1], s.L[1].Apk, s.L[1].u0,
+            gputo::launch_packed_sweep<double>(gputo::MODE_JACOBI, s.lay[1], s.L[1].Apk, s.L[1].u0,
                                                s.L[1].f, s.L[1].diag, s.mask[1], s.L[1].u1, 0.48,
                                                0.7, nullptr, st);
         }
+        if (r && !lst) lst = r;
     };
     launch();  // warm-up
     GPUTO_CUDA(cudaEventRecord(e0, st));
@@ -218,8 +241,9 @@ int gputo_solver_time_kernel(gputo_solver *h, int which, int reps, double *ms, v
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     GPUTO_CUDA(cudaGetLastError());
+    if (lst) return lst;
     *ms = (double)t / reps;
-    return GPUTO_OK;
+    return s.check_error_flags(st);
 }
 
 // ---------------------------------------------------------------------------
@@ -291,13 +315,15 @@ int gputo_mgcg1_ex(const double *Ke0, const double *F, double *U, const double *
         return st;
     }
     const long long nd = s.g[0].ndof(), ne = s.g[0].nel();
-    GPUTO_CUDA(cudaMemcpyAsync(s.Fw, F, sizeof(double) * nd, cudaMemcpyHostToDevice, strm));
+    GPUTO_CUDA(cudaMemcpyAsync(s.Dn, F, sizeof(double) * nd, cudaMemcpyHostToDevice, strm));
+    gputo::launch_pack(s.lay[0], s.Dn, s.Fw, 0, strm);
     GPUTO_CUDA(cudaMemcpyAsync(s.CX, CX, sizeof(double) * ne, cudaMemcpyHostToDevice, strm));
     st = s.setup(s.CX, strm);
     if (!st) st = s.solve(s.Fw, s.Uw, tol, maxit, relres, nit, strm, printLev >= 2 ? log : nullptr);
     if (!st || st == GPUTO_ERR_BREAKDOWN) {
-        gputo::launch_flip_y(s.g[0].nnod(), s.Uw, strm);
-        GPUTO_CUDA(cudaMemcpyAsync(U, s.Uw, sizeof(double) * nd, cudaMemcpyDeviceToHost, strm));
+        // solver frame -> MATLAB frame: y components negated (mgcg1.cu:282-283)
+        gputo::launch_unpack(s.lay[0], s.Uw, s.Dn, 1, strm);
+        GPUTO_CUDA(cudaMemcpyAsync(U, s.Dn, sizeof(double) * nd, cudaMemcpyDeviceToHost, strm));
         GPUTO_CUDA(cudaStreamSynchronize(strm));
     }
     if (log) {

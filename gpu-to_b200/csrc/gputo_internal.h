@@ -28,6 +28,32 @@ struct Grid {
     }
 };
 
+// Row-padded storage of a level's nodal vectors.  Each (i,k) row of ny+1
+// nodes (3(ny+1) values, dofs interleaved as in the reference) is padded to
+// 'pitch' values, a multiple of 8, so that rows start on 64-byte boundaries:
+// TMA needs 16-byte row strides, which 3(ny+1) values never give for odd
+// ny+1.  Padding entries are zero and no kernel writes them.  Vectors cross
+// the C ABI in the reference's dense layout and are packed / unpacked there.
+struct Lay {
+    Grid g;
+    long long pitch;
+    static long long pitch_for(const Grid &g) { return (3LL * (g.ny + 1) + 7) & ~7LL; }
+    static Lay of(const Grid &g) { return Lay{g, pitch_for(g)}; }
+    __host__ __device__ long long row(int i, int k) const { return ((long long)i * (g.nz + 1) + k) * pitch; }
+    __host__ __device__ long long at(int i, int j, int k) const { return row(i, k) + 3LL * j; }
+    __host__ __device__ long long size() const { return (long long)(g.nx + 1) * (g.nz + 1) * pitch; }
+};
+
+// Row-padded element arrays (CX for the TMA-tiled fine sweep): rows of ny
+// elements padded to a multiple of 8.  Padding entries are zero.
+struct ELay {
+    Grid g;
+    long long pitch;
+    static ELay of(const Grid &g) { return ELay{g, ((long long)g.ny + 7) & ~7LL}; }
+    __host__ __device__ long long at(int i, int j, int k) const { return ((long long)i * g.nz + k) * pitch + j; }
+    __host__ __device__ long long size() const { return (long long)g.nx * g.nz * pitch; }
+};
+
 // Element-local node a -> (x,y,z) offset, reference order (mgcg1.c:621-624):
 // 0:(0,0,0) 1:(1,0,0) 2:(1,1,0) 3:(0,1,0) 4:(0,0,1) 5:(1,0,1) 6:(1,1,1) 7:(0,1,1)
 __host__ __device__ constexpr int local_x(int a) { return (a == 1 || a == 2 || a == 5 || a == 6) ? 1 : 0; }
@@ -92,28 +118,38 @@ int upload_quadrature_parts(double nu, cudaStream_t st);
 
 enum SweepMode { MODE_APPLY = 0, MODE_DEFECT = 1, MODE_JACOBI = 2, MODE_JACOBI_PRE = 3 };
 
-// Fine level (K = sum CX_e Ke), FP64 and FP32 instantiations.
+// Fine level (K = sum CX_e Ke), FP64 and FP32 instantiations; CX padded (ELay),
+// vectors padded (Lay).  'err' receives GPUTO_ERR_TIMEOUT if a bounded wait
+// gives up.  Returns a status (tensor-map encoding can fail).
 template <typename T>
-void launch_fine_sweep(int mode, const Grid &g, const T *CX, const T *u, const T *f,
-                       const T *diag, const uint8_t *mask, T *out, T omega, T prerelax,
-                       double *dot_partial, const int *done, cudaStream_t st);
+int launch_fine_sweep(int mode, const Lay &L, const ELay &E, const T *CX, const T *u, const T *f,
+                      const T *diag, const uint8_t *mask, T *out, T omega, T prerelax,
+                      double *dot_partial, const int *done, int *err, cudaStream_t st);
+// Opt the tile kernels into their dynamic shared memory (call once per device).
+int init_fine_kernels();
+// Number of per-CTA partials a MODE_APPLY fine sweep writes.
 int fine_sweep_blocks(const Grid &g);
-// Coarse level (packed element matrices).
+// Coarse level (packed element matrices, natural element order).
 template <typename T>
-void launch_packed_sweep(int mode, const Grid &g, const T *Apk, const T *u, const T *f,
+void launch_packed_sweep(int mode, const Lay &L, const T *Apk, const T *u, const T *f,
                          const T *diag, const uint8_t *mask, T *out, T omega, T prerelax,
                          const int *done, cudaStream_t st);
 
 template <typename T>
-void launch_restrict(const Grid &gc, const T *rf, const uint8_t *maskc, T *fc, const int *done,
-                     cudaStream_t st);
+void launch_restrict(const Lay &Lc, const Lay &Lf, const T *rf, const uint8_t *maskc, T *fc,
+                     const int *done, cudaStream_t st);
 template <typename T>
-void launch_prolong_add(const Grid &gf, const T *uc, const uint8_t *maskf, T *uf, const int *done,
-                        cudaStream_t st);
+void launch_prolong_add(const Lay &Lf, const Lay &Lc, const T *uc, const uint8_t *maskf, T *uf,
+                        const int *done, cudaStream_t st);
 
-void launch_diag_fine(const Grid &g, const double *CX, double *diag, cudaStream_t st);
+void launch_diag_fine(const Lay &L, const double *CX, double *diag, cudaStream_t st);
 template <typename T>
-void launch_diag_packed(const Grid &g, const T *Apk, T *diag, cudaStream_t st);
+void launch_diag_packed(const Lay &L, const T *Apk, T *diag, cudaStream_t st);
+// dense (reference layout) <-> padded, optionally negating y components
+void launch_pack(const Lay &L, const double *dense, double *padded, int flip_y, cudaStream_t st);
+void launch_unpack(const Lay &L, const double *padded, double *dense, int flip_y, cudaStream_t st);
+template <typename T>
+void launch_pack_cx(const ELay &E, const double *CX, T *padded, cudaStream_t st);
 void launch_build_level1(const Grid &gc, const double *CXfine, double *Apk, cudaStream_t st);
 void launch_build_galerkin(const Grid &gc, const double *Afine, double *Apk, cudaStream_t st);
 void launch_coarsest_penalty(const Grid &g, const uint8_t *mask, double *Apk, cudaStream_t st);
@@ -123,8 +159,8 @@ void launch_dense_fine(const Grid &g, const double *CX, double *Apk_tmp, cudaStr
 void launch_cholesky(int n, double *A, int *info, cudaStream_t st);
 void launch_tri_inverse(int n, const double *L, double *Linv, double *LinvT, cudaStream_t st);
 template <typename T>
-void launch_coarse_solve(int n, const double *Linv, const double *LinvT, const T *b, T *x,
-                         double *tmp, const uint8_t *mask, const int *done, cudaStream_t st);
+void launch_coarse_solve(const Lay &L, const double *Linv, const double *LinvT, const T *b, T *x,
+                         double *tmp, const int *done, cudaStream_t st);
 
 void launch_mask_from_list(long long nnod, const double *fixed1b, int nfd, uint8_t *mask,
                            cudaStream_t st);

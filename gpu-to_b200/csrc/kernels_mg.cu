@@ -1,51 +1,22 @@
-// Multigrid kernels: operator sweeps, grid transfers and hierarchy setup.
+// Multigrid kernels for the coarse levels: operator sweeps on packed element
+// matrices, grid transfers, hierarchy setup and the coarsest direct solve.
 //
 // Every operator kernel is a node-centred gather over the (up to) 8 elements
-// around a node, as the reference's multAV0c/defect0c/defectc
-// (Cantilever/TOP3D125MGCGCUDA/mgcg1.cu:941-997,1208-1324): one thread owns a
-// node's three rows, so no atomics are needed.  Unlike the reference (one
-// thread per dof, Ke read with a divergent row index), a thread computes all
-// three rows of its node, the element-local row block is warp-uniform and Ke
-// is read from constant memory as an instruction operand, and the damped
-// Jacobi update (mgcg1.cu:1199-1206) and Dirichlet zeroing (ZeroBCc,
-// :1326-1331) are fused into the sweep's epilogue.
+// around a node, as the reference's defectc
+// (Cantilever/TOP3D125MGCGCUDA/mgcg1.cu:1266-1324): one thread owns a node's
+// three rows, so no atomics are needed, and the damped Jacobi update
+// (:1199-1206) and Dirichlet zeroing (ZeroBCc, :1326-1331) are fused into the
+// epilogue.  Vectors use the padded row layout (Lay); element arrays keep the
+// reference's element order.
 #include "gputo_internal.h"
 
 namespace gputo {
 
-__constant__ double cKe64[576];
-__constant__ float cKe32[576];
 // Level-1 quadrature parts: Kg[g] packed (300), g = 4 ix + 2 iz + iy.
 __constant__ double cKg[8 * 300];
 // Prolongation weights of a coarse element onto its 8 children:
 // cPc[c][b][a] = weight of coarse local node a at child c's local node b.
 __constant__ double cPc[8 * 8 * 8];
-
-template <typename T> __device__ __forceinline__ T ke(int idx);
-template <> __device__ __forceinline__ double ke<double>(int idx) { return cKe64[idx]; }
-template <> __device__ __forceinline__ float ke<float>(int idx) { return cKe32[idx]; }
-
-int upload_fine_ke(const double *Ke_host, cudaStream_t st)
-{
-    static double last[576];
-    static bool have = false;
-    // Ke0 is an argument of every MEX call; skip the copy when it repeats.
-    bool same = have;
-    for (int m = 0; same && m < 576; ++m) same = (last[m] == Ke_host[m]);
-    if (same) return GPUTO_OK;
-    float kf[576];
-    for (int m = 0; m < 576; ++m) {
-        last[m] = Ke_host[m];
-        kf[m] = (float)Ke_host[m];
-    }
-    have = true;
-    GPUTO_CUDA(cudaMemcpyToSymbolAsync(cKe64, last, sizeof(last), 0, cudaMemcpyHostToDevice, st));
-    GPUTO_CUDA(cudaMemcpyToSymbolAsync(cKe32, kf, sizeof(kf), 0, cudaMemcpyHostToDevice, st));
-    const int s2 = upload_design_ke(last, st);
-    if (s2) return s2;
-    GPUTO_CUDA(cudaStreamSynchronize(st));
-    return GPUTO_OK;
-}
 
 // ---------------------------------------------------------------------------
 // host-side element algebra for the constant tables
@@ -124,160 +95,6 @@ int upload_quadrature_parts(double nu, cudaStream_t st)
 }
 
 // ---------------------------------------------------------------------------
-// fine-level sweep: K = sum_e CX_e Ke
-// ---------------------------------------------------------------------------
-
-// CTA tile of nodes: 32 (y) x 4 (z) x 2 (x); halo of one node / element.
-constexpr int TY = 32, TZ = 4, TX = 2;
-constexpr int HY = TY + 2, HZ = TZ + 2, HX = TX + 2;
-constexpr int EY = TY + 1, EZ = TZ + 1, EX = TX + 1;
-
-template <typename T, int MODE>
-__global__ void __launch_bounds__(TY *TZ *TX)
-fine_sweep_kernel(Grid g, const T *__restrict__ CX, const T *__restrict__ u,
-                  const T *__restrict__ f, const T *__restrict__ diag,
-                  const uint8_t *__restrict__ mask, T *__restrict__ out, T omega, T prerelax,
-                  double *__restrict__ dot_partial, const int *__restrict__ done)
-{
-    if (done && *done) return;
-    __shared__ T su[HX][HZ][HY * 3];
-    __shared__ T sc[EX][EZ][EY];
-
-    const int j0 = blockIdx.x * TY, k0 = blockIdx.y * TZ, i0 = blockIdx.z * TX;
-    const int tid = threadIdx.x + TY * (threadIdx.y + TZ * threadIdx.z);
-    constexpr int NT = TY * TZ * TX;
-
-    // halo of u: rows of HY consecutive nodes (3*HY consecutive values in memory)
-    for (int idx = tid; idx < HX * HZ * HY * 3; idx += NT) {
-        const int row = idx / (HY * 3), col = idx - row * (HY * 3);
-        const int hx = row / HZ, hz = row - hx * HZ;
-        const int hy = col / 3, d = col - 3 * hy;
-        const int i = i0 - 1 + hx, k = k0 - 1 + hz, j = j0 - 1 + hy;
-        T v = T(0);
-        if (i >= 0 && i <= g.nx && k >= 0 && k <= g.nz && j >= 0 && j <= g.ny) {
-            const long long dof = 3 * g.node(i, j, k) + d;
-            if (MODE == MODE_JACOBI_PRE)
-                v = prerelax * f[dof] / diag[dof];
-            else
-                v = u[dof];
-        }
-        su[hx][hz][col] = v;
-    }
-    for (int idx = tid; idx < EX * EZ * EY; idx += NT) {
-        const int row = idx / EY, ey = idx - row * EY;
-        const int ex = row / EZ, ez = row - ex * EZ;
-        const int i = i0 - 1 + ex, k = k0 - 1 + ez, j = j0 - 1 + ey;
-        T v = T(0);
-        if (i >= 0 && i < g.nx && k >= 0 && k < g.nz && j >= 0 && j < g.ny) v = CX[g.elem(i, j, k)];
-        sc[ex][ez][ey] = v;
-    }
-    __syncthreads();
-
-    const int ty = threadIdx.x, tz = threadIdx.y, tx = threadIdx.z;
-    const int j = j0 + ty, k = k0 + tz, i = i0 + tx;
-    const bool active = (j <= g.ny) && (k <= g.nz) && (i <= g.nx);
-
-    T acc0 = T(0), acc1 = T(0), acc2 = T(0);
-#pragma unroll
-    for (int ex = 0; ex < 2; ++ex)
-#pragma unroll
-        for (int ez = 0; ez < 2; ++ez)
-#pragma unroll
-            for (int ey = 0; ey < 2; ++ey) {
-                const T c = sc[tx + ex][tz + ez][ty + ey];
-                const int a = local_index(1 - ex, 1 - ey, 1 - ez);
-                T t0 = T(0), t1 = T(0), t2 = T(0);
-#pragma unroll
-                for (int b = 0; b < 8; ++b) {
-                    const T *up = &su[tx + ex + local_x(b)][tz + ez + local_z(b)][(ty + ey + local_y(b)) * 3];
-                    const T u0 = up[0], u1 = up[1], u2 = up[2];
-                    const int r0 = (3 * a) * 24 + 3 * b, r1 = r0 + 24, r2 = r0 + 48;
-                    t0 = fma(ke<T>(r0), u0, fma(ke<T>(r0 + 1), u1, fma(ke<T>(r0 + 2), u2, t0)));
-                    t1 = fma(ke<T>(r1), u0, fma(ke<T>(r1 + 1), u1, fma(ke<T>(r1 + 2), u2, t1)));
-                    t2 = fma(ke<T>(r2), u0, fma(ke<T>(r2 + 1), u1, fma(ke<T>(r2 + 2), u2, t2)));
-                }
-                acc0 = fma(c, t0, acc0);
-                acc1 = fma(c, t1, acc1);
-                acc2 = fma(c, t2, acc2);
-            }
-
-    double dsum = 0.0;
-    if (active) {
-        const long long n = g.node(i, j, k);
-        const unsigned m = mask[n];
-        const T acc[3] = {acc0, acc1, acc2};
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            const long long dof = 3 * n + d;
-            const bool fixed = (m >> d) & 1u;
-            if (MODE == MODE_APPLY) {
-                const T q = fixed ? T(0) : acc[d];
-                out[dof] = q;
-                if (dot_partial) dsum += (double)su[tx + 1][tz + 1][(ty + 1) * 3 + d] * (double)q;
-            } else if (MODE == MODE_DEFECT) {
-                out[dof] = fixed ? T(0) : f[dof] - acc[d];
-            } else {
-                const T r = fixed ? T(0) : f[dof] - acc[d];
-                const T us = su[tx + 1][tz + 1][(ty + 1) * 3 + d];
-                out[dof] = us + omega * r / diag[dof];
-            }
-        }
-    }
-    if (MODE == MODE_APPLY && dot_partial) {
-        // block reduction of p'q in FP64, fixed order
-        __shared__ double red[NT / 32];
-        for (int o = 16; o > 0; o >>= 1) dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
-        if ((tid & 31) == 0) red[tid >> 5] = dsum;
-        __syncthreads();
-        if (tid < 32) {
-            double v = tid < NT / 32 ? red[tid] : 0.0;
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (tid == 0)
-                dot_partial[blockIdx.x + gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z)] = v;
-        }
-    }
-}
-
-template <typename T>
-void launch_fine_sweep(int mode, const Grid &g, const T *CX, const T *u, const T *f, const T *diag,
-                       const uint8_t *mask, T *out, T omega, T prerelax, double *dot_partial,
-                       const int *done, cudaStream_t st)
-{
-    dim3 block(TY, TZ, TX);
-    dim3 grid((g.ny + 1 + TY - 1) / TY, (g.nz + 1 + TZ - 1) / TZ, (g.nx + 1 + TX - 1) / TX);
-    switch (mode) {
-    case MODE_APPLY:
-        fine_sweep_kernel<T, MODE_APPLY><<<grid, block, 0, st>>>(g, CX, u, f, diag, mask, out, omega,
-                                                                 prerelax, dot_partial, done);
-        break;
-    case MODE_DEFECT:
-        fine_sweep_kernel<T, MODE_DEFECT><<<grid, block, 0, st>>>(g, CX, u, f, diag, mask, out, omega,
-                                                                  prerelax, dot_partial, done);
-        break;
-    case MODE_JACOBI:
-        fine_sweep_kernel<T, MODE_JACOBI><<<grid, block, 0, st>>>(g, CX, u, f, diag, mask, out, omega,
-                                                                  prerelax, dot_partial, done);
-        break;
-    default:
-        fine_sweep_kernel<T, MODE_JACOBI_PRE><<<grid, block, 0, st>>>(g, CX, u, f, diag, mask, out,
-                                                                      omega, prerelax, dot_partial, done);
-    }
-    count_launches(1);
-}
-
-int fine_sweep_blocks(const Grid &g)
-{
-    return ((g.ny + 1 + TY - 1) / TY) * ((g.nz + 1 + TZ - 1) / TZ) * ((g.nx + 1 + TX - 1) / TX);
-}
-
-template void launch_fine_sweep<double>(int, const Grid &, const double *, const double *,
-                                        const double *, const double *, const uint8_t *, double *,
-                                        double, double, double *, const int *, cudaStream_t);
-template void launch_fine_sweep<float>(int, const Grid &, const float *, const float *, const float *,
-                                       const float *, const uint8_t *, float *, float, float,
-                                       double *, const int *, cudaStream_t);
-
-// ---------------------------------------------------------------------------
 // coarse-level sweep: packed element matrices [300][nel]
 // ---------------------------------------------------------------------------
 
@@ -291,12 +108,13 @@ __device__ __forceinline__ void node_ijk(const Grid &g, long long n, int &i, int
 
 template <typename T, int MODE>
 __global__ void __launch_bounds__(128)
-packed_sweep_kernel(Grid g, const T *__restrict__ A, const T *__restrict__ u,
+packed_sweep_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u,
                     const T *__restrict__ f, const T *__restrict__ diag,
                     const uint8_t *__restrict__ mask, T *__restrict__ out, T omega, T prerelax,
                     const int *__restrict__ done)
 {
     if (done && *done) return;
+    const Grid &g = L.g;
     const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= g.nnod()) return;
     int i, j, k;
@@ -319,11 +137,11 @@ packed_sweep_kernel(Grid g, const T *__restrict__ A, const T *__restrict__ u,
                 const int a = local_index(1 - ex, 1 - ey, 1 - ez);
 #pragma unroll
                 for (int b = 0; b < 8; ++b) {
-                    const long long nb = g.node(ei + local_x(b), ej + local_y(b), ek + local_z(b));
+                    const long long nb = L.at(ei + local_x(b), ej + local_y(b), ek + local_z(b));
                     T ub[3];
 #pragma unroll
                     for (int q = 0; q < 3; ++q) {
-                        const long long dof = 3 * nb + q;
+                        const long long dof = nb + q;
                         ub[q] = (MODE == MODE_JACOBI_PRE) ? prerelax * f[dof] / diag[dof] : u[dof];
                     }
 #pragma unroll
@@ -336,9 +154,10 @@ packed_sweep_kernel(Grid g, const T *__restrict__ A, const T *__restrict__ u,
         }
     }
     const unsigned m = mask[n];
+    const long long base = L.at(i, j, k);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        const long long dof = 3 * n + d;
+        const long long dof = base + d;
         const bool fixed = (m >> d) & 1u;
         if (MODE == MODE_APPLY) {
             out[dof] = fixed ? T(0) : acc[d];
@@ -353,32 +172,32 @@ packed_sweep_kernel(Grid g, const T *__restrict__ A, const T *__restrict__ u,
 }
 
 template <typename T>
-void launch_packed_sweep(int mode, const Grid &g, const T *Apk, const T *u, const T *f,
+void launch_packed_sweep(int mode, const Lay &L, const T *Apk, const T *u, const T *f,
                          const T *diag, const uint8_t *mask, T *out, T omega, T prerelax,
                          const int *done, cudaStream_t st)
 {
     const int bs = 128;
-    const unsigned nb = (unsigned)((g.nnod() + bs - 1) / bs);
+    const unsigned nb = (unsigned)((L.g.nnod() + bs - 1) / bs);
     switch (mode) {
     case MODE_APPLY:
-        packed_sweep_kernel<T, MODE_APPLY><<<nb, bs, 0, st>>>(g, Apk, u, f, diag, mask, out, omega, prerelax, done);
+        packed_sweep_kernel<T, MODE_APPLY><<<nb, bs, 0, st>>>(L, Apk, u, f, diag, mask, out, omega, prerelax, done);
         break;
     case MODE_DEFECT:
-        packed_sweep_kernel<T, MODE_DEFECT><<<nb, bs, 0, st>>>(g, Apk, u, f, diag, mask, out, omega, prerelax, done);
+        packed_sweep_kernel<T, MODE_DEFECT><<<nb, bs, 0, st>>>(L, Apk, u, f, diag, mask, out, omega, prerelax, done);
         break;
     case MODE_JACOBI:
-        packed_sweep_kernel<T, MODE_JACOBI><<<nb, bs, 0, st>>>(g, Apk, u, f, diag, mask, out, omega, prerelax, done);
+        packed_sweep_kernel<T, MODE_JACOBI><<<nb, bs, 0, st>>>(L, Apk, u, f, diag, mask, out, omega, prerelax, done);
         break;
     default:
-        packed_sweep_kernel<T, MODE_JACOBI_PRE><<<nb, bs, 0, st>>>(g, Apk, u, f, diag, mask, out, omega, prerelax, done);
+        packed_sweep_kernel<T, MODE_JACOBI_PRE><<<nb, bs, 0, st>>>(L, Apk, u, f, diag, mask, out, omega, prerelax, done);
     }
     count_launches(1);
 }
 
-template void launch_packed_sweep<double>(int, const Grid &, const double *, const double *,
+template void launch_packed_sweep<double>(int, const Lay &, const double *, const double *,
                                           const double *, const double *, const uint8_t *, double *,
                                           double, double, const int *, cudaStream_t);
-template void launch_packed_sweep<float>(int, const Grid &, const float *, const float *,
+template void launch_packed_sweep<float>(int, const Lay &, const float *, const float *,
                                          const float *, const float *, const uint8_t *, float *,
                                          float, float, const int *, cudaStream_t);
 
@@ -390,15 +209,17 @@ template void launch_packed_sweep<float>(int, const Grid &, const float *, const
 // fine neighbours of each coarse node (mgcg1.cu:792-831 rstrFc), then the
 // coarse Dirichlet rows are zeroed (ZeroBCc after rstrFc, mgcg1.cu:537).
 template <typename T>
-__global__ void restrict_kernel(Grid gc, const T *__restrict__ rf, const uint8_t *__restrict__ maskc,
-                                T *__restrict__ fc, const int *__restrict__ done)
+__global__ void restrict_kernel(Lay Lc, Lay Lf, const T *__restrict__ rf,
+                                const uint8_t *__restrict__ maskc, T *__restrict__ fc,
+                                const int *__restrict__ done)
 {
     if (done && *done) return;
+    const Grid &gc = Lc.g;
     const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= gc.nnod()) return;
     int i, j, k;
     node_ijk(gc, n, i, j, k);
-    const Grid gf{2 * gc.nx, 2 * gc.ny, 2 * gc.nz};
+    const Grid &gf = Lf.g;
     T acc[3] = {T(0), T(0), T(0)};
     for (int di = -1; di <= 1; ++di) {
         const int fi = 2 * i + di;
@@ -410,109 +231,85 @@ __global__ void restrict_kernel(Grid gc, const T *__restrict__ rf, const uint8_t
                 const int fj = 2 * j + dj;
                 if (fj < 0 || fj > gf.ny) continue;
                 const T w = T(1) / T(1 << (abs(di) + abs(dj) + abs(dk)));
-                const long long nf = gf.node(fi, fj, fk);
+                const long long nf = Lf.at(fi, fj, fk);
 #pragma unroll
-                for (int d = 0; d < 3; ++d) acc[d] = fma(w, rf[3 * nf + d], acc[d]);
+                for (int d = 0; d < 3; ++d) acc[d] = fma(w, rf[nf + d], acc[d]);
             }
         }
     }
     const unsigned m = maskc[n];
+    const long long base = Lc.at(i, j, k);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) fc[3 * n + d] = ((m >> d) & 1u) ? T(0) : acc[d];
+    for (int d = 0; d < 3; ++d) fc[base + d] = ((m >> d) & 1u) ? T(0) : acc[d];
 }
 
 template <typename T>
-void launch_restrict(const Grid &gc, const T *rf, const uint8_t *maskc, T *fc, const int *done,
-                     cudaStream_t st)
+void launch_restrict(const Lay &Lc, const Lay &Lf, const T *rf, const uint8_t *maskc, T *fc,
+                     const int *done, cudaStream_t st)
 {
     const int bs = 128;
-    restrict_kernel<T><<<(unsigned)((gc.nnod() + bs - 1) / bs), bs, 0, st>>>(gc, rf, maskc, fc, done);
+    restrict_kernel<T><<<(unsigned)((Lc.g.nnod() + bs - 1) / bs), bs, 0, st>>>(Lc, Lf, rf, maskc, fc, done);
     count_launches(1);
 }
-template void launch_restrict<double>(const Grid &, const double *, const uint8_t *, double *,
-                                      const int *, cudaStream_t);
-template void launch_restrict<float>(const Grid &, const float *, const uint8_t *, float *,
-                                     const int *, cudaStream_t);
+template void launch_restrict<double>(const Lay &, const Lay &, const double *, const uint8_t *,
+                                      double *, const int *, cudaStream_t);
+template void launch_restrict<float>(const Lay &, const Lay &, const float *, const uint8_t *,
+                                     float *, const int *, cudaStream_t);
 
 // u_f += P u_c, trilinear (mgcg1.cu:1587-1641 interpc), then the fine
 // Dirichlet dofs are zeroed (ZeroBCc after interpc, mgcg1.cu:631).
 template <typename T>
-__global__ void prolong_kernel(Grid gf, const T *__restrict__ uc, const uint8_t *__restrict__ maskf,
-                               T *__restrict__ uf, const int *__restrict__ done)
+__global__ void prolong_kernel(Lay Lf, Lay Lc, const T *__restrict__ uc,
+                               const uint8_t *__restrict__ maskf, T *__restrict__ uf,
+                               const int *__restrict__ done)
 {
     if (done && *done) return;
+    const Grid &gf = Lf.g;
     const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= gf.nnod()) return;
     int i, j, k;
     node_ijk(gf, n, i, j, k);
-    const Grid gc{gf.nx / 2, gf.ny / 2, gf.nz / 2};
     const int ni = (i & 1) + 1, nj = (j & 1) + 1, nk = (k & 1) + 1;
     T acc[3] = {T(0), T(0), T(0)};
     for (int a = 0; a < ni; ++a)
         for (int c = 0; c < nk; ++c)
             for (int b = 0; b < nj; ++b) {
-                const long long nc = gc.node((i >> 1) + a, (j >> 1) + b, (k >> 1) + c);
+                const long long nc = Lc.at((i >> 1) + a, (j >> 1) + b, (k >> 1) + c);
 #pragma unroll
-                for (int d = 0; d < 3; ++d) acc[d] += uc[3 * nc + d];
+                for (int d = 0; d < 3; ++d) acc[d] += uc[nc + d];
             }
     const T w = T(1) / T(ni * nj * nk);
     const unsigned m = maskf[n];
+    const long long base = Lf.at(i, j, k);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        const long long dof = 3 * n + d;
+        const long long dof = base + d;
         uf[dof] = ((m >> d) & 1u) ? T(0) : fma(w, acc[d], uf[dof]);
     }
 }
 
 template <typename T>
-void launch_prolong_add(const Grid &gf, const T *uc, const uint8_t *maskf, T *uf, const int *done,
-                        cudaStream_t st)
+void launch_prolong_add(const Lay &Lf, const Lay &Lc, const T *uc, const uint8_t *maskf, T *uf,
+                        const int *done, cudaStream_t st)
 {
     const int bs = 128;
-    prolong_kernel<T><<<(unsigned)((gf.nnod() + bs - 1) / bs), bs, 0, st>>>(gf, uc, maskf, uf, done);
+    prolong_kernel<T><<<(unsigned)((Lf.g.nnod() + bs - 1) / bs), bs, 0, st>>>(Lf, Lc, uc, maskf, uf, done);
     count_launches(1);
 }
-template void launch_prolong_add<double>(const Grid &, const double *, const uint8_t *, double *,
-                                         const int *, cudaStream_t);
-template void launch_prolong_add<float>(const Grid &, const float *, const uint8_t *, float *,
-                                        const int *, cudaStream_t);
+template void launch_prolong_add<double>(const Lay &, const Lay &, const double *, const uint8_t *,
+                                         double *, const int *, cudaStream_t);
+template void launch_prolong_add<float>(const Lay &, const Lay &, const float *, const uint8_t *,
+                                        float *, const int *, cudaStream_t);
 
 // ---------------------------------------------------------------------------
 // hierarchy setup
 // ---------------------------------------------------------------------------
 
-// diag(K) on the fine level: sum over adjacent elements of CX_e Ke[m][m]
-// (mgcg1.cu:1447-1487 prepAD0c).
-__global__ void diag_fine_kernel(Grid g, const double *__restrict__ CX, double *__restrict__ diag)
-{
-    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= g.nnod()) return;
-    int i, j, k;
-    node_ijk(g, n, i, j, k);
-    double acc[3] = {0, 0, 0};
-    for (int ex = 0; ex < 2; ++ex)
-        for (int ez = 0; ez < 2; ++ez)
-            for (int ey = 0; ey < 2; ++ey) {
-                const int ei = i - 1 + ex, ej = j - 1 + ey, ek = k - 1 + ez;
-                if (ei < 0 || ei >= g.nx || ej < 0 || ej >= g.ny || ek < 0 || ek >= g.nz) continue;
-                const double c = CX[g.elem(ei, ej, ek)];
-                const int a = local_index(1 - ex, 1 - ey, 1 - ez);
-                for (int d = 0; d < 3; ++d) acc[d] += c * cKe64[(3 * a + d) * 25];
-            }
-    for (int d = 0; d < 3; ++d) diag[3 * n + d] = acc[d];
-}
-
-void launch_diag_fine(const Grid &g, const double *CX, double *diag, cudaStream_t st)
-{
-    const int bs = 128;
-    diag_fine_kernel<<<(unsigned)((g.nnod() + bs - 1) / bs), bs, 0, st>>>(g, CX, diag);
-    count_launches(1);
-}
-
 // diag of a packed coarse level (mgcg1.cu:1404-1445 prepADc).
 template <typename T>
-__global__ void diag_packed_kernel(Grid g, const T *__restrict__ A, T *__restrict__ diag)
+__global__ void diag_packed_kernel(Lay L, const T *__restrict__ A, T *__restrict__ diag)
 {
+    const Grid &g = L.g;
     const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= g.nnod()) return;
     int i, j, k;
@@ -528,18 +325,73 @@ __global__ void diag_packed_kernel(Grid g, const T *__restrict__ A, T *__restric
                 const int a = local_index(1 - ex, 1 - ey, 1 - ez);
                 for (int d = 0; d < 3; ++d) acc[d] += A[(long long)packed_index(3 * a + d, 3 * a + d) * nel + e];
             }
-    for (int d = 0; d < 3; ++d) diag[3 * n + d] = acc[d];
+    const long long base = L.at(i, j, k);
+    for (int d = 0; d < 3; ++d) diag[base + d] = acc[d];
 }
 
 template <typename T>
-void launch_diag_packed(const Grid &g, const T *Apk, T *diag, cudaStream_t st)
+void launch_diag_packed(const Lay &L, const T *Apk, T *diag, cudaStream_t st)
 {
     const int bs = 128;
-    diag_packed_kernel<T><<<(unsigned)((g.nnod() + bs - 1) / bs), bs, 0, st>>>(g, Apk, diag);
+    diag_packed_kernel<T><<<(unsigned)((L.g.nnod() + bs - 1) / bs), bs, 0, st>>>(L, Apk, diag);
     count_launches(1);
 }
-template void launch_diag_packed<double>(const Grid &, const double *, double *, cudaStream_t);
-template void launch_diag_packed<float>(const Grid &, const float *, float *, cudaStream_t);
+template void launch_diag_packed<double>(const Lay &, const double *, double *, cudaStream_t);
+template void launch_diag_packed<float>(const Lay &, const float *, float *, cudaStream_t);
+
+// dense reference layout <-> padded layout (y optionally negated)
+__global__ void pack_kernel(Lay L, double *__restrict__ dense, double *__restrict__ padded,
+                            int flip_y, int to_padded)
+{
+    const Grid &g = L.g;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= g.ndof()) return;
+    const long long n = t / 3;
+    const int d = (int)(t - 3 * n);
+    const long long row = n / (g.ny + 1);
+    const int j = (int)(n - row * (g.ny + 1));
+    const long long p = row * L.pitch + 3LL * j + d;
+    const double s = (flip_y && d == 1) ? -1.0 : 1.0;
+    if (to_padded) padded[p] = s * dense[t];
+    else dense[t] = s * padded[p];
+}
+
+void launch_pack(const Lay &L, const double *dense, double *padded, int flip_y, cudaStream_t st)
+{
+    const int bs = 256;
+    pack_kernel<<<(unsigned)((L.g.ndof() + bs - 1) / bs), bs, 0, st>>>(L, const_cast<double *>(dense), padded,
+                                                                        flip_y, 1);
+    count_launches(1);
+}
+
+void launch_unpack(const Lay &L, const double *padded, double *dense, int flip_y, cudaStream_t st)
+{
+    const int bs = 256;
+    pack_kernel<<<(unsigned)((L.g.ndof() + bs - 1) / bs), bs, 0, st>>>(L, dense, const_cast<double *>(padded),
+                                                                        flip_y, 0);
+    count_launches(1);
+}
+
+template <typename T>
+__global__ void pack_cx_kernel(ELay E, const double *__restrict__ CX, T *__restrict__ out)
+{
+    const Grid &g = E.g;
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= g.nel()) return;
+    const long long row = e / g.ny;
+    const int j = (int)(e - row * g.ny);
+    out[row * E.pitch + j] = (T)CX[e];
+}
+
+template <typename T>
+void launch_pack_cx(const ELay &E, const double *CX, T *padded, cudaStream_t st)
+{
+    const int bs = 256;
+    pack_cx_kernel<T><<<(unsigned)((E.g.nel() + bs - 1) / bs), bs, 0, st>>>(E, CX, padded);
+    count_launches(1);
+}
+template void launch_pack_cx<double>(const ELay &, const double *, double *, cudaStream_t);
+template void launch_pack_cx<float>(const ELay &, const double *, float *, cudaStream_t);
 
 // Level 1: A_E = sum_g CX(child containing Gauss point g) Kg[g]
 // (mgcg1.cu:2042-2070 coarseAe2c).  One thread per (element, packed entry).
@@ -615,24 +467,6 @@ __global__ void __launch_bounds__(576) build_galerkin_kernel(Grid gc, const doub
 void launch_build_galerkin(const Grid &gc, const double *Afine, double *Apk, cudaStream_t st)
 {
     build_galerkin_kernel<<<(unsigned)gc.nel(), 576, 0, st>>>(gc, Afine, Apk);
-    count_launches(1);
-}
-
-// Fine level as packed matrices (only for a single-level hierarchy).
-__global__ void dense_fine_kernel(Grid g, const double *__restrict__ CX, double *__restrict__ A)
-{
-    const long long nel = g.nel();
-    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= nel) return;
-    const double c = CX[e];
-    for (int m = 0; m < 24; ++m)
-        for (int n = 0; n <= m; ++n) A[(long long)packed_index(m, n) * nel + e] = c * cKe64[m * 24 + n];
-}
-
-void launch_dense_fine(const Grid &g, const double *CX, double *Apk, cudaStream_t st)
-{
-    const int bs = 128;
-    dense_fine_kernel<<<(unsigned)((g.nel() + bs - 1) / bs), bs, 0, st>>>(g, CX, Apk);
     count_launches(1);
 }
 
@@ -799,38 +633,54 @@ void launch_tri_inverse(int n, const double *L, double *Linv, double *LinvT, cud
 
 // y = M x for a dense row-major n x n matrix, one warp per row, FP64
 // accumulation; the input and output may be FP32 or FP64.
+// Position of dense (reference-order) dof r in the padded layout.
+__device__ __forceinline__ long long padded_pos(const Lay &L, long long r)
+{
+    const long long n = r / 3;
+    const long long row = n / (L.g.ny + 1);
+    const long long j = n - row * (L.g.ny + 1);
+    return row * L.pitch + 3 * j + (r - 3 * n);
+}
+
+// y = M x for a dense row-major n x n triangular matrix, one warp per row,
+// FP64 accumulation.  in_padded / out_padded: x / y live in the level's padded
+// layout (otherwise dense vectors of n).
 template <typename Tin, typename Tout>
-__global__ void gemv_warp_kernel(int n, const double *__restrict__ M, const Tin *__restrict__ x,
-                                 Tout *__restrict__ y, int lower, const int *__restrict__ done)
+__global__ void gemv_warp_kernel(Lay L, const double *__restrict__ M, const Tin *__restrict__ x,
+                                 Tout *__restrict__ y, int lower, int in_padded, int out_padded,
+                                 const int *__restrict__ done)
 {
     if (done && *done) return;
+    const int n = (int)L.g.ndof();
     const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (row >= n) return;
     const int lo = lower ? 0 : row, hi = lower ? row + 1 : n;
     const double *mr = M + (long long)row * n;
     double s = 0.0;
-    for (int c = lo + lane; c < hi; c += 32) s = fma(mr[c], (double)x[c], s);
+    for (int c = lo + lane; c < hi; c += 32)
+        s = fma(mr[c], (double)x[in_padded ? padded_pos(L, c) : c], s);
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) y[row] = (Tout)s;
+    if (lane == 0) y[out_padded ? padded_pos(L, row) : row] = (Tout)s;
 }
 
+// Coarsest solve x = A^-1 b = Linv^T (Linv b) with the explicit inverse of the
+// Cholesky factor (replaces cholsl1's 2n single-block launches, mgcg1.cu:2175-2232).
 template <typename T>
-void launch_coarse_solve(int n, const double *Linv, const double *LinvT, const T *b, T *x,
-                         double *tmp, const uint8_t *, const int *done, cudaStream_t st)
+void launch_coarse_solve(const Lay &L, const double *Linv, const double *LinvT, const T *b, T *x,
+                         double *tmp, const int *done, cudaStream_t st)
 {
+    const int n = (int)L.g.ndof();
     const int bs = 256;
     const unsigned nb = (unsigned)((n * 32 + bs - 1) / bs);
-    gemv_warp_kernel<T, double><<<nb, bs, 0, st>>>(n, Linv, b, tmp, 1, done);
-    gemv_warp_kernel<double, T><<<nb, bs, 0, st>>>(n, LinvT, tmp, x, 0, done);
+    gemv_warp_kernel<T, double><<<nb, bs, 0, st>>>(L, Linv, b, tmp, 1, 1, 0, done);
+    gemv_warp_kernel<double, T><<<nb, bs, 0, st>>>(L, LinvT, tmp, x, 0, 0, 1, done);
     count_launches(2);
 }
-template void launch_coarse_solve<double>(int, const double *, const double *, const double *,
-                                          double *, double *, const uint8_t *, const int *,
-                                          cudaStream_t);
-template void launch_coarse_solve<float>(int, const double *, const double *, const float *,
-                                         float *, double *, const uint8_t *, const int *,
-                                         cudaStream_t);
+template void launch_coarse_solve<double>(const Lay &, const double *, const double *, const double *,
+                                          double *, double *, const int *, cudaStream_t);
+template void launch_coarse_solve<float>(const Lay &, const double *, const double *, const float *,
+                                         float *, double *, const int *, cudaStream_t);
 
 // Fixed-dof mask from the 1-based list (indices validated on the host).
 __global__ void mask_from_list_kernel(const double *__restrict__ fixed1b, int nfd, uint8_t *mask)

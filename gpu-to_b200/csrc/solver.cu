@@ -4,9 +4,12 @@
 // Differences from the reference's host code, all behaviour-preserving:
 //  * buffers are allocated once per solver (64-bit sizes) and reused across
 //    calls instead of cudaDeviceReset + cudaMalloc on every call (:202-215);
+//  * nodal vectors live in a row-padded layout (Lay) so the fine-level sweep
+//    can load its tiles by TMA; the boundary packs / unpacks the reference's
+//    dense layout;
 //  * PCG scalars never leave the device inside an iteration; the host reads a
-//    16-byte status block every opt.check_every iterations (the reference
-//    copies each dot product back, :1033-1041);
+//    status block every opt.check_every iterations (the reference copies each
+//    dot product back, :1033-1041);
 //  * level 1 stores the quadrature operator, levels >= 2 the Galerkin
 //    operator, both packed [300][nel] (structure of arrays, coalesced);
 //  * the coarsest solve is two dense triangular products with the explicitly
@@ -37,14 +40,19 @@ static int checked_malloc(void **p, size_t bytes, size_t &total)
     return GPUTO_OK;
 }
 
-#define ALLOC(ptr, count)                                                                 \
-    do {                                                                                  \
-        int _st = checked_malloc((void **)&(ptr), sizeof(*(ptr)) * (size_t)(count), bytes); \
-        if (_st) return _st;                                                              \
+// Allocate, zero (padding must read as zero) and remember for release.
+#define ALLOC(ptr, count)                                                                   \
+    do {                                                                                    \
+        const size_t _b = sizeof(*(ptr)) * (size_t)(count);                                 \
+        int _st = checked_malloc((void **)&(ptr), _b, bytes);                               \
+        if (_st) return _st;                                                                \
+        owned.push_back((void *)(ptr));                                                     \
+        GPUTO_CUDA(cudaMemsetAsync((void *)(ptr), 0, _b ? _b : 16, own_stream));             \
     } while (0)
 
 Solver::~Solver()
 {
+    if (own_stream) cudaStreamSynchronize(own_stream);
     for (void *p : owned) cudaFree(p);
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (h_sc) cudaFreeHost(h_sc);
@@ -57,23 +65,13 @@ int Solver::alloc_levels(LevelBuf<T> *Lv, bool with_matrices)
     for (int l = 0; l < nl; ++l) {
         LevelBuf<T> &b = Lv[l];
         b.g = g[l];
-        const long long nd = g[l].ndof();
-        ALLOC(b.u0, nd);
-        owned.push_back(b.u0);
-        ALLOC(b.r, nd);
-        owned.push_back(b.r);
-        ALLOC(b.diag, nd);
-        owned.push_back(b.diag);
-        ALLOC(b.u1, nd);
-        owned.push_back(b.u1);
-        ALLOC(b.f, nd);
-        owned.push_back(b.f);
-        if (l > 0) {
-            if (with_matrices) {
-                ALLOC(b.Apk, 300 * g[l].nel());
-                owned.push_back(b.Apk);
-            }
-        }
+        const long long nv = lay[l].size();
+        ALLOC(b.u0, nv);
+        ALLOC(b.r, nv);
+        ALLOC(b.diag, nv);
+        ALLOC(b.u1, nv);
+        ALLOC(b.f, nv);
+        if (l > 0 && with_matrices) ALLOC(b.Apk, 300 * g[l].nel());
         b.mask = mask[l];
     }
     return GPUTO_OK;
@@ -98,7 +96,11 @@ int Solver::create(int nelx, int nely, int nelz, int nl_, const gputo_options *o
         return GPUTO_ERR_ARG;
     }
     nl = nl_;
-    for (int l = 0; l < nl; ++l) g[l] = Grid{nelx >> l, nely >> l, nelz >> l};
+    for (int l = 0; l < nl; ++l) {
+        g[l] = Grid{nelx >> l, nely >> l, nelz >> l};
+        lay[l] = Lay::of(g[l]);
+    }
+    elay = ELay::of(g[0]);
     nc = (int)g[nl - 1].ndof();
     if (nc > opt.max_coarse_dofs) {
         set_error("coarsest grid has " + std::to_string(nc) + " dofs, above max_coarse_dofs=" +
@@ -107,63 +109,41 @@ int Solver::create(int nelx, int nely, int nelz, int nl_, const gputo_options *o
     }
     GPUTO_CUDA(cudaGetDevice(&device));
     GPUTO_CUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
+    int ik = init_fine_kernels();
+    if (ik) return ik;
 
-    const long long nd = g[0].ndof(), ne = g[0].nel();
-    for (int l = 0; l < nl; ++l) {
-        ALLOC(mask[l], (g[l].nnod() + 3) & ~3LL);
-        owned.push_back(mask[l]);
-    }
+    const long long nv = lay[0].size(), ne = g[0].nel();
+    for (int l = 0; l < nl; ++l) ALLOC(mask[l], (g[l].nnod() + 3) & ~3LL);
     ALLOC(CX, ne);
-    owned.push_back(CX);
-    ALLOC(R, nd);
-    owned.push_back(R);
-    ALLOC(P, nd);
-    owned.push_back(P);
-    ALLOC(Q, nd);
-    owned.push_back(Q);
-    ALLOC(Z, nd);
-    owned.push_back(Z);
-    ALLOC(Uw, nd);
-    owned.push_back(Uw);
-    ALLOC(Fw, nd);
-    owned.push_back(Fw);
-    if (opt.precision == GPUTO_PREC_MIXED) {
-        ALLOC(Zold, nd);
-        owned.push_back(Zold);
-    }
+    ALLOC(CXp, elay.size());
+    ALLOC(R, nv);
+    ALLOC(P, nv);
+    ALLOC(Q, nv);
+    ALLOC(Z, nv);
+    ALLOC(Uw, nv);
+    ALLOC(Fw, nv);
+    ALLOC(Dn, g[0].ndof());
+    if (opt.precision == GPUTO_PREC_MIXED) ALLOC(Zold, nv);
     int st = alloc_levels<double>(L, true);
     if (st) return st;
     if (opt.precision == GPUTO_PREC_MIXED) {
         st = alloc_levels<float>(Lf, true);
         if (st) return st;
-        ALLOC(CXf, ne);
-        owned.push_back(CXf);
+        ALLOC(CXpf, elay.size());
     }
     ALLOC(AQ, (long long)nc * nc);
-    owned.push_back(AQ);
     ALLOC(Linv, (long long)nc * nc);
-    owned.push_back(Linv);
     ALLOC(LinvT, (long long)nc * nc);
-    owned.push_back(LinvT);
     ALLOC(ctmp, nc);
-    owned.push_back(ctmp);
-    if (nl == 1) {
-        ALLOC(Apk0, 300 * g[0].nel());
-        owned.push_back(Apk0);
-    }
-    partial_cap = std::max(fine_sweep_blocks(g[0]), 1 << 12);  // dot2 needs 2 per CTA
+    if (nl == 1) ALLOC(Apk0, 300 * g[0].nel());
+    partial_cap = std::max(fine_sweep_blocks(g[0]), 1 << 12);
     ALLOC(partial, partial_cap);
-    owned.push_back(partial);
     ALLOC(ticket, 4);
-    owned.push_back(ticket);
     ALLOC(sc, 1);
-    owned.push_back(sc);
     ALLOC(info, 4);
-    owned.push_back(info);
+    ALLOC(err, 4);
     ALLOC(fixed_dev, 1);
-    owned.push_back(fixed_dev);
     GPUTO_CUDA(cudaMallocHost((void **)&h_sc, sizeof(PcgScalars)));
-    GPUTO_CUDA(cudaMemsetAsync(ticket, 0, 16, own_stream));
     GPUTO_CUDA(cudaStreamSynchronize(own_stream));
     return GPUTO_OK;
 }
@@ -197,14 +177,15 @@ int Solver::set_problem(const double *Ke0, const double *fixed1b, int nfd, cudaS
     if (s1) return s1;
     // the fixed list: unchanged lists are not re-uploaded
     std::vector<double> list(fixed1b, fixed1b + nfd);
-    if (list != fixed_host) {
+    if (list != fixed_host || !have_problem) {
         if ((long long)list.size() > fixed_cap) {
+            cudaStreamSynchronize(st);
             cudaFree(fixed_dev);
             owned.erase(std::find(owned.begin(), owned.end(), (void *)fixed_dev));
             fixed_dev = nullptr;
             ALLOC(fixed_dev, list.size());
-            owned.push_back(fixed_dev);
             fixed_cap = (long long)list.size();
+            GPUTO_CUDA(cudaStreamSynchronize(own_stream));
         }
         if (nfd > 0)
             GPUTO_CUDA(cudaMemcpyAsync(fixed_dev, list.data(), sizeof(double) * nfd,
@@ -218,21 +199,36 @@ int Solver::set_problem(const double *Ke0, const double *fixed1b, int nfd, cudaS
     return GPUTO_OK;
 }
 
+int Solver::check_error_flags(cudaStream_t st)
+{
+    int h_err = 0;
+    GPUTO_CUDA(cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    GPUTO_CUDA(cudaStreamSynchronize(st));
+    if (h_err) {
+        set_error("a bounded wait for a TMA tile load gave up");
+        cudaMemsetAsync(err, 0, sizeof(int), st);
+        return h_err;
+    }
+    return GPUTO_OK;
+}
+
 int Solver::setup(const double *CX_in, cudaStream_t st)
 {
     if (!have_problem) {
         set_error("gputo_solver_set_problem must come before setup");
         return GPUTO_ERR_ARG;
     }
+    ready = false;
     const long long ne = g[0].nel();
     if (CX_in != CX)
         GPUTO_CUDA(cudaMemcpyAsync(CX, CX_in, sizeof(double) * ne, cudaMemcpyDeviceToDevice, st));
-    launch_diag_fine(g[0], CX, L[0].diag, st);
+    launch_pack_cx<double>(elay, CX, CXp, st);
+    launch_diag_fine(lay[0], CX, L[0].diag, st);
     for (int l = 1; l < nl; ++l) {
         if (l == 1) launch_build_level1(g[1], CX, L[1].Apk, st);
         else launch_build_galerkin(g[l], L[l - 1].Apk, L[l].Apk, st);
         if (l == nl - 1) launch_coarsest_penalty(g[l], mask[l], L[l].Apk, st);
-        launch_diag_packed<double>(g[l], L[l].Apk, L[l].diag, st);
+        launch_diag_packed<double>(lay[l], L[l].Apk, L[l].diag, st);
     }
     const double *Acoarse = (nl > 1) ? L[nl - 1].Apk : Apk0;
     if (nl == 1) {
@@ -243,11 +239,11 @@ int Solver::setup(const double *CX_in, cudaStream_t st)
     launch_cholesky(nc, AQ, info, st);
     launch_tri_inverse(nc, AQ, Linv, LinvT, st);
     if (opt.precision == GPUTO_PREC_MIXED) {
-        launch_cast_f32(ne, CX, CXf, st);
-        launch_cast_f32(g[0].ndof(), L[0].diag, Lf[0].diag, st);
+        launch_pack_cx<float>(elay, CX, CXpf, st);
+        launch_cast_f32(lay[0].size(), L[0].diag, Lf[0].diag, st);
         for (int l = 1; l < nl; ++l) {
             launch_cast_f32(300 * g[l].nel(), L[l].Apk, Lf[l].Apk, st);
-            launch_cast_f32(g[l].ndof(), L[l].diag, Lf[l].diag, st);
+            launch_cast_f32(lay[l].size(), L[l].diag, Lf[l].diag, st);
         }
     }
     int h_info = 0;
@@ -256,7 +252,6 @@ int Solver::setup(const double *CX_in, cudaStream_t st)
     GPUTO_CUDA(cudaGetLastError());
     if (h_info) {
         set_error("coarsest-grid Cholesky met a non-positive pivot at row " + std::to_string(h_info));
-        ready = false;
         return GPUTO_ERR_NOT_SPD;
     }
     ready = true;
@@ -276,9 +271,11 @@ void Solver::vcycle_impl(LevelBuf<T> *Lv, const T *CXl, const T *r0, T *z0, cons
     const T om = (T)opt.omega, pr = (T)opt.prerelax;
     auto sweep = [&](int l, int mode, const T *u, const T *f, T *out, T w) {
         if (l == 0)
-            launch_fine_sweep<T>(mode, g[0], CXl, u, f, Lv[0].diag, mask[0], out, w, pr, nullptr, done, st);
+            note(launch_fine_sweep<T>(mode, lay[0], elay, CXl, u, f, Lv[0].diag, mask[0], out, w, pr,
+                                      nullptr, done, err, st));
         else
-            launch_packed_sweep<T>(mode, g[l], Lv[l].Apk, u, f, Lv[l].diag, mask[l], out, w, pr, done, st);
+            launch_packed_sweep<T>(mode, lay[l], Lv[l].Apk, u, f, Lv[l].diag, mask[l], out, w, pr, done,
+                                   st);
     };
     auto bufs = [&](int l, int which) -> T * {
         if (l == 0) return which ? z0 : Lv[0].u0;
@@ -286,7 +283,7 @@ void Solver::vcycle_impl(LevelBuf<T> *Lv, const T *CXl, const T *r0, T *z0, cons
     };
     for (int l = 0; l < nl; ++l) {
         const T *f = (l == 0) ? r0 : Lv[l].f;
-        if (l > 0) launch_restrict<T>(g[l], Lv[l - 1].r, mask[l], Lv[l].f, done, st);
+        if (l > 0) launch_restrict<T>(lay[l], lay[l - 1], Lv[l - 1].r, mask[l], Lv[l].f, done, st);
         if (l < nl - 1) {
             if (ns == 0) {
                 sweep(l, MODE_JACOBI_PRE, nullptr, f, bufs(l, 1), T(0));  // U = prerelax F / diag
@@ -298,13 +295,13 @@ void Solver::vcycle_impl(LevelBuf<T> *Lv, const T *CXl, const T *r0, T *z0, cons
             const T *upre = (ns == 0) ? bufs(l, 1) : bufs(l, (ns - 1) & 1);
             sweep(l, MODE_DEFECT, upre, f, Lv[l].r, om);
         } else {
-            launch_coarse_solve<T>(nc, Linv, LinvT, f, bufs(l, 1), ctmp, mask[l], done, st);
+            launch_coarse_solve<T>(lay[l], Linv, LinvT, f, bufs(l, 1), ctmp, done, st);
         }
     }
     for (int l = nl - 2; l >= 0; --l) {
         const T *f = (l == 0) ? r0 : Lv[l].f;
         int cur = (ns == 0) ? 1 : ((ns - 1) & 1);
-        launch_prolong_add<T>(g[l], bufs(l + 1, 1), mask[l], bufs(l, cur), done, st);
+        launch_prolong_add<T>(lay[l], lay[l + 1], bufs(l + 1, 1), mask[l], bufs(l, cur), done, st);
         for (int s = 0; s < ns; ++s) {
             sweep(l, MODE_JACOBI, bufs(l, cur), f, bufs(l, cur ^ 1), om);
             cur ^= 1;
@@ -312,46 +309,43 @@ void Solver::vcycle_impl(LevelBuf<T> *Lv, const T *CXl, const T *r0, T *z0, cons
     }
 }
 
-int Solver::vcycle(const double *r, double *z, const int *done, cudaStream_t st)
+void Solver::vcycle(const double *r, double *z, const int *done, cudaStream_t st)
 {
     if (opt.precision == GPUTO_PREC_MIXED) {
         // FP32 V-cycle between FP64 vectors
-        launch_convert<double, float>(g[0].ndof(), r, Lf[0].f, done, st);
-        vcycle_impl<float>(Lf, CXf, Lf[0].f, Lf[0].u1, done, st);
-        launch_convert<float, double>(g[0].ndof(), Lf[0].u1, z, done, st);
+        launch_convert<double, float>(lay[0].size(), r, Lf[0].f, done, st);
+        vcycle_impl<float>(Lf, CXpf, Lf[0].f, Lf[0].u1, done, st);
+        launch_convert<float, double>(lay[0].size(), Lf[0].u1, z, done, st);
     } else {
-        vcycle_impl<double>(L, CX, r, z, done, st);
+        vcycle_impl<double>(L, CXp, r, z, done, st);
     }
-    return GPUTO_OK;
 }
 
-int Solver::apply(const double *u, double *r, cudaStream_t st)
+void Solver::apply(const double *u, double *r, double *dot_partial, const int *done, cudaStream_t st)
 {
-    launch_fine_sweep<double>(MODE_APPLY, g[0], CX, u, nullptr, L[0].diag, mask[0], r, 1.0, 0.0,
-                              nullptr, nullptr, st);
-    return GPUTO_OK;
+    note(launch_fine_sweep<double>(MODE_APPLY, lay[0], elay, CXp, u, nullptr, L[0].diag, mask[0], r,
+                                   1.0, 0.0, dot_partial, done, err, st));
 }
 
 // One PCG iteration (mgcg1.cu:254-275), every scalar on the device.
 void Solver::iteration(cudaStream_t st)
 {
-    const long long nd = g[0].ndof();
+    const long long nv = lay[0].size();
     const int *done = &sc->done;
-    launch_fine_sweep<double>(MODE_APPLY, g[0], CX, P, nullptr, L[0].diag, mask[0], Q, 1.0, 0.0,
-                              partial, done, st);
+    apply(P, Q, partial, done, st);
     launch_finish_apply_dot(fine_sweep_blocks(g[0]), partial, ticket, sc, st);
-    launch_pcg_update(nd, Uw, R, P, Q, partial, ticket, sc, st);
+    launch_pcg_update(nv, Uw, R, P, Q, partial, ticket, sc, st);
     vcycle(R, Z, done, st);
     if (Zold) {
-        launch_dot2(nd, R, Z, Zold, partial, ticket, sc, done, st);
-        launch_p_update(nd, Z, P, Zold, sc, st);
+        launch_dot2(nv, R, Z, Zold, partial, ticket, sc, done, st);
+        launch_p_update(nv, Z, P, Zold, sc, st);
     } else {
-        launch_dot(nd, R, Z, partial, ticket, sc, 2 /*DOT_RZ*/, done, st);
-        launch_p_update(nd, Z, P, nullptr, sc, st);
+        launch_dot(nv, R, Z, partial, ticket, sc, 2 /*DOT_RZ*/, done, st);
+        launch_p_update(nv, Z, P, nullptr, sc, st);
     }
 }
 
-int Solver::solve(const double *F, double *U, double tol, int maxit, double *relres, int *nit,
+int Solver::solve(const double *Fp, double *Up, double tol, int maxit, double *relres, int *nit,
                   cudaStream_t st, FILE *log)
 {
     if (!ready) {
@@ -362,13 +356,15 @@ int Solver::solve(const double *F, double *U, double tol, int maxit, double *rel
         set_error("maxit must be >= 0 and tol >= 0");
         return GPUTO_ERR_ARG;
     }
-    const long long nd = g[0].ndof();
+    launch_status = GPUTO_OK;
+    const long long nv = lay[0].size();
     const int *done = &sc->done;
-    launch_pcg_init(nd, F, Uw, R, partial, ticket, sc, tol, maxit,
-                    opt.precision == GPUTO_PREC_MIXED, st);
+    launch_pcg_init(nv, Fp, Uw, R, partial, ticket, sc, tol, maxit, opt.precision == GPUTO_PREC_MIXED,
+                    st);
     vcycle(R, P, done, st);
-    launch_dot(nd, R, P, partial, ticket, sc, 1 /*DOT_RHO0*/, done, st);
-    if (Zold) launch_copy(nd, P, Zold, done, st);
+    launch_dot(nv, R, P, partial, ticket, sc, 1 /*DOT_RHO0*/, done, st);
+    if (Zold) launch_copy(nv, P, Zold, done, st);
+    if (launch_status) return launch_status;
 
     const bool graph = opt.use_graph != 0;
     int it = 0;
@@ -383,13 +379,15 @@ int Solver::solve(const double *F, double *U, double tol, int maxit, double *rel
             if (gs) return gs;
         } else {
             for (int b = 0; b < batch; ++b) iteration(st);
+            if (launch_status) return launch_status;
         }
         it += batch;
     }
     GPUTO_CUDA(cudaGetLastError());
-    if (U != Uw)
-        GPUTO_CUDA(cudaMemcpyAsync(U, Uw, sizeof(double) * nd, cudaMemcpyDeviceToDevice, st));
-    GPUTO_CUDA(cudaStreamSynchronize(st));
+    if (Up != Uw)
+        GPUTO_CUDA(cudaMemcpyAsync(Up, Uw, sizeof(double) * nv, cudaMemcpyDeviceToDevice, st));
+    int fe = check_error_flags(st);
+    if (fe) return fe;
     *relres = h_sc->relres;
     *nit = h_sc->nit;
     last_res0 = h_sc->res0;
@@ -411,9 +409,14 @@ int Solver::run_graph(int batch, cudaStream_t st)
             graph_exec = nullptr;
         }
         cudaGraph_t gr;
+        launch_status = GPUTO_OK;
         GPUTO_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         iteration(st);
         GPUTO_CUDA(cudaStreamEndCapture(st, &gr));
+        if (launch_status) {
+            cudaGraphDestroy(gr);
+            return launch_status;
+        }
         cudaError_t e = cudaGraphInstantiate(&graph_exec, gr, 0);
         cudaGraphDestroy(gr);
         GPUTO_CUDA(e);

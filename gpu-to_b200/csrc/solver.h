@@ -12,6 +12,8 @@ struct Solver {
     gputo_options opt{};
     int nl = 0, device = 0, nc = 0;
     Grid g[kMaxLevels]{};
+    Lay lay[kMaxLevels]{};     // padded vector layout per level
+    ELay elay{};               // padded element layout of the fine level
     cudaStream_t own_stream = nullptr;
 
     double Ke[576]{};
@@ -20,23 +22,29 @@ struct Solver {
     double *fixed_dev = nullptr;
     long long fixed_cap = 1;
 
-    // fine-level PCG vectors (FP64) and solver-owned copies of CX, F, U
-    double *CX = nullptr, *R = nullptr, *P = nullptr, *Q = nullptr, *Z = nullptr, *Zold = nullptr;
+    // fine-level PCG vectors (FP64, padded layout)
+    double *R = nullptr, *P = nullptr, *Q = nullptr, *Z = nullptr, *Zold = nullptr;
     double *Uw = nullptr, *Fw = nullptr;
+    // staging in the reference's dense layout (MEX / device API boundary)
+    double *Dn = nullptr;
+    // element scales: natural order (setup kernels) and padded (fine sweeps)
+    double *CX = nullptr, *CXp = nullptr;
+    float *CXpf = nullptr;
     uint8_t *mask[kMaxLevels]{};
     LevelBuf<double> L[kMaxLevels];
     // FP32 preconditioner copies (mixed precision)
     LevelBuf<float> Lf[kMaxLevels];
-    float *CXf = nullptr;
     // coarsest grid
     double *AQ = nullptr, *Linv = nullptr, *LinvT = nullptr, *ctmp = nullptr, *Apk0 = nullptr;
     int *info = nullptr;
+    int *err = nullptr;        // device error flag (bounded waits)
     // device scalars and reduction scratch
     PcgScalars *sc = nullptr, *h_sc = nullptr;
     double *partial = nullptr;
     int partial_cap = 0;
     unsigned *ticket = nullptr;
     double last_res0 = 0.0;
+    int launch_status = GPUTO_OK;   // first failure seen while enqueuing kernels
 
     cudaGraphExec_t graph_exec = nullptr;
     cudaStream_t graph_stream = nullptr;
@@ -47,12 +55,16 @@ struct Solver {
     ~Solver();
     int create(int nelx, int nely, int nelz, int nl, const gputo_options *o);
     int set_problem(const double *Ke0, const double *fixed1b, int nfd, cudaStream_t st);
+    // CX in natural element order (device).
     int setup(const double *CX_dev, cudaStream_t st);
-    int solve(const double *F, double *U, double tol, int maxit, double *relres, int *nit,
+    // F, U in the padded layout (solver-owned or compatible buffers).
+    int solve(const double *Fp, double *Up, double tol, int maxit, double *relres, int *nit,
               cudaStream_t st, FILE *log);
-    int vcycle(const double *r, double *z, const int *done, cudaStream_t st);
-    int apply(const double *u, double *r, cudaStream_t st);
+    // Padded-layout preconditioner and operator.
+    void vcycle(const double *r, double *z, const int *done, cudaStream_t st);
+    void apply(const double *u, double *r, double *dot_partial, const int *done, cudaStream_t st);
     cudaStream_t stream(void *s) const { return s ? (cudaStream_t)s : own_stream; }
+    int check_error_flags(cudaStream_t st);
 
   private:
     template <typename T>
@@ -62,6 +74,10 @@ struct Solver {
                      cudaStream_t st);
     void iteration(cudaStream_t st);
     int run_graph(int batch, cudaStream_t st);
+    void note(int s)
+    {
+        if (s && !launch_status) launch_status = s;
+    }
 };
 
 }  // namespace gputo
