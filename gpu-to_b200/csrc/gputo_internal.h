@@ -191,6 +191,10 @@ void launch_flip_y(long long nnod, double *U, cudaStream_t st);
 void launch_element_energy(const Grid &g, const double *U, const double *CX, const double *dsK,
                            double *ce, double *dc, double *partial, unsigned *ticket,
                            double *compliance, cudaStream_t st);
+void launch_element_energy_blocks(const Grid &g, const double *U, const double *CX,
+                                  const double *dsK, double *ce, double *dc, double *partial,
+                                  unsigned *ticket, double *compliance, int nblocks,
+                                  cudaStream_t st);
 int launch_filter(const Grid &g, const double *in, const double *div, double *out, double rmin,
                   int normalize, cudaStream_t st);
 void launch_simp(long long n, const double *x, double penal, double E0, double Emin, double *CX,

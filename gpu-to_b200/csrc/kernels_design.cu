@@ -96,6 +96,17 @@ void launch_element_energy(const Grid &g, const double *U, const double *CX, con
     count_launches(1);
 }
 
+// Same kernel with an explicit number of CTAs (one partial slot per CTA).
+void launch_element_energy_blocks(const Grid &g, const double *U, const double *CX,
+                                  const double *dsK, double *ce, double *dc, double *partial,
+                                  unsigned *ticket, double *compliance, int nblocks,
+                                  cudaStream_t st)
+{
+    element_energy_kernel<<<(unsigned)nblocks, 256, 0, st>>>(g, U, CX, dsK, ce, dc, partial, ticket,
+                                                              compliance);
+    count_launches(1);
+}
+
 // MATLAB 'symmetric' padding: mirror including the edge sample.
 __device__ __forceinline__ int mirror_index(int i, int n)
 {

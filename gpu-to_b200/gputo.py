@@ -74,6 +74,7 @@ SIGNATURES = {
     "gputo_solver_time_kernel": (_i, [_vp, _i, _i, _dp, _vp]),
     "gputo_compliance_sens_dev": (_i, [_dp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _dp, _vp]),
     "gputo_compliance_sens": (_i, [_dp, _dp, _dp, _dp, _i, _i, _i, _dp, _dp, _dp]),
+    "gputo_compliance_sens_noalloc_dev": (_i, [_dp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _dp, _vp]),
     "gputo_density_filter_dev": (_i, [_vp, _vp, _vp, _i, _i, _i, _d, _i, _vp]),
     "gputo_density_filter": (_i, [_dp, _dp, _dp, _i, _i, _i, _d, _i]),
     "gputo_simp_dev": (_i, [_vp, ctypes.c_longlong, _d, _d, _d, _vp, _vp, _vp]),

@@ -180,6 +180,29 @@ int gputo_compliance_sens(const double *Ke0, const double *U, const double *CX,
                           const double *dsK, int nelx, int nely, int nelz, double *ce,
                           double *dc, double *compliance);
 
+/* gputo_compliance_sens_dev for callers that cannot allocate device memory.
+ * No counterpart in the reference: its sensitivity step is MATLAB code.
+ *
+ * gputo_compliance_sens_dev creates reduction scratch and a stream the first
+ * time it runs.  Code inside a CUDA stream capture, hosts whose memory manager
+ * owns the whole device (a MATLAB gpuArray workspace, a caching allocator) and
+ * real-time loops that must not hit cudaMalloc's implicit synchronisation
+ * cannot allow that.  This variant takes the same arguments and gives the same
+ * results, but keeps its scratch in a fixed device array compiled into the
+ * library (about 64 KB, held by every GPU that loads the library until the
+ * process exits) and calls no allocator.
+ *  - Grids above 16,777,216 elements are rejected with GPUTO_ERR_ARG.
+ *  - The first call on a device looks up the array's device address; make that
+ *    first call before any stream capture.
+ *  - Every call shares the array: calls that overlap on the GPU (different
+ *    streams, or different host threads on one device) race and must be
+ *    serialised by the caller.
+ * 'stream' may be NULL (the legacy default stream); the call returns after
+ * the stream has finished the work. */
+int gputo_compliance_sens_noalloc_dev(const double *Ke0, const double *U, const double *CX,
+                                      const double *dsK, int nelx, int nely, int nelz, double *ce,
+                                      double *dc, double *compliance, void *stream);
+
 /* Density filter, the three imfilter calls of the driver
  * (top3D125modCuda.m:95-96,109,140-141):
  *   out = imfilter(reshape(in ./ divisor, nely,nelz,nelx), h, 'symmetric')   [./ Hs]
