@@ -95,6 +95,7 @@ struct LevelBuf {
     T *r = nullptr;                  // defect after pre-smoothing (restriction input)
     T *diag = nullptr;               // operator diagonal
     T *Apk = nullptr;                // packed element matrices, [300][nel] (levels >= 1)
+    T *yq = nullptr;                 // level-1 element outputs, [24][nel] (matrix-free level 1)
     uint8_t *mask = nullptr;         // fixed-dof bits per node (bit d = dof d fixed)
 };
 
@@ -125,6 +126,17 @@ template <typename T>
 int launch_fine_sweep(int mode, const Lay &L, const ELay &E, const T *CX, const T *u, const T *f,
                       const T *diag, const uint8_t *mask, T *out, T omega, T prerelax,
                       double *dot_partial, const int *done, int *err, cudaStream_t st);
+// Level-1 quadrature operator applied matrix-free (L: level-1 layout, Ef: the
+// fine element layout of the padded CX, yscratch: 24 values per level-1
+// element, nu: Poisson ratio of the quadrature operator).
+template <typename T>
+int launch_quad_sweep(int mode, const Lay &L, const ELay &Ef, const T *CX, const T *u, const T *f,
+                      const T *diag, const uint8_t *mask, T *out, T omega, T prerelax, double nu,
+                      T *yscratch, const int *done, int *err, cudaStream_t st);
+void launch_diag_quad(const Lay &L, const double *CXf, double *diag, cudaStream_t st);
+int upload_quadrature_fine(const double *kg_packed, cudaStream_t st);
+// Level-2 Galerkin operator directly from the fine CX (level 1 not stored).
+void launch_build_galerkin_from_quad(const Grid &g2, const double *CXfine, double *Apk, cudaStream_t st);
 // Opt the tile kernels into their dynamic shared memory (call once per device).
 int init_fine_kernels();
 // Number of per-CTA partials a MODE_APPLY fine sweep writes.

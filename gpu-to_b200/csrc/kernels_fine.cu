@@ -56,22 +56,48 @@ int upload_fine_ke(const double *Ke_host, cudaStream_t st)
 }
 
 // ---------------------------------------------------------------------------
-// tile geometry
+// level-1 quadrature parts (constant memory, this translation unit's copy)
 // ---------------------------------------------------------------------------
 
-constexpr int TY = 32, TZ = 8, TX = 4;          // nodes per tile
+// Kg[g] packed lower triangle (300), g = 4 ix + 2 iz + iy: the 2h element's
+// stiffness evaluated at one Gauss point (mgcg1.cu:2000-2040 prepAelm); used
+// here for the diagonal of the level-1 operator.
+__constant__ double cKq64[8 * 300];
+
+int upload_quadrature_fine(const double *kg_packed, cudaStream_t st)
+{
+    GPUTO_CUDA(cudaMemcpyToSymbolAsync(cKq64, kg_packed, sizeof(double) * 8 * 300, 0,
+                                       cudaMemcpyHostToDevice, st));
+    GPUTO_CUDA(cudaStreamSynchronize(st));
+    return GPUTO_OK;
+}
+
+// ---------------------------------------------------------------------------
+// tile geometry
+// ---------------------------------------------------------------------------
+//
+// OP_FINE: K = sum_e CX_e Ke (the fine level).  The operator is a template
+// parameter so that other element operators can share the tile machinery.
+
+constexpr int OP_FINE = 0;
+constexpr int TY = 32, TZ = 8;                    // nodes per tile in y, z
 constexpr int NT = TY * TZ;                       // threads per CTA (one x-column each)
 constexpr int UW = 104;                           // u box width: 3*(TY+2) = 102 values from
                                                   // 3(j0-1)-1 (16-byte aligned start)
 constexpr int UOFF = 1;                           // value offset of halo node 0 in a u row
-template <typename T> struct CxBox;               // CX box width / offset (alignment per type)
-template <> struct CxBox<double> { static constexpr int W = 34, OFF = 1; };
-template <> struct CxBox<float> { static constexpr int W = 36, OFF = 3; };
+constexpr int TX_FINE = 4;                        // nodes per thread column along x
 
-template <typename T>
+// CX box width / offset (16-byte aligned start per element type)
+template <typename T, int OP> struct CxBox;
+template <> struct CxBox<double, OP_FINE> { static constexpr int W = 34, OFF = 1; };
+template <> struct CxBox<float, OP_FINE> { static constexpr int W = 36, OFF = 3; };
+
+template <typename T, int OP, int TXN>
 struct TileSmem {
-    static constexpr int U = (TX + 2) * (TZ + 2) * UW;       // values
-    static constexpr int C = (TX + 1) * (TZ + 1) * CxBox<T>::W;
+    static constexpr int CZ = TZ + 1;                                   // CX box rows in z
+    static constexpr int CX_ = TXN + 1;                                 // CX box planes in x
+    static constexpr int U = (TXN + 2) * (TZ + 2) * UW;                // values
+    static constexpr int C = CX_ * CZ * CxBox<T, OP>::W;
     static constexpr size_t u_bytes = sizeof(T) * U;
     static constexpr size_t c_bytes = sizeof(T) * C;
     static constexpr size_t u_off = 0;
@@ -83,18 +109,33 @@ struct TileSmem {
 
 constexpr uint32_t kWaitPolls = 1u << 22;   // bounded mbarrier wait (seconds, not forever)
 
-template <typename T, int MODE>
+// rows (3a..3a+2) of one element operator times its 24 displacements
+template <typename T, int OP>
+__device__ __forceinline__ void element_rows(int a, const T (&ue)[24], const T *cg, T &t0, T &t1, T &t2)
+{
+#pragma unroll
+    for (int q = 0; q < 24; ++q) {
+        t0 = fma(ke<T>((3 * a) * 24 + q), ue[q], t0);
+        t1 = fma(ke<T>((3 * a + 1) * 24 + q), ue[q], t1);
+        t2 = fma(ke<T>((3 * a + 2) * 24 + q), ue[q], t2);
+    }
+    t0 *= cg[0];
+    t1 *= cg[0];
+    t2 *= cg[0];
+}
+
+template <typename T, int MODE, int OP, int TXN>
 __global__ void __launch_bounds__(NT, 2)
-fine_tile_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ CUtensorMap tm_d,
-                 const __grid_constant__ CUtensorMap tm_c, Lay L, const T *__restrict__ f,
-                 const T *__restrict__ diag, const uint8_t *__restrict__ mask, T *__restrict__ out,
-                 T omega, T prerelax, double *__restrict__ dot_partial, const int *__restrict__ done,
-                 int *__restrict__ err)
+tile_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ CUtensorMap tm_d,
+            const __grid_constant__ CUtensorMap tm_c, Lay L, const T *__restrict__ f,
+            const T *__restrict__ diag, const uint8_t *__restrict__ mask, T *__restrict__ out,
+            T omega, T prerelax, double *__restrict__ dot_partial, const int *__restrict__ done,
+            int *__restrict__ err)
 {
     if (done && *done) return;
     constexpr bool PRE = (MODE == MODE_JACOBI_PRE);
-    using S = TileSmem<T>;
-    constexpr int CW = CxBox<T>::W, COFF = CxBox<T>::OFF;
+    using S = TileSmem<T, OP, TXN>;
+    constexpr int CW = CxBox<T, OP>::W, COFF = CxBox<T, OP>::OFF;
     extern __shared__ __align__(128) unsigned char smem[];
     T *su = reinterpret_cast<T *>(smem + S::u_off);
     T *sd = reinterpret_cast<T *>(smem + S::d_off);
@@ -102,7 +143,7 @@ fine_tile_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem + S::bar_off(PRE));
 
     const Grid &g = L.g;
-    const int j0 = blockIdx.x * TY, k0 = blockIdx.y * TZ, i0 = blockIdx.z * TX;
+    const int j0 = blockIdx.x * TY, k0 = blockIdx.y * TZ, i0 = blockIdx.z * TXN;
     const int tid = threadIdx.x;
 
     if (tid == 0) {
@@ -133,17 +174,18 @@ fine_tile_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant
     }
 
     const int ty = tid & 31, tz = tid >> 5;
-    T acc[TX][3];
+    T acc[TXN][3];
 #pragma unroll
-    for (int n = 0; n < TX; ++n) acc[n][0] = acc[n][1] = acc[n][2] = T(0);
+    for (int n = 0; n < TXN; ++n) acc[n][0] = acc[n][1] = acc[n][2] = T(0);
 
 #pragma unroll
-    for (int l = 0; l <= TX; ++l) {          // element x-layer i0-1+l
+    for (int l = 0; l <= TXN; ++l) {          // element x-layer i0-1+l
 #pragma unroll
         for (int ez = 0; ez < 2; ++ez) {
 #pragma unroll
             for (int ey = 0; ey < 2; ++ey) {
-                const T c = sc[(l * (TZ + 1) + tz + ez) * CW + COFF + ty + ey];
+                T cg[1];
+                cg[0] = sc[(l * S::CZ + tz + ez) * CW + COFF + ty + ey];
                 T ue[24];
 #pragma unroll
                 for (int b = 0; b < 8; ++b) {
@@ -158,18 +200,13 @@ fine_tile_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant
                     // side 0: the element's x = 0 face node (column node l-1);
                     // side 1: its x = 1 face node (column node l)
                     const int n = side ? l : l - 1;
-                    if (n < 0 || n >= TX) continue;
+                    if (n < 0 || n >= TXN) continue;
                     const int a = local_index(side, 1 - ey, 1 - ez);
                     T t0 = T(0), t1 = T(0), t2 = T(0);
-#pragma unroll
-                    for (int q = 0; q < 24; ++q) {
-                        t0 = fma(ke<T>((3 * a) * 24 + q), ue[q], t0);
-                        t1 = fma(ke<T>((3 * a + 1) * 24 + q), ue[q], t1);
-                        t2 = fma(ke<T>((3 * a + 2) * 24 + q), ue[q], t2);
-                    }
-                    acc[n][0] = fma(c, t0, acc[n][0]);
-                    acc[n][1] = fma(c, t1, acc[n][1]);
-                    acc[n][2] = fma(c, t2, acc[n][2]);
+                    element_rows<T, OP>(a, ue, cg, t0, t1, t2);
+                    acc[n][0] += t0;
+                    acc[n][1] += t1;
+                    acc[n][2] += t2;
                 }
             }
         }
@@ -178,7 +215,7 @@ fine_tile_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant
     double dsum = 0.0;
     const int j = j0 + ty, k = k0 + tz;
 #pragma unroll
-    for (int n = 0; n < TX; ++n) {
+    for (int n = 0; n < TXN; ++n) {
         const int i = i0 + n;
         if (j >= g.ny || k >= g.nz || i >= g.nx) continue;   // far faces: face kernel
         const unsigned m = mask[g.node(i, j, k)];
@@ -213,14 +250,16 @@ fine_tile_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant
     }
 }
 
+
 // Nodes on the far faces j = ny, k = nz, i = nx: a direct gather, one thread
 // per node.  Face A: j = ny; face B: k = nz, j < ny; face C: i = nx, j < ny, k < nz.
-template <typename T, int MODE>
+// E is the layout of the CX array.
+template <typename T, int MODE, int OP>
 __global__ void __launch_bounds__(128)
-fine_face_kernel(Lay L, ELay E, const T *__restrict__ CX, const T *__restrict__ u,
-                 const T *__restrict__ f, const T *__restrict__ diag,
-                 const uint8_t *__restrict__ mask, T *__restrict__ out, T omega, T prerelax,
-                 double *__restrict__ dot_partial, const int *__restrict__ done)
+face_kernel(Lay L, ELay E, const T *__restrict__ CX, const T *__restrict__ u,
+            const T *__restrict__ f, const T *__restrict__ diag,
+            const uint8_t *__restrict__ mask, T *__restrict__ out, T omega, T prerelax,
+            double *__restrict__ dot_partial, const int *__restrict__ done)
 {
     if (done && *done) return;
     const Grid &g = L.g;
@@ -256,26 +295,27 @@ fine_face_kernel(Lay L, ELay E, const T *__restrict__ CX, const T *__restrict__ 
                 for (int ey = 0; ey < 2; ++ey) {
                     const int ej = j - 1 + ey;
                     if (ej < 0 || ej >= g.ny) continue;
-                    const T c = CX[E.at(ei, ej, ek)];
+                    T cg[1] = {CX[E.at(ei, ej, ek)]};
                     const int a = local_index(1 - ex, 1 - ey, 1 - ez);
-                    T tt[3] = {T(0), T(0), T(0)};
+                    T ue[24];
 #pragma unroll
                     for (int b = 0; b < 8; ++b) {
                         const long long nb = L.at(ei + local_x(b), ej + local_y(b), ek + local_z(b));
 #pragma unroll
                         for (int q = 0; q < 3; ++q) {
-                            T ub;
                             if (MODE == MODE_JACOBI_PRE) {
                                 const T dv = diag[nb + q];
-                                ub = dv != T(0) ? prerelax * f[nb + q] / dv : T(0);
+                                ue[3 * b + q] = dv != T(0) ? prerelax * f[nb + q] / dv : T(0);
                             } else {
-                                ub = u[nb + q];
+                                ue[3 * b + q] = u[nb + q];
                             }
-#pragma unroll
-                            for (int d = 0; d < 3; ++d) tt[d] = fma(ke<T>((3 * a + d) * 24 + 3 * b + q), ub, tt[d]);
                         }
                     }
-                    for (int d = 0; d < 3; ++d) acc[d] = fma(c, tt[d], acc[d]);
+                    T t0 = T(0), t1 = T(0), t2 = T(0);
+                    element_rows<T, OP>(a, ue, cg, t0, t1, t2);
+                    acc[0] += t0;
+                    acc[1] += t1;
+                    acc[2] += t2;
                 }
             }
         }
@@ -311,9 +351,10 @@ fine_face_kernel(Lay L, ELay E, const T *__restrict__ CX, const T *__restrict__ 
     }
 }
 
+template <int TXN>
 static dim3 tile_grid(const Grid &g)
 {
-    return dim3((g.ny + TY - 1) / TY, (g.nz + TZ - 1) / TZ, (g.nx + TX - 1) / TX);
+    return dim3((g.ny + TY - 1) / TY, (g.nz + TZ - 1) / TZ, (g.nx + TXN - 1) / TXN);
 }
 
 static long long face_nodes(const Grid &g)
@@ -323,55 +364,66 @@ static long long face_nodes(const Grid &g)
 
 int fine_sweep_blocks(const Grid &g)
 {
-    const dim3 tg = tile_grid(g);
+    const dim3 tg = tile_grid<TX_FINE>(g);
     return (int)(tg.x * tg.y * tg.z + (face_nodes(g) + 127) / 128);
 }
 
-template <typename T>
+// Tensor maps for one sweep: u (or f), diag (PRE only) and CX (layout E).
+template <typename T, int OP, int TXN>
 static int make_maps(const Lay &L, const ELay &E, const T *u, const T *d, const T *CX, CUtensorMap *mu,
                      CUtensorMap *md, CUtensorMap *mc)
 {
+    using S = TileSmem<T, OP, TXN>;
     const Grid &g = L.g;
     const uint64_t es = sizeof(T);
     int st = make_tmap_3d(mu, u, (int)es, (uint64_t)L.pitch, (uint64_t)g.nz + 1, (uint64_t)g.nx + 1,
-                          L.pitch * es, L.pitch * es * (g.nz + 1), UW, TZ + 2, TX + 2);
+                          L.pitch * es, L.pitch * es * (g.nz + 1), UW, TZ + 2, TXN + 2);
     if (!st && d)
         st = make_tmap_3d(md, d, (int)es, (uint64_t)L.pitch, (uint64_t)g.nz + 1, (uint64_t)g.nx + 1,
-                          L.pitch * es, L.pitch * es * (g.nz + 1), UW, TZ + 2, TX + 2);
+                          L.pitch * es, L.pitch * es * (g.nz + 1), UW, TZ + 2, TXN + 2);
     if (!st)
-        st = make_tmap_3d(mc, CX, (int)es, (uint64_t)E.pitch, (uint64_t)g.nz, (uint64_t)g.nx,
-                          E.pitch * es, E.pitch * es * g.nz, CxBox<T>::W, TZ + 1, TX + 1);
+        st = make_tmap_3d(mc, CX, (int)es, (uint64_t)E.pitch, (uint64_t)E.g.nz, (uint64_t)E.g.nx,
+                          E.pitch * es, E.pitch * es * E.g.nz, CxBox<T, OP>::W, S::CZ, S::CX_);
     return st;
 }
 
-template <typename T, int MODE>
+template <typename T, int MODE, int OP, int TXN>
 static int launch_mode(const Lay &L, const ELay &E, const T *CX, const T *u, const T *f, const T *diag,
                        const uint8_t *mask, T *out, T omega, T prerelax, double *dot_partial,
                        const int *done, int *err, cudaStream_t st)
 {
     constexpr bool PRE = (MODE == MODE_JACOBI_PRE);
     CUtensorMap mu, md, mc;
-    int s = make_maps<T>(L, E, PRE ? f : u, PRE ? diag : nullptr, CX, &mu, &md, &mc);
+    int s = make_maps<T, OP, TXN>(L, E, PRE ? f : u, PRE ? diag : nullptr, CX, &mu, &md, &mc);
     if (s) return s;
     if (!PRE) md = mu;
-    const size_t smem = TileSmem<T>::bytes(PRE);
-    const dim3 tg = tile_grid(L.g);
-    fine_tile_kernel<T, MODE><<<tg, NT, smem, st>>>(mu, md, mc, L, f, diag, mask, out, omega, prerelax,
-                                                    dot_partial, done, err);
+    const size_t smem = TileSmem<T, OP, TXN>::bytes(PRE);
+    const dim3 tg = tile_grid<TXN>(L.g);
+    tile_kernel<T, MODE, OP, TXN><<<tg, NT, smem, st>>>(mu, md, mc, L, f, diag, mask, out, omega, prerelax,
+                                                        dot_partial, done, err);
     const long long nf = face_nodes(L.g);
     const unsigned fb = (unsigned)((nf + 127) / 128);
     double *fp = dot_partial ? dot_partial + (long long)tg.x * tg.y * tg.z : nullptr;
-    fine_face_kernel<T, MODE><<<fb, 128, 0, st>>>(L, E, CX, u, f, diag, mask, out, omega, prerelax, fp,
-                                                  done);
+    face_kernel<T, MODE, OP><<<fb, 128, 0, st>>>(L, E, CX, u, f, diag, mask, out, omega, prerelax, fp, done);
     count_launches(2);
     return GPUTO_OK;
 }
 
-template <typename T, int MODE>
+template <typename T, int MODE, int OP, int TXN>
 static cudaError_t set_smem_attr()
 {
-    return cudaFuncSetAttribute(fine_tile_kernel<T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)TileSmem<T>::bytes(MODE == MODE_JACOBI_PRE));
+    return cudaFuncSetAttribute(tile_kernel<T, MODE, OP, TXN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)TileSmem<T, OP, TXN>::bytes(MODE == MODE_JACOBI_PRE));
+}
+
+template <typename T, int OP, int TXN>
+static cudaError_t set_attrs_all_modes()
+{
+    cudaError_t e;
+    if ((e = set_smem_attr<T, MODE_APPLY, OP, TXN>()) != cudaSuccess) return e;
+    if ((e = set_smem_attr<T, MODE_DEFECT, OP, TXN>()) != cudaSuccess) return e;
+    if ((e = set_smem_attr<T, MODE_JACOBI, OP, TXN>()) != cudaSuccess) return e;
+    return set_smem_attr<T, MODE_JACOBI_PRE, OP, TXN>();
 }
 
 // Dynamic shared-memory opt-in for every tile-kernel instance, once per
@@ -384,16 +436,31 @@ int init_fine_kernels()
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 64 && done_dev[dev]) return GPUTO_OK;
-    GPUTO_CUDA((set_smem_attr<double, MODE_APPLY>()));
-    GPUTO_CUDA((set_smem_attr<double, MODE_DEFECT>()));
-    GPUTO_CUDA((set_smem_attr<double, MODE_JACOBI>()));
-    GPUTO_CUDA((set_smem_attr<double, MODE_JACOBI_PRE>()));
-    GPUTO_CUDA((set_smem_attr<float, MODE_APPLY>()));
-    GPUTO_CUDA((set_smem_attr<float, MODE_DEFECT>()));
-    GPUTO_CUDA((set_smem_attr<float, MODE_JACOBI>()));
-    GPUTO_CUDA((set_smem_attr<float, MODE_JACOBI_PRE>()));
+    GPUTO_CUDA((set_attrs_all_modes<double, OP_FINE, TX_FINE>()));
+    GPUTO_CUDA((set_attrs_all_modes<float, OP_FINE, TX_FINE>()));
     if (dev < 64) done_dev[dev] = true;
     return GPUTO_OK;
+}
+
+template <typename T, int OP, int TXN>
+static int launch_any(int mode, const Lay &L, const ELay &E, const T *CX, const T *u, const T *f,
+                      const T *diag, const uint8_t *mask, T *out, T omega, T prerelax,
+                      double *dot_partial, const int *done, int *err, cudaStream_t st)
+{
+    switch (mode) {
+    case MODE_APPLY:
+        return launch_mode<T, MODE_APPLY, OP, TXN>(L, E, CX, u, f, diag, mask, out, omega, prerelax,
+                                                   dot_partial, done, err, st);
+    case MODE_DEFECT:
+        return launch_mode<T, MODE_DEFECT, OP, TXN>(L, E, CX, u, f, diag, mask, out, omega, prerelax,
+                                                    nullptr, done, err, st);
+    case MODE_JACOBI:
+        return launch_mode<T, MODE_JACOBI, OP, TXN>(L, E, CX, u, f, diag, mask, out, omega, prerelax,
+                                                    nullptr, done, err, st);
+    default:
+        return launch_mode<T, MODE_JACOBI_PRE, OP, TXN>(L, E, CX, u, f, diag, mask, out, omega, prerelax,
+                                                        nullptr, done, err, st);
+    }
 }
 
 template <typename T>
@@ -401,20 +468,8 @@ int launch_fine_sweep(int mode, const Lay &L, const ELay &E, const T *CX, const 
                       const T *diag, const uint8_t *mask, T *out, T omega, T prerelax,
                       double *dot_partial, const int *done, int *err, cudaStream_t st)
 {
-    switch (mode) {
-    case MODE_APPLY:
-        return launch_mode<T, MODE_APPLY>(L, E, CX, u, f, diag, mask, out, omega, prerelax, dot_partial,
-                                          done, err, st);
-    case MODE_DEFECT:
-        return launch_mode<T, MODE_DEFECT>(L, E, CX, u, f, diag, mask, out, omega, prerelax, nullptr,
-                                           done, err, st);
-    case MODE_JACOBI:
-        return launch_mode<T, MODE_JACOBI>(L, E, CX, u, f, diag, mask, out, omega, prerelax, nullptr,
-                                           done, err, st);
-    default:
-        return launch_mode<T, MODE_JACOBI_PRE>(L, E, CX, u, f, diag, mask, out, omega, prerelax,
-                                               nullptr, done, err, st);
-    }
+    return launch_any<T, OP_FINE, TX_FINE>(mode, L, E, CX, u, f, diag, mask, out, omega, prerelax,
+                                           dot_partial, done, err, st);
 }
 
 template int launch_fine_sweep<double>(int, const Lay &, const ELay &, const double *, const double *,
@@ -423,6 +478,45 @@ template int launch_fine_sweep<double>(int, const Lay &, const ELay &, const dou
 template int launch_fine_sweep<float>(int, const Lay &, const ELay &, const float *, const float *,
                                       const float *, const float *, const uint8_t *, float *, float,
                                       float, double *, const int *, int *, cudaStream_t);
+
+// diag of the level-1 quadrature operator from the fine CX (natural order):
+// sum over adjacent coarse elements and Gauss points of CX_g Kg[g][m][m].
+__global__ void diag_quad_kernel(Lay L, const double *__restrict__ CXf, double *__restrict__ diag)
+{
+    const Grid &g = L.g;
+    const Grid gf{2 * g.nx, 2 * g.ny, 2 * g.nz};
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= g.nnod()) return;
+    const long long t = n / (g.ny + 1);
+    const int j = (int)(n - t * (g.ny + 1));
+    const int i = (int)(t / (g.nz + 1));
+    const int k = (int)(t - (long long)i * (g.nz + 1));
+    double acc[3] = {0, 0, 0};
+    for (int ex = 0; ex < 2; ++ex)
+        for (int ez = 0; ez < 2; ++ez)
+            for (int ey = 0; ey < 2; ++ey) {
+                const int ei = i - 1 + ex, ej = j - 1 + ey, ek = k - 1 + ez;
+                if (ei < 0 || ei >= g.nx || ej < 0 || ej >= g.ny || ek < 0 || ek >= g.nz) continue;
+                const int a = local_index(1 - ex, 1 - ey, 1 - ez);
+                for (int ix = 0; ix < 2; ++ix)
+                    for (int iz = 0; iz < 2; ++iz)
+                        for (int iy = 0; iy < 2; ++iy) {
+                            const double c = CXf[gf.elem(2 * ei + ix, 2 * ej + iy, 2 * ek + iz)];
+                            const int gq = 4 * ix + 2 * iz + iy;
+                            for (int d = 0; d < 3; ++d)
+                                acc[d] += c * cKq64[gq * 300 + packed_index(3 * a + d, 3 * a + d)];
+                        }
+            }
+    const long long base = L.at(i, j, k);
+    for (int d = 0; d < 3; ++d) diag[base + d] = acc[d];
+}
+
+void launch_diag_quad(const Lay &L, const double *CXf, double *diag, cudaStream_t st)
+{
+    const int bs = 128;
+    diag_quad_kernel<<<(unsigned)((L.g.nnod() + bs - 1) / bs), bs, 0, st>>>(L, CXf, diag);
+    count_launches(1);
+}
 
 // ---------------------------------------------------------------------------
 // fine-level setup kernels that need Ke

@@ -90,6 +90,8 @@ int upload_quadrature_parts(double nu, cudaStream_t st)
     GPUTO_CUDA(cudaMemcpyToSymbolAsync(cKg, kg, sizeof(kg), 0, cudaMemcpyHostToDevice, st));
     GPUTO_CUDA(cudaMemcpyToSymbolAsync(cPc, pc, sizeof(pc), 0, cudaMemcpyHostToDevice, st));
     GPUTO_CUDA(cudaStreamSynchronize(st));
+    const int s2 = upload_quadrature_fine(kg, st);   // the sweep kernels' copy
+    if (s2) return s2;
     last_nu = nu;
     return GPUTO_OK;
 }
@@ -427,7 +429,10 @@ void launch_build_level1(const Grid &gc, const double *CXfine, double *Apk, cuda
 // Levels >= 2: Galerkin P^T A P over the 8 children of each coarse element
 // (mgcg1.cu:1678-1743 coarseAe3c), computed child by child as
 // A_E = sum_c Pc^T A_c Pc with the 8x8 node weights Pc.  One CTA of 576
-// threads per coarse element; thread t owns entry (t/24, t%24).
+// threads per coarse element; thread t owns entry (t/24, t%24).  FROM_QUAD:
+// the children are level-1 quadrature elements, formed on the fly from the
+// fine CX (sum_g CX_g Kg[g]) because level 1 is applied without storage.
+template <bool FROM_QUAD>
 __global__ void __launch_bounds__(576) build_galerkin_kernel(Grid gc, const double *__restrict__ Af,
                                                              double *__restrict__ A)
 {
@@ -438,17 +443,32 @@ __global__ void __launch_bounds__(576) build_galerkin_kernel(Grid gc, const doub
     const int i = (int)(t / gc.nz);
     const int k = (int)(t - (long long)i * gc.nz);
     const Grid gf{2 * gc.nx, 2 * gc.ny, 2 * gc.nz};
+    const Grid gff{4 * gc.nx, 4 * gc.ny, 4 * gc.nz};   // fine grid under level 1 (FROM_QUAD)
     const long long nelf = gf.nel();
     __shared__ double S[576];
     __shared__ double Tm[576];
+    __shared__ double cxs[8];
     const int tid = threadIdx.x;
     const int m = tid / 24, n = tid - 24 * (tid / 24);
     const int am = m / 3, p = m - 3 * am;   // row: coarse local node, component
     const int an = n / 3, q = n - 3 * an;   // column
     double acc = 0.0;
     for (int c = 0; c < 8; ++c) {
-        const long long ec = gf.elem(2 * i + local_x(c), 2 * j + local_y(c), 2 * k + local_z(c));
-        S[tid] = Af[(long long)packed_index(m, n) * nelf + ec];
+        const int ci = 2 * i + local_x(c), cj = 2 * j + local_y(c), ck = 2 * k + local_z(c);
+        if (FROM_QUAD) {
+            if (tid < 8) {
+                const int ix = tid >> 2, iz = (tid >> 1) & 1, iy = tid & 1;   // tid = 4 ix + 2 iz + iy
+                cxs[tid] = Af[gff.elem(2 * ci + ix, 2 * cj + iy, 2 * ck + iz)];
+            }
+            __syncthreads();
+            double v = 0.0;
+            const int pk = packed_index(m, n);
+#pragma unroll
+            for (int gq = 0; gq < 8; ++gq) v = fma(cxs[gq], cKg[gq * 300 + pk], v);
+            S[tid] = v;
+        } else {
+            S[tid] = Af[(long long)packed_index(m, n) * nelf + gf.elem(ci, cj, ck)];
+        }
         __syncthreads();
         // Tm[(b,p)][(an,q)] = sum_b' S[(b,p)][(b',q)] Pc[b'][an]   (here m = (b,p))
         double tv = 0.0;
@@ -466,7 +486,13 @@ __global__ void __launch_bounds__(576) build_galerkin_kernel(Grid gc, const doub
 
 void launch_build_galerkin(const Grid &gc, const double *Afine, double *Apk, cudaStream_t st)
 {
-    build_galerkin_kernel<<<(unsigned)gc.nel(), 576, 0, st>>>(gc, Afine, Apk);
+    build_galerkin_kernel<false><<<(unsigned)gc.nel(), 576, 0, st>>>(gc, Afine, Apk);
+    count_launches(1);
+}
+
+void launch_build_galerkin_from_quad(const Grid &g2, const double *CXfine, double *Apk, cudaStream_t st)
+{
+    build_galerkin_kernel<true><<<(unsigned)g2.nel(), 576, 0, st>>>(g2, CXfine, Apk);
     count_launches(1);
 }
 

@@ -71,7 +71,9 @@ int Solver::alloc_levels(LevelBuf<T> *Lv, bool with_matrices)
         ALLOC(b.diag, nv);
         ALLOC(b.u1, nv);
         ALLOC(b.f, nv);
-        if (l > 0 && with_matrices) ALLOC(b.Apk, 300 * g[l].nel());
+        // level 1 is applied matrix-free unless it is the coarsest level
+        if (l > 0 && with_matrices && !(l == 1 && quad_level1())) ALLOC(b.Apk, 300 * g[l].nel());
+        if (l == 1 && quad_level1()) ALLOC(b.yq, 24 * g[l].nel());
         b.mask = mask[l];
     }
     return GPUTO_OK;
@@ -225,7 +227,12 @@ int Solver::setup(const double *CX_in, cudaStream_t st)
     launch_pack_cx<double>(elay, CX, CXp, st);
     launch_diag_fine(lay[0], CX, L[0].diag, st);
     for (int l = 1; l < nl; ++l) {
+        if (l == 1 && quad_level1()) {
+            launch_diag_quad(lay[1], CX, L[1].diag, st);
+            continue;
+        }
         if (l == 1) launch_build_level1(g[1], CX, L[1].Apk, st);
+        else if (l == 2 && quad_level1()) launch_build_galerkin_from_quad(g[2], CX, L[2].Apk, st);
         else launch_build_galerkin(g[l], L[l - 1].Apk, L[l].Apk, st);
         if (l == nl - 1) launch_coarsest_penalty(g[l], mask[l], L[l].Apk, st);
         launch_diag_packed<double>(lay[l], L[l].Apk, L[l].diag, st);
@@ -242,7 +249,7 @@ int Solver::setup(const double *CX_in, cudaStream_t st)
         launch_pack_cx<float>(elay, CX, CXpf, st);
         launch_cast_f32(lay[0].size(), L[0].diag, Lf[0].diag, st);
         for (int l = 1; l < nl; ++l) {
-            launch_cast_f32(300 * g[l].nel(), L[l].Apk, Lf[l].Apk, st);
+            if (L[l].Apk) launch_cast_f32(300 * g[l].nel(), L[l].Apk, Lf[l].Apk, st);
             launch_cast_f32(lay[l].size(), L[l].diag, Lf[l].diag, st);
         }
     }
@@ -273,6 +280,9 @@ void Solver::vcycle_impl(LevelBuf<T> *Lv, const T *CXl, const T *r0, T *z0, cons
         if (l == 0)
             note(launch_fine_sweep<T>(mode, lay[0], elay, CXl, u, f, Lv[0].diag, mask[0], out, w, pr,
                                       nullptr, done, err, st));
+        else if (l == 1 && quad_level1())
+            note(launch_quad_sweep<T>(mode, lay[1], elay, CXl, u, f, Lv[1].diag, mask[1], out, w, pr,
+                                      opt.nu, Lv[1].yq, done, err, st));
         else
             launch_packed_sweep<T>(mode, lay[l], Lv[l].Apk, u, f, Lv[l].diag, mask[l], out, w, pr, done,
                                    st);

@@ -64,6 +64,9 @@ struct Solver {
     void vcycle(const double *r, double *z, const int *done, cudaStream_t st);
     void apply(const double *u, double *r, double *dot_partial, const int *done, cudaStream_t st);
     cudaStream_t stream(void *s) const { return s ? (cudaStream_t)s : own_stream; }
+    // Level 1 is applied matrix-free from the fine CX whenever it is not the
+    // coarsest level (then it needs assembled matrices for the direct solve).
+    bool quad_level1() const { return nl >= 3; }
     int check_error_flags(cudaStream_t st);
 
   private:
