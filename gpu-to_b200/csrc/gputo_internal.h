@@ -147,6 +147,14 @@ void launch_packed_sweep(int mode, const Lay &L, const T *Apk, const T *u, const
                          const T *diag, const uint8_t *mask, T *out, T omega, T prerelax,
                          const int *done, cudaStream_t st);
 
+// Element-centric form of the same sweep (yscratch: 24 values per element).
+template <typename T>
+void launch_packed_sweep_ec(int mode, const Lay &L, const T *Apk, const T *u, const T *f, const T *diag,
+                            const uint8_t *mask, T *out, T omega, T prerelax, T *yscratch,
+                            const int *done, cudaStream_t st);
+// Levels at least this many elements use the element-centric sweep.
+constexpr long long kElementCentricMinElems = 16384;
+
 template <typename T>
 void launch_restrict(const Lay &Lc, const Lay &Lf, const T *rf, const uint8_t *maskc, T *fc,
                      const int *done, cudaStream_t st);

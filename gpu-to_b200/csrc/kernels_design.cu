@@ -167,12 +167,17 @@ int launch_filter(const Grid &g, const double *in, const double *div, double *ou
                 h[((a + R) * W + (b + R)) * W + (c + R)] = w;
                 hs += w;
             }
-    static double last_rmin = -1.0;
-    if (rmin != last_rmin) {
+    static double last_rmin[64];
+    static bool have[64] = {};
+    int dev = 0;
+    GPUTO_CUDA(cudaGetDevice(&dev));
+    const int slot = dev < 64 ? dev : 63;
+    if (!have[slot] || rmin != last_rmin[slot] || dev >= 64) {   // constant memory is per device
         GPUTO_CUDA(cudaMemcpyToSymbolAsync(cFilterH, h.data(), sizeof(double) * h.size(), 0,
                                            cudaMemcpyHostToDevice, st));
         GPUTO_CUDA(cudaStreamSynchronize(st));
-        last_rmin = rmin;
+        last_rmin[slot] = rmin;
+        have[slot] = true;
     }
     const double scale = normalize ? 1.0 / hs : 1.0;
     const int bs = 256;

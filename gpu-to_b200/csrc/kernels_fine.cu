@@ -33,23 +33,27 @@ template <> __device__ __forceinline__ float ke<float>(int idx) { return cKe32[i
 
 int upload_fine_ke(const double *Ke_host, cudaStream_t st)
 {
+    // constant memory is per device: remember what each device holds
     static std::mutex mu;
-    static double last[576];
-    static bool have = false;
+    static double last[64][576];
+    static bool have[64] = {};
     std::lock_guard<std::mutex> lock(mu);
+    int dev = 0;
+    GPUTO_CUDA(cudaGetDevice(&dev));
+    const int slot = dev < 64 ? dev : 63;
     // Ke0 is an argument of every MEX call; skip the copy when it repeats.
-    bool same = have;
-    for (int m = 0; same && m < 576; ++m) same = (last[m] == Ke_host[m]);
+    bool same = have[slot] && dev < 64;
+    for (int m = 0; same && m < 576; ++m) same = (last[slot][m] == Ke_host[m]);
     if (same) return GPUTO_OK;
     float kf[576];
     for (int m = 0; m < 576; ++m) {
-        last[m] = Ke_host[m];
+        last[slot][m] = Ke_host[m];
         kf[m] = (float)Ke_host[m];
     }
-    have = true;
-    GPUTO_CUDA(cudaMemcpyToSymbolAsync(cKe64, last, sizeof(last), 0, cudaMemcpyHostToDevice, st));
+    have[slot] = true;
+    GPUTO_CUDA(cudaMemcpyToSymbolAsync(cKe64, last[slot], sizeof(double) * 576, 0, cudaMemcpyHostToDevice, st));
     GPUTO_CUDA(cudaMemcpyToSymbolAsync(cKe32, kf, sizeof(kf), 0, cudaMemcpyHostToDevice, st));
-    const int s2 = upload_design_ke(last, st);
+    const int s2 = upload_design_ke(last[slot], st);
     if (s2) return s2;
     GPUTO_CUDA(cudaStreamSynchronize(st));
     return GPUTO_OK;

@@ -62,10 +62,21 @@ void gauss_part(double nu, double h, int ix, int iy, int iz, double K[24][24])
         }
 }
 
+// Level-2 Galerkin blocks of the quadrature level: the 2h-element matrix of
+// level 1 is sum_g CX_g Kg[g], so the level-2 element matrix is
+//   A_E = sum_{c,g} CX(fine element g of level-1 child c) * Pc^T Kg[g] Pc,
+// a fixed combination of 64 constant matrices Mq[c*8+g] = Pc^T Kg[g] Pc
+// (packed, 300 each), weighted by the 64 fine densities under E.
+static double *g_mq_dev[64] = {};
+static double g_mq_nu[64];
+
+const double *quad_galerkin_blocks(int dev) { return dev >= 0 && dev < 64 ? g_mq_dev[dev] : nullptr; }
+
 int upload_quadrature_parts(double nu, cudaStream_t st)
 {
-    static double last_nu = -1.0;
-    if (nu == last_nu) return GPUTO_OK;
+    int dev = 0;
+    GPUTO_CUDA(cudaGetDevice(&dev));
+    if (dev < 64 && g_mq_dev[dev] && g_mq_nu[dev] == nu) return GPUTO_OK;   // per device
     static double kg[8 * 300];
     for (int ix = 0; ix < 2; ++ix)
         for (int iz = 0; iz < 2; ++iz)
@@ -92,7 +103,31 @@ int upload_quadrature_parts(double nu, cudaStream_t st)
     GPUTO_CUDA(cudaStreamSynchronize(st));
     const int s2 = upload_quadrature_fine(kg, st);   // the sweep kernels' copy
     if (s2) return s2;
-    last_nu = nu;
+    // Mq[c][g] = Pc^T Kg[g] Pc
+    static double mq[64 * 300];
+    for (int c = 0; c < 8; ++c)
+        for (int gq = 0; gq < 8; ++gq)
+            for (int m = 0; m < 24; ++m)
+                for (int n = 0; n <= m; ++n) {
+                    const int am = m / 3, p = m % 3, an = n / 3, q = n % 3;
+                    double acc = 0.0;
+                    for (int b = 0; b < 8; ++b) {
+                        const double wb = pc[(c * 8 + b) * 8 + am];
+                        if (wb == 0.0) continue;
+                        for (int b2 = 0; b2 < 8; ++b2) {
+                            const double wb2 = pc[(c * 8 + b2) * 8 + an];
+                            if (wb2 == 0.0) continue;
+                            acc += wb * wb2 * kg[gq * 300 + packed_index(3 * b + p, 3 * b2 + q)];
+                        }
+                    }
+                    mq[(c * 8 + gq) * 300 + packed_index(m, n)] = acc;
+                }
+    if (dev < 64) {
+        if (!g_mq_dev[dev]) GPUTO_CUDA(cudaMalloc(&g_mq_dev[dev], sizeof(mq)));
+        GPUTO_CUDA(cudaMemcpyAsync(g_mq_dev[dev], mq, sizeof(mq), cudaMemcpyHostToDevice, st));
+        GPUTO_CUDA(cudaStreamSynchronize(st));
+        g_mq_nu[dev] = nu;
+    }
     return GPUTO_OK;
 }
 
@@ -173,12 +208,100 @@ packed_sweep_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u,
     }
 }
 
+// Small levels: one warp per node.  Lane l takes element l/4 of the 8 around
+// the node and a quarter (6 columns) of its 24, i.e. 18 products, and the
+// warp sums the three rows with shuffles -- 32x the parallelism of a thread
+// per node, for levels with too few nodes to fill the GPU.
+template <typename T, int MODE>
+__global__ void __launch_bounds__(128)
+packed_sweep_warp_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u,
+                         const T *__restrict__ f, const T *__restrict__ diag,
+                         const uint8_t *__restrict__ mask, T *__restrict__ out, T omega, T prerelax,
+                         const int *__restrict__ done)
+{
+    if (done && *done) return;
+    const Grid &g = L.g;
+    const long long n = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (n >= g.nnod()) return;
+    int i, j, k;
+    node_ijk(g, n, i, j, k);
+    const int eidx = lane >> 2, quarter = lane & 3;
+    const int ex = (eidx >> 2) & 1, ez = (eidx >> 1) & 1, ey = eidx & 1;
+    const int ei = i - 1 + ex, ej = j - 1 + ey, ek = k - 1 + ez;
+    T acc[3] = {T(0), T(0), T(0)};
+    if (ei >= 0 && ei < g.nx && ej >= 0 && ej < g.ny && ek >= 0 && ek < g.nz) {
+        const long long nel = g.nel();
+        const long long e = g.elem(ei, ej, ek);
+        const int a = local_index(1 - ex, 1 - ey, 1 - ez);
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            const int col = quarter * 6 + c, b = col / 3, q = col - 3 * b;
+            const long long dof = L.at(ei + local_x(b), ej + local_y(b), ek + local_z(b)) + q;
+            T ub;
+            if (MODE == MODE_JACOBI_PRE) {
+                const T dv = diag[dof];
+                ub = dv != T(0) ? prerelax * f[dof] / dv : T(0);
+            } else {
+                ub = u[dof];
+            }
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+                acc[d] = fma(A[(long long)packed_index(3 * a + d, col) * nel + e], ub, acc[d]);
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+        for (int o = 16; o > 0; o >>= 1) acc[d] += __shfl_xor_sync(0xffffffffu, acc[d], o);
+    if (lane != 0) return;
+    const unsigned m = mask[n];
+    const long long base = L.at(i, j, k);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const long long dof = base + d;
+        const bool fixed = (m >> d) & 1u;
+        if (MODE == MODE_APPLY) {
+            out[dof] = fixed ? T(0) : acc[d];
+        } else if (MODE == MODE_DEFECT) {
+            out[dof] = fixed ? T(0) : f[dof] - acc[d];
+        } else {
+            const T r = fixed ? T(0) : f[dof] - acc[d];
+            T us;
+            if (MODE == MODE_JACOBI_PRE) {
+                const T dv = diag[dof];
+                us = dv != T(0) ? prerelax * f[dof] / dv : T(0);
+            } else {
+                us = u[dof];
+            }
+            out[dof] = us + omega * r / diag[dof];
+        }
+    }
+}
+
 template <typename T>
 void launch_packed_sweep(int mode, const Lay &L, const T *Apk, const T *u, const T *f,
                          const T *diag, const uint8_t *mask, T *out, T omega, T prerelax,
                          const int *done, cudaStream_t st)
 {
     const int bs = 128;
+    if (L.g.nnod() < 65536) {
+        const unsigned wb = (unsigned)((L.g.nnod() * 32 + bs - 1) / bs);
+        switch (mode) {
+        case MODE_APPLY:
+            packed_sweep_warp_kernel<T, MODE_APPLY><<<wb, bs, 0, st>>>(L, Apk, u, f, diag, mask, out, omega, prerelax, done);
+            break;
+        case MODE_DEFECT:
+            packed_sweep_warp_kernel<T, MODE_DEFECT><<<wb, bs, 0, st>>>(L, Apk, u, f, diag, mask, out, omega, prerelax, done);
+            break;
+        case MODE_JACOBI:
+            packed_sweep_warp_kernel<T, MODE_JACOBI><<<wb, bs, 0, st>>>(L, Apk, u, f, diag, mask, out, omega, prerelax, done);
+            break;
+        default:
+            packed_sweep_warp_kernel<T, MODE_JACOBI_PRE><<<wb, bs, 0, st>>>(L, Apk, u, f, diag, mask, out, omega, prerelax, done);
+        }
+        count_launches(1);
+        return;
+    }
     const unsigned nb = (unsigned)((L.g.nnod() + bs - 1) / bs);
     switch (mode) {
     case MODE_APPLY:
@@ -429,10 +552,7 @@ void launch_build_level1(const Grid &gc, const double *CXfine, double *Apk, cuda
 // Levels >= 2: Galerkin P^T A P over the 8 children of each coarse element
 // (mgcg1.cu:1678-1743 coarseAe3c), computed child by child as
 // A_E = sum_c Pc^T A_c Pc with the 8x8 node weights Pc.  One CTA of 576
-// threads per coarse element; thread t owns entry (t/24, t%24).  FROM_QUAD:
-// the children are level-1 quadrature elements, formed on the fly from the
-// fine CX (sum_g CX_g Kg[g]) because level 1 is applied without storage.
-template <bool FROM_QUAD>
+// threads per coarse element; thread t owns entry (t/24, t%24).
 __global__ void __launch_bounds__(576) build_galerkin_kernel(Grid gc, const double *__restrict__ Af,
                                                              double *__restrict__ A)
 {
@@ -443,11 +563,9 @@ __global__ void __launch_bounds__(576) build_galerkin_kernel(Grid gc, const doub
     const int i = (int)(t / gc.nz);
     const int k = (int)(t - (long long)i * gc.nz);
     const Grid gf{2 * gc.nx, 2 * gc.ny, 2 * gc.nz};
-    const Grid gff{4 * gc.nx, 4 * gc.ny, 4 * gc.nz};   // fine grid under level 1 (FROM_QUAD)
     const long long nelf = gf.nel();
     __shared__ double S[576];
     __shared__ double Tm[576];
-    __shared__ double cxs[8];
     const int tid = threadIdx.x;
     const int m = tid / 24, n = tid - 24 * (tid / 24);
     const int am = m / 3, p = m - 3 * am;   // row: coarse local node, component
@@ -455,20 +573,7 @@ __global__ void __launch_bounds__(576) build_galerkin_kernel(Grid gc, const doub
     double acc = 0.0;
     for (int c = 0; c < 8; ++c) {
         const int ci = 2 * i + local_x(c), cj = 2 * j + local_y(c), ck = 2 * k + local_z(c);
-        if (FROM_QUAD) {
-            if (tid < 8) {
-                const int ix = tid >> 2, iz = (tid >> 1) & 1, iy = tid & 1;   // tid = 4 ix + 2 iz + iy
-                cxs[tid] = Af[gff.elem(2 * ci + ix, 2 * cj + iy, 2 * ck + iz)];
-            }
-            __syncthreads();
-            double v = 0.0;
-            const int pk = packed_index(m, n);
-#pragma unroll
-            for (int gq = 0; gq < 8; ++gq) v = fma(cxs[gq], cKg[gq * 300 + pk], v);
-            S[tid] = v;
-        } else {
-            S[tid] = Af[(long long)packed_index(m, n) * nelf + gf.elem(ci, cj, ck)];
-        }
+        S[tid] = Af[(long long)packed_index(m, n) * nelf + gf.elem(ci, cj, ck)];
         __syncthreads();
         // Tm[(b,p)][(an,q)] = sum_b' S[(b,p)][(b',q)] Pc[b'][an]   (here m = (b,p))
         double tv = 0.0;
@@ -486,13 +591,44 @@ __global__ void __launch_bounds__(576) build_galerkin_kernel(Grid gc, const doub
 
 void launch_build_galerkin(const Grid &gc, const double *Afine, double *Apk, cudaStream_t st)
 {
-    build_galerkin_kernel<false><<<(unsigned)gc.nel(), 576, 0, st>>>(gc, Afine, Apk);
+    build_galerkin_kernel<<<(unsigned)gc.nel(), 576, 0, st>>>(gc, Afine, Apk);
     count_launches(1);
+}
+
+// Level 2 from the fine CX: A_E[p] = sum_{f<64} CX_f Mq[f][p], one CTA per
+// level-2 element, one thread per packed entry.
+__global__ void __launch_bounds__(320) build_level2_quad_kernel(Grid g2, const double *__restrict__ CXf,
+                                                                const double *__restrict__ Mq,
+                                                                double *__restrict__ A)
+{
+    const long long E = blockIdx.x;
+    const long long nel = g2.nel();
+    const long long t = E / g2.ny;
+    const int j = (int)(E - t * g2.ny);
+    const int i = (int)(t / g2.nz);
+    const int k = (int)(t - (long long)i * g2.nz);
+    const Grid gff{4 * g2.nx, 4 * g2.ny, 4 * g2.nz};
+    __shared__ double cx[64];
+    const int tid = threadIdx.x;
+    if (tid < 64) {
+        const int c = tid >> 3, gq = tid & 7;
+        const int ix = gq >> 2, iz = (gq >> 1) & 1, iy = gq & 1;   // gq = 4 ix + 2 iz + iy
+        cx[tid] = CXf[gff.elem(2 * (2 * i + local_x(c)) + ix, 2 * (2 * j + local_y(c)) + iy,
+                               2 * (2 * k + local_z(c)) + iz)];
+    }
+    __syncthreads();
+    if (tid >= 300) return;
+    double acc = 0.0;
+#pragma unroll 8
+    for (int f = 0; f < 64; ++f) acc = fma(cx[f], Mq[f * 300 + tid], acc);
+    A[(long long)tid * nel + E] = acc;
 }
 
 void launch_build_galerkin_from_quad(const Grid &g2, const double *CXfine, double *Apk, cudaStream_t st)
 {
-    build_galerkin_kernel<true><<<(unsigned)g2.nel(), 576, 0, st>>>(g2, CXfine, Apk);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    build_level2_quad_kernel<<<(unsigned)g2.nel(), 320, 0, st>>>(g2, CXfine, quad_galerkin_blocks(dev), Apk);
     count_launches(1);
 }
 
@@ -567,58 +703,123 @@ void launch_assemble_dense(const Grid &g, const double *Apk, double *AQ, cudaStr
     count_launches(1);
 }
 
-// Right-looking Cholesky of the dense coarsest matrix by one CTA, in place
-// (lower triangle).  Textbook algorithm: scale the pivot column, stage it in
-// shared memory, then one warp per trailing row subtracts the rank-1 update
-// with coalesced row accesses.  info = 1-based index of the first non-positive
-// pivot, 0 on success.  (The reference launches one kernel per row,
-// mgcg1.cu:2099-2142.)
-__global__ void __launch_bounds__(1024) cholesky_kernel(int n, double *__restrict__ A, int *info)
+// Blocked left-looking Cholesky A = L L^T of the dense coarsest matrix, in
+// place in the lower triangle, 32-column panels (textbook algorithm; the
+// reference launches one kernel per row, mgcg1.cu:2099-2142):
+//   for each panel [c0, c0+w):
+//     update:  A[r][c0+j] -= sum_{k<c0} L[r][k] L[c0+j][k]   for r >= c0+j
+//              (a tiled FP64 GEMM over all rows below the panel, many CTAs)
+//     factor:  the w x w diagonal block in shared memory, then each row below
+//              solves L[r][panel] D^T = A[r][panel] (one CTA)
+// info = 1-based index of the first non-positive pivot, 0 on success; once
+// set, every later kernel returns at once.
+constexpr int kCholB = 32;
+
+__global__ void __launch_bounds__(256) chol_update_kernel(int n, int c0, int w, double *__restrict__ A,
+                                                          const int *__restrict__ info)
 {
-    extern __shared__ double colv[];
-    __shared__ double piv;
-    __shared__ int bad;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
-    if (tid == 0) bad = 0;
-    __syncthreads();
-    for (int c = 0; c < n; ++c) {
-        if (tid == 0) {
-            const double s = A[(long long)c * n + c];
-            if (!(s > 0.0)) {
-                bad = c + 1;
-                piv = 1.0;
-            } else {
-                piv = sqrt(s);
-            }
-            A[(long long)c * n + c] = piv;
+    if (*info) return;
+    __shared__ double Ar[kCholB][kCholB + 1];
+    __shared__ double Ac[kCholB][kCholB + 1];
+    const int r0 = c0 + blockIdx.x * kCholB;   // row block (rows >= c0)
+    const int ty = threadIdx.x >> 3, tx = threadIdx.x & 7;   // 32 rows x 8 threads, 4 cols each
+    double acc[4] = {0, 0, 0, 0};
+    for (int kk = 0; kk < c0; kk += kCholB) {
+        for (int idx = threadIdx.x; idx < kCholB * kCholB; idx += 256) {
+            const int rr = idx / kCholB, k = idx - rr * kCholB;
+            const int gr = r0 + rr, gc = c0 + rr, gk = kk + k;
+            Ar[rr][k] = (gr < n && gk < c0) ? A[(long long)gr * n + gk] : 0.0;
+            Ac[rr][k] = (rr < w && gk < c0) ? A[(long long)gc * n + gk] : 0.0;
         }
         __syncthreads();
-        if (bad) break;
-        const double dinv = 1.0 / piv;
-        for (int r = c + 1 + tid; r < n; r += nt) {
-            const double v = A[(long long)r * n + c] * dinv;
-            A[(long long)r * n + c] = v;
-            colv[r] = v;
-        }
-        __syncthreads();
-        for (int r = c + 1 + warp; r < n; r += nw) {
-            const double lr = colv[r];
-            double *row = A + (long long)r * n;
-            for (int col = c + 1 + lane; col <= r; col += 32) row[col] = fma(-lr, colv[col], row[col]);
+#pragma unroll 8
+        for (int k = 0; k < kCholB; ++k) {
+            const double a = Ar[ty][k];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[q] = fma(a, Ac[tx * 4 + q][k], acc[q]);
         }
         __syncthreads();
     }
-    if (tid == 0) *info = bad;
+    const int r = r0 + ty;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int j = tx * 4 + q, col = c0 + j;
+        if (r < n && j < w && r >= col) A[(long long)r * n + col] -= acc[q];
+    }
+}
+
+__global__ void __launch_bounds__(512) chol_factor_kernel(int n, int c0, int w, double *__restrict__ A,
+                                                          int *__restrict__ info)
+{
+    if (*info) return;
+    __shared__ double D[kCholB][kCholB + 1];
+    __shared__ int bad;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    if (tid == 0) bad = 0;
+    for (int idx = tid; idx < kCholB * kCholB; idx += nt) {
+        const int r = idx / kCholB, c = idx - r * kCholB;
+        D[r][c] = (r < w && c <= r) ? A[(long long)(c0 + r) * n + c0 + c] : 0.0;
+    }
+    __syncthreads();
+    for (int c = 0; c < w; ++c) {
+        if (tid == 0) {
+            const double s = D[c][c];
+            if (!(s > 0.0)) {
+                bad = c0 + c + 1;
+                D[c][c] = 1.0;
+            } else {
+                D[c][c] = sqrt(s);
+            }
+        }
+        __syncthreads();
+        if (bad) break;
+        if (tid > c && tid < w) D[tid][c] /= D[c][c];
+        __syncthreads();
+        // trailing update inside the block: D[r][cc] -= D[r][c] D[cc][c], c < cc <= r < w
+        for (int idx = tid; idx < kCholB * kCholB; idx += nt) {
+            const int r = idx / kCholB, cc = idx - r * kCholB;
+            if (cc > c && cc <= r && r < w) D[r][cc] = fma(-D[r][c], D[cc][c], D[r][cc]);
+        }
+        __syncthreads();
+    }
+    if (bad) {
+        if (tid == 0) atomicCAS(info, 0, bad);
+        return;
+    }
+    for (int idx = tid; idx < kCholB * kCholB; idx += nt) {
+        const int r = idx / kCholB, c = idx - r * kCholB;
+        if (r < w && c <= r) A[(long long)(c0 + r) * n + c0 + c] = D[r][c];
+    }
+    // rows below the block: x D^T = a  (forward substitution, one row per thread)
+    for (int r = c0 + w + tid; r < n; r += nt) {
+        double x[kCholB];
+        double *row = A + (long long)r * n + c0;
+#pragma unroll
+        for (int c = 0; c < kCholB; ++c) {
+            if (c < w) {
+                double s = row[c];
+#pragma unroll
+                for (int k = 0; k < c; ++k) s = fma(-x[k], D[c][k], s);
+                x[c] = s / D[c][c];
+                row[c] = x[c];
+            }
+        }
+    }
 }
 
 void launch_cholesky(int n, double *A, int *info, cudaStream_t st)
 {
-    const size_t smem = sizeof(double) * (size_t)n;
-    if (smem > 48 * 1024)
-        cudaFuncSetAttribute(cholesky_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cholesky_kernel<<<1, 1024, smem, st>>>(n, A, info);
-    count_launches(1);
+    cudaMemsetAsync(info, 0, sizeof(int), st);
+    for (int c0 = 0; c0 < n; c0 += kCholB) {
+        const int w = (n - c0) < kCholB ? (n - c0) : kCholB;
+        if (c0 > 0) {
+            const unsigned blocks = (unsigned)((n - c0 + kCholB - 1) / kCholB);
+            chol_update_kernel<<<blocks, 256, 0, st>>>(n, c0, w, A, info);
+            count_launches(1);
+        }
+        chol_factor_kernel<<<1, 512, 0, st>>>(n, c0, w, A, info);
+        count_launches(1);
+    }
 }
 
 // Explicit inverse of the lower Cholesky factor, one warp per column

@@ -207,3 +207,91 @@ template int launch_quad_sweep<float>(int, const Lay &, const ELay &, const floa
                                       double, float *, const int *, int *, cudaStream_t);
 
 }  // namespace gputo
+
+namespace gputo {
+
+// Element-centric sweep for a level with stored (packed) element matrices:
+// one thread per element reads its 300 matrix entries once (coalesced,
+// structure of arrays) and writes y_E = A_E u_E; the node pass is the same
+// deterministic gather as for level 1.  Used for the large coarse levels,
+// where the node-centred form re-reads every entry from the 8 nodes around it.
+template <typename T, bool PRE>
+__global__ void __launch_bounds__(128)
+packed_element_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u, const T *__restrict__ f,
+                      const T *__restrict__ diag, T prerelax, T *__restrict__ y, const int *__restrict__ done)
+{
+    if (done && *done) return;
+    const Grid &g = L.g;
+    const long long nel = g.nel();
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nel) return;
+    const long long t = e / g.ny;
+    const int j = (int)(e - t * g.ny);
+    const int i = (int)(t / g.nz);
+    const int k = (int)(t - (long long)i * g.nz);
+    T ue[24];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        const long long nb = L.at(i + local_x(a), j + local_y(a), k + local_z(a));
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            if (PRE) {
+                const T dv = diag[nb + q];
+                ue[3 * a + q] = dv != T(0) ? prerelax * f[nb + q] / dv : T(0);
+            } else {
+                ue[3 * a + q] = u[nb + q];
+            }
+        }
+    }
+    T ye[24];
+#pragma unroll
+    for (int m = 0; m < 24; ++m) ye[m] = T(0);
+#pragma unroll
+    for (int m = 0; m < 24; ++m) {
+#pragma unroll
+        for (int n = 0; n <= m; ++n) {
+            const T amn = A[(long long)packed_index(m, n) * nel + e];
+            ye[m] = fma(amn, ue[n], ye[m]);
+            if (n != m) ye[n] = fma(amn, ue[m], ye[n]);
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < 24; ++m) y[(long long)m * nel + e] = ye[m];
+}
+
+template <typename T>
+void launch_packed_sweep_ec(int mode, const Lay &L, const T *Apk, const T *u, const T *f, const T *diag,
+                            const uint8_t *mask, T *out, T omega, T prerelax, T *yscratch,
+                            const int *done, cudaStream_t st)
+{
+    const int bs = 128;
+    const unsigned eb = (unsigned)((L.g.nel() + bs - 1) / bs);
+    const unsigned nb = (unsigned)((L.g.nnod() + bs - 1) / bs);
+    if (mode == MODE_JACOBI_PRE)
+        packed_element_kernel<T, true><<<eb, bs, 0, st>>>(L, Apk, u, f, diag, prerelax, yscratch, done);
+    else
+        packed_element_kernel<T, false><<<eb, bs, 0, st>>>(L, Apk, u, f, diag, prerelax, yscratch, done);
+    switch (mode) {
+    case MODE_APPLY:
+        quad_node_kernel<T, MODE_APPLY><<<nb, bs, 0, st>>>(L, yscratch, u, f, diag, mask, out, omega, prerelax, done);
+        break;
+    case MODE_DEFECT:
+        quad_node_kernel<T, MODE_DEFECT><<<nb, bs, 0, st>>>(L, yscratch, u, f, diag, mask, out, omega, prerelax, done);
+        break;
+    case MODE_JACOBI:
+        quad_node_kernel<T, MODE_JACOBI><<<nb, bs, 0, st>>>(L, yscratch, u, f, diag, mask, out, omega, prerelax, done);
+        break;
+    default:
+        quad_node_kernel<T, MODE_JACOBI_PRE><<<nb, bs, 0, st>>>(L, yscratch, u, f, diag, mask, out, omega, prerelax, done);
+    }
+    count_launches(2);
+}
+
+template void launch_packed_sweep_ec<double>(int, const Lay &, const double *, const double *,
+                                             const double *, const double *, const uint8_t *, double *,
+                                             double, double, double *, const int *, cudaStream_t);
+template void launch_packed_sweep_ec<float>(int, const Lay &, const float *, const float *, const float *,
+                                            const float *, const uint8_t *, float *, float, float, float *,
+                                            const int *, cudaStream_t);
+
+}  // namespace gputo

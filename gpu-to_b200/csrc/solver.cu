@@ -73,7 +73,8 @@ int Solver::alloc_levels(LevelBuf<T> *Lv, bool with_matrices)
         ALLOC(b.f, nv);
         // level 1 is applied matrix-free unless it is the coarsest level
         if (l > 0 && with_matrices && !(l == 1 && quad_level1())) ALLOC(b.Apk, 300 * g[l].nel());
-        if (l == 1 && quad_level1()) ALLOC(b.yq, 24 * g[l].nel());
+        if (l >= 1 && (l == 1 ? quad_level1() : g[l].nel() >= kElementCentricMinElems))
+            ALLOC(b.yq, 24 * g[l].nel());
         b.mask = mask[l];
     }
     return GPUTO_OK;
@@ -283,6 +284,9 @@ void Solver::vcycle_impl(LevelBuf<T> *Lv, const T *CXl, const T *r0, T *z0, cons
         else if (l == 1 && quad_level1())
             note(launch_quad_sweep<T>(mode, lay[1], elay, CXl, u, f, Lv[1].diag, mask[1], out, w, pr,
                                       opt.nu, Lv[1].yq, done, err, st));
+        else if (Lv[l].yq)
+            launch_packed_sweep_ec<T>(mode, lay[l], Lv[l].Apk, u, f, Lv[l].diag, mask[l], out, w, pr,
+                                      Lv[l].yq, done, st);
         else
             launch_packed_sweep<T>(mode, lay[l], Lv[l].Apk, u, f, Lv[l].diag, mask[l], out, w, pr, done,
                                    st);
