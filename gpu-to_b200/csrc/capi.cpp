@@ -363,13 +363,28 @@ struct Scratch {
     double *partial = nullptr;
     unsigned *ticket = nullptr;
     double *scalar = nullptr;
+    int *err = nullptr;
+    double *big = nullptr;      // grown on demand (tensor-core partials)
+    long long big_cap = 0;
     cudaStream_t st = nullptr;
+    int reserve_big(long long n)
+    {
+        if (n <= big_cap) return GPUTO_OK;
+        cudaFree(big);
+        big = nullptr;
+        big_cap = 0;
+        GPUTO_CUDA(cudaMalloc(&big, sizeof(double) * (size_t)n));
+        big_cap = n;
+        return GPUTO_OK;
+    }
     int init()
     {
         if (partial) return GPUTO_OK;
         GPUTO_CUDA(cudaMalloc(&partial, sizeof(double) * 2048));
         GPUTO_CUDA(cudaMalloc(&ticket, 16));
         GPUTO_CUDA(cudaMalloc(&scalar, sizeof(double)));
+        GPUTO_CUDA(cudaMalloc(&err, sizeof(int)));
+        GPUTO_CUDA(cudaMemset(err, 0, sizeof(int)));
         GPUTO_CUDA(cudaMemset(ticket, 0, 16));
         GPUTO_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         return GPUTO_OK;
@@ -406,6 +421,44 @@ int gputo_compliance_sens_dev(const double *Ke0, const double *U, const double *
                                    cudaMemcpyDeviceToHost, s));
     GPUTO_CUDA(cudaStreamSynchronize(s));
     GPUTO_CUDA(cudaGetLastError());
+    return GPUTO_OK;
+}
+
+int gputo_compliance_sens_tc_dev(const double *Ke0, const double *U, const double *CX,
+                                 const double *dsK, int nelx, int nely, int nelz, double *ce,
+                                 double *dc, double *compliance, void *stream)
+{
+    if (!Ke0 || !U || !grid_ok(nelx, nely, nelz) || (dc && !dsK) || (compliance && !CX))
+        return GPUTO_ERR_ARG;
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    int st = gputo::check_device();
+    if (st) return st;
+    st = g_scratch.init();
+    if (st) return st;
+    Grid g{nelx, nely, nelz};
+    if (!gputo::element_energy_tc_fits(g)) {
+        gputo::set_error("grid too large for the tensor-core contraction (2^31 dofs)");
+        return GPUTO_ERR_ARG;
+    }
+    st = g_scratch.reserve_big(gputo::element_energy_tc_partials(g));
+    if (st) return st;
+    cudaStream_t s = stream ? (cudaStream_t)stream : g_scratch.st;
+    st = gputo::upload_fine_ke(Ke0, s);
+    if (st) return st;
+    gputo::launch_element_energy_tc(g, U, CX, dsK, ce, dc, g_scratch.big,
+                                    compliance ? g_scratch.scalar : nullptr, g_scratch.err, s);
+    if (compliance)
+        GPUTO_CUDA(cudaMemcpyAsync(compliance, g_scratch.scalar, sizeof(double),
+                                   cudaMemcpyDeviceToHost, s));
+    int h_err = 0;
+    GPUTO_CUDA(cudaMemcpyAsync(&h_err, g_scratch.err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    GPUTO_CUDA(cudaStreamSynchronize(s));
+    GPUTO_CUDA(cudaGetLastError());
+    if (h_err) {
+        cudaMemset(g_scratch.err, 0, sizeof(int));
+        gputo::set_error("tensor-core MMA completion wait gave up");
+        return GPUTO_ERR_TIMEOUT;
+    }
     return GPUTO_OK;
 }
 

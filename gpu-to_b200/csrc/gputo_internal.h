@@ -112,6 +112,7 @@ int cuda_status(cudaError_t e, const char *what);
 // Level-0 element matrix in constant memory (FP64 and FP32 copies).
 int upload_fine_ke(const double *Ke_host, cudaStream_t st);
 int upload_design_ke(const double *Ke_host, cudaStream_t st);
+int upload_tc_ke(const double *Ke_host, cudaStream_t st);
 // B^T D B w at one Gauss point (ix,iy,iz) of an h-cube, E = 1 (host).
 void gauss_part(double nu, double h, int ix, int iy, int iz, double K[24][24]);
 // Level-1 quadrature parts Kg[g] (packed 300 each) for nu, h = 2.
@@ -211,6 +212,13 @@ void launch_flip_y(long long nnod, double *U, cudaStream_t st);
 void launch_element_energy(const Grid &g, const double *U, const double *CX, const double *dsK,
                            double *ce, double *dc, double *partial, unsigned *ticket,
                            double *compliance, cudaStream_t st);
+// ce / dc / compliance with the element contraction on the tensor cores
+// (tcgen05, BF16 splits, FP32 accumulate): kernels_tc.cu.
+long long element_energy_tc_partials(const Grid &g);
+bool element_energy_tc_fits(const Grid &g);   // 32-bit dof indexing
+void launch_element_energy_tc(const Grid &g, const double *U, const double *CX, const double *dsK,
+                              double *ce, double *dc, double *partial, double *compliance, int *err,
+                              cudaStream_t st);
 void launch_element_energy_blocks(const Grid &g, const double *U, const double *CX,
                                   const double *dsK, double *ce, double *dc, double *partial,
                                   unsigned *ticket, double *compliance, int nblocks,

@@ -53,7 +53,8 @@ int upload_fine_ke(const double *Ke_host, cudaStream_t st)
     have[slot] = true;
     GPUTO_CUDA(cudaMemcpyToSymbolAsync(cKe64, last[slot], sizeof(double) * 576, 0, cudaMemcpyHostToDevice, st));
     GPUTO_CUDA(cudaMemcpyToSymbolAsync(cKe32, kf, sizeof(kf), 0, cudaMemcpyHostToDevice, st));
-    const int s2 = upload_design_ke(last[slot], st);
+    int s2 = upload_design_ke(last[slot], st);
+    if (!s2) s2 = upload_tc_ke(last[slot], st);
     if (s2) return s2;
     GPUTO_CUDA(cudaStreamSynchronize(st));
     return GPUTO_OK;

@@ -74,6 +74,7 @@ SIGNATURES = {
     "gputo_solver_time_kernel": (_i, [_vp, _i, _i, _dp, _vp]),
     "gputo_compliance_sens_dev": (_i, [_dp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _dp, _vp]),
     "gputo_compliance_sens": (_i, [_dp, _dp, _dp, _dp, _i, _i, _i, _dp, _dp, _dp]),
+    "gputo_compliance_sens_tc_dev": (_i, [_dp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _dp, _vp]),
     "gputo_compliance_sens_noalloc_dev": (_i, [_dp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _dp, _vp]),
     "gputo_density_filter_dev": (_i, [_vp, _vp, _vp, _i, _i, _i, _d, _i, _vp]),
     "gputo_density_filter": (_i, [_dp, _dp, _dp, _i, _i, _i, _d, _i]),
@@ -290,6 +291,16 @@ def compliance_sens_dev(Ke0, U, CX, dsK, nelx, nely, nelz, ce=None, dc=None, str
     _check(_lib.gputo_compliance_sens_dev(_p(Ke0), _ptr(U), _ptr(CX), _ptr(dsK), nelx, nely, nelz,
                                           _ptr(ce), _ptr(dc), ctypes.byref(c), _ptr_stream(stream)),
            "gputo_compliance_sens_dev")
+    return c.value
+
+
+def compliance_sens_tc_dev(Ke0, U, CX, dsK, nelx, nely, nelz, ce=None, dc=None, stream=None):
+    """Tensor-core form of compliance_sens_dev (U in the solver frame)."""
+    Ke0 = np.ascontiguousarray(Ke0, dtype=np.float64).reshape(-1)
+    c = ctypes.c_double(0.0)
+    _check(_lib.gputo_compliance_sens_tc_dev(_p(Ke0), _ptr(U), _ptr(CX), _ptr(dsK), nelx, nely, nelz,
+                                             _ptr(ce), _ptr(dc), ctypes.byref(c), _ptr_stream(stream)),
+           "gputo_compliance_sens_tc_dev")
     return c.value
 
 

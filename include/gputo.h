@@ -180,6 +180,14 @@ int gputo_compliance_sens(const double *Ke0, const double *U, const double *CX,
                           const double *dsK, int nelx, int nely, int nelz, double *ce,
                           double *dc, double *compliance);
 
+/* gputo_compliance_sens_dev with the element contraction U Ke on the tensor
+ * cores: the [n_elem x 24] x [24 x 24] product runs as tcgen05 BF16 MMAs with
+ * FP32 accumulation (U and Ke each split into three BF16 parts), then
+ * ce = u . (Ke u) in FP64.  About 1e-7 relative accuracy. */
+int gputo_compliance_sens_tc_dev(const double *Ke0, const double *U, const double *CX,
+                                 const double *dsK, int nelx, int nely, int nelz, double *ce,
+                                 double *dc, double *compliance, void *stream);
+
 /* gputo_compliance_sens_dev for callers that cannot allocate device memory.
  * No counterpart in the reference: its sensitivity step is MATLAB code.
  *
