@@ -109,6 +109,8 @@ void gputo_default_options(gputo_options *o)
     o->check_every = 1;
     o->use_graph = 1;
     o->max_coarse_dofs = 12000;
+    o->tc_parts = 0;
+    o->tc_xchunk = 0;
 }
 
 int gputo_solver_create(gputo_solver **out, int nelx, int nely, int nelz, int nl,
@@ -192,14 +194,42 @@ int gputo_solver_apply_dev(gputo_solver *h, const double *u, double *r, void *st
     return s.check_error_flags(st);
 }
 
+int gputo_solver_apply_fp32_dev(gputo_solver *h, const double *u, double *r, int tc_parts, void *stream)
+{
+    if (!h || !u || !r || tc_parts < 0 || tc_parts > 2) return GPUTO_ERR_ARG;
+    Solver &s = h->s;
+    if (!s.ready || s.opt.precision != GPUTO_PREC_MIXED) return GPUTO_ERR_ARG;
+    cudaStream_t st = s.stream(stream);
+    s.launch_status = GPUTO_OK;
+    const long long nv = s.lay[0].size();
+    gputo::launch_pack(s.lay[0], u, s.P, 0, st);
+    gputo::launch_convert<double, float>(nv, s.P, s.Lf[0].u0, nullptr, st);
+    int rs;
+    if (tc_parts == 0)
+        rs = gputo::launch_fine_sweep<float>(gputo::MODE_APPLY, s.lay[0], s.elay, s.CXpf, s.Lf[0].u0, nullptr,
+                                             s.Lf[0].diag, s.mask[0], s.Lf[0].u1, 1.f, 0.f, nullptr, nullptr,
+                                             s.err, st);
+    else
+        rs = gputo::launch_tc_sweep(tc_parts, gputo::MODE_APPLY, s.lay[0], s.elay, s.CXpf, s.Lf[0].u0, nullptr,
+                                    s.Lf[0].diag, s.mask[0], s.Lf[0].u1, 1.f, 0.f, s.opt.tc_xchunk, nullptr,
+                                    s.err, st);
+    if (rs) return rs;
+    gputo::launch_convert<float, double>(nv, s.Lf[0].u1, s.Q, nullptr, st);
+    gputo::launch_unpack(s.lay[0], s.Q, r, 0, st);
+    GPUTO_CUDA(cudaStreamSynchronize(st));
+    GPUTO_CUDA(cudaGetLastError());
+    if (s.launch_status) return s.launch_status;
+    return s.check_error_flags(st);
+}
+
 long long gputo_solver_launch_count(const gputo_solver *) { return gputo::launches_issued(); }
 
 int gputo_solver_time_kernel(gputo_solver *h, int which, int reps, double *ms, void *stream)
 {
-    if (!h || !ms || reps < 1 || which < 0 || which > 3) return GPUTO_ERR_ARG;
+    if (!h || !ms || reps < 1 || which < 0 || which > 4) return GPUTO_ERR_ARG;
     Solver &s = h->s;
     if (!s.ready) return GPUTO_ERR_ARG;
-    if ((which == 1 || which == 2) && s.opt.precision != GPUTO_PREC_MIXED) return GPUTO_ERR_ARG;
+    if ((which == 1 || which == 2 || which == 4) && s.opt.precision != GPUTO_PREC_MIXED) return GPUTO_ERR_ARG;
     if ((which == 2 || which == 3) && s.nl < 2) return GPUTO_ERR_ARG;
     cudaStream_t st = s.stream(stream);
     cudaEvent_t e0, e1;
@@ -218,6 +248,11 @@ int gputo_solver_time_kernel(gputo_solver *h, int which, int reps, double *ms, v
             r = gputo::launch_fine_sweep<float>(gputo::MODE_JACOBI, s.lay[0], s.elay, s.CXpf, s.Lf[0].u0,
                                                 s.Lf[0].f, s.Lf[0].diag, s.mask[0], s.Lf[0].u1, 0.48f,
                                                 0.7f, nullptr, nullptr, s.err, st);
+            break;
+        case 4:
+            r = gputo::launch_tc_sweep(s.opt.tc_parts > 0 ? s.opt.tc_parts : 1, gputo::MODE_JACOBI, s.lay[0],
+                                       s.elay, s.CXpf, s.Lf[0].u0, s.Lf[0].f, s.Lf[0].diag, s.mask[0],
+                                       s.Lf[0].u1, 0.48f, 0.7f, s.opt.tc_xchunk, nullptr, s.err, st);
             break;
         case 2:
             if (s.quad_level1())

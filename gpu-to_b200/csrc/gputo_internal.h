@@ -113,6 +113,7 @@ int cuda_status(cudaError_t e, const char *what);
 int upload_fine_ke(const double *Ke_host, cudaStream_t st);
 int upload_design_ke(const double *Ke_host, cudaStream_t st);
 int upload_tc_ke(const double *Ke_host, cudaStream_t st);
+int upload_tcsweep_ke(const double *Ke_host, cudaStream_t st);
 // B^T D B w at one Gauss point (ix,iy,iz) of an h-cube, E = 1 (host).
 void gauss_part(double nu, double h, int ix, int iy, int iz, double K[24][24]);
 // Level-1 quadrature parts Kg[g] (packed 300 each) for nu, h = 2.
@@ -130,6 +131,19 @@ int launch_fine_sweep(int mode, const Lay &L, const ELay &E, const T *CX, const 
 // Level-1 quadrature operator applied matrix-free (L: level-1 layout, Ef: the
 // fine element layout of the padded CX, yscratch: 24 values per level-1
 // element, nu: Poisson ratio of the quadrature operator).
+// Far-face nodes of a fine sweep only (kernels_fine.cu).
+template <typename T>
+int launch_fine_faces(int mode, const Lay &L, const ELay &E, const T *CX, const T *u, const T *f, const T *diag,
+                      const uint8_t *mask, T *out, T omega, T prerelax, const int *done, cudaStream_t st);
+
+// FP32 fine sweep with the element contraction on the tensor cores
+// (kernels_tcsweep.cu).  parts: u and Ke each split into 1 or 2 BF16 parts.
+// xchunk: node planes per CTA along x.
+int init_tc_sweep_kernels();
+int launch_tc_sweep(int parts, int mode, const Lay &L, const ELay &E, const float *CX, const float *u,
+                    const float *f, const float *diag, const uint8_t *mask, float *out, float omega,
+                    float prerelax, int xchunk, const int *done, int *err, cudaStream_t st);
+
 template <typename T>
 int launch_quad_sweep(int mode, const Lay &L, const ELay &Ef, const T *CX, const T *u, const T *f,
                       const T *diag, const uint8_t *mask, T *out, T omega, T prerelax, double nu,

@@ -55,6 +55,7 @@ int upload_fine_ke(const double *Ke_host, cudaStream_t st)
     GPUTO_CUDA(cudaMemcpyToSymbolAsync(cKe32, kf, sizeof(kf), 0, cudaMemcpyHostToDevice, st));
     int s2 = upload_design_ke(last[slot], st);
     if (!s2) s2 = upload_tc_ke(last[slot], st);
+    if (!s2) s2 = upload_tcsweep_ke(last[slot], st);
     if (s2) return s2;
     GPUTO_CUDA(cudaStreamSynchronize(st));
     return GPUTO_OK;
@@ -476,6 +477,37 @@ int launch_fine_sweep(int mode, const Lay &L, const ELay &E, const T *CX, const 
     return launch_any<T, OP_FINE, TX_FINE>(mode, L, E, CX, u, f, diag, mask, out, omega, prerelax,
                                            dot_partial, done, err, st);
 }
+
+// The far-face gather alone (nodes j = ny, k = nz, i = nx), for sweeps whose
+// interior comes from another kernel.
+template <typename T>
+int launch_fine_faces(int mode, const Lay &L, const ELay &E, const T *CX, const T *u, const T *f, const T *diag,
+                      const uint8_t *mask, T *out, T omega, T prerelax, const int *done, cudaStream_t st)
+{
+    const unsigned fb = (unsigned)((face_nodes(L.g) + 127) / 128);
+    switch (mode) {
+    case MODE_APPLY:
+        face_kernel<T, MODE_APPLY, OP_FINE><<<fb, 128, 0, st>>>(L, E, CX, u, f, diag, mask, out, omega, prerelax,
+                                                                nullptr, done);
+        break;
+    case MODE_DEFECT:
+        face_kernel<T, MODE_DEFECT, OP_FINE><<<fb, 128, 0, st>>>(L, E, CX, u, f, diag, mask, out, omega, prerelax,
+                                                                 nullptr, done);
+        break;
+    case MODE_JACOBI:
+        face_kernel<T, MODE_JACOBI, OP_FINE><<<fb, 128, 0, st>>>(L, E, CX, u, f, diag, mask, out, omega, prerelax,
+                                                                 nullptr, done);
+        break;
+    default:
+        face_kernel<T, MODE_JACOBI_PRE, OP_FINE><<<fb, 128, 0, st>>>(L, E, CX, u, f, diag, mask, out, omega,
+                                                                     prerelax, nullptr, done);
+    }
+    count_launches(1);
+    return GPUTO_OK;
+}
+template int launch_fine_faces<float>(int, const Lay &, const ELay &, const float *, const float *, const float *,
+                                      const float *, const uint8_t *, float *, float, float, const int *,
+                                      cudaStream_t);
 
 template int launch_fine_sweep<double>(int, const Lay &, const ELay &, const double *, const double *,
                                        const double *, const double *, const uint8_t *, double *,

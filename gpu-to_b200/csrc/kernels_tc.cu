@@ -269,12 +269,14 @@ element_energy_tc_kernel(Grid g, const double *__restrict__ U,
 #pragma unroll
         for (int c0 = 0; c0 < 72; c0 += 16) {
             uint32_t r[16];
+            // the wait is in the same statement: no use of r can move above it
             asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n\t"
+                "tcgen05.wait::ld.sync.aligned;"
                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-                : "r"(tmem + row_addr_off + (uint32_t)c0));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                : "r"(tmem + row_addr_off + (uint32_t)c0)
+                : "memory");
 #pragma unroll
             for (int q = 0; q < 16; ++q) {
                 const int c = c0 + q;

@@ -18,6 +18,8 @@
 //    built with atomics (:747-790).
 #include "solver.h"
 
+#include <type_traits>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -93,7 +95,8 @@ int Solver::create(int nelx, int nely, int nelz, int nl_, const gputo_options *o
         set_error("nelx, nely, nelz must be divisible by 2^(nl-1)");
         return GPUTO_ERR_ARG;
     }
-    if (opt.nswp < 0 || opt.check_every < 1 || !(opt.omega > 0) ||
+    if (opt.nswp < 0 || opt.check_every < 1 || !(opt.omega > 0) || opt.tc_parts < 0 || opt.tc_parts > 2 ||
+        opt.tc_xchunk < 0 ||
         (opt.precision != GPUTO_PREC_FP64 && opt.precision != GPUTO_PREC_MIXED)) {
         set_error("invalid solver options");
         return GPUTO_ERR_ARG;
@@ -113,6 +116,7 @@ int Solver::create(int nelx, int nely, int nelz, int nl_, const gputo_options *o
     GPUTO_CUDA(cudaGetDevice(&device));
     GPUTO_CUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
     int ik = init_fine_kernels();
+    if (!ik && opt.precision == GPUTO_PREC_MIXED) ik = init_tc_sweep_kernels();
     if (ik) return ik;
 
     const long long nv = lay[0].size(), ne = g[0].nel();
@@ -278,9 +282,17 @@ void Solver::vcycle_impl(LevelBuf<T> *Lv, const T *CXl, const T *r0, T *z0, cons
     const int ns = opt.nswp;
     const T om = (T)opt.omega, pr = (T)opt.prerelax;
     auto sweep = [&](int l, int mode, const T *u, const T *f, T *out, T w) {
-        if (l == 0)
+        if (l == 0) {
+            if constexpr (std::is_same<T, float>::value) {
+                if (opt.tc_parts > 0) {
+                    note(launch_tc_sweep(opt.tc_parts, mode, lay[0], elay, CXl, u, f, Lv[0].diag, mask[0], out, w,
+                                         pr, opt.tc_xchunk, done, err, st));
+                    return;
+                }
+            }
             note(launch_fine_sweep<T>(mode, lay[0], elay, CXl, u, f, Lv[0].diag, mask[0], out, w, pr,
                                       nullptr, done, err, st));
+        }
         else if (l == 1 && quad_level1())
             note(launch_quad_sweep<T>(mode, lay[1], elay, CXl, u, f, Lv[1].diag, mask[1], out, w, pr,
                                       opt.nu, Lv[1].yq, done, err, st));

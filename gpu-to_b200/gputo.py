@@ -50,7 +50,8 @@ _d = ctypes.c_double
 
 class Options(ctypes.Structure):
     _fields_ = [("precision", _i), ("nswp", _i), ("omega", _d), ("prerelax", _d), ("nu", _d),
-                ("check_every", _i), ("use_graph", _i), ("max_coarse_dofs", _i)]
+                ("check_every", _i), ("use_graph", _i), ("max_coarse_dofs", _i), ("tc_parts", _i),
+                ("tc_xchunk", _i)]
 
 
 SIGNATURES = {
@@ -64,6 +65,7 @@ SIGNATURES = {
                             ctypes.POINTER(Options), _dp, _ip]),
     "gputo_solver_create": (_i, [ctypes.POINTER(_vp), _i, _i, _i, _i, ctypes.POINTER(Options)]),
     "gputo_solver_destroy": (None, [_vp]),
+    "gputo_solver_apply_fp32_dev": (_i, [_vp, _vp, _vp, _i, _vp]),
     "gputo_solver_device_bytes": (ctypes.c_size_t, [_vp]),
     "gputo_solver_set_problem": (_i, [_vp, _dp, _dp, _i]),
     "gputo_solver_setup_dev": (_i, [_vp, _vp, _vp]),
@@ -255,6 +257,11 @@ class Solver:
     def apply(self, u, r, stream=None):
         _check(_lib.gputo_solver_apply_dev(self._h, _ptr(u), _ptr(r), _ptr_stream(stream)),
                "gputo_solver_apply_dev")
+
+    def apply_fp32(self, u, r, tc_parts=0, stream=None):
+        """The mixed V-cycle's FP32 fine operator (0: CUDA cores, 1-3: tensor cores)."""
+        _check(_lib.gputo_solver_apply_fp32_dev(self._h, _ptr(u), _ptr(r), int(tc_parts), _ptr_stream(stream)),
+               "gputo_solver_apply_fp32_dev")
 
 
 def _ptr_stream(stream):

@@ -69,6 +69,13 @@ typedef struct {
     int check_every;     /* PCG iterations between host convergence checks (>=1) */
     int use_graph;       /* capture the PCG iteration in a CUDA graph (0/1)      */
     int max_coarse_dofs; /* reject hierarchies whose coarsest grid is larger      */
+    int tc_parts;        /* GPUTO_PREC_MIXED only: fine-level smoother on the
+                            tensor cores, u and Ke each split into this many
+                            BF16 parts (1: plain BF16, about 2e-3 relative;
+                            2: about 1e-5), FP32 accumulation; 0 = FP32 CUDA
+                            cores                                                 */
+    int tc_xchunk;       /* node planes per CTA of the tensor-core smoother
+                            (0 = 16)                                              */
 } gputo_options;
 
 void gputo_default_options(gputo_options *opt);
@@ -127,6 +134,12 @@ typedef struct gputo_solver gputo_solver;
 int gputo_solver_create(gputo_solver **out, int nelx, int nely, int nelz, int nl,
                         const gputo_options *opt);
 void gputo_solver_destroy(gputo_solver *s);
+/* r = K u with the fine-level FP32 operator of the mixed-precision V-cycle
+ * (precision GPUTO_PREC_MIXED only): tc_parts = 0 uses the CUDA-core tile
+ * kernel, 1 or 2 the tensor-core sweep with u and Ke split into that many
+ * BF16 parts.  u
+ * and r are ndof doubles on the device (converted to and from FP32). */
+int gputo_solver_apply_fp32_dev(gputo_solver *s, const double *u, double *r, int tc_parts, void *stream);
 /* Bytes of device memory the solver holds. */
 size_t gputo_solver_device_bytes(const gputo_solver *s);
 
@@ -159,7 +172,8 @@ long long gputo_solver_launch_count(const gputo_solver *s);
 /* Time 'reps' back-to-back launches of one solver kernel on the current
  * hierarchy with CUDA events on 'stream' and return the mean launch time in
  * milliseconds.  which: 0 fine-level FP64 apply (p -> K p), 1 fine-level FP32
- * Jacobi sweep, 2 level-1 FP32 sweep, 3 level-1 FP64 sweep.  Inputs are the
+ * Jacobi sweep, 2 level-1 FP32 sweep, 3 level-1 FP64 sweep, 4 fine-level
+ * tensor-core Jacobi sweep (tc_parts of the options, 1 if 0).  Inputs are the
  * solver's own work vectors; results are discarded.  Needs setup first. */
 int gputo_solver_time_kernel(gputo_solver *s, int which, int reps, double *ms_per_launch,
                              void *stream);
