@@ -30,7 +30,8 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", f"-I{CSRC
           f"-I{os.path.join(ROOT, 'include')}"]
 
 SOURCES = ["kernels_fine.cu", "kernels_mg.cu", "kernels_blas.cu", "kernels_design.cu", "solver.cu",
-           "capi.cpp", "noalloc.cu", "kernels_quad.cu", "kernels_tc.cu", "kernels_tcsweep.cu"]
+           "capi.cpp", "noalloc.cu", "kernels_quad.cu", "kernels_tc.cu", "kernels_tcsweep.cu",
+           "kernels_learned.cu"]
 HEADERS = ["gputo_internal.h", "solver.h", "tma.h"]
 
 

@@ -7,6 +7,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <new>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -18,6 +19,10 @@ using gputo::Solver;
 
 struct gputo_solver {
     Solver s;
+};
+
+struct gputo_net {
+    gputo::Net n;
 };
 
 namespace gputo {
@@ -220,6 +225,177 @@ int gputo_solver_apply_fp32_dev(gputo_solver *h, const double *u, double *r, int
     GPUTO_CUDA(cudaGetLastError());
     if (s.launch_status) return s.launch_status;
     return s.check_error_flags(st);
+}
+
+// ---------------------------------------------------------------------------
+// learned coarse-grid correction
+// ---------------------------------------------------------------------------
+
+long long gputo_net_num_params(void) { return gputo::Net::num_params(); }
+
+int gputo_net_create(gputo_net **out, unsigned long long seed)
+{
+    if (!out) return GPUTO_ERR_ARG;
+    *out = nullptr;
+    int st = gputo::check_device();
+    if (st) return st;
+    auto *h = new (std::nothrow) gputo_net();
+    if (!h) return GPUTO_ERR_OOM;
+    st = h->n.create(seed);
+    if (st) {
+        delete h;
+        return st;
+    }
+    *out = h;
+    return GPUTO_OK;
+}
+
+void gputo_net_destroy(gputo_net *h) { delete h; }
+
+int gputo_net_get_params(const gputo_net *h, float *host)
+{
+    if (!h || !host) return GPUTO_ERR_ARG;
+    GPUTO_CUDA(cudaMemcpy(host, h->n.params, sizeof(float) * gputo::Net::num_params(), cudaMemcpyDeviceToHost));
+    return GPUTO_OK;
+}
+
+int gputo_net_set_params(gputo_net *h, const float *host)
+{
+    if (!h || !host) return GPUTO_ERR_ARG;
+    const size_t b = sizeof(float) * gputo::Net::num_params();
+    GPUTO_CUDA(cudaMemcpy(h->n.params, host, b, cudaMemcpyHostToDevice));
+    GPUTO_CUDA(cudaMemset(h->n.grads, 0, b));
+    GPUTO_CUDA(cudaMemset(h->n.m1, 0, b));
+    GPUTO_CUDA(cudaMemset(h->n.m2, 0, b));
+    h->n.step = 0;
+    return GPUTO_OK;
+}
+
+int gputo_net_forward_dev(gputo_net *h, const float *x, int X, int Z, int Y, float *y, void *stream)
+{
+    if (!h || !x || !y || X < 1 || Z < 1 || Y < 1) return GPUTO_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    int s = gputo::init_net_kernels();
+    if (!s) s = h->n.forward(x, gputo::NetDims{X, Z, Y}, y, st);
+    if (s) return s;
+    GPUTO_CUDA(cudaStreamSynchronize(st));
+    GPUTO_CUDA(cudaGetLastError());
+    return GPUTO_OK;
+}
+
+int gputo_net_train_step_dev(gputo_net *h, const float *x, const float *t, const float *m, int nsamples, int X,
+                             int Z, int Y, float lr, double *loss, float *grads_out, void *stream)
+{
+    if (!h || !x || !t || !m || nsamples < 1 || X < 1 || Z < 1 || Y < 1 || lr < 0.f) return GPUTO_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    const gputo::NetDims d{X, Z, Y};
+    const long long n = d.n();
+    int s = gputo::init_net_kernels();
+    if (s) return s;
+    GPUTO_CUDA(cudaMemsetAsync(h->n.loss_acc, 0, sizeof(double), st));
+    for (int q = 0; q < nsamples; ++q) {
+        s = h->n.accumulate(x + (size_t)q * 4 * n, t + (size_t)q * 3 * n, m + (size_t)q * 3 * n, d, st);
+        if (s) return s;
+    }
+    if (grads_out)
+        GPUTO_CUDA(cudaMemcpyAsync(grads_out, h->n.grads, sizeof(float) * gputo::Net::num_params(),
+                                   cudaMemcpyDeviceToHost, st));
+    if (lr > 0.f) {
+        s = h->n.adam(lr, nsamples, st);
+        if (s) return s;
+    } else {
+        GPUTO_CUDA(cudaMemsetAsync(h->n.grads, 0, sizeof(float) * gputo::Net::num_params(), st));
+    }
+    double l = 0.0;
+    GPUTO_CUDA(cudaMemcpyAsync(&l, h->n.loss_acc, sizeof(double), cudaMemcpyDeviceToHost, st));
+    GPUTO_CUDA(cudaStreamSynchronize(st));
+    GPUTO_CUDA(cudaGetLastError());
+    if (loss) *loss = l / nsamples;
+    return GPUTO_OK;
+}
+
+int gputo_solver_set_net(gputo_solver *h, gputo_net *net, int mode)
+{
+    if (!h) return GPUTO_ERR_ARG;
+    return h->s.attach_net(net ? &net->n : nullptr, net ? mode : 0);
+}
+
+int gputo_solver_net_state(const gputo_solver *h, int *on, int *plain_nit, int *net_nit)
+{
+    if (!h) return GPUTO_ERR_ARG;
+    if (on) *on = h->s.net_on ? 1 : 0;
+    if (plain_nit) *plain_nit = h->s.ref_plain_nit;
+    if (net_nit) *net_nit = h->s.ref_net_nit;
+    return GPUTO_OK;
+}
+
+int gputo_solver_net_dims(const gputo_solver *h, int *X, int *Z, int *Y)
+{
+    if (!h || !X || !Z || !Y) return GPUTO_ERR_ARG;
+    const Solver &s = h->s;
+    if (!s.net_x) return GPUTO_ERR_ARG;
+    *X = s.nd.X;
+    *Z = s.nd.Z;
+    *Y = s.nd.Y;
+    return GPUTO_OK;
+}
+
+int gputo_solver_net_features_dev(gputo_solver *h, const double *r, float *x, float *m, float *dsq, float *scale,
+                                  void *stream)
+{
+    if (!h || !r || !x) return GPUTO_ERR_ARG;
+    Solver &s = h->s;
+    if (!s.ready || !s.net_x) return GPUTO_ERR_ARG;
+    cudaStream_t st = s.stream(stream);
+    gputo::launch_pack(s.lay[0], r, s.P, 0, st);
+    gputo::launch_convert<double, float>(s.lay[0].size(), s.P, s.Lf[0].f, nullptr, st);
+    gputo::launch_restrict<float>(s.lay[1], s.lay[0], s.Lf[0].f, s.mask[1], s.Lf[1].f, nullptr, st);
+    gputo::launch_restrict<float>(s.lay[2], s.lay[1], s.Lf[1].f, s.mask[2], s.Lf[2].f, nullptr, st);
+    gputo::launch_net_features(s.lay[2], s.Lf[2].f, s.Lf[2].diag, s.dens2, x, dsq, s.net_s, nullptr, st);
+    if (m) gputo::launch_net_mask(s.g[2], s.mask[2], m, st);
+    float sc = 0.f;
+    GPUTO_CUDA(cudaMemcpyAsync(&sc, s.net_s, sizeof(float), cudaMemcpyDeviceToHost, st));
+    GPUTO_CUDA(cudaStreamSynchronize(st));
+    GPUTO_CUDA(cudaGetLastError());
+    if (scale) *scale = sc;
+    return GPUTO_OK;
+}
+
+int gputo_solver_net_energy_rhs_dev(gputo_solver *h, const double *w, float scale, float *gt, void *stream)
+{
+    if (!h || !w || !gt || !(scale > 0.f)) return GPUTO_ERR_ARG;
+    Solver &s = h->s;
+    if (!s.ready || !s.net_x) return GPUTO_ERR_ARG;
+    cudaStream_t st = s.stream(stream);
+    gputo::launch_pack(s.lay[0], w, s.P, 0, st);
+    gputo::launch_convert<double, float>(s.lay[0].size(), s.P, s.Lf[0].f, nullptr, st);
+    gputo::launch_restrict<float>(s.lay[1], s.lay[0], s.Lf[0].f, s.mask[1], s.Lf[1].f, nullptr, st);
+    gputo::launch_restrict<float>(s.lay[2], s.lay[1], s.Lf[1].f, s.mask[2], s.Lf[2].f, nullptr, st);
+    gputo::launch_net_energy_rhs(s.lay[2], s.Lf[2].f, s.Lf[2].diag, s.mask[2], scale, gt, st);
+    GPUTO_CUDA(cudaStreamSynchronize(st));
+    GPUTO_CUDA(cudaGetLastError());
+    return GPUTO_OK;
+}
+
+int gputo_solver_net_train_step_dev(gputo_solver *h, gputo_net *net, const float *x, const float *gt, int nsamples,
+                                    float lr, double *loss, float *grads_out, void *stream)
+{
+    if (!h || !net || !x || !gt || nsamples < 1 || lr < 0.f) return GPUTO_ERR_ARG;
+    Solver &s = h->s;
+    if (!s.ready || !s.net_x) return GPUTO_ERR_ARG;
+    return s.net_train_energy(&net->n, x, gt, nsamples, lr, loss, grads_out, s.stream(stream));
+}
+
+int gputo_solver_level2_inject_dev(gputo_solver *h, const double *v, float *out, void *stream)
+{
+    if (!h || !v || !out) return GPUTO_ERR_ARG;
+    Solver &s = h->s;
+    if (s.nl < 3) return GPUTO_ERR_ARG;
+    cudaStream_t st = s.stream(stream);
+    gputo::launch_level2_inject(s.g[2], s.g[0], v, out, st);
+    GPUTO_CUDA(cudaStreamSynchronize(st));
+    GPUTO_CUDA(cudaGetLastError());
+    return GPUTO_OK;
 }
 
 long long gputo_solver_launch_count(const gputo_solver *) { return gputo::launches_issued(); }

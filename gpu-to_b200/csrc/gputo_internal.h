@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cstddef>
 #include <string>
+#include <vector>
 
 #include "gputo.h"
 
@@ -249,5 +250,62 @@ void launch_oc_update(long long n, const double *x, const double *dc, const doub
 // Counter of kernel launches issued by this library (per process).
 void count_launches(long long n);
 long long launches_issued();
+
+// ---------------------------------------------------------------------------
+// learned coarse-grid correction (kernels_learned.cu)
+// ---------------------------------------------------------------------------
+
+// Node grid of the network, channels-first [C][X][Z][Y] (Y fastest).
+struct NetDims {
+    int X, Z, Y;
+    __host__ __device__ long long n() const { return (long long)X * Z * Y; }
+};
+
+// The network's parameters, Adam state and activation buffers on one device.
+struct Net {
+    int device = 0;
+    float *params = nullptr, *grads = nullptr, *m1 = nullptr, *m2 = nullptr;
+    double *part = nullptr, *loss_acc = nullptr;   // loss reduction scratch, summed loss
+    float *gscale = nullptr;
+    float *act[5] = {};                            // act[0] = input (not owned), act[1..4] owned
+    float *gA = nullptr, *gB = nullptr;            // gradient ping-pong, 64 channels each
+    long long cap_n = 0, step = 0;
+    std::vector<void *> owned;
+
+    static long long num_params();
+    static long long param_offset(int layer, bool bias);
+    ~Net();
+    int create(unsigned long long seed);
+    int reserve(long long nodes);   // activation buffers (never inside a stream capture)
+    // y = net(x) (y may be null: the output stays in act[4])
+    int forward(const float *x, const NetDims &d, float *y, cudaStream_t st);
+    // one sample's masked mean-square loss added to *loss_acc, its gradient to grads
+    int accumulate(const float *x, const float *t, const float *m, const NetDims &d, cudaStream_t st);
+    // gradient of the last forward's output in gA ([3][n]) -> added to grads
+    int backward_from(const NetDims &d, cudaStream_t st);
+    // Adam step with the mean gradient of nsamples accumulated samples; clears grads
+    int adam(float lr, int nsamples, cudaStream_t st);
+};
+
+int init_net_kernels();
+// Level-2 node features of the learned correction: log-density of the
+// element scales, then the restricted residual in Jacobi-scaled units divided
+// by its RMS (device s); dsq (optional) receives sqrt(diag), channels-first.
+void launch_net_density(const Grid &g2, const Grid &gf, const double *CXf, float *dens2, cudaStream_t st);
+void launch_net_features(const Lay &L2, const float *r2, const float *diag2, const float *dens2, float *x,
+                         float *dsq, float *s, const int *done, cudaStream_t st);
+void launch_net_output(const Lay &L2, const float *y, const float *diag2, const float *s, const uint8_t *mask2,
+                       float *e2, const int *done, cudaStream_t st);
+void launch_add_f2d(long long n, const float *e, double *z, const int *done, cudaStream_t st);
+void launch_net_mask(const Grid &g2, const uint8_t *mask2, float *m, cudaStream_t st);
+void launch_level2_inject(const Grid &g2, const Grid &gf, const double *v, float *out, cudaStream_t st);
+// Energy loss of the correction: w = D^-1/2 y (padded), and with q = A2 w the
+// output gradient gy = 2 (D^-1/2 q - g~) and loss += y'D^-1/2 q - 2 y'g~.
+void launch_net_to_padded(const Lay &L2, const float *y, const float *diag2, const uint8_t *mask2, float *w,
+                          cudaStream_t st);
+void launch_net_energy_rhs(const Lay &L2, const float *v2, const float *diag2, const uint8_t *mask2, float scale,
+                           float *gt, cudaStream_t st);
+int launch_net_energy(const Lay &L2, const float *y, const float *q, const float *diag2, const float *gt,
+                      const uint8_t *mask2, float *gy, double *part, int part_cap, double *loss_acc, cudaStream_t st);
 
 }  // namespace gputo

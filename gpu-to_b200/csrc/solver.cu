@@ -137,6 +137,13 @@ int Solver::create(int nelx, int nely, int nelz, int nl_, const gputo_options *o
         st = alloc_levels<float>(Lf, true);
         if (st) return st;
         ALLOC(CXpf, elay.size());
+        if (nl >= 3) {
+            nd = NetDims{g[2].nx + 1, g[2].nz + 1, g[2].ny + 1};
+            ALLOC(net_x, 4 * nd.n());
+            ALLOC(net_y, 3 * nd.n());
+            ALLOC(dens2, nd.n());
+            ALLOC(net_s, 4);
+        }
     }
     ALLOC(AQ, (long long)nc * nc);
     ALLOC(Linv, (long long)nc * nc);
@@ -251,6 +258,7 @@ int Solver::setup(const double *CX_in, cudaStream_t st)
     launch_cholesky(nc, AQ, info, st);
     launch_tri_inverse(nc, AQ, Linv, LinvT, st);
     if (opt.precision == GPUTO_PREC_MIXED) {
+        if (dens2) launch_net_density(g[2], g[0], CX, dens2, st);
         launch_pack_cx<float>(elay, CX, CXpf, st);
         launch_cast_f32(lay[0].size(), L[0].diag, Lf[0].diag, st);
         for (int l = 1; l < nl; ++l) {
@@ -342,9 +350,112 @@ void Solver::vcycle(const double *r, double *z, const int *done, cudaStream_t st
         launch_convert<double, float>(lay[0].size(), r, Lf[0].f, done, st);
         vcycle_impl<float>(Lf, CXpf, Lf[0].f, Lf[0].u1, done, st);
         launch_convert<float, double>(lay[0].size(), Lf[0].u1, z, done, st);
+        if (net_on) learned_correction(z, done, st);
     } else {
         vcycle_impl<double>(L, CXp, r, z, done, st);
     }
+}
+
+// z += P0 P1 e2 with e2 = s D2^-1/2 net(density, D2^-1/2 R1 R0 r / s) on level 2
+// (D2 the level-2 diagonal, s the RMS of the scaled residual), after the
+// FP32 V-cycle (which leaves float(r) in Lf[0].f and no longer needs its level
+// 1/2 buffers).  Additive, so the preconditioner stays a function of r alone;
+// the flexible PCG absorbs that it is not exactly symmetric.
+void Solver::learned_correction(double *z, const int *done, cudaStream_t st)
+{
+    launch_restrict<float>(lay[1], lay[0], Lf[0].f, mask[1], Lf[1].f, done, st);
+    launch_restrict<float>(lay[2], lay[1], Lf[1].f, mask[2], Lf[2].f, done, st);
+    launch_net_features(lay[2], Lf[2].f, Lf[2].diag, dens2, net_x, nullptr, net_s, done, st);
+    note(net->forward(net_x, nd, net_y, st));
+    launch_net_output(lay[2], net_y, Lf[2].diag, net_s, mask[2], Lf[2].u0, done, st);
+    cudaMemsetAsync(Lf[1].u0, 0, sizeof(float) * lay[1].size(), st);
+    launch_prolong_add<float>(lay[1], lay[2], Lf[2].u0, mask[1], Lf[1].u0, done, st);
+    cudaMemsetAsync(Lf[0].u0, 0, sizeof(float) * lay[0].size(), st);
+    launch_prolong_add<float>(lay[0], lay[1], Lf[1].u0, mask[0], Lf[0].u0, done, st);
+    launch_add_f2d(lay[0].size(), Lf[0].u0, z, done, st);
+}
+
+void Solver::apply_level_f32(int l, const float *u, float *out, cudaStream_t st)
+{
+    if (Lf[l].yq)
+        launch_packed_sweep_ec<float>(MODE_APPLY, lay[l], Lf[l].Apk, u, nullptr, Lf[l].diag, mask[l], out, 1.f, 0.f,
+                                      Lf[l].yq, nullptr, st);
+    else
+        launch_packed_sweep<float>(MODE_APPLY, lay[l], Lf[l].Apk, u, nullptr, Lf[l].diag, mask[l], out, 1.f, 0.f,
+                                   nullptr, st);
+}
+
+// Energy loss L = y'A~y - 2 y'g~ per sample (see launch_net_energy), summed
+// over the samples; Adam with the mean gradient when lr > 0.  Uses Lf[2].u0/u1
+// as scratch: not during a solve.
+int Solver::net_train_energy(Net *n, const float *x, const float *gt, int ns, float lr, double *loss,
+                             float *grads_out, cudaStream_t st)
+{
+    if (!n || !net_x || ns < 1) return GPUTO_ERR_ARG;
+    int s = init_net_kernels();
+    if (!s) s = n->reserve(nd.n());
+    if (s) return s;
+    const long long nn = nd.n();
+    GPUTO_CUDA(cudaMemsetAsync(n->loss_acc, 0, sizeof(double), st));
+    for (int q = 0; q < ns; ++q) {
+        s = n->forward(x + (size_t)q * 4 * nn, nd, nullptr, st);
+        if (s) return s;
+        launch_net_to_padded(lay[2], n->act[4], Lf[2].diag, mask[2], Lf[2].u0, st);
+        apply_level_f32(2, Lf[2].u0, Lf[2].u1, st);
+        s = launch_net_energy(lay[2], n->act[4], Lf[2].u1, Lf[2].diag, gt + (size_t)q * 3 * nn, mask[2], n->gA,
+                              n->part, 2048, n->loss_acc, st);
+        if (!s) s = n->backward_from(nd, st);
+        if (s) return s;
+    }
+    if (grads_out)
+        GPUTO_CUDA(cudaMemcpyAsync(grads_out, n->grads, sizeof(float) * Net::num_params(), cudaMemcpyDeviceToHost, st));
+    if (lr > 0.f) {
+        s = n->adam(lr, ns, st);
+        if (s) return s;
+    } else {
+        GPUTO_CUDA(cudaMemsetAsync(n->grads, 0, sizeof(float) * Net::num_params(), st));
+    }
+    double l = 0.0;
+    GPUTO_CUDA(cudaMemcpyAsync(&l, n->loss_acc, sizeof(double), cudaMemcpyDeviceToHost, st));
+    GPUTO_CUDA(cudaStreamSynchronize(st));
+    GPUTO_CUDA(cudaGetLastError());
+    if (loss) *loss = l / ns;
+    return GPUTO_OK;
+}
+
+int Solver::attach_net(Net *n, int mode)
+{
+    if (n && (opt.precision != GPUTO_PREC_MIXED || nl < 3 || !net_x)) {
+        set_error("the learned correction needs precision GPUTO_PREC_MIXED and nl >= 3");
+        return GPUTO_ERR_ARG;
+    }
+    if (mode < 0 || mode > 2) {
+        set_error("net mode must be 0 (off), 1 (on) or 2 (auto)");
+        return GPUTO_ERR_ARG;
+    }
+    if (n) {
+        int d = 0;
+        GPUTO_CUDA(cudaGetDevice(&d));
+        if (d != n->device) {
+            set_error("the network lives on another device");
+            return GPUTO_ERR_ARG;
+        }
+        // everything the captured iteration needs exists before any capture
+        int s = init_net_kernels();
+        if (!s) s = n->reserve(nd.n());
+        if (s) return s;
+    }
+    net = n;
+    net_mode = n ? mode : 0;
+    ref_plain_nit = ref_net_nit = -1;
+    net_solves = 0;
+    const bool want = net_mode == 1;
+    if (want != net_on && graph_exec) {
+        cudaGraphExecDestroy(graph_exec);
+        graph_exec = nullptr;
+    }
+    net_on = want;
+    return GPUTO_OK;
 }
 
 void Solver::apply(const double *u, double *r, double *dot_partial, const int *done, cudaStream_t st)
@@ -383,6 +494,22 @@ int Solver::solve(const double *Fp, double *Up, double tol, int maxit, double *r
         return GPUTO_ERR_ARG;
     }
     launch_status = GPUTO_OK;
+    // auto mode: measure a plain solve and a solve with the network, keep
+    // whichever needed fewer iterations, re-measure the other every 8 solves
+    if (net && net_mode == 2) {
+        bool want;
+        if (ref_plain_nit < 0) want = false;
+        else if (ref_net_nit < 0) want = true;
+        else {
+            want = ref_net_nit < ref_plain_nit;
+            if (net_solves % 8 == 7) want = !want;
+        }
+        if (want != net_on && graph_exec) {
+            cudaGraphExecDestroy(graph_exec);
+            graph_exec = nullptr;
+        }
+        net_on = want;
+    }
     const long long nv = lay[0].size();
     const int *done = &sc->done;
     launch_pcg_init(nv, Fp, Uw, R, partial, ticket, sc, tol, maxit, opt.precision == GPUTO_PREC_MIXED,
@@ -417,6 +544,10 @@ int Solver::solve(const double *Fp, double *Up, double tol, int maxit, double *r
     *relres = h_sc->relres;
     *nit = h_sc->nit;
     last_res0 = h_sc->res0;
+    if (net && net_mode == 2) {
+        (net_on ? ref_net_nit : ref_plain_nit) = h_sc->nit;
+        ++net_solves;
+    }
     if (h_sc->status) {
         set_error("PCG breakdown: p'q <= 0 or a non-finite scalar at iteration " +
                   std::to_string(h_sc->nit));

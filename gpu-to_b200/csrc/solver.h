@@ -49,6 +49,21 @@ struct Solver {
     cudaGraphExec_t graph_exec = nullptr;
     cudaStream_t graph_stream = nullptr;
 
+    // learned coarse-grid correction (mixed precision, nl >= 3): z += P P net(R R r)
+    Net *net = nullptr;
+    int net_mode = 0;          // 0 off, 1 always, 2 auto: kept only while it lowers the iteration count
+    bool net_on = false;       // part of the captured iteration
+    int ref_plain_nit = -1, ref_net_nit = -1, net_solves = 0;
+    float *net_x = nullptr, *net_y = nullptr, *dens2 = nullptr, *net_s = nullptr;
+    NetDims nd{};
+    int attach_net(Net *n, int mode);
+    void learned_correction(double *z, const int *done, cudaStream_t st);
+    // FP32 operator of level l >= 2 (packed Galerkin): out = A_l u, padded layout
+    void apply_level_f32(int l, const float *u, float *out, cudaStream_t st);
+    // One training step of n on the energy loss: x [ns][4][n2], gt [ns][3][n2]
+    int net_train_energy(Net *n, const float *x, const float *gt, int ns, float lr, double *loss, float *grads_out,
+                         cudaStream_t st);
+
     size_t bytes = 0;
     std::vector<void *> owned;
 

@@ -46,6 +46,7 @@ _vp = ctypes.c_void_p
 _ip = ctypes.POINTER(ctypes.c_int)
 _i = ctypes.c_int
 _d = ctypes.c_double
+_fp = ctypes.POINTER(ctypes.c_float)
 
 
 class Options(ctypes.Structure):
@@ -66,6 +67,20 @@ SIGNATURES = {
     "gputo_solver_create": (_i, [ctypes.POINTER(_vp), _i, _i, _i, _i, ctypes.POINTER(Options)]),
     "gputo_solver_destroy": (None, [_vp]),
     "gputo_solver_apply_fp32_dev": (_i, [_vp, _vp, _vp, _i, _vp]),
+    "gputo_net_num_params": (ctypes.c_longlong, []),
+    "gputo_net_create": (_i, [ctypes.POINTER(_vp), ctypes.c_ulonglong]),
+    "gputo_net_destroy": (None, [_vp]),
+    "gputo_net_get_params": (_i, [_vp, _fp]),
+    "gputo_net_set_params": (_i, [_vp, _fp]),
+    "gputo_net_forward_dev": (_i, [_vp, _vp, _i, _i, _i, _vp, _vp]),
+    "gputo_net_train_step_dev": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _i, ctypes.c_float, _dp, _fp, _vp]),
+    "gputo_solver_set_net": (_i, [_vp, _vp, _i]),
+    "gputo_solver_net_state": (_i, [_vp, _ip, _ip, _ip]),
+    "gputo_solver_net_dims": (_i, [_vp, _ip, _ip, _ip]),
+    "gputo_solver_net_features_dev": (_i, [_vp, _vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_float), _vp]),
+    "gputo_solver_level2_inject_dev": (_i, [_vp, _vp, _vp, _vp]),
+    "gputo_solver_net_energy_rhs_dev": (_i, [_vp, _vp, ctypes.c_float, _vp, _vp]),
+    "gputo_solver_net_train_step_dev": (_i, [_vp, _vp, _vp, _vp, _i, ctypes.c_float, _dp, _fp, _vp]),
     "gputo_solver_device_bytes": (ctypes.c_size_t, [_vp]),
     "gputo_solver_set_problem": (_i, [_vp, _dp, _dp, _i]),
     "gputo_solver_setup_dev": (_i, [_vp, _vp, _vp]),
@@ -258,10 +273,169 @@ class Solver:
         _check(_lib.gputo_solver_apply_dev(self._h, _ptr(u), _ptr(r), _ptr_stream(stream)),
                "gputo_solver_apply_dev")
 
+    # learned coarse-grid correction -------------------------------------------------
+    def set_net(self, net, mode=1):
+        """Attach a Net (mode 1 always, 2 auto with plain-V-cycle fallback) or detach (None)."""
+        self._net = net
+        _check(_lib.gputo_solver_set_net(self._h, net._h if net is not None else None, int(mode)),
+               "gputo_solver_set_net")
+
+    def net_state(self):
+        on, a, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(_lib.gputo_solver_net_state(self._h, ctypes.byref(on), ctypes.byref(a), ctypes.byref(b)),
+               "gputo_solver_net_state")
+        return bool(on.value), a.value, b.value
+
+    def net_dims(self):
+        X, Z, Y = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(_lib.gputo_solver_net_dims(self._h, ctypes.byref(X), ctypes.byref(Z), ctypes.byref(Y)),
+               "gputo_solver_net_dims")
+        return X.value, Z.value, Y.value
+
+    def net_features(self, r, x, m=None, dsq=None, stream=None):
+        s = ctypes.c_float()
+        _check(_lib.gputo_solver_net_features_dev(self._h, _ptr(r), _ptr(x), _ptr(m), _ptr(dsq), ctypes.byref(s),
+                                                  _ptr_stream(stream)), "gputo_solver_net_features_dev")
+        return s.value
+
+    def net_energy_rhs(self, w, scale, gt, stream=None):
+        _check(_lib.gputo_solver_net_energy_rhs_dev(self._h, _ptr(w), float(scale), _ptr(gt), _ptr_stream(stream)),
+               "gputo_solver_net_energy_rhs_dev")
+
+    def net_train_step(self, net, x, gt, nsamples, lr, grads_out=None, stream=None):
+        loss = ctypes.c_double()
+        gp = grads_out.ctypes.data_as(_fp) if grads_out is not None else None
+        _check(_lib.gputo_solver_net_train_step_dev(self._h, net._h, _ptr(x), _ptr(gt), int(nsamples), float(lr),
+                                                    ctypes.byref(loss), gp, _ptr_stream(stream)),
+               "gputo_solver_net_train_step_dev")
+        return loss.value
+
+    def level2_inject(self, v, out, stream=None):
+        _check(_lib.gputo_solver_level2_inject_dev(self._h, _ptr(v), _ptr(out), _ptr_stream(stream)),
+               "gputo_solver_level2_inject_dev")
+
     def apply_fp32(self, u, r, tc_parts=0, stream=None):
         """The mixed V-cycle's FP32 fine operator (0: CUDA cores, 1-3: tensor cores)."""
         _check(_lib.gputo_solver_apply_fp32_dev(self._h, _ptr(u), _ptr(r), int(tc_parts), _ptr_stream(stream)),
                "gputo_solver_apply_fp32_dev")
+
+
+class Net:
+    """The learned coarse-grid correction network (gputo_net_*) on the current device."""
+
+    def __init__(self, seed=0):
+        self._h = ctypes.c_void_p()
+        _check(_lib.gputo_net_create(ctypes.byref(self._h), int(seed)), "gputo_net_create")
+
+    def close(self):
+        if self._h:
+            _lib.gputo_net_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def num_params() -> int:
+        return int(_lib.gputo_net_num_params())
+
+    def get_params(self) -> np.ndarray:
+        p = np.zeros(self.num_params(), dtype=np.float32)
+        _check(_lib.gputo_net_get_params(self._h, p.ctypes.data_as(_fp)), "gputo_net_get_params")
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32).reshape(-1)
+        if p.size != self.num_params():
+            raise ValueError("wrong parameter count")
+        _check(_lib.gputo_net_set_params(self._h, p.ctypes.data_as(_fp)), "gputo_net_set_params")
+
+    def forward(self, x, dims, y, stream=None):
+        _check(_lib.gputo_net_forward_dev(self._h, _ptr(x), *dims, _ptr(y), _ptr_stream(stream)),
+               "gputo_net_forward_dev")
+
+    def train_step(self, x, t, m, nsamples, dims, lr, grads_out=None, stream=None):
+        """Summed loss/gradient over nsamples stacked samples, then one Adam step (lr > 0)."""
+        loss = ctypes.c_double()
+        gp = grads_out.ctypes.data_as(_fp) if grads_out is not None else None
+        _check(_lib.gputo_net_train_step_dev(self._h, _ptr(x), _ptr(t), _ptr(m), int(nsamples), *dims,
+                                             float(lr), ctypes.byref(loss), gp, _ptr_stream(stream)),
+               "gputo_net_train_step_dev")
+        return loss.value
+
+
+def random_field_density(nelx, nely, nelz, seed=0, corr_len=8.0, lo=1e-3, hi=1.0):
+    """Seeded Gaussian random field with correlation length corr_len (elements),
+    mapped through a sigmoid to [lo, hi]; element order of the solver."""
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal((nelx, nelz, nely))
+    k = [np.fft.fftfreq(n) * 2 * np.pi for n in (nelx, nelz, nely)]
+    kk = k[0][:, None, None] ** 2 + k[1][None, :, None] ** 2 + k[2][None, None, :] ** 2
+    f = np.real(np.fft.ifftn(np.fft.fftn(w) * np.exp(-0.5 * kk * corr_len ** 2)))
+    f = (f - f.mean()) / (f.std() + 1e-30)
+    x = lo + (hi - lo) / (1.0 + np.exp(-3.0 * f))
+    return np.ascontiguousarray(x.reshape(-1))
+
+
+def harvest_net_samples(solver, F, iters=40):
+    """Training samples of the learned correction from one plain PCG solve
+    with the solver's own V-cycle (network detached): at iteration k the input
+    x_k is built from the residual r_k and the loss data from the residual the
+    V-cycle leaves, g_k = D^-1/2 P'P'(r_k - A V(r_k)) / s_k.  F: device float64
+    right-hand side (dense layout).  Returns [(x_k, g_k)]."""
+    import torch
+
+    X, Z, Y = solver.net_dims()
+    n = X * Z * Y
+    dev = F.device
+    u = torch.zeros_like(F)
+    r = F.clone()
+    z = torch.empty_like(F)
+    q = torch.empty_like(F)
+    solver.vcycle(r, z)
+    p = z.clone()
+    rz = torch.dot(r, z)
+    out = []
+    for _ in range(iters):
+        x = torch.empty(4 * n, dtype=torch.float32, device=dev)
+        s = solver.net_features(r, x)
+        solver.apply(z, q)
+        g = torch.empty(3 * n, dtype=torch.float32, device=dev)
+        solver.net_energy_rhs(r - q, s, g)
+        out.append((x, g))
+        solver.apply(p, q)
+        alpha = rz / torch.dot(p, q)
+        u += alpha * p
+        r -= alpha * q
+        if float(torch.linalg.norm(r)) <= 1e-10 * float(torch.linalg.norm(F)):
+            break
+        solver.vcycle(r, z)
+        rz_new = torch.dot(r, z)
+        p = z + (rz_new / rz) * p
+        rz = rz_new
+    return out
+
+
+def train_net(solver, net, samples, epochs=20, lr=1e-3, batch=8, seed=0):
+    """Adam on the energy loss of samples harvested with this solver's current
+    hierarchy; returns the mean loss of every epoch (0 = the plain V-cycle)."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    X = torch.stack([s[0] for s in samples])
+    G = torch.stack([s[1] for s in samples])
+    hist = []
+    for _ in range(epochs):
+        order = rng.permutation(len(samples))
+        tot = 0.0
+        for b0 in range(0, len(order), batch):
+            idx = torch.as_tensor(order[b0:b0 + batch], device=X.device)
+            tot += solver.net_train_step(net, X[idx].contiguous(), G[idx].contiguous(), len(idx), lr) * len(idx)
+        hist.append(tot / len(samples))
+    return hist
 
 
 def _ptr_stream(stream):

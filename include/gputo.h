@@ -179,6 +179,71 @@ int gputo_solver_time_kernel(gputo_solver *s, int which, int reps, double *ms_pe
                              void *stream);
 
 /* ---------------------------------------------------------------------- */
+/* Learned coarse-grid correction (no reference counterpart)                */
+/* ---------------------------------------------------------------------- */
+
+/* A small 3D convolutional network on the level-2 node grid: three 3x3x3
+ * convolutions 4 -> 16 -> 32 -> 64 with ReLU and a 1x1x1 convolution 64 -> 3;
+ * FP32 master weights used rounded to BF16, FP32 activations.  Tensors are
+ * channels-first [C][X][Z][Y] with Y fastest (the solver's node order); the
+ * input channels are a density feature and the residual restricted twice in
+ * Jacobi-scaled units, the output the level-2 error estimate in those units.
+ * Flat parameter layout: per layer w[co][ci][tap] then b[co], tap = 9 (dx+1)
+ * + 3 (dz+1) + (dy+1). */
+typedef struct gputo_net gputo_net;
+long long gputo_net_num_params(void);
+int gputo_net_create(gputo_net **out, unsigned long long seed);
+void gputo_net_destroy(gputo_net *net);
+int gputo_net_get_params(const gputo_net *net, float *host);
+/* Replaces the parameters and resets the optimizer state. */
+int gputo_net_set_params(gputo_net *net, const float *host);
+/* y[3][n] = net(x[4][n]) on device buffers, n = X Z Y. */
+int gputo_net_forward_dev(gputo_net *net, const float *x, int X, int Z, int Y, float *y, void *stream);
+/* One training step on nsamples samples stored back to back (x: [4][n] each,
+ * target t and loss mask m: [3][n] each): the masked mean-square losses and
+ * their gradients are summed; if lr > 0 one Adam step with the mean gradient
+ * follows.  loss receives the mean loss, grads_out (host, optional) the summed
+ * gradient before the step. */
+int gputo_net_train_step_dev(gputo_net *net, const float *x, const float *t, const float *m, int nsamples,
+                             int X, int Z, int Y, float lr, double *loss, float *grads_out, void *stream);
+
+/* Attach a network to a solver (precision GPUTO_PREC_MIXED, nl >= 3), or
+ * detach it (net = NULL).  mode 1 adds z += P P e2 with e2 = net(R R r) after
+ * every V-cycle of the flexible PCG; mode 2 (auto) measures solves with and
+ * without it and keeps the plain V-cycle whenever the network does not lower
+ * the iteration count, re-measuring every 8 solves.  The solution is
+ * unchanged: CG still converges to the same tolerance. */
+int gputo_solver_set_net(gputo_solver *s, gputo_net *net, int mode);
+/* Whether the correction is on for the next solve, and the last measured
+ * iteration counts without / with it (-1 if not measured yet). */
+int gputo_solver_net_state(const gputo_solver *s, int *on, int *plain_nit, int *net_nit);
+/* The network's grid for this solver: level-2 nodes (nelx/4+1, nelz/4+1, nely/4+1). */
+int gputo_solver_net_dims(const gputo_solver *s, int *X, int *Z, int *Y);
+/* Network input [4][n] for a fine residual r (ndof doubles, device), as the
+ * preconditioner builds it: the residual is restricted twice, scaled to
+ * D^-1/2 r with the level-2 diagonal D and divided by its RMS s.  m
+ * (optional, [3][n]) receives the loss mask (1 on free dofs), dsq (optional,
+ * [3][n]) sqrt(D), scale s: a level-2 error e enters the loss as
+ * e sqrt(D) / s.  Uses the solver's work buffers: not during a solve. */
+int gputo_solver_net_features_dev(gputo_solver *s, const double *r, float *x, float *m, float *dsq,
+                                  float *scale, void *stream);
+/* Energy-loss data for a post-V-cycle residual w = r - A V(r) (fine dense
+ * doubles, device): gt [3][n] = D^-1/2 P'P' w / scale at the level-2 nodes,
+ * with scale the value gputo_solver_net_features_dev returned for r. */
+int gputo_solver_net_energy_rhs_dev(gputo_solver *s, const double *w, float scale, float *gt, void *stream);
+/* One training step on the energy of the error left after the V-cycle and
+ * the correction: per sample L = y'A~y - 2 y'g~ (A~ = D^-1/2 A2 D^-1/2 with the
+ * solver's Galerkin level-2 operator A2, y the network output for x, g~ = gt),
+ * the optimum being the exact two-grid correction and L = 0 the plain V-cycle;
+ * summed over nsamples stacked samples (grads_out, host, optional: the summed
+ * gradient), then one Adam step (lr > 0).  The solver's hierarchy (setup)
+ * must be the one the samples came from. */
+int gputo_solver_net_train_step_dev(gputo_solver *s, gputo_net *net, const float *x, const float *gt,
+                                    int nsamples, float lr, double *loss, float *grads_out, void *stream);
+/* Values of a fine dense vector v at the level-2 nodes, [3][n] floats. */
+int gputo_solver_level2_inject_dev(gputo_solver *s, const double *v, float *out, void *stream);
+
+/* ---------------------------------------------------------------------- */
 /* Design-loop steps that the MATLAB drivers run around the solve          */
 /* ---------------------------------------------------------------------- */
 
