@@ -482,8 +482,7 @@ void Solver::iteration(cudaStream_t st)
     }
 }
 
-int Solver::solve(const double *Fp, double *Up, double tol, int maxit, double *relres, int *nit,
-                  cudaStream_t st, FILE *log)
+int Solver::solve_begin(const double *Fp, double tol, int maxit, cudaStream_t st)
 {
     if (!ready) {
         set_error("solver setup has not succeeded");
@@ -512,33 +511,27 @@ int Solver::solve(const double *Fp, double *Up, double tol, int maxit, double *r
     }
     const long long nv = lay[0].size();
     const int *done = &sc->done;
-    launch_pcg_init(nv, Fp, Uw, R, partial, ticket, sc, tol, maxit, opt.precision == GPUTO_PREC_MIXED,
-                    st);
+    launch_pcg_init(nv, Fp, Uw, R, partial, ticket, sc, tol, maxit, opt.precision == GPUTO_PREC_MIXED, st);
     vcycle(R, P, done, st);
     launch_dot(nv, R, P, partial, ticket, sc, 1 /*DOT_RHO0*/, done, st);
     if (Zold) launch_copy(nv, P, Zold, done, st);
-    if (launch_status) return launch_status;
+    return launch_status;
+}
 
-    const bool graph = opt.use_graph != 0;
-    int it = 0;
-    for (;;) {
-        GPUTO_CUDA(cudaMemcpyAsync(h_sc, sc, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
-        GPUTO_CUDA(cudaStreamSynchronize(st));
-        if (log && it > 0) std::fprintf(log, "CG It %d  %12.6g\n", h_sc->iter - 1, h_sc->relres);
-        if (h_sc->done || it >= maxit) break;
-        const int batch = std::min(opt.check_every, maxit - it);
-        if (graph) {
-            int gs = run_graph(batch, st);
-            if (gs) return gs;
-        } else {
-            for (int b = 0; b < batch; ++b) iteration(st);
-            if (launch_status) return launch_status;
-        }
-        it += batch;
-    }
+// Device scalars -> host (h_sc); true once the solve has converged or failed.
+int Solver::solve_poll(cudaStream_t st, bool *finished)
+{
+    GPUTO_CUDA(cudaMemcpyAsync(h_sc, sc, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+    GPUTO_CUDA(cudaStreamSynchronize(st));
+    *finished = h_sc->done != 0;
+    return GPUTO_OK;
+}
+
+int Solver::solve_end(double *Up, double *relres, int *nit, cudaStream_t st)
+{
     GPUTO_CUDA(cudaGetLastError());
     if (Up != Uw)
-        GPUTO_CUDA(cudaMemcpyAsync(Up, Uw, sizeof(double) * nv, cudaMemcpyDeviceToDevice, st));
+        GPUTO_CUDA(cudaMemcpyAsync(Up, Uw, sizeof(double) * lay[0].size(), cudaMemcpyDeviceToDevice, st));
     int fe = check_error_flags(st);
     if (fe) return fe;
     *relres = h_sc->relres;
@@ -549,9 +542,56 @@ int Solver::solve(const double *Fp, double *Up, double tol, int maxit, double *r
         ++net_solves;
     }
     if (h_sc->status) {
-        set_error("PCG breakdown: p'q <= 0 or a non-finite scalar at iteration " +
-                  std::to_string(h_sc->nit));
+        set_error("PCG breakdown: p'q <= 0 or a non-finite scalar at iteration " + std::to_string(h_sc->nit));
         return h_sc->status;
+    }
+    return GPUTO_OK;
+}
+
+int Solver::solve(const double *Fp, double *Up, double tol, int maxit, double *relres, int *nit,
+                  cudaStream_t st, FILE *log)
+{
+    int s = solve_begin(Fp, tol, maxit, st);
+    if (s) return s;
+    const bool graph = opt.use_graph != 0;
+    int it = 0;
+    for (;;) {
+        bool fin = false;
+        s = solve_poll(st, &fin);
+        if (s) return s;
+        if (log && it > 0) std::fprintf(log, "CG It %d  %12.6g\n", h_sc->iter - 1, h_sc->relres);
+        if (fin || it >= maxit) break;
+        const int batch = std::min(opt.check_every, maxit - it);
+        if (graph) {
+            int gs = run_graph(batch, st);
+            if (gs) return gs;
+        } else {
+            for (int b = 0; b < batch; ++b) iteration(st);
+            if (launch_status) return launch_status;
+        }
+        it += batch;
+    }
+    return solve_end(Up, relres, nit, st);
+}
+
+// Options that change neither the hierarchy nor its buffers.
+int Solver::set_tunables(const gputo_options &o)
+{
+    if (o.nswp < 0 || o.check_every < 1 || !(o.omega > 0) || o.tc_parts < 0 || o.tc_parts > 2 || o.tc_xchunk < 0 ||
+        (o.tc_parts > 0 && opt.precision != GPUTO_PREC_MIXED)) {
+        set_error("invalid solver options");
+        return GPUTO_ERR_ARG;
+    }
+    opt.nswp = o.nswp;
+    opt.omega = o.omega;
+    opt.prerelax = o.prerelax;
+    opt.check_every = o.check_every;
+    opt.use_graph = o.use_graph;
+    opt.tc_parts = o.tc_parts;
+    opt.tc_xchunk = o.tc_xchunk;
+    if (graph_exec) {
+        cudaGraphExecDestroy(graph_exec);
+        graph_exec = nullptr;
     }
     return GPUTO_OK;
 }

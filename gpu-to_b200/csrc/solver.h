@@ -75,6 +75,14 @@ struct Solver {
     // F, U in the padded layout (solver-owned or compatible buffers).
     int solve(const double *Fp, double *Up, double tol, int maxit, double *relres, int *nit,
               cudaStream_t st, FILE *log);
+    // The same solve in phases, for drivers that interleave several solvers:
+    // begin (initial residual and V-cycle), then iteration() steps, poll
+    // (device scalars to h_sc), end (result, status).
+    int solve_begin(const double *Fp, double tol, int maxit, cudaStream_t st);
+    int solve_poll(cudaStream_t st, bool *finished);
+    int solve_end(double *Up, double *relres, int *nit, cudaStream_t st);
+    void iteration(cudaStream_t st);
+    int set_tunables(const gputo_options &o);
     // Padded-layout preconditioner and operator.
     void vcycle(const double *r, double *z, const int *done, cudaStream_t st);
     void apply(const double *u, double *r, double *dot_partial, const int *done, cudaStream_t st);
@@ -90,7 +98,6 @@ struct Solver {
     template <typename T>
     void vcycle_impl(LevelBuf<T> *Lv, const T *CXl, const T *r0, T *z0, const int *done,
                      cudaStream_t st);
-    void iteration(cudaStream_t st);
     int run_graph(int batch, cudaStream_t st);
     void note(int s)
     {

@@ -67,6 +67,11 @@ SIGNATURES = {
     "gputo_solver_create": (_i, [ctypes.POINTER(_vp), _i, _i, _i, _i, ctypes.POINTER(Options)]),
     "gputo_solver_destroy": (None, [_vp]),
     "gputo_solver_apply_fp32_dev": (_i, [_vp, _vp, _vp, _i, _vp]),
+    "gputo_batch_create": (_i, [ctypes.POINTER(_vp), ctypes.POINTER(_vp), _i]),
+    "gputo_batch_destroy": (None, [_vp]),
+    "gputo_batch_solve_dev": (_i, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp), _d, _i, _i, _dp, _ip]),
+    "gputo_solver_set_options": (_i, [_vp, ctypes.POINTER(Options)]),
+    "gputo_autotune_dev": (_i, [_vp, _vp, _vp, _d, _i, ctypes.POINTER(Options), _dp, _dp, _ip, _i, _ip]),
     "gputo_net_num_params": (ctypes.c_longlong, []),
     "gputo_net_create": (_i, [ctypes.POINTER(_vp), ctypes.c_ulonglong]),
     "gputo_net_destroy": (None, [_vp]),
@@ -274,6 +279,11 @@ class Solver:
                "gputo_solver_apply_dev")
 
     # learned coarse-grid correction -------------------------------------------------
+    def set_options(self, options):
+        """Change the options that need no new hierarchy (see gputo_solver_set_options)."""
+        _check(_lib.gputo_solver_set_options(self._h, ctypes.byref(options)), "gputo_solver_set_options")
+        self.options = options
+
     def set_net(self, net, mode=1):
         """Attach a Net (mode 1 always, 2 auto with plain-V-cycle fallback) or detach (None)."""
         self._net = net
@@ -318,6 +328,52 @@ class Solver:
         """The mixed V-cycle's FP32 fine operator (0: CUDA cores, 1-3: tensor cores)."""
         _check(_lib.gputo_solver_apply_fp32_dev(self._h, _ptr(u), _ptr(r), int(tc_parts), _ptr_stream(stream)),
                "gputo_solver_apply_fp32_dev")
+
+
+class Batch:
+    """Several Solvers solved together, one CUDA graph launch per CG step (gputo_batch_*)."""
+
+    def __init__(self, solvers):
+        self.solvers = list(solvers)
+        self._h = ctypes.c_void_p()
+        arr = (_vp * len(self.solvers))(*[s._h.value for s in self.solvers])
+        _check(_lib.gputo_batch_create(ctypes.byref(self._h), arr, len(self.solvers)), "gputo_batch_create")
+
+    def close(self):
+        if self._h:
+            _lib.gputo_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def solve(self, Fs, Us, tol, maxit, check_every=8):
+        n = len(self.solvers)
+        fa = (_vp * n)(*[_ptr(f) for f in Fs])
+        ua = (_vp * n)(*[_ptr(u) for u in Us])
+        rr = (_d * n)()
+        it = (_i * n)()
+        _check(_lib.gputo_batch_solve_dev(self._h, fa, ua, float(tol), int(maxit), int(check_every), rr, it),
+               "gputo_batch_solve_dev")
+        return list(rr), list(it)
+
+
+def autotune(solver, F, U, tol, maxit):
+    """Time complete solves over the tunable options and apply the fastest;
+    returns (best Options, best ms, [(ms, nit)] per candidate)."""
+    best = Options()
+    bms = ctypes.c_double()
+    cap = 64
+    tms = (_d * cap)()
+    tnit = (_i * cap)()
+    nc = ctypes.c_int()
+    _check(_lib.gputo_autotune_dev(solver._h, _ptr(F), _ptr(U), float(tol), int(maxit), ctypes.byref(best),
+                                   ctypes.byref(bms), tms, tnit, cap, ctypes.byref(nc)), "gputo_autotune_dev")
+    solver.options = best
+    return best, bms.value, [(tms[i], tnit[i]) for i in range(min(nc.value, cap))]
 
 
 class Net:

@@ -179,6 +179,40 @@ int gputo_solver_time_kernel(gputo_solver *s, int which, int reps, double *ms_pe
                              void *stream);
 
 /* ---------------------------------------------------------------------- */
+/* Batched solves and the option autotuner (no reference counterpart)       */
+/* ---------------------------------------------------------------------- */
+
+/* Several solvers (any grid sizes, same device) solved together: one PCG
+ * iteration of every member is one branch of a single CUDA graph, so each CG
+ * step of the batch is one graph launch.  The solvers stay owned by the
+ * caller and must outlive the batch. */
+typedef struct gputo_batch gputo_batch;
+int gputo_batch_create(gputo_batch **out, gputo_solver **solvers, int n);
+void gputo_batch_destroy(gputo_batch *b);
+/* F[i], U[i]: device vectors (dense layout) of member i; relres[i], nit[i] as
+ * gputo_solver_solve_dev returns them.  Results equal the members' own
+ * solves; the host checks convergence every check_every CG steps. */
+int gputo_batch_solve_dev(gputo_batch *b, const double *const *F, double *const *U, double tol, int maxit,
+                          int check_every, double *relres, int *nit);
+
+/* Change the options that need no new hierarchy (nswp, omega, prerelax,
+ * check_every, use_graph, tc_parts, tc_xchunk) on an existing solver, e.g. to
+ * reuse what gputo_autotune_dev chose for another solver of the same shape. */
+int gputo_solver_set_options(gputo_solver *s, const gputo_options *opt);
+
+/* Choose the options that change neither the hierarchy nor its buffers
+ * (Jacobi sweeps per smoothing step; for GPUTO_PREC_MIXED also the CUDA-core
+ * or tensor-core fine smoother and its x-chunk; host check interval) by
+ * timing complete solves of this solver's problem (F, U: device vectors as
+ * for gputo_solver_solve_dev) with CUDA events.  The fastest candidate that
+ * converges is applied to the solver and returned in best (best_ms: its solve
+ * time).  table_ms / table_nit (optional, table_cap entries) receive every
+ * candidate's time and iteration count (-1: did not converge), ncand the
+ * number of candidates. */
+int gputo_autotune_dev(gputo_solver *s, const double *F, double *U, double tol, int maxit, gputo_options *best,
+                       double *best_ms, double *table_ms, int *table_nit, int table_cap, int *ncand);
+
+/* ---------------------------------------------------------------------- */
 /* Learned coarse-grid correction (no reference counterpart)                */
 /* ---------------------------------------------------------------------- */
 
