@@ -5,13 +5,14 @@
 
 Outputs (git-ignored, shipped with the tree):
   gpu-to_b200/lib/libgputo.so       the product: kernels + solver + C ABI
-  gpu-to_b200/lib/libgputo_mex.so   the MEX gateway (mexFunction) linked
+  gpu-to_b200/lib/libgputo_mex.so   the MEX gateway of mgcg1 (mexFunction) linked
                                     against libgputo.so.  It is compiled
                                     against MATLAB's mex.h when MATLAB_ROOT is
                                     set, else against the project's stand-in
                                     declarations (oracle/shim/mex.h); the mx*
                                     symbols stay undefined and resolve from
                                     MATLAB's libmx (or the stand-in) at load.
+  gpu-to_b200/lib/libgputo_mex9.so  the same for the MEX mgcg9 (18 arguments)
 """
 from __future__ import annotations
 
@@ -69,11 +70,12 @@ def build(force: bool = False, verbose: bool = False) -> str:
     # MEX gateway
     mex_inc = os.path.join(os.environ["MATLAB_ROOT"], "extern", "include") if os.environ.get(
         "MATLAB_ROOT") else os.path.join(ROOT, "oracle", "shim")
-    gw_src = os.path.join(CSRC, "mex_gateway.cpp")
-    gw = os.path.join(LIB, "libgputo_mex.so")
-    if force or _newer(gw, [gw_src, so]):
-        _run(["g++", "-O2", "-fPIC", "-shared", f"-I{mex_inc}", f"-I{os.path.join(ROOT, 'include')}",
-              gw_src, "-o", gw, f"-L{LIB}", "-lgputo", f"-Wl,-rpath,{LIB}", "-Wl,-rpath,$ORIGIN"])
+    for src, out in (("mex_gateway.cpp", "libgputo_mex.so"), ("mex_gateway9.cpp", "libgputo_mex9.so")):
+        gw_src = os.path.join(CSRC, src)
+        gw = os.path.join(LIB, out)
+        if force or _newer(gw, [gw_src, so]):
+            _run(["g++", "-O2", "-fPIC", "-shared", f"-I{mex_inc}", f"-I{os.path.join(ROOT, 'include')}",
+                  gw_src, "-o", gw, f"-L{LIB}", "-lgputo", f"-Wl,-rpath,{LIB}", "-Wl,-rpath,$ORIGIN"])
     return so
 
 

@@ -116,6 +116,7 @@ void gputo_default_options(gputo_options *o)
     o->max_coarse_dofs = 12000;
     o->tc_parts = 0;
     o->tc_xchunk = 0;
+    o->coarse = GPUTO_COARSE_GALERKIN;
 }
 
 int gputo_solver_create(gputo_solver **out, int nelx, int nely, int nelz, int nl,
@@ -472,7 +473,9 @@ int gputo_solver_time_kernel(gputo_solver *h, int which, int reps, double *ms, v
 // ---------------------------------------------------------------------------
 
 namespace {
-using Key = std::tuple<int, int, int, int, int, int, int, double, double, double, int, int>;
+// every option is part of the key: a call must never reuse a solver built
+// with other options
+using Key = std::tuple<int, int, int, int, int, int, int, double, double, double, int, int, int, int, int, int>;
 std::mutex g_cache_mu;
 std::map<Key, std::unique_ptr<gputo_solver>> g_cache;
 std::vector<Key> g_cache_order;
@@ -482,7 +485,7 @@ gputo_solver *cached_solver(int nelx, int nely, int nelz, int nl, const gputo_op
     int dev = 0;
     cudaGetDevice(&dev);
     Key k{dev, nelx, nely, nelz, nl, o.precision, o.nswp, o.omega, o.prerelax, o.nu,
-          o.check_every, o.use_graph};
+          o.check_every, o.use_graph, o.max_coarse_dofs, o.tc_parts, o.tc_xchunk, o.coarse};
     auto it = g_cache.find(k);
     if (it != g_cache.end()) return it->second.get();
     // keep at most two shapes resident
@@ -506,10 +509,53 @@ gputo_solver *cached_solver(int nelx, int nely, int nelz, int nl, const gputo_op
 }
 }  // namespace
 
+// One MEX-style solve on host buffers with the cached solver of these
+// options; the log file (printLev >= 1) gets per-iteration lines from
+// printLev >= cg_lines on.
+static int mex_solve(const char *log_name, int cg_lines, const double *Ke0, const double *F, double *U,
+                     const double *CX, const double *fixed1b, int nfd, int nelx, int nely, int nelz, int nl,
+                     double tol, int maxit, int printLev, const gputo_options &o, double *relres, int *nit);
+
 int gputo_mgcg1_ex(const double *Ke0, const double *F, double *U, const double *CX,
                    const double *fixed1b, int nfd, int nelx, int nely, int nelz, int nl,
                    double tol, int maxit, int printLev, const gputo_options *opt, double *relres,
                    int *nit)
+{
+    gputo_options o;
+    if (opt) o = *opt;
+    else gputo_default_options(&o);
+    return mex_solve("mgcg1.log", 2, Ke0, F, U, CX, fixed1b, nfd, nelx, nely, nelz, nl, tol, maxit, printLev, o,
+                     relres, nit);
+}
+
+int gputo_mgcg9(const double *Ae, const double *F, double *U, const double *CX, const double *fixed1b, int nfd,
+                int nelx, int nely, int nelz, int nl, double tol, int maxit, int nswp, int printLev, double nu,
+                double hx, double hy, double hz, double *relres, int *nit)
+{
+    (void)nu;   // read by the reference (mgcg9.cu:167-170) and not used on its solve path
+    (void)hx;
+    (void)hy;
+    (void)hz;
+    if (nswp < 0 || nl < 2) {
+        if (relres) *relres = 0.0;
+        if (nit) *nit = -1;
+        gputo::set_error("mgcg9 needs nswp >= 0 and nl >= 2");
+        return GPUTO_ERR_ARG;
+    }
+    gputo_options o;
+    gputo_default_options(&o);
+    o.coarse = GPUTO_COARSE_REDISCRETIZED;
+    o.nswp = nswp;
+    o.omega = 0.33;            // mgcg9.cu:929-935 Jacobc: U = 0.67 U + 0.33 (R + D U) / D
+    o.prerelax = 0.7;          // mgcg9.cu:920-927 preRelc
+    o.max_coarse_dofs = 19999; // mgcg9.cu:74,400 maxDofs0: direct coarsest solve below 20000 dofs
+    return mex_solve("mgcg9.log", 3, Ae, F, U, CX, fixed1b, nfd, nelx, nely, nelz, nl, tol, maxit, printLev, o,
+                     relres, nit);
+}
+
+static int mex_solve(const char *log_name, int cg_lines, const double *Ke0, const double *F, double *U,
+                     const double *CX, const double *fixed1b, int nfd, int nelx, int nely, int nelz, int nl,
+                     double tol, int maxit, int printLev, const gputo_options &o, double *relres, int *nit)
 {
     if (relres) *relres = 0.0;
     if (nit) *nit = -1;
@@ -517,9 +563,6 @@ int gputo_mgcg1_ex(const double *Ke0, const double *F, double *U, const double *
         gputo::set_error("null argument");
         return GPUTO_ERR_ARG;
     }
-    gputo_options o;
-    if (opt) o = *opt;
-    else gputo_default_options(&o);
     auto t0 = std::chrono::steady_clock::now();
     std::lock_guard<std::mutex> lock(g_cache_mu);
     int st = gputo::check_device();
@@ -529,7 +572,7 @@ int gputo_mgcg1_ex(const double *Ke0, const double *F, double *U, const double *
     Solver &s = h->s;
     cudaStream_t strm = s.own_stream;
     FILE *log = nullptr;
-    if (printLev >= 1) log = std::fopen("mgcg1.log", "w");
+    if (printLev >= 1) log = std::fopen(log_name, "w");
     st = s.set_problem(Ke0, fixed1b, nfd, strm);
     if (st) {
         if (log) std::fclose(log);
@@ -540,7 +583,7 @@ int gputo_mgcg1_ex(const double *Ke0, const double *F, double *U, const double *
     gputo::launch_pack(s.lay[0], s.Dn, s.Fw, 0, strm);
     GPUTO_CUDA(cudaMemcpyAsync(s.CX, CX, sizeof(double) * ne, cudaMemcpyHostToDevice, strm));
     st = s.setup(s.CX, strm);
-    if (!st) st = s.solve(s.Fw, s.Uw, tol, maxit, relres, nit, strm, printLev >= 2 ? log : nullptr);
+    if (!st) st = s.solve(s.Fw, s.Uw, tol, maxit, relres, nit, strm, printLev >= cg_lines ? log : nullptr);
     if (!st || st == GPUTO_ERR_BREAKDOWN) {
         // solver frame -> MATLAB frame: y components negated (mgcg1.cu:282-283)
         gputo::launch_unpack(s.lay[0], s.Uw, s.Dn, 1, strm);

@@ -191,6 +191,10 @@ void launch_build_galerkin(const Grid &gc, const double *Afine, double *Apk, cud
 void launch_coarsest_penalty(const Grid &g, const uint8_t *mask, double *Apk, cudaStream_t st);
 void launch_assemble_dense(const Grid &g, const double *Apk, double *AQ, cudaStream_t st);
 void launch_dense_fine(const Grid &g, const double *CX, double *Apk_tmp, cudaStream_t st);
+// re-discretised hierarchy (mgcg9): coarse CX = 2 mean(children); fixed dofs
+// of the dense coarsest matrix as zero rows/columns with 1e10 on the diagonal
+void launch_coarse_cx(const Grid &gc, const double *CXf, double *CXc, cudaStream_t st);
+void launch_dense_fix(const Grid &g, const uint8_t *mask, double *AQ, cudaStream_t st);
 // Cholesky + explicit inverse of the lower factor; info[0] = 0 or bad pivot (1-based).
 void launch_cholesky(int n, double *A, int *info, cudaStream_t st);
 void launch_tri_inverse(int n, const double *L, double *Linv, double *LinvT, cudaStream_t st);

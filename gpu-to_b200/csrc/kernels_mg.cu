@@ -703,6 +703,52 @@ void launch_assemble_dense(const Grid &g, const double *Apk, double *AQ, cudaStr
     count_launches(1);
 }
 
+// Re-discretised coarse levels (Homogenization/QNC/mgcg9.cu:753-781 formCXc):
+// a coarse element's scale is twice the mean of its eight children, the 2
+// being Ke(2h) = 2 Ke(h) for the unit-modulus hex8 (the reference's choice
+// among the mean forms it tried).
+__global__ void coarse_cx_kernel(Grid gc, const double *__restrict__ CXf, double *__restrict__ CXc)
+{
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= gc.nel()) return;
+    const int j = (int)(e % gc.ny);
+    const long long r = e / gc.ny;
+    const int k = (int)(r % gc.nz), i = (int)(r / gc.nz);
+    const Grid gf{2 * gc.nx, 2 * gc.ny, 2 * gc.nz};
+    double s = 0.0;
+    for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b)
+            for (int c = 0; c < 2; ++c) s += CXf[gf.elem(2 * i + a, 2 * j + c, 2 * k + b)];
+    CXc[e] = 2.0 * (s / 8.0);
+}
+
+void launch_coarse_cx(const Grid &gc, const double *CXf, double *CXc, cudaStream_t st)
+{
+    const int bs = 256;
+    coarse_cx_kernel<<<(unsigned)((gc.nel() + bs - 1) / bs), bs, 0, st>>>(gc, CXf, CXc);
+    count_launches(1);
+}
+
+// Fixed dofs of a dense coarsest matrix, the mgcg9 way (mgcg9.cu:1005-1028
+// CorrCsAQc): their rows and columns become zero and the diagonal 1e10.
+__global__ void dense_fix_kernel(Grid g, const uint8_t *__restrict__ mask, double *__restrict__ AQ)
+{
+    const long long N = g.ndof();
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= N * N) return;
+    const long long r = idx / N, c = idx - r * N;
+    const bool fr = (mask[r / 3] >> (r % 3)) & 1u, fc = (mask[c / 3] >> (c % 3)) & 1u;
+    if (fr || fc) AQ[idx] = (r == c) ? 1e10 : 0.0;
+}
+
+void launch_dense_fix(const Grid &g, const uint8_t *mask, double *AQ, cudaStream_t st)
+{
+    const long long n2 = g.ndof() * g.ndof();
+    const int bs = 256;
+    dense_fix_kernel<<<(unsigned)((n2 + bs - 1) / bs), bs, 0, st>>>(g, mask, AQ);
+    count_launches(1);
+}
+
 // Blocked left-looking Cholesky A = L L^T of the dense coarsest matrix, in
 // place in the lower triangle, 32-column panels (textbook algorithm; the
 // reference launches one kernel per row, mgcg1.cu:2099-2142):

@@ -73,7 +73,13 @@ int Solver::alloc_levels(LevelBuf<T> *Lv, bool with_matrices)
         ALLOC(b.diag, nv);
         ALLOC(b.u1, nv);
         ALLOC(b.f, nv);
-        // level 1 is applied matrix-free unless it is the coarsest level
+        // level 1 is applied matrix-free unless it is the coarsest level; the
+        // re-discretised hierarchy stores element matrices for the coarsest only
+        if (redisc()) {
+            if (l > 0 && l == nl - 1 && with_matrices) ALLOC(b.Apk, 300 * g[l].nel());
+            b.mask = mask[l];
+            continue;
+        }
         if (l > 0 && with_matrices && !(l == 1 && quad_level1())) ALLOC(b.Apk, 300 * g[l].nel());
         if (l >= 1 && (l == 1 ? quad_level1() : g[l].nel() >= kElementCentricMinElems))
             ALLOC(b.yq, 24 * g[l].nel());
@@ -96,7 +102,7 @@ int Solver::create(int nelx, int nely, int nelz, int nl_, const gputo_options *o
         return GPUTO_ERR_ARG;
     }
     if (opt.nswp < 0 || opt.check_every < 1 || !(opt.omega > 0) || opt.tc_parts < 0 || opt.tc_parts > 2 ||
-        opt.tc_xchunk < 0 ||
+        opt.tc_xchunk < 0 || (opt.coarse != GPUTO_COARSE_GALERKIN && opt.coarse != GPUTO_COARSE_REDISCRETIZED) ||
         (opt.precision != GPUTO_PREC_FP64 && opt.precision != GPUTO_PREC_MIXED)) {
         set_error("invalid solver options");
         return GPUTO_ERR_ARG;
@@ -131,6 +137,15 @@ int Solver::create(int nelx, int nely, int nelz, int nl_, const gputo_options *o
     ALLOC(Fw, nv);
     ALLOC(Dn, g[0].ndof());
     if (opt.precision == GPUTO_PREC_MIXED) ALLOC(Zold, nv);
+    if (redisc())
+        for (int l = 1; l < nl; ++l) {
+            elayr[l] = ELay::of(g[l]);
+            ALLOC(CXr[l], g[l].nel());
+            if (l < nl - 1) {
+                ALLOC(CXrp[l], elayr[l].size());
+                if (opt.precision == GPUTO_PREC_MIXED) ALLOC(CXrpf[l], elayr[l].size());
+            }
+        }
     int st = alloc_levels<double>(L, true);
     if (st) return st;
     if (opt.precision == GPUTO_PREC_MIXED) {
@@ -238,7 +253,13 @@ int Solver::setup(const double *CX_in, cudaStream_t st)
         GPUTO_CUDA(cudaMemcpyAsync(CX, CX_in, sizeof(double) * ne, cudaMemcpyDeviceToDevice, st));
     launch_pack_cx<double>(elay, CX, CXp, st);
     launch_diag_fine(lay[0], CX, L[0].diag, st);
-    for (int l = 1; l < nl; ++l) {
+    for (int l = 1; l < nl && redisc(); ++l) {
+        launch_coarse_cx(g[l], l == 1 ? CX : CXr[l - 1], CXr[l], st);
+        launch_diag_fine(lay[l], CXr[l], L[l].diag, st);
+        if (l < nl - 1) launch_pack_cx<double>(elayr[l], CXr[l], CXrp[l], st);
+        else launch_dense_fine(g[l], CXr[l], L[l].Apk, st);
+    }
+    for (int l = 1; l < nl && !redisc(); ++l) {
         if (l == 1 && quad_level1()) {
             launch_diag_quad(lay[1], CX, L[1].diag, st);
             continue;
@@ -252,14 +273,16 @@ int Solver::setup(const double *CX_in, cudaStream_t st)
     const double *Acoarse = (nl > 1) ? L[nl - 1].Apk : Apk0;
     if (nl == 1) {
         launch_dense_fine(g[0], CX, Apk0, st);
-        launch_coarsest_penalty(g[0], mask[0], Apk0, st);
+        if (!redisc()) launch_coarsest_penalty(g[0], mask[0], Apk0, st);
     }
     launch_assemble_dense(g[nl - 1], Acoarse, AQ, st);
+    if (redisc()) launch_dense_fix(g[nl - 1], mask[nl - 1], AQ, st);
     launch_cholesky(nc, AQ, info, st);
     launch_tri_inverse(nc, AQ, Linv, LinvT, st);
     if (opt.precision == GPUTO_PREC_MIXED) {
         if (dens2) launch_net_density(g[2], g[0], CX, dens2, st);
         launch_pack_cx<float>(elay, CX, CXpf, st);
+        for (int l = 1; l < nl - 1 && redisc(); ++l) launch_pack_cx<float>(elayr[l], CXr[l], CXrpf[l], st);
         launch_cast_f32(lay[0].size(), L[0].diag, Lf[0].diag, st);
         for (int l = 1; l < nl; ++l) {
             if (L[l].Apk) launch_cast_f32(300 * g[l].nel(), L[l].Apk, Lf[l].Apk, st);
@@ -301,7 +324,13 @@ void Solver::vcycle_impl(LevelBuf<T> *Lv, const T *CXl, const T *r0, T *z0, cons
             note(launch_fine_sweep<T>(mode, lay[0], elay, CXl, u, f, Lv[0].diag, mask[0], out, w, pr,
                                       nullptr, done, err, st));
         }
-        else if (l == 1 && quad_level1())
+        else if (redisc()) {
+            const T *cxl;
+            if constexpr (std::is_same<T, float>::value) cxl = CXrpf[l];
+            else cxl = CXrp[l];
+            note(launch_fine_sweep<T>(mode, lay[l], elayr[l], cxl, u, f, Lv[l].diag, mask[l], out, w, pr, nullptr,
+                                      done, err, st));
+        } else if (l == 1 && quad_level1())
             note(launch_quad_sweep<T>(mode, lay[1], elay, CXl, u, f, Lv[1].diag, mask[1], out, w, pr,
                                       opt.nu, Lv[1].yq, done, err, st));
         else if (Lv[l].yq)
@@ -391,7 +420,7 @@ void Solver::apply_level_f32(int l, const float *u, float *out, cudaStream_t st)
 int Solver::net_train_energy(Net *n, const float *x, const float *gt, int ns, float lr, double *loss,
                              float *grads_out, cudaStream_t st)
 {
-    if (!n || !net_x || ns < 1) return GPUTO_ERR_ARG;
+    if (!n || !net_x || ns < 1 || redisc()) return GPUTO_ERR_ARG;
     int s = init_net_kernels();
     if (!s) s = n->reserve(nd.n());
     if (s) return s;
@@ -425,8 +454,8 @@ int Solver::net_train_energy(Net *n, const float *x, const float *gt, int ns, fl
 
 int Solver::attach_net(Net *n, int mode)
 {
-    if (n && (opt.precision != GPUTO_PREC_MIXED || nl < 3 || !net_x)) {
-        set_error("the learned correction needs precision GPUTO_PREC_MIXED and nl >= 3");
+    if (n && (opt.precision != GPUTO_PREC_MIXED || nl < 3 || !net_x || redisc())) {
+        set_error("the learned correction needs precision GPUTO_PREC_MIXED, nl >= 3 and Galerkin coarse levels");
         return GPUTO_ERR_ARG;
     }
     if (mode < 0 || mode > 2) {

@@ -89,7 +89,13 @@ struct Solver {
     cudaStream_t stream(void *s) const { return s ? (cudaStream_t)s : own_stream; }
     // Level 1 is applied matrix-free from the fine CX whenever it is not the
     // coarsest level (then it needs assembled matrices for the direct solve).
-    bool quad_level1() const { return nl >= 3; }
+    bool quad_level1() const { return nl >= 3 && !redisc(); }
+    // mgcg9's hierarchy: every level is K_l = sum_e CX_l Ke, CX_l = 2 mean(children)
+    bool redisc() const { return opt.coarse == GPUTO_COARSE_REDISCRETIZED; }
+    double *CXr[kMaxLevels]{};     // re-discretised element scales, natural order (l >= 1)
+    double *CXrp[kMaxLevels]{};    // ... padded for the tile kernels (1 <= l < nl-1)
+    float *CXrpf[kMaxLevels]{};    // ... and their FP32 copies (mixed precision)
+    ELay elayr[kMaxLevels]{};
     int check_error_flags(cudaStream_t st);
 
   private:

@@ -52,7 +52,7 @@ _fp = ctypes.POINTER(ctypes.c_float)
 class Options(ctypes.Structure):
     _fields_ = [("precision", _i), ("nswp", _i), ("omega", _d), ("prerelax", _d), ("nu", _d),
                 ("check_every", _i), ("use_graph", _i), ("max_coarse_dofs", _i), ("tc_parts", _i),
-                ("tc_xchunk", _i)]
+                ("tc_xchunk", _i), ("coarse", _i)]
 
 
 SIGNATURES = {
@@ -64,6 +64,7 @@ SIGNATURES = {
     "gputo_mgcg1": (_i, [_dp, _dp, _dp, _dp, _dp, _i, _i, _i, _i, _i, _d, _i, _i, _dp, _ip]),
     "gputo_mgcg1_ex": (_i, [_dp, _dp, _dp, _dp, _dp, _i, _i, _i, _i, _i, _d, _i, _i,
                             ctypes.POINTER(Options), _dp, _ip]),
+    "gputo_mgcg9": (_i, [_dp, _dp, _dp, _dp, _dp, _i, _i, _i, _i, _i, _d, _i, _i, _i, _d, _d, _d, _d, _dp, _ip]),
     "gputo_solver_create": (_i, [ctypes.POINTER(_vp), _i, _i, _i, _i, ctypes.POINTER(Options)]),
     "gputo_solver_destroy": (None, [_vp]),
     "gputo_solver_apply_fp32_dev": (_i, [_vp, _vp, _vp, _i, _vp]),
@@ -208,6 +209,31 @@ def mgcg1(Ke0, F1, U, CX, fixed, nfd, nelx, nely, nelz, nl, cgtol, cgmax, printL
         return 0.0, -1
     if st not in (GPUTO_OK, GPUTO_ERR_BREAKDOWN):
         raise GputoError(st, "mgcg1")
+    return rr.value, nit.value
+
+
+def mgcg9(Ae, F, U, CX, FDofs, nFD, nelx, nely, nelz, nl, tol, maxit, nswp, printLev=1, nu=0.3, hx=1.0,
+          hy=1.0, hz=1.0):
+    """The MEX mgcg9 call (18 arguments).  Returns (cgres, cgiters); U is written in place."""
+    Ae = np.ascontiguousarray(Ae, dtype=np.float64).reshape(-1)
+    F = np.ascontiguousarray(F, dtype=np.float64).reshape(-1)
+    CX = np.ascontiguousarray(CX, dtype=np.float64).reshape(-1)
+    FDofs = np.ascontiguousarray(FDofs, dtype=np.float64).reshape(-1)
+    if not (isinstance(U, np.ndarray) and U.dtype == np.float64 and U.flags.c_contiguous):
+        raise TypeError("U must be a C-contiguous float64 ndarray (written in place)")
+    nd = 3 * (int(nelx) + 1) * (int(nely) + 1) * (int(nelz) + 1)
+    if F.size != nd or U.size != nd or CX.size != int(nelx) * int(nely) * int(nelz) or Ae.size != 576 \
+            or FDofs.size < int(nFD):
+        raise ValueError("argument sizes do not match nelx/nely/nelz/nFD")
+    rr = ctypes.c_double(0.0)
+    nit = ctypes.c_int(-1)
+    st = _lib.gputo_mgcg9(_p(Ae), _p(F), _p(U.reshape(-1)), _p(CX), _p(FDofs), int(nFD), int(nelx), int(nely),
+                          int(nelz), int(nl), float(tol), int(maxit), int(nswp), int(printLev), float(nu), float(hx),
+                          float(hy), float(hz), ctypes.byref(rr), ctypes.byref(nit))
+    if st == GPUTO_ERR_OOM:
+        return 0.0, -1
+    if st not in (GPUTO_OK, GPUTO_ERR_BREAKDOWN):
+        raise GputoError(st, "mgcg9")
     return rr.value, nit.value
 
 

@@ -57,6 +57,13 @@ typedef enum {
                               flexible PCG                                       */
 } gputo_precision;
 
+/* Coarse operators of the hierarchy. */
+typedef enum {
+    GPUTO_COARSE_GALERKIN = 0,       /* mgcg1: level 1 by quadrature, Galerkin above   */
+    GPUTO_COARSE_REDISCRETIZED = 1   /* mgcg9: every level K_l = sum_e CX_l Ke with
+                                        CX_l = 2 mean(children) (no stored matrices)  */
+} gputo_coarse;
+
 /* Solver options.  gputo_default_options() gives the constants that the MEX
  * hard-codes (mgcg1.cu:188 nswp=3, :1199-1206 omega=0.48, :1190-1197
  * pre-relaxation 0.7, :331 nu=0.3 for the level-1 quadrature). */
@@ -76,6 +83,7 @@ typedef struct {
                             cores                                                 */
     int tc_xchunk;       /* node planes per CTA of the tensor-core smoother
                             (0 = 16)                                              */
+    int coarse;          /* gputo_coarse                                          */
 } gputo_options;
 
 void gputo_default_options(gputo_options *opt);
@@ -121,6 +129,25 @@ int gputo_mgcg1_ex(const double *Ke0, const double *F, double *U, const double *
                    const double *fixed1b, int nfd, int nelx, int nely, int nelz, int nl,
                    double tol, int maxit, int printLev, const gputo_options *opt,
                    double *relres, int *nit);
+
+/*
+ * Replaces the MEX mgcg9 (Homogenization/QNC/mgcg9.cu:124-305), used by the
+ * QNC homogenization and CrossWalk drivers: the same PCG with a re-discretised
+ * hierarchy (every level K_l = sum_e CX_l Ae with CX_l twice the mean of its
+ * eight children, mgcg9.cu:753-781; damped Jacobi with weight 0.33 and
+ * pre-relaxation 0.7, nswp sweeps, mgcg9.cu:920-935; dense coarsest solve
+ * with zero rows/columns and 1e10 on fixed dofs, mgcg9.cu:1005-1028).  The
+ * 18 MEX arguments in order: Ae F U CX FDofs nFD nelx nely nelz nl tol maxit
+ * nswp printLev nu hx hy hz; nu and hx/hy/hz are accepted and, as in the
+ * reference, not used by the solve.  Outputs and U follow gputo_mgcg1 (y
+ * negated, nit the 0-based break index); printLev >= 1 writes mgcg9.log.
+ * Coarsest grids of 20,000 dofs or more are rejected (the reference switches
+ * to 10 nswp Jacobi sweeps there), and so is nl = 1 (the reference then
+ * smooths without a coarse solve).
+ */
+int gputo_mgcg9(const double *Ae, const double *F, double *U, const double *CX, const double *fixed1b, int nfd,
+                int nelx, int nely, int nelz, int nl, double tol, int maxit, int nswp, int printLev, double nu,
+                double hx, double hy, double hz, double *relres, int *nit);
 
 /* ---------------------------------------------------------------------- */
 /* Device-resident solver (the same solve without host copies)             */

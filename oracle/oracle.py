@@ -51,7 +51,7 @@ def build(force: bool = False) -> None:
 
 class _Opts(ctypes.Structure):
     _fields_ = [("nswp", ctypes.c_int), ("omega", ctypes.c_double),
-                ("prerelax", ctypes.c_double), ("nu", ctypes.c_double)]
+                ("prerelax", ctypes.c_double), ("nu", ctypes.c_double), ("coarse", ctypes.c_int)]
 
 
 _lib = None
@@ -180,12 +180,13 @@ def simp(xphys, penal=3.0, E0=1.0, Emin=1e-9):
 # --------------------------------------------------------------------------
 
 def mgcg1(p: Problem, CX, nl, tol, maxit, nswp=3, omega=0.48, prerelax=0.7, nu=0.3,
-          history=False):
-    """Restatement of the MEX: returns (U, relres, nit[, res_history])."""
+          history=False, coarse=0):
+    """Restatement of the MEX: returns (U, relres, nit[, res_history]).
+    coarse=1 gives the mgcg9 hierarchy (re-discretised levels)."""
     U = np.zeros(p.ndof)
     rr = ctypes.c_double(0.0)
     nit = ctypes.c_int(0)
-    o = _Opts(nswp, omega, prerelax, nu)
+    o = _Opts(nswp, omega, prerelax, nu, coarse)
     hist = np.zeros(max(maxit, 1) + 1)
     CX = np.ascontiguousarray(CX, dtype=np.float64)
     st = lib().or_mgcg1(_ptr(p.Ke0.reshape(-1).copy()), _ptr(p.F), _ptr(U), _ptr(CX),
@@ -198,9 +199,9 @@ def mgcg1(p: Problem, CX, nl, tol, maxit, nswp=3, omega=0.48, prerelax=0.7, nu=0
     return U, rr.value, nit.value
 
 
-def vcycle(p: Problem, CX, nl, r, nswp=3, omega=0.48, prerelax=0.7, nu=0.3):
+def vcycle(p: Problem, CX, nl, r, nswp=3, omega=0.48, prerelax=0.7, nu=0.3, coarse=0):
     z = np.zeros(p.ndof)
-    o = _Opts(nswp, omega, prerelax, nu)
+    o = _Opts(nswp, omega, prerelax, nu, coarse)
     st = lib().or_vcycle_apply(_ptr(p.Ke0.reshape(-1).copy()), _ptr(np.ascontiguousarray(CX)),
                                _ptr(p.fixed), len(p.fixed), p.nelx, p.nely, p.nelz, nl,
                                ctypes.byref(o), _ptr(np.ascontiguousarray(r)), _ptr(z))
@@ -214,6 +215,13 @@ def apply_fine(p: Problem, CX, u):
     lib().or_apply_fine(_ptr(p.Ke0.reshape(-1).copy()), _ptr(np.ascontiguousarray(CX)),
                         _ptr(np.ascontiguousarray(u)), _ptr(r), p.nelx, p.nely, p.nelz)
     return r
+
+
+def mgcg9(p: Problem, CX, nl, tol, maxit, nswp=2, history=False):
+    """Restatement of the MEX mgcg9 (Homogenization/QNC/mgcg9.cu): the mgcg1
+    PCG with re-discretised coarse levels and damped Jacobi omega = 0.33
+    (mgcg9.cu:929-935), nswp from the call."""
+    return mgcg1(p, CX, nl, tol, maxit, nswp=nswp, omega=0.33, prerelax=0.7, history=history, coarse=1)
 
 
 def ref_mgcg1(p: Problem, CX, nl, tol, maxit, workdir=None):

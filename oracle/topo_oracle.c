@@ -488,6 +488,7 @@ typedef struct {
     unsigned char *mask[16];
     double *diag[16], *U[16], *F[16], *R[16];
     double *Ael[16];
+    double *CXr[16];  /* mgcg9 hierarchy: re-discretised element scales */
     double *L;  /* coarsest Cholesky factor */
 } mg_t;
 
@@ -501,6 +502,7 @@ static void mg_free(mg_t *mg)
             free(mg->U[l]);
             free(mg->F[l]);
             free(mg->Ael[l]);
+            free(mg->CXr[l]);
         }
     }
     free(mg->L);
@@ -539,6 +541,24 @@ static int mg_build(mg_t *mg, const double *Ke0, const double *CX, const double 
         if (l == 0) {
             mg->op[0].Ke = Ke0;
             mg->op[0].CX = CX;
+        } else if (o->coarse) {
+            /* mgcg9.cu:753-781 formCXc: CX_l = 2 * mean of the 8 children */
+            const grid_t *gf = &mg->g[l - 1];
+            const double *CXf = (l == 1) ? CX : mg->CXr[l - 1];
+            mg->CXr[l] = malloc(sizeof(double) * g->nel);
+            for (int i = 0; i < g->nx; ++i)
+                for (int k = 0; k < g->nz; ++k)
+                    for (int j = 0; j < g->ny; ++j) {
+                        double s = 0.0;
+                        for (int a = 0; a < 2; ++a)
+                            for (int b = 0; b < 2; ++b)
+                                for (int c = 0; c < 2; ++c) s += CXf[elem_id(gf, 2 * i + a, 2 * j + c, 2 * k + b)];
+                        mg->CXr[l][elem_id(g, i, j, k)] = 2.0 * (s / 8.0);
+                    }
+            mg->op[l].Ke = Ke0;
+            mg->op[l].CX = mg->CXr[l];
+            mg->U[l] = calloc(g->ndof, sizeof(double));
+            mg->F[l] = calloc(g->ndof, sizeof(double));
         } else {
             mg->Ael[l] = malloc(sizeof(double) * 576 * g->nel);
             if (l == 1)
@@ -551,7 +571,26 @@ static int mg_build(mg_t *mg, const double *Ke0, const double *CX, const double 
         }
         mg->R[l] = calloc(g->ndof, sizeof(double));
         mg->diag[l] = calloc(g->ndof, sizeof(double));
-        if (l == nl - 1) {
+        if (l == nl - 1 && o->coarse) {
+            if (g->ndof >= 20000) return 2;
+            /* mgcg9.cu:1243-1300 assembAQc and :1005-1028 CorrCsAQc: the
+             * re-discretised operator, then zero rows/columns and 1e10 on
+             * every fixed dof */
+            const double *CXc = (l == 0) ? CX : mg->CXr[l];
+            double *Ael = malloc(sizeof(double) * 576 * g->nel);
+            for (long e = 0; e < g->nel; ++e)
+                for (int m = 0; m < 576; ++m) Ael[e * 576 + m] = CXc[e] * Ke0[m];
+            mg->L = malloc(sizeof(double) * g->ndof * g->ndof);
+            assemble_dense(g, Ael, mg->L);
+            free(Ael);
+            const long N = g->ndof;
+            for (long r = 0; r < N; ++r)
+                for (long q = 0; q < N; ++q) {
+                    const int fr = (mg->mask[l][r / 3] >> (r % 3)) & 1, fq = (mg->mask[l][q / 3] >> (q % 3)) & 1;
+                    if (fr || fq) mg->L[r * N + q] = (r == q) ? 1e10 : 0.0;
+                }
+            if (cholesky(g->ndof, mg->L)) return 3;
+        } else if (l == nl - 1) {
             if (l > 0) coarsest_penalty(g, mg->mask[l], mg->Ael[l]);
             if (g->ndof > 20000) return 2;
             mg->L = malloc(sizeof(double) * g->ndof * g->ndof);
@@ -628,6 +667,7 @@ void or_default_opts(or_opts *o)
     o->omega = 0.48;
     o->prerelax = 0.7;
     o->nu = 0.3;
+    o->coarse = 0;
 }
 
 static int check_args(int nelx, int nely, int nelz, int nl)

@@ -40,6 +40,11 @@ typedef struct {
     double omega;      /* damped Jacobi weight                        (0.48) */
     double prerelax;   /* initial relaxation factor U = c F / diag    (0.7)  */
     double nu;         /* Poisson ratio of the level-1 quadrature     (0.3)  */
+    int coarse;        /* 0: mgcg1 hierarchy (level-1 quadrature, Galerkin,
+                          element penalty); 1: mgcg9 hierarchy
+                          (Homogenization/QNC/mgcg9.cu: every level CX_l Ke with
+                          CX_l = 2 mean(children), dense coarsest with zero
+                          rows/columns and 1e10 on fixed dofs)        (0)    */
 } or_opts;
 
 void or_default_opts(or_opts *o);
