@@ -77,7 +77,7 @@ def test_no_device_returns_status_not_crash(gputo):
         gputo.density_filter(np.ones(8), 2, 2, 2, 1.5)
 
 
-def _load_mex():
+def _load_mex(name="libgputo_mex.so"):
     """Load the gateway the way MATLAB would: its mx* symbols resolve from a
     globally loaded libmx -- here the project's stand-in, built on the fly."""
     shim = os.path.join(ROOT, "oracle", "shim")
@@ -88,7 +88,7 @@ def _load_mex():
         subprocess.run(["gcc", "-O2", "-fPIC", "-shared", f"-I{shim}", os.path.join(shim, "mex_shim.c"),
                         "-o", so], check=True)
     ctypes.CDLL(so, mode=ctypes.RTLD_GLOBAL)
-    return ctypes.CDLL(os.path.join(ROOT, "gpu-to_b200", "lib", "libgputo_mex.so")), ctypes.CDLL(so)
+    return ctypes.CDLL(os.path.join(ROOT, "gpu-to_b200", "lib", name)), ctypes.CDLL(so)
 
 
 class MxArray(ctypes.Structure):
@@ -121,4 +121,14 @@ def test_mex_gateway_exports_mexfunction_and_rejects_bad_calls(gputo):
     # mismatched sizes: rejected before any buffer is touched
     res, it = call_mex(mex, [np.zeros(576), np.zeros(10), np.zeros(10), np.zeros(3), np.ones(1),
                              1, 2, 2, 2, 2, 1e-8, 10])
+    assert it == -1.0
+
+
+def test_mgcg9_gateway_exports_mexfunction_and_rejects_bad_calls(gputo):
+    mex, _ = _load_mex("libgputo_mex9.so")
+    assert hasattr(mex, "mexFunction")
+    res, it = call_mex(mex, [np.zeros(576)] * 12)      # mgcg9 needs 18 arguments
+    assert it == -1.0
+    res, it = call_mex(mex, [np.zeros(576), np.zeros(10), np.zeros(10), np.zeros(3), np.ones(1),
+                             1, 2, 2, 2, 2, 1e-8, 10, 2, 0, 0.3, 1.0, 1.0, 1.0])
     assert it == -1.0

@@ -165,3 +165,20 @@ def test_restatement_vs_live_reference_random(oracle):
         Uo, rr_o, n_o = oracle.mgcg1(p, CX, nl, 1e-9, 100)
         assert n_r == n_o
         assert np.linalg.norm(Ur - Uo) <= 1e-10 * np.linalg.norm(Ur)
+
+
+MGCG9_CASES = ["mgcg9_16x8x8_rand_nl3", "mgcg9_32x16x16_unif_nl4", "mgcg9_24x16x8_rand_nl3_nswp3",
+               "mgcg9_16x8x8_maxit3_nl2"]
+
+
+@pytest.mark.parametrize("name", MGCG9_CASES)
+def test_mgcg9_restatement_matches_reference_golden(oracle, name):
+    """The oracle's mgcg9 (re-discretised hierarchy) against the reference's own
+    CUDA mgcg9 run on a B200 (tests/golden/make_golden_mgcg9.py)."""
+    d = load_golden(name)
+    p = oracle.cantilever(int(d["nelx"]), int(d["nely"]), int(d["nelz"]))
+    assert np.array_equal(p.F, d["F"]) and np.array_equal(p.fixed, d["fixed"])
+    U, rr, nit = oracle.mgcg9(p, d["CX"], int(d["nl"]), float(d["tol"]), int(d["maxit"]), nswp=int(d["nswp"]))
+    assert nit == int(d["nit"])
+    assert abs(rr - float(d["relres"])) <= 1e-6 * float(d["relres"])
+    assert np.linalg.norm(U - d["U"]) <= 1e-9 * np.linalg.norm(d["U"])
