@@ -307,7 +307,9 @@ def run_ours(args):
                    "nelx": NELX, "nely": NELY, "nelz": NELZ, "ndof": ndof, "nl": NL,
                    "tol": TOL, "rmin": RMIN, "volfrac": VOLFRAC,
                    "l2": "inputs larger than L2 (12.8M-DOF FP64 vectors of 103 MB; ~4 GB per step)",
-                   "parallelism": f"replicas x{ws}"},
+                   "parallelism": f"replicas x{ws}",
+                   "learned": "off: the learned correction does not lower the iteration count on the designs "
+                              "measured, so its auto mode keeps the plain mixed V-cycle"},
         "fp64": {"value": round(s_fp64, 5), "unit": "s/design-iter",
                  "nit": [i["nit"] for i in inf_d], "speedup_mixed_vs_fp64": round(s_fp64 / s_mixed, 3)},
         "nit": [i["nit"] for i in inf_m],
