@@ -446,7 +446,8 @@ def run_reference(args):
     print(json.dumps(out))
 
 
-KERNELS = {"apply64": 0, "jacobi32": 1, "level1_32": 2, "level1_64": 3}
+KERNELS = {"apply64": 0, "jacobi32": 1, "level1_32": 2, "level1_64": 3, "jacobi_tc": 4, "energy64": -1,
+           "energy_tc": -2}
 
 
 def run_micro(args):
@@ -460,8 +461,9 @@ def run_micro(args):
     F, fixed = gputo.cantilever(nelx, nely, nelz)
     x0 = bench_design(nelx, nely, nelz)
     kinds = list(KERNELS) if args.micro == "all" else [args.micro]
-    mixed = any(k in ("jacobi32", "level1_32") for k in kinds)
-    opts = gputo.default_options(precision=gputo.PREC_MIXED if mixed else gputo.PREC_FP64)
+    mixed = any(k in ("jacobi32", "level1_32", "jacobi_tc") for k in kinds)
+    opts = gputo.default_options(precision=gputo.PREC_MIXED if mixed else gputo.PREC_FP64,
+                                 tc_parts=2 if "jacobi_tc" in kinds else 0)
     s = gputo.Solver(nelx, nely, nelz, nl, opts)
     s.set_problem(gputo.hex8_stiffness(), fixed)
     xd = torch.as_tensor(x0, dtype=torch.float64, device="cuda")
@@ -472,7 +474,24 @@ def run_micro(args):
     s.setup(CX)
     out = {"micro": args.micro, "size": args.size, "nl": nl, "device_bytes": s.device_bytes}
     for k in kinds:
-        out[k + "_ms"] = s.time_kernel(KERNELS[k], args.reps)
+        if KERNELS[k] >= 0:
+            out[k + "_ms"] = s.time_kernel(KERNELS[k], args.reps)
+            continue
+        # compliance sensitivity of a random displacement field: FP64 kernel or tensor cores
+        U = torch.randn(3 * (nelx + 1) * (nely + 1) * (nelz + 1), dtype=torch.float64, device="cuda")
+        dsK = -3.0 * xp * xp
+        ce, dc = torch.empty_like(xd), torch.empty_like(xd)
+        fn = gputo.compliance_sens_dev if KERNELS[k] == -1 else gputo.compliance_sens_tc_dev
+        Ke = gputo.hex8_stiffness()
+        fn(Ke, U, CX, dsK, nelx, nely, nelz, ce, dc)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.reps):
+            fn(Ke, U, CX, dsK, nelx, nely, nelz, ce, dc)
+        e1.record()
+        torch.cuda.synchronize()
+        out[k + "_ms_per_call"] = e0.elapsed_time(e1) / args.reps
     print(json.dumps(out))
 
 
