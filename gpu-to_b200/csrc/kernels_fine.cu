@@ -26,6 +26,7 @@ namespace gputo {
 
 __constant__ double cKe64[576];
 __constant__ float cKe32[576];
+__constant__ float2 cKe32p[288];   // the same FP32 rows as (q, q+1) pairs for packed FMAs
 
 template <typename T> __device__ __forceinline__ T ke(int idx);
 template <> __device__ __forceinline__ double ke<double>(int idx) { return cKe64[idx]; }
@@ -53,6 +54,7 @@ int upload_fine_ke(const double *Ke_host, cudaStream_t st)
     have[slot] = true;
     GPUTO_CUDA(cudaMemcpyToSymbolAsync(cKe64, last[slot], sizeof(double) * 576, 0, cudaMemcpyHostToDevice, st));
     GPUTO_CUDA(cudaMemcpyToSymbolAsync(cKe32, kf, sizeof(kf), 0, cudaMemcpyHostToDevice, st));
+    GPUTO_CUDA(cudaMemcpyToSymbolAsync(cKe32p, kf, sizeof(kf), 0, cudaMemcpyHostToDevice, st));
     int s2 = upload_design_ke(last[slot], st);
     if (!s2) s2 = upload_tc_ke(last[slot], st);
     if (!s2) s2 = upload_tcsweep_ke(last[slot], st);
@@ -130,8 +132,31 @@ __device__ __forceinline__ void element_rows(int a, const T (&ue)[24], const T *
     t2 *= cg[0];
 }
 
+// FP32: packed two-wide FMAs (sm_100 FFMA2), each row summed as two interleaved
+// partial sums over (q, q+1) pairs, so one instruction issues two FMAs; the
+// FP32 sweep is issue-bound, not FMA-bound.
+template <>
+__device__ __forceinline__ void element_rows<float, OP_FINE>(int a, const float (&ue)[24], const float *cg, float &t0,
+                                                             float &t1, float &t2)
+{
+    float2 s0 = make_float2(0.f, 0.f), s1 = s0, s2 = s0;
+#pragma unroll
+    for (int q = 0; q < 24; q += 2) {
+        const float2 u2 = make_float2(ue[q], ue[q + 1]);
+        s0 = __ffma2_rn(cKe32p[((3 * a) * 24 + q) >> 1], u2, s0);
+        s1 = __ffma2_rn(cKe32p[((3 * a + 1) * 24 + q) >> 1], u2, s1);
+        s2 = __ffma2_rn(cKe32p[((3 * a + 2) * 24 + q) >> 1], u2, s2);
+    }
+    t0 = fmaf(s0.x + s0.y, cg[0], t0);
+    t1 = fmaf(s1.x + s1.y, cg[0], t1);
+    t2 = fmaf(s2.x + s2.y, cg[0], t2);
+}
+
+// FP32 instances are held to 3 CTAs per SM (85 registers): with packed FMAs
+// the sweep is latency-bound, and the third CTA hides more than the spare
+// registers would.
 template <typename T, int MODE, int OP, int TXN>
-__global__ void __launch_bounds__(NT, 2)
+__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 3 : 2)
 tile_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ CUtensorMap tm_d,
             const __grid_constant__ CUtensorMap tm_c, Lay L, const T *__restrict__ f,
             const T *__restrict__ diag, const uint8_t *__restrict__ mask, T *__restrict__ out,
