@@ -844,6 +844,7 @@ struct OcScratch {
 };
 std::mutex g_oc_mu;
 OcScratch g_oc;
+constexpr int kHeavisideSteps = 60;   // Newton steps queued for the projection threshold
 }  // namespace
 
 int gputo_oc_update_dev(const double *x, const double *dc, const double *dV0, long long n,
@@ -864,6 +865,44 @@ int gputo_oc_update_dev(const double *x, const double *dc, const double *dV0, lo
     GPUTO_CUDA(cudaStreamSynchronize(s));
     GPUTO_CUDA(cudaGetLastError());
     if (lmid) *lmid = hst[2];
+    return GPUTO_OK;
+}
+
+int gputo_heaviside_dev(const double *xTilde, long long n, double volfrac, double beta, double *eta,
+                        double *xPhys, double *dprj, void *stream)
+{
+    if (!xTilde || !xPhys || !eta || n <= 0 || xTilde == xPhys || !(volfrac > 0 && volfrac < 1) || !(beta > 0))
+        return GPUTO_ERR_ARG;
+    std::lock_guard<std::mutex> lock(g_oc_mu);
+    int st = gputo::check_device();
+    if (st) return st;
+    st = g_oc.reserve(n);
+    if (st) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    gputo::launch_heaviside(n, xTilde, volfrac, beta, *eta, xPhys, dprj, g_oc.partial, g_oc.ticket, g_oc.state,
+                            kHeavisideSteps, s);
+    struct {
+        double eta;
+        int steps, done;
+    } hst{};
+    GPUTO_CUDA(cudaMemcpyAsync(&hst, g_oc.state, sizeof(hst), cudaMemcpyDeviceToHost, s));
+    GPUTO_CUDA(cudaStreamSynchronize(s));
+    GPUTO_CUDA(cudaGetLastError());
+    *eta = hst.eta;
+    if (!hst.done) {
+        gputo::set_error("Heaviside threshold: the eta Newton iteration did not reach |f| <= 1e-6");
+        return GPUTO_ERR_BREAKDOWN;
+    }
+    return GPUTO_OK;
+}
+
+int gputo_mul_dev(const double *a, const double *b, double *out, long long n, void *stream)
+{
+    if (!a || !b || !out || n <= 0) return GPUTO_ERR_ARG;
+    int st = gputo::check_device();
+    if (st) return st;
+    gputo::launch_mul(n, a, b, out, (cudaStream_t)stream);
+    GPUTO_CUDA(cudaGetLastError());
     return GPUTO_OK;
 }
 

@@ -247,6 +247,10 @@ int launch_filter(const Grid &g, const double *in, const double *div, double *ou
 void launch_simp(long long n, const double *x, double penal, double E0, double Emin, double *CX,
                  double *dsK, cudaStream_t st);
 int oc_state_bytes();
+int proj_state_bytes();
+void launch_heaviside(long long n, const double *xt, double volfrac, double beta, double eta0, double *xphys,
+                      double *dprj, double *partial, unsigned *ticket, void *state, int max_steps, cudaStream_t st);
+void launch_mul(long long n, const double *a, const double *b, double *out, cudaStream_t st);
 void launch_oc_update(long long n, const double *x, const double *dc, const double *dv0,
                       double volfrac, double move, double *ocp, double *xnew, double *partial,
                       unsigned *ticket, void *state, int max_steps, cudaStream_t st);

@@ -342,6 +342,133 @@ __global__ void copy_if_untouched_kernel(long long n, const double *__restrict__
 
 int oc_state_bytes() { return (int)sizeof(OcState); }
 
+// ---------------------------------------------------------------------------
+// Heaviside projection with the volume-preserving threshold
+// (top3D125modCuda.m:60-64 prj/deta/dprj, :111-119 the eta Newton loop):
+//   while |mean(prj(xTilde, eta, beta)) - volfrac| > 1e-6:
+//       eta -= f / mean(deta(xTilde, eta, beta))
+//   xPhys = prj(xTilde, eta, beta),  dprj(xTilde, eta, beta) for the chain rule
+// Each Newton step is one pass with a fixed-order sum; the threshold lives
+// on the device, so the loop needs no host round trip.
+// ---------------------------------------------------------------------------
+struct ProjState {
+    double eta;
+    int steps, done;
+};
+
+__device__ __forceinline__ double prj_v(double v, double eta, double beta)
+{
+    return (tanh(beta * eta) + tanh(beta * (v - eta))) / (tanh(beta * eta) + tanh(beta * (1.0 - eta)));
+}
+
+__device__ __forceinline__ double deta_v(double v, double eta, double beta)
+{
+    const double c = cosh(beta * (v - eta));
+    return -beta / sinh(beta) / (c * c) * sinh(v * beta) * sinh((1.0 - v) * beta);
+}
+
+__device__ __forceinline__ double dprj_v(double v, double eta, double beta)
+{
+    const double t = tanh(beta * (v - eta));
+    return beta * (1.0 - t * t) / (tanh(beta * eta) + tanh(beta * (1.0 - eta)));
+}
+
+__global__ void proj_init_kernel(ProjState *state, double eta0)
+{
+    state->eta = eta0;
+    state->steps = 0;
+    state->done = 0;
+}
+
+__global__ void __launch_bounds__(kOcThreads)
+proj_newton_kernel(long long n, const double *__restrict__ xt, double beta, double volfrac,
+                   double *__restrict__ partial, unsigned *ticket, ProjState *state)
+{
+    if (state->done) return;
+    __shared__ double rp[kOcThreads / 32], rd[kOcThreads / 32];
+    __shared__ bool is_last;
+    const double eta = state->eta;
+    double sp = 0.0, sd = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        sp += prj_v(xt[i], eta, beta);
+        sd += deta_v(xt[i], eta, beta);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        sp += __shfl_xor_sync(0xffffffffu, sp, o);
+        sd += __shfl_xor_sync(0xffffffffu, sd, o);
+    }
+    if ((threadIdx.x & 31) == 0) rp[threadIdx.x >> 5] = sp, rd[threadIdx.x >> 5] = sd;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int w = 0; w < kOcThreads / 32; ++w) a += rp[w], b += rd[w];
+        partial[2 * blockIdx.x] = a;
+        partial[2 * blockIdx.x + 1] = b;
+        __threadfence();
+        is_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (is_last && threadIdx.x == 0) {
+        __threadfence();
+        double a = 0.0, b = 0.0;
+        for (unsigned q = 0; q < gridDim.x; ++q) a += partial[2 * q], b += partial[2 * q + 1];
+        const double f = a / (double)n - volfrac;
+        ProjState z = *state;
+        if (fabs(f) > 1e-6) {
+            z.eta = eta - f / (b / (double)n);
+            z.steps += 1;
+        } else {
+            z.done = 1;
+        }
+        *state = z;
+        *ticket = 0;
+    }
+}
+
+__global__ void proj_apply_kernel(long long n, const double *__restrict__ xt, double beta,
+                                  const ProjState *__restrict__ state, double *__restrict__ xphys,
+                                  double *__restrict__ dprj)
+{
+    const double eta = state->eta;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        xphys[i] = prj_v(xt[i], eta, beta);
+        if (dprj) dprj[i] = dprj_v(xt[i], eta, beta);
+    }
+}
+
+int proj_state_bytes() { return (int)sizeof(ProjState); }
+
+void launch_heaviside(long long n, const double *xt, double volfrac, double beta, double eta0, double *xphys,
+                      double *dprj, double *partial, unsigned *ticket, void *state, int max_steps, cudaStream_t st)
+{
+    long long nb = (n + kOcThreads - 1) / kOcThreads;
+    if (nb > kOcBlocks / 2) nb = kOcBlocks / 2;   // partial holds 2 sums per CTA
+    ProjState *s = (ProjState *)state;
+    proj_init_kernel<<<1, 1, 0, st>>>(s, eta0);
+    for (int k = 0; k < max_steps; ++k)
+        proj_newton_kernel<<<(unsigned)nb, kOcThreads, 0, st>>>(n, xt, beta, volfrac, partial, ticket, s);
+    proj_apply_kernel<<<(unsigned)nb, kOcThreads, 0, st>>>(n, xt, beta, s, xphys, dprj);
+    count_launches(2 + max_steps);
+}
+
+__global__ void mul_kernel(long long n, const double *__restrict__ a, const double *__restrict__ b,
+                           double *__restrict__ out)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = a[i] * b[i];
+}
+
+void launch_mul(long long n, const double *a, const double *b, double *out, cudaStream_t st)
+{
+    long long nb = (n + 255) / 256;
+    if (nb > 4096) nb = 4096;
+    mul_kernel<<<(unsigned)nb, 256, 0, st>>>(n, a, b, out);
+    count_launches(1);
+}
+
 void launch_oc_update(long long n, const double *x, const double *dc, const double *dv0,
                       double volfrac, double move, double *ocp, double *xnew, double *partial,
                       unsigned *ticket, void *state, int max_steps, cudaStream_t st)

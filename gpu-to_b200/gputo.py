@@ -64,6 +64,8 @@ SIGNATURES = {
     "gputo_mgcg1": (_i, [_dp, _dp, _dp, _dp, _dp, _i, _i, _i, _i, _i, _d, _i, _i, _dp, _ip]),
     "gputo_mgcg1_ex": (_i, [_dp, _dp, _dp, _dp, _dp, _i, _i, _i, _i, _i, _d, _i, _i,
                             ctypes.POINTER(Options), _dp, _ip]),
+    "gputo_heaviside_dev": (_i, [_vp, ctypes.c_longlong, _d, _d, _dp, _vp, _vp, _vp]),
+    "gputo_mul_dev": (_i, [_vp, _vp, _vp, ctypes.c_longlong, _vp]),
     "gputo_mgcg9": (_i, [_dp, _dp, _dp, _dp, _dp, _i, _i, _i, _i, _i, _d, _i, _i, _i, _d, _d, _d, _d, _dp, _ip]),
     "gputo_solver_create": (_i, [ctypes.POINTER(_vp), _i, _i, _i, _i, ctypes.POINTER(Options)]),
     "gputo_solver_destroy": (None, [_vp]),
@@ -608,9 +610,22 @@ def oc_update(x, dc, dv0, volfrac, move):
     return xn, lm.value
 
 
+def heaviside_dev(xTilde, xPhys, volfrac, beta, eta, dprj=None, stream=None):
+    """Volume-preserving Heaviside projection on device tensors; returns the final eta."""
+    e = ctypes.c_double(float(eta))
+    _check(_lib.gputo_heaviside_dev(_ptr(xTilde), xTilde.numel(), float(volfrac), float(beta), ctypes.byref(e),
+                                    _ptr(xPhys), _ptr(dprj), _ptr_stream(stream)), "gputo_heaviside_dev")
+    return e.value
+
+
+def mul_dev(a, b, out, stream=None):
+    _check(_lib.gputo_mul_dev(_ptr(a), _ptr(b), _ptr(out), a.numel(), _ptr_stream(stream)), "gputo_mul_dev")
+
+
 class DesignLoop:
     """The top3D125 optimisation loop with every field resident on the GPU
-    (Cantilever/TOP3D125MGCGCUDA/top3D125modCuda.m:105-166, density filter ft=1):
+    (Cantilever/TOP3D125MGCGCUDA/top3D125modCuda.m:105-166; ft=1 density filter,
+    ft=3 density filter plus volume-preserving Heaviside projection):
 
         xPhys = imfilter(x, h, 'symmetric') ./ Hs          density filter
         CX, dsK = SIMP(xPhys)                               stiffness
@@ -627,7 +642,7 @@ class DesignLoop:
 
     def __init__(self, nelx, nely, nelz, nl, F, fixed, Ke0, volfrac=0.12, penal=3.0,
                  rmin=3 ** 0.5, move=0.2, tol=1e-6, maxit=200, E0=1.0, Emin=1e-9,
-                 options: Options | None = None, x0=None, stream=None):
+                 options: Options | None = None, x0=None, stream=None, ft=1, eta=0.4, beta=2.0):
         import torch
         self.torch = torch
         self.shape = (nelx, nely, nelz)
@@ -652,20 +667,40 @@ class DesignLoop:
         self.dV = torch.full((self.nel,), 1.0 / self.nel / volfrac, **f64)
         self.dV0 = torch.empty_like(self.x)
         self.U = torch.zeros(self.ndof, **f64)
+        if ft not in (1, 3):
+            raise ValueError("ft must be 1 (density filter) or 3 (plus Heaviside projection)")
+        self.ft, self.eta, self.beta = ft, eta, beta
+        if ft == 3:
+            self.xTilde = torch.empty_like(self.x)
+            self.dprj = torch.empty_like(self.x)
+            self.dVp = torch.empty_like(self.x)
         self.solver = Solver(nelx, nely, nelz, nl, options)
         self.solver.set_problem(self.Ke0, fixed)
 
     def step(self):
         nelx, nely, nelz = self.shape
         s = self.stream
-        density_filter_dev(self.x, self.xPhys, nelx, nely, nelz, self.rmin, stream=s)
+        if self.ft == 3:
+            # xTilde = filtered x; eta keeps the volume; xPhys = prj(xTilde) (top3D125modCuda.m:109-119)
+            density_filter_dev(self.x, self.xTilde, nelx, nely, nelz, self.rmin, stream=s)
+            self.eta = heaviside_dev(self.xTilde, self.xPhys, self.volfrac, self.beta, self.eta, self.dprj,
+                                     stream=s)
+        else:
+            density_filter_dev(self.x, self.xPhys, nelx, nely, nelz, self.rmin, stream=s)
         simp_dev(self.xPhys, self.CX, self.dsK, self.penal, self.E0, self.Emin, stream=s)
         self.solver.setup(self.CX, stream=s)
         relres, nit = self.solver.solve(self.F, self.U, self.tol, self.maxit, stream=s)
         c = compliance_sens_dev(self.Ke0, self.U, self.CX, self.dsK, nelx, nely, nelz,
                                 ce=self.ce, dc=self.dc, stream=s)
-        density_filter_dev(self.dc, self.dcf, nelx, nely, nelz, self.rmin, stream=s)
-        density_filter_dev(self.dV, self.dV0, nelx, nely, nelz, self.rmin, stream=s)
+        if self.ft == 3:
+            # dc ./ dHs with dHs = Hs ./ dprj: filter(dc .* dprj) / Hs (top3D125modCuda.m:117,140-141)
+            mul_dev(self.dc, self.dprj, self.dc, stream=s)
+            mul_dev(self.dV, self.dprj, self.dVp, stream=s)
+            density_filter_dev(self.dc, self.dcf, nelx, nely, nelz, self.rmin, stream=s)
+            density_filter_dev(self.dVp, self.dV0, nelx, nely, nelz, self.rmin, stream=s)
+        else:
+            density_filter_dev(self.dc, self.dcf, nelx, nely, nelz, self.rmin, stream=s)
+            density_filter_dev(self.dV, self.dV0, nelx, nely, nelz, self.rmin, stream=s)
         lmid = oc_update_dev(self.x, self.dcf, self.dV0, self.xnew, self.volfrac, self.move,
                              stream=s)
         self.x, self.xnew = self.xnew, self.x

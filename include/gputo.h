@@ -381,6 +381,20 @@ int gputo_oc_update_dev(const double *x, const double *dc, const double *dV0, lo
 int gputo_oc_update(const double *x, const double *dc, const double *dV0, long long n,
                     double volfrac, double move, double *xnew, double *lmid);
 
+/* Heaviside projection with the volume-preserving threshold (ft = 3,
+ * top3D125modCuda.m:60-64,111-119) on device arrays of n elements:
+ *   while |mean(prj(xTilde, eta, beta)) - volfrac| > 1e-6:
+ *       eta = eta - f / mean(deta(xTilde, eta, beta))
+ *   xPhys = prj(xTilde, eta, beta);  dprj (optional) = dprj(xTilde, eta, beta)
+ * with prj(v) = (tanh(beta eta) + tanh(beta (v - eta))) / (tanh(beta eta) +
+ * tanh(beta (1 - eta))).  eta: the starting threshold in (the previous design
+ * iteration's), the final one out.  The sensitivity chain rule of the driver,
+ * dc ./ dHs with dHs = Hs ./ dprj, is the filtered dc .* dprj (gputo_mul_dev). */
+int gputo_heaviside_dev(const double *xTilde, long long n, double volfrac, double beta, double *eta,
+                        double *xPhys, double *dprj, void *stream);
+/* out = a .* b on device arrays of n (out may alias a or b). */
+int gputo_mul_dev(const double *a, const double *b, double *out, long long n, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
