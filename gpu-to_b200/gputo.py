@@ -64,6 +64,9 @@ SIGNATURES = {
     "gputo_mgcg1": (_i, [_dp, _dp, _dp, _dp, _dp, _i, _i, _i, _i, _i, _d, _i, _i, _dp, _ip]),
     "gputo_mgcg1_ex": (_i, [_dp, _dp, _dp, _dp, _dp, _i, _i, _i, _i, _i, _d, _i, _i,
                             ctypes.POINTER(Options), _dp, _ip]),
+    "gputo_design_save": (_i, [ctypes.c_char_p, _i, _i, _i, _i, _dp, _i, _dp, _dp]),
+    "gputo_design_load": (_i, [ctypes.c_char_p, _ip, _ip, _ip, _ip, _dp, _ip, _dp, _dp]),
+    "gputo_design_export_volume": (_i, [ctypes.c_char_p, _i, _i, _i, _dp]),
     "gputo_heaviside_dev": (_i, [_vp, ctypes.c_longlong, _d, _d, _dp, _vp, _vp, _vp]),
     "gputo_mul_dev": (_i, [_vp, _vp, _vp, ctypes.c_longlong, _vp]),
     "gputo_mgcg9": (_i, [_dp, _dp, _dp, _dp, _dp, _i, _i, _i, _i, _i, _d, _i, _i, _i, _d, _d, _d, _d, _dp, _ip]),
@@ -610,6 +613,35 @@ def oc_update(x, dc, dv0, volfrac, move):
     return xn, lm.value
 
 
+def design_save(path, shape, iteration, params, x, xPhys):
+    """Write a design-state file (host arrays in element order)."""
+    x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+    xPhys = np.ascontiguousarray(xPhys, dtype=np.float64).reshape(-1)
+    params = np.ascontiguousarray(params, dtype=np.float64).reshape(-1)
+    _check(_lib.gputo_design_save(os.fsencode(path), *shape, int(iteration), _p(params) if params.size else None,
+                                  params.size, _p(x), _p(xPhys)), "gputo_design_save")
+
+
+def design_load(path):
+    """Read a design-state file: (shape, iteration, params, x, xPhys)."""
+    nx, ny, nz, it, npar = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int(0)
+    _check(_lib.gputo_design_load(os.fsencode(path), ctypes.byref(nx), ctypes.byref(ny), ctypes.byref(nz),
+                                  ctypes.byref(it), None, ctypes.byref(npar), None, None), "gputo_design_load")
+    nel = nx.value * ny.value * nz.value
+    params = np.zeros(max(npar.value, 1))
+    x, xp = np.zeros(nel), np.zeros(nel)
+    cap = ctypes.c_int(params.size)
+    _check(_lib.gputo_design_load(os.fsencode(path), ctypes.byref(nx), ctypes.byref(ny), ctypes.byref(nz),
+                                  ctypes.byref(it), _p(params), ctypes.byref(cap), _p(x), _p(xp)),
+           "gputo_design_load")
+    return (nx.value, ny.value, nz.value), it.value, params[:cap.value], x, xp
+
+
+def design_export_volume(base, shape, xPhys):
+    xPhys = np.ascontiguousarray(xPhys, dtype=np.float64).reshape(-1)
+    _check(_lib.gputo_design_export_volume(os.fsencode(base), *shape, _p(xPhys)), "gputo_design_export_volume")
+
+
 def heaviside_dev(xTilde, xPhys, volfrac, beta, eta, dprj=None, stream=None):
     """Volume-preserving Heaviside projection on device tensors; returns the final eta."""
     e = ctypes.c_double(float(eta))
@@ -676,6 +708,25 @@ class DesignLoop:
             self.dVp = torch.empty_like(self.x)
         self.solver = Solver(nelx, nely, nelz, nl, options)
         self.solver.set_problem(self.Ke0, fixed)
+
+    def save(self, path, iteration):
+        """Design state (x, xPhys and the loop parameters) for a later resume."""
+        params = [self.volfrac, self.penal, self.rmin, self.move, float(self.ft), self.eta, self.beta]
+        design_save(path, self.shape, iteration, params, self.x.cpu().numpy(), self.xPhys.cpu().numpy())
+
+    def resume(self, path):
+        """Continue from a saved design state (the drivers' warm start); returns its iteration."""
+        shape, it, params, x, xp = design_load(path)
+        if tuple(shape) != tuple(self.shape):
+            raise ValueError(f"saved design is {shape}, this loop is {self.shape}")
+        if len(params) < 7 or int(params[4]) != self.ft:
+            raise ValueError("saved design was not written by a loop with this filter type")
+        self.volfrac, self.penal, self.rmin, self.move = (float(v) for v in params[:4])
+        self.eta, self.beta = float(params[5]), float(params[6])
+        self.dV.fill_(1.0 / self.nel / self.volfrac)
+        self.x.copy_(self.torch.as_tensor(x, device=self.x.device))
+        self.xPhys.copy_(self.torch.as_tensor(xp, device=self.x.device))
+        return it
 
     def step(self):
         nelx, nely, nelz = self.shape

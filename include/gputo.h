@@ -395,6 +395,27 @@ int gputo_heaviside_dev(const double *xTilde, long long n, double volfrac, doubl
 /* out = a .* b on device arrays of n (out may alias a or b). */
 int gputo_mul_dev(const double *a, const double *b, double *out, long long n, void *stream);
 
+/* ---------------------------------------------------------------------- */
+/* Design-state files (host buffers; no GPU needed)                         */
+/* ---------------------------------------------------------------------- */
+
+/* Save / resume a design: the reference's drivers warm-start from a MATLAB
+ * file (CrossWalk/crosswalk.m:135, load x46.mat).  Binary file: 64-byte header
+ * (magic "GPUTODS1", version 1, nelx, nely, nelz, iteration, nparams), then
+ * params[nparams], x[nel], xPhys[nel] as little-endian doubles in element
+ * order.  params holds whatever loop state the caller keeps (e.g. volfrac,
+ * penal, rmin, eta, beta). */
+int gputo_design_save(const char *path, int nelx, int nely, int nelz, int iteration, const double *params,
+                      int nparams, const double *x, const double *xPhys);
+/* Reads the header; with x, xPhys and params all NULL it only reports the
+ * sizes.  *nparams: in, the capacity of params; out, the saved count.
+ * Truncated or foreign files give GPUTO_ERR_ARG with a message. */
+int gputo_design_load(const char *path, int *nelx, int *nely, int *nelz, int *iteration, double *params,
+                      int *nparams, double *x, double *xPhys);
+/* xPhys as a volume for external viewers (replaces the drivers' isosurface
+ * plot): <base>.raw (float32, y fastest, then z, then x) and <base>.nhdr. */
+int gputo_design_export_volume(const char *base, int nelx, int nely, int nelz, const double *xPhys);
+
 #ifdef __cplusplus
 }
 #endif

@@ -52,3 +52,25 @@ def test_design_loop_with_projection_matches_oracle(oracle, gputo, torch):
     assert max(abs(a - b) for a, b in zip(nits, h["nit"])) <= 1
     assert np.abs(dl.xPhys.cpu().numpy() - h["xPhys"]).max() <= 1e-6
     assert np.abs(dl.x.cpu().numpy() - h["x"]).max() <= 1e-6
+
+
+def test_design_loop_resume_is_seamless(gputo, torch, tmp_path):
+    """Save after three ft = 3 iterations, resume in a fresh loop, run three
+    more: the design and compliance match six uninterrupted iterations
+    (the drivers' warm start, CrossWalk/crosswalk.m:135)."""
+    F, fixed = gputo.cantilever(32, 16, 16)
+    kw = dict(volfrac=0.12, tol=1e-9, maxit=200, ft=3, eta=0.4, beta=2.0)
+    a = gputo.DesignLoop(32, 16, 16, 3, F, fixed, gputo.hex8_stiffness(), **kw)
+    ca = [a.step()["c"] for _ in range(6)]
+    b = gputo.DesignLoop(32, 16, 16, 3, F, fixed, gputo.hex8_stiffness(), **kw)
+    for _ in range(3):
+        b.step()
+    path = tmp_path / "it3.gds"
+    b.save(path, 3)
+    c = gputo.DesignLoop(32, 16, 16, 3, F, fixed, gputo.hex8_stiffness(), volfrac=0.3, tol=1e-9, maxit=200,
+                         ft=3, eta=0.5, beta=2.0)
+    assert c.resume(path) == 3
+    assert c.volfrac == 0.12 and c.eta == b.eta
+    cc = [c.step()["c"] for _ in range(3)]
+    np.testing.assert_allclose(cc, ca[3:], rtol=1e-9)
+    assert np.abs(c.x.cpu().numpy() - a.x.cpu().numpy()).max() <= 1e-9
