@@ -117,6 +117,19 @@ void gputo_default_options(gputo_options *o)
     o->tc_parts = 0;
     o->tc_xchunk = 0;
     o->coarse = GPUTO_COARSE_GALERKIN;
+    o->fine_op = 0;
+}
+
+int gputo_fine_op_constants(const double *Ke, double *c8)
+{
+    if (!Ke || !c8) return GPUTO_ERR_ARG;
+    gputo::HadamardKe hk;
+    if (!gputo::hadamard_ke(Ke, &hk)) {
+        gputo::set_error("Ke does not have the Hadamard-basis pattern of an isotropic cube element");
+        return GPUTO_ERR_ARG;
+    }
+    for (int q = 0; q < 8; ++q) c8[q] = hk.c[q];
+    return GPUTO_OK;
 }
 
 int gputo_solver_create(gputo_solver **out, int nelx, int nely, int nelz, int nl,
@@ -212,9 +225,8 @@ int gputo_solver_apply_fp32_dev(gputo_solver *h, const double *u, double *r, int
     gputo::launch_convert<double, float>(nv, s.P, s.Lf[0].u0, nullptr, st);
     int rs;
     if (tc_parts == 0)
-        rs = gputo::launch_fine_sweep<float>(gputo::MODE_APPLY, s.lay[0], s.elay, s.CXpf, s.Lf[0].u0, nullptr,
-                                             s.Lf[0].diag, s.mask[0], s.Lf[0].u1, 1.f, 0.f, nullptr, nullptr,
-                                             s.err, st);
+        rs = s.fine_sweep<float>(0, gputo::MODE_APPLY, s.lay[0], s.elay, s.CXpf, s.Lf[0].u0, nullptr, s.Lf[0],
+                                 s.Lf[0].u1, 1.f, 0.f, nullptr, nullptr, st);
     else
         rs = gputo::launch_tc_sweep(tc_parts, gputo::MODE_APPLY, s.lay[0], s.elay, s.CXpf, s.Lf[0].u0, nullptr,
                                     s.Lf[0].diag, s.mask[0], s.Lf[0].u1, 1.f, 0.f, s.opt.tc_xchunk, nullptr,
@@ -417,14 +429,12 @@ int gputo_solver_time_kernel(gputo_solver *h, int which, int reps, double *ms, v
         int r = GPUTO_OK;
         switch (which) {
         case 0:
-            r = gputo::launch_fine_sweep<double>(gputo::MODE_APPLY, s.lay[0], s.elay, s.CXp, s.P, nullptr,
-                                                 s.L[0].diag, s.mask[0], s.Q, 1.0, 0.0, nullptr, nullptr,
-                                                 s.err, st);
+            r = s.fine_sweep<double>(0, gputo::MODE_APPLY, s.lay[0], s.elay, s.CXp, s.P, nullptr, s.L[0], s.Q, 1.0,
+                                     0.0, nullptr, nullptr, st);
             break;
         case 1:
-            r = gputo::launch_fine_sweep<float>(gputo::MODE_JACOBI, s.lay[0], s.elay, s.CXpf, s.Lf[0].u0,
-                                                s.Lf[0].f, s.Lf[0].diag, s.mask[0], s.Lf[0].u1, 0.48f,
-                                                0.7f, nullptr, nullptr, s.err, st);
+            r = s.fine_sweep<float>(0, gputo::MODE_JACOBI, s.lay[0], s.elay, s.CXpf, s.Lf[0].u0, s.Lf[0].f, s.Lf[0],
+                                    s.Lf[0].u1, 0.48f, 0.7f, nullptr, nullptr, st);
             break;
         case 4:
             r = gputo::launch_tc_sweep(s.opt.tc_parts > 0 ? s.opt.tc_parts : 1, gputo::MODE_JACOBI, s.lay[0],
@@ -475,7 +485,7 @@ int gputo_solver_time_kernel(gputo_solver *h, int which, int reps, double *ms, v
 namespace {
 // every option is part of the key: a call must never reuse a solver built
 // with other options
-using Key = std::tuple<int, int, int, int, int, int, int, double, double, double, int, int, int, int, int, int>;
+using Key = std::tuple<int, int, int, int, int, int, int, double, double, double, int, int, int, int, int, int, int>;
 std::mutex g_cache_mu;
 std::map<Key, std::unique_ptr<gputo_solver>> g_cache;
 std::vector<Key> g_cache_order;
@@ -485,7 +495,7 @@ gputo_solver *cached_solver(int nelx, int nely, int nelz, int nl, const gputo_op
     int dev = 0;
     cudaGetDevice(&dev);
     Key k{dev, nelx, nely, nelz, nl, o.precision, o.nswp, o.omega, o.prerelax, o.nu,
-          o.check_every, o.use_graph, o.max_coarse_dofs, o.tc_parts, o.tc_xchunk, o.coarse};
+          o.check_every, o.use_graph, o.max_coarse_dofs, o.tc_parts, o.tc_xchunk, o.coarse, o.fine_op};
     auto it = g_cache.find(k);
     if (it != g_cache.end()) return it->second.get();
     // keep at most two shapes resident

@@ -95,6 +95,7 @@ struct LevelBuf {
     T *f = nullptr;                  // right-hand side of this level
     T *r = nullptr;                  // defect after pre-smoothing (restriction input)
     T *diag = nullptr;               // operator diagonal
+    T *rdiag = nullptr;              // 1 / diag (0 where diag is 0), levels with fine sweeps
     T *Apk = nullptr;                // packed element matrices, [300][nel] (levels >= 1)
     T *yq = nullptr;                 // level-1 element outputs, [24][nel] (matrix-free level 1)
     uint8_t *mask = nullptr;         // fixed-dof bits per node (bit d = dof d fixed)
@@ -153,6 +154,26 @@ void launch_diag_quad(const Lay &L, const double *CXf, double *diag, cudaStream_
 int upload_quadrature_fine(const double *kg_packed, cudaStream_t st);
 // Level-2 Galerkin operator directly from the fine CX (level 1 not stored).
 void launch_build_galerkin_from_quad(const Grid &g2, const double *CXfine, double *Apk, cudaStream_t st);
+// Fine sweeps with Ke in its Hadamard basis (kernels_hsweep.cu).  hadamard_ke
+// derives the eight constants of T Ke T from a cube element's Ke and returns
+// false when Ke lacks that structure.  hsweep_fits: the grid suits the kernel
+// (ny <= 256) and its clusters are resident on this device.
+struct HadamardKe {
+    bool ok = false;
+    double c[8] = {};   // a, b, c, d, e, f, g, h
+};
+bool hadamard_ke(const double *Ke, HadamardKe *hk);
+int init_hsweep_kernels();
+template <typename T> bool hsweep_fits(const Grid &g);
+template <typename T> int hsweep_blocks(const Grid &g);
+// rdiag: 1/diag (launch_recip); maskp: the Dirichlet bytes with rows padded
+// to 16 bytes (launch_pad_mask; hsweep_mask_bytes of storage).
+template <typename T>
+int launch_hsweep(int mode, const Lay &L, const ELay &E, const HadamardKe &hk, const T *CX, const T *u, const T *f,
+                  const T *rdiag, const uint8_t *mask, const uint8_t *maskp, T *out, T omega, T prerelax,
+                  double *dot_partial, const int *done, int *err, cudaStream_t st);
+long long hsweep_mask_bytes(const Grid &g);
+void launch_pad_mask(const Grid &g, const uint8_t *mask, uint8_t *maskp, cudaStream_t st);
 // Opt the tile kernels into their dynamic shared memory (call once per device).
 int init_fine_kernels();
 // Number of per-CTA partials a MODE_APPLY fine sweep writes.
@@ -208,6 +229,9 @@ void launch_mask_restrict(const Grid &gc, const uint8_t *maskf, uint8_t *maskc, 
 template <typename Tin, typename Tout>
 void launch_convert(long long n, const Tin *in, Tout *out, const int *done, cudaStream_t st);
 void launch_cast_f32(long long n, const double *in, float *out, cudaStream_t st);
+// out = 1 / in (0 where in is 0), rounded once to T
+template <typename T>
+void launch_recip(long long n, const double *in, T *out, cudaStream_t st);
 
 // PCG vector kernels (kernels_blas.cu).
 int reduce_partials_capacity();

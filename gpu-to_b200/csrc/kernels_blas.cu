@@ -354,6 +354,22 @@ void launch_convert(long long n, const Tin *in, Tout *out, const int *done, cuda
 template void launch_convert<double, float>(long long, const double *, float *, const int *, cudaStream_t);
 template void launch_convert<float, double>(long long, const float *, double *, const int *, cudaStream_t);
 
+template <typename T>
+__global__ void recip_kernel(long long n, const double *__restrict__ in, T *__restrict__ out)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = in[i] != 0.0 ? (T)(1.0 / in[i]) : T(0);
+}
+
+template <typename T>
+void launch_recip(long long n, const double *in, T *out, cudaStream_t st)
+{
+    recip_kernel<T><<<red_blocks(n), kRedThreads, 0, st>>>(n, in, out);
+    count_launches(1);
+}
+template void launch_recip<double>(long long, const double *, double *, cudaStream_t);
+template void launch_recip<float>(long long, const double *, float *, cudaStream_t);
+
 void launch_cast_f32(long long n, const double *in, float *out, cudaStream_t st)
 {
     launch_convert<double, float>(n, in, out, nullptr, st);

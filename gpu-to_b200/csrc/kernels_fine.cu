@@ -671,8 +671,9 @@ int make_tmap_3d(CUtensorMap *m, const void *base, int elem_bytes, uint64_t d0, 
     const cuuint64_t strides[2] = {stride1_bytes, stride2_bytes};
     const cuuint32_t box[3] = {b0, b1, b2};
     const cuuint32_t estr[3] = {1, 1, 1};
-    const CUtensorMapDataType dt =
-        elem_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    const CUtensorMapDataType dt = elem_bytes == 8   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                                   : elem_bytes == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                                     : CU_TENSOR_MAP_DATA_TYPE_UINT8;
     CUresult r = fn(m, dt, 3, const_cast<void *>(base), dims, strides, box, estr,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);

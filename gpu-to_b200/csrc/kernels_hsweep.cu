@@ -1,0 +1,760 @@
+// Fine-level operator sweeps with the element matrix in its Hadamard basis.
+//
+// Same modes and results as tile_kernel (K u, f - K u, damped Jacobi with the
+// Dirichlet rows zeroed: mgcg1.cu:941-997,1199-1264,1326-1331), with far
+// fewer operations per element.
+//
+// The algebra.  Let H be the 2x2 Hadamard matrix and T = H (x) H (x) H act on
+// the eight corners of an element (corner (cx, cy, cz), mode (px, py, pz),
+// sign (-1)^(px cx + py cy + pz cz)).  For the trilinear hex8 of an isotropic
+// material on a cube, Ke is a sum of Kronecker products of the 1-D mass,
+// stiffness and gradient matrices [a b; b a] / [a a; -a -a], which H turns
+// into diagonal / single-entry matrices.  So S = T Ke T' (per displacement
+// component, 24x24) has only 45 non-zeros in a fixed pattern:
+//   three 2x2 blocks a [1 1; 1 1], two 3x3 blocks (b - c) I + c 11', three 2x2
+//   blocks [f g; g f], the diagonal h on mode (1,1,1), and zero on mode
+//   (0,0,0) (rigid translation).
+// Ke u = T' S T u / 64.  T factors into butterflies: two per face (y, z),
+// shared by the two elements that meet at the face, and one across the
+// element (x).  Per element: 24 + 24 operations forward, 41 in S (with the
+// element's CX folded into eight scaled constants), 36 + 24 back, against
+// 576 FMAs for the dense 24x24 product.  The host derives the eight
+// constants from the caller's Ke and checks the pattern to 1e-12; any other
+// Ke runs on the dense kernel.
+//
+// The tiling.  A thread owns one element column along x (lane = y, warp = z)
+// and marches through an x chunk of HTX node planes, one element per step:
+//  * node planes arrive by TMA into a ring of HRING shared-memory slots (u,
+//    or f and diag for MODE_JACOBI_PRE, plus the CX plane), each slot on its
+//    own mbarrier, with bounded waits;
+//  * the back face of element i is the front face of element i + 1, so each
+//    face is loaded and transformed once and its accumulator carries over;
+//  * when a node plane is complete, the four corner partials of each column
+//    are summed across columns: over y by a warp shuffle, over z through
+//    shared memory (one barrier per plane, which also frees the ring slot);
+//  * a cluster of CTAs spans all of y (ny <= 256): the partial of the node
+//    column on the seam between two CTAs goes to the right neighbour's
+//    shared memory (DSMEM), which finishes those nodes after one cluster
+//    barrier at the end of the chunk; in z, tiles overlap by one element
+//    column; in x, chunks overlap by one element.
+// No atomics: results are deterministic.  Nodes on the far faces need no
+// separate kernel.
+#include <cooperative_groups.h>
+
+#include <cmath>
+#include <mutex>
+
+#include "gputo_internal.h"
+#include "tma.h"
+
+namespace cg = cooperative_groups;
+
+namespace gputo {
+
+namespace {
+
+constexpr int HY = 32;           // element columns per CTA along y (one per lane)
+constexpr int HUW = 100;         // u box width in values: 3 (HY + 1) = 99, rounded to 16 bytes
+constexpr int HRING = 5;         // ring slots; loads run HRING - 2 node planes ahead
+constexpr int HM = 48;           // mask box width in bytes: HY + 1 = 33 nodes, rounded to 16
+constexpr int HTX = 32;          // node planes per x chunk
+constexpr int HMAXP = HTX + 1;   // planes one chunk may finish (the last chunk also takes plane nx)
+constexpr int HMAXCY = 8;        // CTAs per cluster (portable limit): ny <= 256
+constexpr uint32_t kHWaitPolls = 1u << 22;
+
+template <typename T> struct HC {
+    T a, bc, c, de, e, f, g, h;   // S constants / 64: a, b - c, c, d - e, e, f, g, h
+};
+
+__host__ __device__ constexpr size_t al128(size_t x) { return (x + 127) & ~size_t(127); }
+
+// What each mode reads besides u: f (defect, Jacobi, pre-relaxation) and
+// 1/diag (Jacobi, pre-relaxation) at the node plane being finished.
+template <int MODE> struct HNeeds {
+    static constexpr bool PRE = MODE == MODE_JACOBI_PRE;
+    static constexpr bool F = MODE != MODE_APPLY;
+    static constexpr bool D = MODE == MODE_JACOBI || MODE == MODE_JACOBI_PRE;
+};
+
+// Shared memory of one CTA.  Ring slot s holds: the face tile of node plane
+// E0 + s (u; f and diag for pre-relaxation), the CX tile of element plane
+// E0 + s - 1, and the epilogue tiles of node plane E0 + s - 1 (f, diag, the
+// Dirichlet mask), which that stage finishes.
+template <typename T, int WZ, int MODE>
+struct HSmem {
+    using N = HNeeds<MODE>;
+    // every TMA destination starts on a 128-byte boundary
+    static constexpr size_t u_bytes = sizeof(T) * (WZ + 1) * HUW;   // one node plane tile
+    static constexpr size_t ua = al128(u_bytes);
+    static constexpr size_t c_bytes = sizeof(T) * WZ * HY;          // one CX plane tile
+    static constexpr size_t m_bytes = (size_t)WZ * HM;              // one mask plane tile
+    static constexpr size_t d_off = ua;                               // face 1/diag (pre-relaxation)
+    static constexpr size_t ef_off = d_off + (N::PRE ? ua : 0);       // epilogue f
+    static constexpr size_t ed_off = ef_off + (N::F ? ua : 0);        // epilogue 1/diag
+    static constexpr size_t c_off = ed_off + (N::D ? ua : 0);
+    static constexpr size_t m_off = c_off + al128(c_bytes);
+    static constexpr size_t slot = al128(m_off + m_bytes);
+    static constexpr int ZROW = HY + 1;                               // lanes + the seam column
+    static constexpr size_t z_off = HRING * slot;
+    static constexpr size_t z_bytes = sizeof(T) * 2 * WZ * ZROW * 3;
+    static constexpr int SEAM = HMAXP * WZ * 3;
+    static constexpr size_t s_off = al128(z_off + z_bytes);
+    static constexpr size_t s_bytes = sizeof(T) * 3 * SEAM;         // own, own u, received
+    static constexpr size_t bar_off = al128(s_off + s_bytes);
+    static constexpr size_t red_off = bar_off + 8 * HRING;            // per-warp dot partials
+    static constexpr size_t bytes = red_off + 8 * WZ;
+    static_assert(ua % 128 == 0 && c_off % 128 == 0 && m_off % 128 == 0 && slot % 128 == 0,
+                  "TMA shared-memory destinations must be 128-byte aligned");
+};
+
+// (y, z) butterflies of one face: x[(cy 2 + cz) 3 + d] -> x[(py 2 + pz) 3 + d];
+// applied twice it multiplies by 4.
+template <typename T>
+__device__ __forceinline__ void face_h(T (&x)[12])
+{
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const T u00 = x[d], u01 = x[3 + d], u10 = x[6 + d], u11 = x[9 + d];
+        const T s0 = u00 + u10, d0 = u00 - u10, s1 = u01 + u11, d1 = u01 - u11;
+        x[d] = s0 + s1;
+        x[3 + d] = s0 - s1;
+        x[6 + d] = d0 + d1;
+        x[9 + d] = d0 - d1;
+    }
+}
+
+// One element in the Hadamard basis.  Fp, Fn: transformed front (x = 0) and
+// back (x = 1) faces.  Adds the element's front-face output (still in face
+// modes) to A and sets An to its back-face output.  Mode m = 4 px + 2 py + pz
+// with px selecting v0 / v1 and (py, pz, d) the index (py 2 + pz) 3 + d.
+template <typename T>
+__device__ __forceinline__ void element_h(const T (&Fp)[12], const T (&Fn)[12], T cx, const HC<T> &k, T (&A)[12],
+                                          T (&An)[12])
+{
+    T v0[12], v1[12], w0[12], w1[12];
+#pragma unroll
+    for (int q = 0; q < 12; ++q) {
+        v0[q] = Fp[q] + Fn[q];
+        v1[q] = Fp[q] - Fn[q];
+    }
+    const T ka = k.a * cx, kbc = k.bc * cx, kc = k.c * cx, kde = k.de * cx, ke = k.e * cx, kf = k.f * cx,
+            kg = k.g * cx, kh = k.h * cx;
+    T t;
+    w0[0] = w0[1] = w0[2] = T(0);   // mode (0,0,0): rigid translation
+    // a [1 1; 1 1]: {(m1,x),(m4,z)}, {(m1,y),(m2,z)}, {(m2,x),(m4,y)}
+    t = ka * (v0[3] + v1[2]);
+    w0[3] = t, w1[2] = t;
+    t = ka * (v0[4] + v0[8]);
+    w0[4] = t, w0[8] = t;
+    t = ka * (v0[6] + v1[1]);
+    w0[6] = t, w1[1] = t;
+    // (b - c) I + c 11': {(m1,z),(m2,y),(m4,x)}
+    t = kc * (v0[5] + v0[7] + v1[0]);
+    w0[5] = fma(kbc, v0[5], t);
+    w0[7] = fma(kbc, v0[7], t);
+    w1[0] = fma(kbc, v1[0], t);
+    // (d - e) I + e 11': {(m3,x),(m5,y),(m6,z)}
+    t = ke * (v0[9] + v1[4] + v1[8]);
+    w0[9] = fma(kde, v0[9], t);
+    w1[4] = fma(kde, v1[4], t);
+    w1[8] = fma(kde, v1[8], t);
+    // [f g; g f]: {(m3,y),(m5,x)}, {(m3,z),(m6,x)}, {(m5,z),(m6,y)}
+    w0[10] = fma(kf, v0[10], kg * v1[3]);
+    w1[3] = fma(kf, v1[3], kg * v0[10]);
+    w0[11] = fma(kf, v0[11], kg * v1[6]);
+    w1[6] = fma(kf, v1[6], kg * v0[11]);
+    w1[5] = fma(kf, v1[5], kg * v1[7]);
+    w1[7] = fma(kf, v1[7], kg * v1[5]);
+    // h I on mode (1,1,1)
+    w1[9] = kh * v1[9];
+    w1[10] = kh * v1[10];
+    w1[11] = kh * v1[11];
+#pragma unroll
+    for (int q = 0; q < 12; ++q) {
+        A[q] += w0[q] + w1[q];
+        An[q] = w0[q] - w1[q];
+    }
+}
+
+// One node's result from K u (ku), u, f, 1/diag and its Dirichlet bits m; fv
+// and rv point at that node's three f and 1/diag values (shared or global).
+template <typename T, int MODE>
+__device__ __forceinline__ void h_store(long long base, unsigned m, const T (&ku)[3], const T (&u)[3], const T *fv,
+                                        const T *rv, T *__restrict__ out, T omega, double &dsum)
+{
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const bool fixed = (m >> d) & 1u;
+        if (MODE == MODE_APPLY) {
+            const T q = fixed ? T(0) : ku[d];
+            out[base + d] = q;
+            dsum += (double)u[d] * (double)q;
+        } else if (MODE == MODE_DEFECT) {
+            out[base + d] = fixed ? T(0) : fv[d] - ku[d];
+        } else {
+            const T r = fixed ? T(0) : fv[d] - ku[d];
+            out[base + d] = u[d] + omega * r * rv[d];
+        }
+    }
+}
+
+// Grid: x = rank along y inside the cluster (the cluster spans all of y),
+// y = z tile (element columns kc0 .. kc0 + WZ - 1, kc0 = (WZ - 1) tile),
+// z = x chunk (node planes [c htx, (c + 1) htx), the last one up to nx;
+// htx <= HTX).  The Dirichlet bits come by TMA from a copy with rows padded
+// to 16 bytes (tm_m); rdiag = 1/diag.
+template <typename T, int MODE, int WZ>
+__global__ void __launch_bounds__(32 * WZ, sizeof(T) == 4 ? 2 : 1)
+hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ CUtensorMap tm_d,
+              const __grid_constant__ CUtensorMap tm_f, const __grid_constant__ CUtensorMap tm_c,
+              const __grid_constant__ CUtensorMap tm_m, Lay L, HC<T> hc, int htx, const T *__restrict__ f,
+              const T *__restrict__ rdiag, const uint8_t *__restrict__ mask, T *__restrict__ out, T omega,
+              T prerelax, double *__restrict__ dot_partial, const int *__restrict__ done, int *__restrict__ err)
+{
+    if (done && *done) return;   // the same value for every CTA of the cluster
+    using N = HNeeds<MODE>;
+    constexpr int NT = 32 * WZ;
+    using S = HSmem<T, WZ, MODE>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    if (smem_u32(smem) & 127u) {   // TMA destinations need 128-byte alignment (same for every CTA)
+        if (threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && err)
+            atomicExch(err, GPUTO_ERR_CUDA);
+        return;
+    }
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + S::bar_off);
+    T *zb = reinterpret_cast<T *>(smem + S::z_off);
+    T *s_own = reinterpret_cast<T *>(smem + S::s_off);
+    T *s_ownu = s_own + S::SEAM;
+    T *s_recv = s_own + 2 * S::SEAM;
+
+    cg::cluster_group cluster = cg::this_cluster();
+    const Grid &g = L.g;
+    const int tid = threadIdx.x, l = tid & 31, w = tid >> 5;
+    const int r = blockIdx.x, CY = gridDim.x;
+    const int jc0 = HY * r;
+    const int zt = blockIdx.y, kc0 = (WZ - 1) * zt;
+    const int P0 = blockIdx.z * htx;
+    const int P1 = (blockIdx.z == gridDim.z - 1) ? g.nx + 1 : P0 + htx;
+    const int E0 = P0 > 0 ? P0 - 1 : 0, E1 = P1 < g.nx ? P1 : g.nx;
+    const int nE = E1 - E0;                          // elements of the chunk (>= 1)
+    const bool last_plane = E1 == g.nx && E1 < P1;   // plane nx: only element nx - 1 touches it
+    const int nst = nE + 1 + (last_plane ? 1 : 0);   // ring stages
+    const bool tail_owner = (r == CY - 1) && (jc0 + HY == g.ny);
+    const bool zok = (w >= 1 || zt == 0) && kc0 + w <= g.nz;   // this warp's node row is output here
+
+    if (tid == 0) {
+        for (int s = 0; s < HRING; ++s) mbar_init(&bar[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    int issued = 0;   // meaningful on thread 0
+    auto issue = [&](int s) {
+        unsigned char *sb = smem + (s % HRING) * S::slot;
+        uint64_t *b = &bar[s % HRING];
+        const bool face = s <= nE, cxp = s >= 1 && s <= nE, epi = s >= 1 && E0 + s - 1 >= P0;
+        uint32_t bytes = 0;
+        if (face) bytes += (uint32_t)(S::u_bytes * (N::PRE ? 2 : 1));
+        if (cxp) bytes += (uint32_t)S::c_bytes;
+        if (epi) bytes += (uint32_t)(S::u_bytes * ((N::F ? 1 : 0) + (N::D ? 1 : 0)) + S::m_bytes);
+        mbar_arrive_expect_tx(b, bytes);
+        if (face) {
+            tma_load_3d(sb, &tm_u, 3 * jc0, kc0, E0 + s, b);
+            if (N::PRE) tma_load_3d(sb + S::d_off, &tm_d, 3 * jc0, kc0, E0 + s, b);
+        }
+        if (cxp) tma_load_3d(sb + S::c_off, &tm_c, jc0, kc0, E0 + s - 1, b);
+        if (epi) {
+            if (N::F) tma_load_3d(sb + S::ef_off, &tm_f, 3 * jc0, kc0, E0 + s - 1, b);
+            if (N::D) tma_load_3d(sb + S::ed_off, &tm_d, 3 * jc0, kc0, E0 + s - 1, b);
+            tma_load_3d(sb + S::m_off, &tm_m, jc0, kc0, E0 + s - 1, b);
+        }
+        issued = s + 1;
+    };
+    if (tid == 0)
+        for (int s = 0; s < HRING && s < nst; ++s) issue(s);
+    cluster.sync();   // every CTA of the cluster is running before any remote store
+
+    bool bad = false;
+    auto wait_stage = [&](int s) {
+        if (!bad && !mbar_wait_bounded(&bar[s % HRING], (uint32_t)((s / HRING) & 1), kHWaitPolls)) bad = true;
+    };
+    auto load_face = [&](int s, T (&U)[12]) {
+        const unsigned char *sb = smem + (s % HRING) * S::slot;
+        const T *su = reinterpret_cast<const T *>(sb);
+        const T *sd = reinterpret_cast<const T *>(sb + S::d_off);
+#pragma unroll
+        for (int cy = 0; cy < 2; ++cy)
+#pragma unroll
+            for (int cz = 0; cz < 2; ++cz)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const int idx = (w + cz) * HUW + 3 * (l + cy) + d;
+                    T v = su[idx];
+                    if (N::PRE) v = prerelax * v * sd[idx];   // 1/diag is 0 outside the grid
+                    U[(cy * 2 + cz) * 3 + d] = v;
+                }
+    };
+    double dsum = 0.0;
+    // Corner partials P of node plane p -> y sums through the warp, z partner
+    // values into the exchange buffer (read after the next barrier).
+    auto reduce_y = [&](int p, T (&P)[12], T (&q0)[3]) {
+        T *z = zb + (p & 1) * (WZ * S::ZROW * 3);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const T a0 = __shfl_up_sync(0xffffffffu, P[6 + d], 1);
+            const T a1 = __shfl_up_sync(0xffffffffu, P[9 + d], 1);
+            q0[d] = P[d] + (l > 0 ? a0 : T(0));
+            z[(w * S::ZROW + l) * 3 + d] = P[3 + d] + (l > 0 ? a1 : T(0));
+            if (l == HY - 1) z[(w * S::ZROW + HY) * 3 + d] = P[9 + d];
+        }
+    };
+    // Finish node plane p with the epilogue tiles of ring stage s.
+    auto emit = [&](int p, int s, const T (&P)[12], const T (&q0)[3], const T (&Uu)[12]) {
+        if (!zok) return;
+        const unsigned char *sb = smem + (s % HRING) * S::slot;
+        const T *ef = reinterpret_cast<const T *>(sb + S::ef_off) + w * HUW;
+        const T *ed = reinterpret_cast<const T *>(sb + S::ed_off) + w * HUW;
+        const uint8_t *em = sb + S::m_off + w * HM;
+        const T *z = zb + (p & 1) * (WZ * S::ZROW * 3);
+        const int k = kc0 + w, j = jc0 + l, at = ((p - P0) * WZ + w) * 3;
+        T R[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) R[d] = q0[d] + (w > 0 ? z[((w - 1) * S::ZROW + l) * 3 + d] : T(0));
+        if (l == 0 && r > 0) {   // seam node: finished after the cluster barrier
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                s_own[at + d] = R[d];
+                s_ownu[at + d] = Uu[d];
+            }
+        } else if (j <= g.ny) {
+            const T uu[3] = {Uu[0], Uu[1], Uu[2]};
+            h_store<T, MODE>(L.at(p, j, k), em[l], R, uu, ef + 3 * l, ed + 3 * l, out, omega, dsum);
+        }
+        if (l == HY - 1) {   // this CTA's part of node column jc0 + HY
+            T Sd[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) Sd[d] = P[6 + d] + (w > 0 ? z[((w - 1) * S::ZROW + HY) * 3 + d] : T(0));
+            if (r + 1 < CY) {
+                T *rem = cluster.map_shared_rank(s_recv, r + 1);
+#pragma unroll
+                for (int d = 0; d < 3; ++d) rem[at + d] = Sd[d];
+            } else if (tail_owner) {
+                const T uu[3] = {Uu[6], Uu[7], Uu[8]};
+                h_store<T, MODE>(L.at(p, g.ny, k), em[HY], Sd, uu, ef + 3 * HY, ed + 3 * HY, out, omega, dsum);
+            }
+        }
+    };
+
+    // One march step: element E0 + t - 1 between faces (Uc, Fc) and the next
+    // face (Un, Fn); Ac collects node plane E0 + t - 1, An starts plane E0 + t.
+    // The loop runs two steps per trip with the roles swapped, so no arrays
+    // are copied.
+    int cur = 0;   // the stage being consumed
+    bool fail = false;
+    auto step = [&](int t, T (&Uc)[12], T (&Fc)[12], T (&Ac)[12], T (&Un)[12], T (&Fn)[12], T (&An)[12]) {
+        cur = t;
+        wait_stage(t);
+        load_face(t, Un);
+#pragma unroll
+        for (int q = 0; q < 12; ++q) Fn[q] = Un[q];
+        face_h(Fn);
+        const T cx = reinterpret_cast<const T *>(smem + (t % HRING) * S::slot + S::c_off)[w * HY + l];
+        element_h(Fc, Fn, cx, hc, Ac, An);
+        const int p = E0 + t - 1;   // node plane finished by this element
+        const bool out_plane = p >= P0;
+        T q0[3];
+        if (out_plane) {
+            face_h(Ac);   // node partials of plane p
+            reduce_y(p, Ac, q0);
+        }
+        fail = __syncthreads_or(bad);   // z partners visible; ring slot t - 1 free
+        if (!fail && tid == 0 && t - 1 + HRING < nst) issue(t - 1 + HRING);
+        if (!fail && out_plane) emit(p, t, Ac, q0, Uc);
+    };
+    auto finish_last = [&](T (&Uc)[12], T (&Ac)[12]) {   // plane nx: only element nx - 1 touches it
+        cur = nE + 1;
+        wait_stage(nE + 1);
+        T q0[3];
+        face_h(Ac);
+        reduce_y(E1, Ac, q0);
+        fail = __syncthreads_or(bad);
+        if (!fail) emit(E1, nE + 1, Ac, q0, Uc);
+    };
+
+    T U0[12], F0[12], A0[12], U1[12], F1[12], A1[12];
+    wait_stage(0);
+    load_face(0, U0);
+#pragma unroll
+    for (int q = 0; q < 12; ++q) {
+        F0[q] = U0[q];
+        A0[q] = T(0);
+    }
+    face_h(F0);
+    fail = __syncthreads_or(bad);
+    int t = 1;
+    for (; !fail && t + 1 <= nE; t += 2) {
+        step(t, U0, F0, A0, U1, F1, A1);
+        if (!fail) step(t + 1, U1, F1, A1, U0, F0, A0);
+    }
+    if (!fail && t <= nE) {   // odd count: one more step, the state ends in set 1
+        step(t, U0, F0, A0, U1, F1, A1);
+        if (!fail && last_plane) finish_last(U1, A1);
+    } else if (!fail && last_plane) {
+        finish_last(U0, A0);
+    }
+    if (fail && tid == 0) {
+        // let the loads still in flight (stages cur .. issued - 1, each the
+        // latest phase of its slot) land before the CTA ends (bounded)
+        for (int s = cur; s < issued; ++s)
+            (void)mbar_wait_bounded(&bar[s % HRING], (uint32_t)((s / HRING) & 1), kHWaitPolls);
+        if (err) atomicExch(err, GPUTO_ERR_TIMEOUT);
+    }
+    cluster.sync();   // seam partials from the left neighbour have arrived
+    if (!fail && r > 0) {   // node column jc0, from both sides of the seam
+        const int np = P1 - P0;
+        for (int idx = tid; idx < np * WZ; idx += NT) {
+            const int pp = idx / WZ, ww = idx - pp * WZ;
+            const int k = kc0 + ww, p = P0 + pp, at = idx * 3;
+            if (!((ww >= 1 || zt == 0) && k <= g.nz)) continue;
+            T v[3], uu[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                v[d] = s_own[at + d] + s_recv[at + d];
+                uu[d] = s_ownu[at + d];
+            }
+            const long long base = L.at(p, jc0, k);
+            h_store<T, MODE>(base, mask[g.node(p, jc0, k)], v, uu, f + base, rdiag + base, out, omega, dsum);
+        }
+    }
+    if (MODE == MODE_APPLY && dot_partial) {
+        double *red = reinterpret_cast<double *>(smem + S::red_off);
+        for (int o = 16; o > 0; o >>= 1) dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
+        if (l == 0) red[w] = dsum;
+        __syncthreads();
+        if (tid == 0) {
+            double v = 0.0;
+            for (int q = 0; q < WZ; ++q) v += red[q];
+            dot_partial[blockIdx.x + gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z)] = v;
+        }
+    }
+}
+
+template <typename T> constexpr int hwz() { return 8; }
+
+// Row pitch of the padded mask copy: TMA needs 16-byte row strides.
+long long hmask_pitch(const Grid &g) { return ((long long)g.ny + 1 + 15) & ~15LL; }
+
+template <typename T>
+int hztiles(const Grid &g)
+{
+    constexpr int WZ = hwz<T>();
+    const int rest = g.nz + 1 - WZ;
+    return 1 + (rest > 0 ? (rest + WZ - 2) / (WZ - 1) : 0);
+}
+
+struct HState {
+    bool init = false, ok = false;
+    int resident[2][4][HMAXCY + 1] = {};   // [FP64?][mode][cluster size]: clusters resident on the device
+};
+
+HState &hstate(int dev)
+{
+    static HState st[64];
+    return st[dev < 64 ? dev : 63];
+}
+
+// Node planes per x chunk: whole rounds of resident clusters, few overlapping
+// elements, and a fixed cost per CTA of about four planes.
+template <typename T>
+int hchunk(const Grid &g, int mode)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int cy = (g.ny + HY - 1) / HY;
+    const int res = cy <= HMAXCY ? hstate(dev).resident[sizeof(T) == 8][mode & 3][cy] : 0;
+    if (res <= 0 || g.nx <= HTX) return g.nx <= HTX ? (g.nx > 0 ? g.nx : 1) : HTX;
+    const long long nzt = hztiles<T>(g);
+    long long best = -1;
+    int bh = HTX;
+    for (int ncx = (g.nx + HTX - 1) / HTX; ncx <= g.nx; ++ncx) {
+        const int htx = (g.nx + ncx - 1) / ncx;
+        const long long chunks = (g.nx + htx - 1) / htx;
+        const long long rounds = (nzt * chunks + res - 1) / res;
+        const long long cost = rounds * (htx + 1 + 4);
+        if (best < 0 || cost < best) {
+            best = cost;
+            bh = htx;
+        }
+        if (htx == 1) break;
+    }
+    return bh;
+}
+
+template <typename T>
+dim3 hgrid(const Grid &g, int htx)
+{
+    const int cy = (g.ny + HY - 1) / HY;
+    const int ncx = g.nx > htx ? (g.nx + htx - 1) / htx : 1;
+    return dim3((unsigned)cy, (unsigned)hztiles<T>(g), (unsigned)ncx);
+}
+
+template <typename T, int MODE>
+int hlaunch(const Lay &L, const ELay &E, const HadamardKe &hk, const T *CX, const T *u, const T *f, const T *rdiag,
+            const uint8_t *mask, const uint8_t *maskp, T *out, T omega, T prerelax, double *dot_partial,
+            const int *done, int *err, cudaStream_t st)
+{
+    constexpr int WZ = hwz<T>();
+    using N = HNeeds<MODE>;
+    using S = HSmem<T, WZ, MODE>;
+    const Grid &g = L.g;
+    const uint64_t es = sizeof(T);
+    // node-plane maps (u, f, diag) share one box: WZ + 1 rows of HUW values
+    auto node_map = [&](CUtensorMap *m, const T *base) {
+        return make_tmap_3d(m, base, (int)es, (uint64_t)L.pitch, (uint64_t)g.nz + 1, (uint64_t)g.nx + 1,
+                            L.pitch * es, L.pitch * es * (g.nz + 1), HUW, WZ + 1, 1);
+    };
+    CUtensorMap mu, md, mf, mc, mm;
+    int s = node_map(&mu, N::PRE ? f : u);
+    if (!s && N::D) s = node_map(&md, rdiag);
+    if (!s && N::F) s = node_map(&mf, f);
+    if (!s)
+        s = make_tmap_3d(&mc, CX, (int)es, (uint64_t)E.pitch, (uint64_t)E.g.nz, (uint64_t)E.g.nx, E.pitch * es,
+                         E.pitch * es * E.g.nz, HY, WZ, 1);
+    const uint64_t mp = hmask_pitch(g);
+    if (!s)
+        s = make_tmap_3d(&mm, maskp, 1, mp, (uint64_t)g.nz + 1, (uint64_t)g.nx + 1, mp, mp * (g.nz + 1), HM, WZ, 1);
+    if (s) return s;
+    if (!N::D) md = mu;
+    if (!N::F) mf = mu;
+    HC<T> hc;
+    hc.a = (T)(hk.c[0] / 64.0);
+    hc.bc = (T)((hk.c[1] - hk.c[2]) / 64.0);
+    hc.c = (T)(hk.c[2] / 64.0);
+    hc.de = (T)((hk.c[3] - hk.c[4]) / 64.0);
+    hc.e = (T)(hk.c[4] / 64.0);
+    hc.f = (T)(hk.c[5] / 64.0);
+    hc.g = (T)(hk.c[6] / 64.0);
+    hc.h = (T)(hk.c[7] / 64.0);
+    const int htx = hchunk<T>(g, MODE);
+    const dim3 grid = hgrid<T>(g, htx);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(32 * WZ);
+    cfg.dynamicSmemBytes = S::bytes;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = grid.x;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    GPUTO_CUDA(cudaLaunchKernelEx(&cfg, hsweep_kernel<T, MODE, WZ>, mu, md, mf, mc, mm, L, hc, htx, f, rdiag, mask,
+                                  out, omega, prerelax, dot_partial, done, err));
+    count_launches(1);
+    return GPUTO_OK;
+}
+
+template <typename T, int MODE>
+cudaError_t hset_attr()
+{
+    return cudaFuncSetAttribute(hsweep_kernel<T, MODE, hwz<T>()>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)HSmem<T, hwz<T>(), MODE>::bytes);
+}
+
+template <typename T>
+cudaError_t hset_attrs()
+{
+    cudaError_t e;
+    if ((e = hset_attr<T, MODE_APPLY>()) != cudaSuccess) return e;
+    if ((e = hset_attr<T, MODE_DEFECT>()) != cudaSuccess) return e;
+    if ((e = hset_attr<T, MODE_JACOBI>()) != cudaSuccess) return e;
+    return hset_attr<T, MODE_JACOBI_PRE>();
+}
+
+// Clusters of 'cy' CTAs of one kernel instance that the device holds at once
+// (0: none fit).
+template <typename T, int MODE>
+int hresident(int cy)
+{
+    constexpr int WZ = hwz<T>();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)cy, 1, 1);
+    cfg.blockDim = dim3(32 * WZ);
+    cfg.dynamicSmemBytes = HSmem<T, WZ, MODE>::bytes;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)cy;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, hsweep_kernel<T, MODE, WZ>, &cfg) != cudaSuccess) return 0;
+    return n;
+}
+
+template <typename T>
+void hresident_all(HState &s, int cy)
+{
+    const int p = sizeof(T) == 8;
+    s.resident[p][MODE_APPLY][cy] = hresident<T, MODE_APPLY>(cy);
+    s.resident[p][MODE_DEFECT][cy] = hresident<T, MODE_DEFECT>(cy);
+    s.resident[p][MODE_JACOBI][cy] = hresident<T, MODE_JACOBI>(cy);
+    s.resident[p][MODE_JACOBI_PRE][cy] = hresident<T, MODE_JACOBI_PRE>(cy);
+}
+
+__global__ void pad_mask_kernel(Grid g, const uint8_t *__restrict__ mask, uint8_t *__restrict__ maskp, long long mp)
+{
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= g.nnod()) return;
+    const long long row = n / (g.ny + 1);
+    maskp[row * mp + (n - row * (g.ny + 1))] = mask[n];
+}
+
+}  // namespace
+
+bool hadamard_ke(const double *Ke, HadamardKe *hk)
+{
+    hk->ok = false;
+    // S = T Ke T' with T[m][b] = (-1)^(px x_b + py y_b + pz z_b), m = 4 px + 2 py + pz
+    double T8[8][8];
+    for (int m = 0; m < 8; ++m)
+        for (int b = 0; b < 8; ++b) {
+            const int e = ((m >> 2) & 1) * local_x(b) + ((m >> 1) & 1) * local_y(b) + (m & 1) * local_z(b);
+            T8[m][b] = (e & 1) ? -1.0 : 1.0;
+        }
+    static thread_local double S[24][24], tmp[24][24];
+    for (int m = 0; m < 8; ++m)
+        for (int d = 0; d < 3; ++d)
+            for (int col = 0; col < 24; ++col) {
+                double s = 0.0;
+                for (int b = 0; b < 8; ++b) s += T8[m][b] * Ke[(3 * b + d) * 24 + col];
+                tmp[3 * m + d][col] = s;
+            }
+    double big = 0.0;
+    for (int row = 0; row < 24; ++row)
+        for (int n = 0; n < 8; ++n)
+            for (int d = 0; d < 3; ++d) {
+                double s = 0.0;
+                for (int b = 0; b < 8; ++b) s += tmp[row][3 * b + d] * T8[n][b];
+                S[row][3 * n + d] = s;
+                big = std::fmax(big, std::fabs(s));
+            }
+    if (!(big > 0.0)) return false;
+    auto R = [](int m, int d) { return 3 * m + d; };
+    const double a = S[R(1, 0)][R(1, 0)], b = S[R(1, 2)][R(1, 2)], c = S[R(1, 2)][R(2, 1)],
+                 dd = S[R(3, 0)][R(3, 0)], e = S[R(3, 0)][R(5, 1)], f = S[R(3, 1)][R(3, 1)],
+                 gg = S[R(3, 1)][R(5, 0)], h = S[R(7, 0)][R(7, 0)];
+    static thread_local double M[24][24];
+    for (int i = 0; i < 24; ++i)
+        for (int j = 0; j < 24; ++j) M[i][j] = 0.0;
+    const int pa[3][2][2] = {{{1, 0}, {4, 2}}, {{1, 1}, {2, 2}}, {{2, 0}, {4, 1}}};
+    for (auto &gp : pa)
+        for (auto &x : gp)
+            for (auto &y : gp) M[R(x[0], x[1])][R(y[0], y[1])] = a;
+    const int tb[2][3][2] = {{{1, 2}, {2, 1}, {4, 0}}, {{3, 0}, {5, 1}, {6, 2}}};
+    for (int q = 0; q < 2; ++q)
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                M[R(tb[q][i][0], tb[q][i][1])][R(tb[q][j][0], tb[q][j][1])] =
+                    i == j ? (q ? dd : b) : (q ? e : c);
+    const int pf[3][2][2] = {{{3, 1}, {5, 0}}, {{3, 2}, {6, 0}}, {{5, 2}, {6, 1}}};
+    for (auto &gp : pf)
+        for (int i = 0; i < 2; ++i)
+            for (int j = 0; j < 2; ++j) M[R(gp[i][0], gp[i][1])][R(gp[j][0], gp[j][1])] = i == j ? f : gg;
+    for (int d = 0; d < 3; ++d) M[R(7, d)][R(7, d)] = h;
+    double dev = 0.0;
+    for (int i = 0; i < 24; ++i)
+        for (int j = 0; j < 24; ++j) dev = std::fmax(dev, std::fabs(S[i][j] - M[i][j]));
+    if (!(dev <= 1e-12 * big)) return false;
+    const double v[8] = {a, b, c, dd, e, f, gg, h};
+    for (int q = 0; q < 8; ++q) hk->c[q] = v[q];
+    hk->ok = true;
+    return true;
+}
+
+int init_hsweep_kernels()
+{
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    int dev = 0;
+    GPUTO_CUDA(cudaGetDevice(&dev));
+    HState &s = hstate(dev);
+    if (s.init) return GPUTO_OK;
+    s.init = true;
+    if (hset_attrs<float>() != cudaSuccess || hset_attrs<double>() != cudaSuccess) {
+        cudaGetLastError();
+        return GPUTO_OK;   // the dense kernel serves every sweep
+    }
+    for (int cy = 1; cy <= HMAXCY; ++cy) {
+        hresident_all<float>(s, cy);
+        hresident_all<double>(s, cy);
+    }
+    cudaGetLastError();
+    s.ok = true;
+    return GPUTO_OK;
+}
+
+template <typename T>
+bool hsweep_fits(const Grid &g)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    const HState &s = hstate(dev);
+    const int cy = (g.ny + HY - 1) / HY;
+    if (!s.ok || cy < 1 || cy > HMAXCY || g.nx < 1 || g.nz < 1) return false;
+    const int p = sizeof(T) == 8;
+    for (int m = 0; m < 4; ++m)
+        if (s.resident[p][m][cy] <= 0) return false;
+    return true;
+}
+
+template <typename T>
+int hsweep_blocks(const Grid &g)
+{
+    const dim3 gr = hgrid<T>(g, hchunk<T>(g, MODE_APPLY));
+    return (int)(gr.x * gr.y * gr.z);
+}
+
+long long hsweep_mask_bytes(const Grid &g) { return hmask_pitch(g) * (g.nz + 1) * (g.nx + 1); }
+
+void launch_pad_mask(const Grid &g, const uint8_t *mask, uint8_t *maskp, cudaStream_t st)
+{
+    pad_mask_kernel<<<(unsigned)((g.nnod() + 255) / 256), 256, 0, st>>>(g, mask, maskp, hmask_pitch(g));
+    count_launches(1);
+}
+
+template <typename T>
+int launch_hsweep(int mode, const Lay &L, const ELay &E, const HadamardKe &hk, const T *CX, const T *u, const T *f,
+                  const T *rdiag, const uint8_t *mask, const uint8_t *maskp, T *out, T omega, T prerelax,
+                  double *dot_partial, const int *done, int *err, cudaStream_t st)
+{
+    switch (mode) {
+    case MODE_APPLY:
+        return hlaunch<T, MODE_APPLY>(L, E, hk, CX, u, f, rdiag, mask, maskp, out, omega, prerelax, dot_partial, done,
+                                      err, st);
+    case MODE_DEFECT:
+        return hlaunch<T, MODE_DEFECT>(L, E, hk, CX, u, f, rdiag, mask, maskp, out, omega, prerelax, nullptr, done,
+                                       err, st);
+    case MODE_JACOBI:
+        return hlaunch<T, MODE_JACOBI>(L, E, hk, CX, u, f, rdiag, mask, maskp, out, omega, prerelax, nullptr, done,
+                                       err, st);
+    default:
+        return hlaunch<T, MODE_JACOBI_PRE>(L, E, hk, CX, u, f, rdiag, mask, maskp, out, omega, prerelax, nullptr,
+                                           done, err, st);
+    }
+}
+
+template bool hsweep_fits<float>(const Grid &);
+template bool hsweep_fits<double>(const Grid &);
+template int hsweep_blocks<float>(const Grid &);
+template int hsweep_blocks<double>(const Grid &);
+template int launch_hsweep<float>(int, const Lay &, const ELay &, const HadamardKe &, const float *, const float *,
+                                  const float *, const float *, const uint8_t *, const uint8_t *, float *, float,
+                                  float, double *, const int *, int *, cudaStream_t);
+template int launch_hsweep<double>(int, const Lay &, const ELay &, const HadamardKe &, const double *,
+                                   const double *, const double *, const double *, const uint8_t *,
+                                   const uint8_t *, double *, double, double, double *, const int *, int *,
+                                   cudaStream_t);
+
+}  // namespace gputo

@@ -71,6 +71,7 @@ int Solver::alloc_levels(LevelBuf<T> *Lv, bool with_matrices)
         ALLOC(b.u0, nv);
         ALLOC(b.r, nv);
         ALLOC(b.diag, nv);
+        if (l == 0 || (redisc() && l < nl - 1)) ALLOC(b.rdiag, nv);   // levels with fine sweeps
         ALLOC(b.u1, nv);
         ALLOC(b.f, nv);
         // level 1 is applied matrix-free unless it is the coarsest level; the
@@ -122,11 +123,15 @@ int Solver::create(int nelx, int nely, int nelz, int nl_, const gputo_options *o
     GPUTO_CUDA(cudaGetDevice(&device));
     GPUTO_CUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
     int ik = init_fine_kernels();
+    if (!ik) ik = init_hsweep_kernels();
     if (!ik && opt.precision == GPUTO_PREC_MIXED) ik = init_tc_sweep_kernels();
     if (ik) return ik;
 
     const long long nv = lay[0].size(), ne = g[0].nel();
-    for (int l = 0; l < nl; ++l) ALLOC(mask[l], (g[l].nnod() + 3) & ~3LL);
+    for (int l = 0; l < nl; ++l) {
+        ALLOC(mask[l], (g[l].nnod() + 3) & ~3LL);
+        ALLOC(maskp[l], hsweep_mask_bytes(g[l]));
+    }
     ALLOC(CX, ne);
     ALLOC(CXp, elay.size());
     ALLOC(R, nv);
@@ -165,7 +170,7 @@ int Solver::create(int nelx, int nely, int nelz, int nl_, const gputo_options *o
     ALLOC(LinvT, (long long)nc * nc);
     ALLOC(ctmp, nc);
     if (nl == 1) ALLOC(Apk0, 300 * g[0].nel());
-    partial_cap = std::max(fine_sweep_blocks(g[0]), 1 << 12);
+    partial_cap = std::max({fine_sweep_blocks(g[0]), hsweep_blocks<double>(g[0]), 1 << 12});
     ALLOC(partial, partial_cap);
     ALLOC(ticket, 4);
     ALLOC(sc, 1);
@@ -202,6 +207,13 @@ int Solver::set_problem(const double *Ke0, const double *fixed1b, int nfd, cudaS
     std::memcpy(Ke, Ke0, sizeof(Ke));
     int s1 = upload_fine_ke(Ke, st);
     if (s1) return s1;
+    HadamardKe nhk;
+    hadamard_ke(Ke, &nhk);
+    if (graph_exec && (nhk.ok != hk.ok || std::memcmp(nhk.c, hk.c, sizeof(hk.c)) != 0)) {
+        cudaGraphExecDestroy(graph_exec);   // the captured sweeps carry the constants
+        graph_exec = nullptr;
+    }
+    hk = nhk;
     s1 = upload_quadrature_parts(opt.nu, st);
     if (s1) return s1;
     // the fixed list: unchanged lists are not re-uploaded
@@ -221,6 +233,7 @@ int Solver::set_problem(const double *Ke0, const double *fixed1b, int nfd, cudaS
                                        cudaMemcpyHostToDevice, st));
         launch_mask_from_list((g[0].nnod() + 3) & ~3LL, fixed_dev, nfd, mask[0], st);
         for (int l = 1; l < nl; ++l) launch_mask_restrict(g[l], mask[l - 1], mask[l], st);
+        for (int l = 0; l < nl; ++l) launch_pad_mask(g[l], mask[l], maskp[l], st);
         GPUTO_CUDA(cudaStreamSynchronize(st));
         fixed_host.swap(list);
     }
@@ -234,7 +247,8 @@ int Solver::check_error_flags(cudaStream_t st)
     GPUTO_CUDA(cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st));
     GPUTO_CUDA(cudaStreamSynchronize(st));
     if (h_err) {
-        set_error("a bounded wait for a TMA tile load gave up");
+        set_error(h_err == GPUTO_ERR_TIMEOUT ? "a bounded wait for a TMA tile load gave up"
+                                             : "a fine sweep found its shared memory misaligned for TMA");
         cudaMemsetAsync(err, 0, sizeof(int), st);
         return h_err;
     }
@@ -288,7 +302,11 @@ int Solver::setup(const double *CX_in, cudaStream_t st)
             if (L[l].Apk) launch_cast_f32(300 * g[l].nel(), L[l].Apk, Lf[l].Apk, st);
             launch_cast_f32(lay[l].size(), L[l].diag, Lf[l].diag, st);
         }
+        for (int l = 0; l < nl; ++l)
+            if (Lf[l].rdiag) launch_recip<float>(lay[l].size(), L[l].diag, Lf[l].rdiag, st);
     }
+    for (int l = 0; l < nl; ++l)
+        if (L[l].rdiag) launch_recip<double>(lay[l].size(), L[l].diag, L[l].rdiag, st);
     int h_info = 0;
     GPUTO_CUDA(cudaMemcpyAsync(&h_info, info, sizeof(int), cudaMemcpyDeviceToHost, st));
     GPUTO_CUDA(cudaStreamSynchronize(st));
@@ -321,15 +339,13 @@ void Solver::vcycle_impl(LevelBuf<T> *Lv, const T *CXl, const T *r0, T *z0, cons
                     return;
                 }
             }
-            note(launch_fine_sweep<T>(mode, lay[0], elay, CXl, u, f, Lv[0].diag, mask[0], out, w, pr,
-                                      nullptr, done, err, st));
+            note(fine_sweep<T>(0, mode, lay[0], elay, CXl, u, f, Lv[0], out, w, pr, nullptr, done, st));
         }
         else if (redisc()) {
             const T *cxl;
             if constexpr (std::is_same<T, float>::value) cxl = CXrpf[l];
             else cxl = CXrp[l];
-            note(launch_fine_sweep<T>(mode, lay[l], elayr[l], cxl, u, f, Lv[l].diag, mask[l], out, w, pr, nullptr,
-                                      done, err, st));
+            note(fine_sweep<T>(l, mode, lay[l], elayr[l], cxl, u, f, Lv[l], out, w, pr, nullptr, done, st));
         } else if (l == 1 && quad_level1())
             note(launch_quad_sweep<T>(mode, lay[1], elay, CXl, u, f, Lv[1].diag, mask[1], out, w, pr,
                                       opt.nu, Lv[1].yq, done, err, st));
@@ -489,8 +505,7 @@ int Solver::attach_net(Net *n, int mode)
 
 void Solver::apply(const double *u, double *r, double *dot_partial, const int *done, cudaStream_t st)
 {
-    note(launch_fine_sweep<double>(MODE_APPLY, lay[0], elay, CXp, u, nullptr, L[0].diag, mask[0], r,
-                                   1.0, 0.0, dot_partial, done, err, st));
+    note(fine_sweep<double>(0, MODE_APPLY, lay[0], elay, CXp, u, nullptr, L[0], r, 1.0, 0.0, dot_partial, done, st));
 }
 
 // One PCG iteration (mgcg1.cu:254-275), every scalar on the device.
@@ -499,7 +514,7 @@ void Solver::iteration(cudaStream_t st)
     const long long nv = lay[0].size();
     const int *done = &sc->done;
     apply(P, Q, partial, done, st);
-    launch_finish_apply_dot(fine_sweep_blocks(g[0]), partial, ticket, sc, st);
+    launch_finish_apply_dot(apply_blocks(), partial, ticket, sc, st);
     launch_pcg_update(nv, Uw, R, P, Q, partial, ticket, sc, st);
     vcycle(R, Z, done, st);
     if (Zold) {
@@ -607,6 +622,7 @@ int Solver::solve(const double *Fp, double *Up, double tol, int maxit, double *r
 int Solver::set_tunables(const gputo_options &o)
 {
     if (o.nswp < 0 || o.check_every < 1 || !(o.omega > 0) || o.tc_parts < 0 || o.tc_parts > 2 || o.tc_xchunk < 0 ||
+        o.fine_op < 0 || o.fine_op > 1 ||
         (o.tc_parts > 0 && opt.precision != GPUTO_PREC_MIXED)) {
         set_error("invalid solver options");
         return GPUTO_ERR_ARG;
@@ -618,6 +634,7 @@ int Solver::set_tunables(const gputo_options &o)
     opt.use_graph = o.use_graph;
     opt.tc_parts = o.tc_parts;
     opt.tc_xchunk = o.tc_xchunk;
+    opt.fine_op = o.fine_op;
     if (graph_exec) {
         cudaGraphExecDestroy(graph_exec);
         graph_exec = nullptr;

@@ -17,6 +17,7 @@ struct Solver {
     cudaStream_t own_stream = nullptr;
 
     double Ke[576]{};
+    HadamardKe hk{};           // Ke in its Hadamard basis (ok = false: dense sweeps only)
     bool have_problem = false, ready = false;
     std::vector<double> fixed_host;
     double *fixed_dev = nullptr;
@@ -31,6 +32,7 @@ struct Solver {
     double *CX = nullptr, *CXp = nullptr;
     float *CXpf = nullptr;
     uint8_t *mask[kMaxLevels]{};
+    uint8_t *maskp[kMaxLevels]{};   // the same, rows padded to 16 bytes (Hadamard-basis sweeps)
     LevelBuf<double> L[kMaxLevels];
     // FP32 preconditioner copies (mixed precision)
     LevelBuf<float> Lf[kMaxLevels];
@@ -87,6 +89,26 @@ struct Solver {
     void vcycle(const double *r, double *z, const int *done, cudaStream_t st);
     void apply(const double *u, double *r, double *dot_partial, const int *done, cudaStream_t st);
     cudaStream_t stream(void *s) const { return s ? (cudaStream_t)s : own_stream; }
+    // Fine-operator sweep on a grid with K = sum CX_e Ke: the Hadamard-basis
+    // kernel when it applies, else the dense element rows.
+    template <typename T>
+    bool use_hsweep(const Grid &gr) const { return opt.fine_op == 0 && hk.ok && hsweep_fits<T>(gr); }
+    template <typename T>
+    int fine_sweep(int l, int mode, const Lay &Lo, const ELay &E, const T *CXl, const T *u, const T *f,
+                   const LevelBuf<T> &B, T *out, T omega, T pr, double *dot_partial, const int *done,
+                   cudaStream_t st) const
+    {
+        if (use_hsweep<T>(Lo.g) && B.rdiag)
+            return launch_hsweep<T>(mode, Lo, E, hk, CXl, u, f, B.rdiag, mask[l], maskp[l], out, omega, pr,
+                                    dot_partial, done, err, st);
+        return launch_fine_sweep<T>(mode, Lo, E, CXl, u, f, B.diag, mask[l], out, omega, pr, dot_partial, done, err,
+                                    st);
+    }
+    // Per-CTA partials written by the FP64 fine apply.
+    int apply_blocks() const
+    {
+        return use_hsweep<double>(g[0]) && L[0].rdiag ? hsweep_blocks<double>(g[0]) : fine_sweep_blocks(g[0]);
+    }
     // Level 1 is applied matrix-free from the fine CX whenever it is not the
     // coarsest level (then it needs assembled matrices for the direct solve).
     bool quad_level1() const { return nl >= 3 && !redisc(); }

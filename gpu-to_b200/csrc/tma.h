@@ -9,7 +9,8 @@
 
 namespace gputo {
 
-// Encode a 3-D tiled tensor map over a row-padded array:
+// Encode a 3-D tiled tensor map over a row-padded array of doubles, floats or
+// bytes (elem_bytes 8, 4 or 1):
 //   dims (inner, mid, outer) in elements, byte strides of mid and outer,
 //   box (b0, b1, b2) in elements.  Out-of-range elements of a box read as 0.
 // Returns 0 on success.

@@ -52,7 +52,7 @@ _fp = ctypes.POINTER(ctypes.c_float)
 class Options(ctypes.Structure):
     _fields_ = [("precision", _i), ("nswp", _i), ("omega", _d), ("prerelax", _d), ("nu", _d),
                 ("check_every", _i), ("use_graph", _i), ("max_coarse_dofs", _i), ("tc_parts", _i),
-                ("tc_xchunk", _i), ("coarse", _i)]
+                ("tc_xchunk", _i), ("coarse", _i), ("fine_op", _i)]
 
 
 SIGNATURES = {
@@ -61,6 +61,7 @@ SIGNATURES = {
     "gputo_version": (ctypes.c_char_p, []),
     "gputo_default_options": (None, [ctypes.POINTER(Options)]),
     "gputo_hex8_stiffness": (_i, [_d, _d, _dp]),
+    "gputo_fine_op_constants": (_i, [_dp, _dp]),
     "gputo_mgcg1": (_i, [_dp, _dp, _dp, _dp, _dp, _i, _i, _i, _i, _i, _d, _i, _i, _dp, _ip]),
     "gputo_mgcg1_ex": (_i, [_dp, _dp, _dp, _dp, _dp, _i, _i, _i, _i, _i, _d, _i, _i,
                             ctypes.POINTER(Options), _dp, _ip]),
@@ -164,6 +165,15 @@ def hex8_stiffness(nu=0.3, h=1.0) -> np.ndarray:
     Ke = np.zeros(576)
     _check(_lib.gputo_hex8_stiffness(float(nu), float(h), _p(Ke)), "gputo_hex8_stiffness")
     return Ke.reshape(24, 24)
+
+
+def fine_op_constants(Ke):
+    """The eight Hadamard-basis constants of Ke, or None when Ke lacks the
+    pattern (then the fine sweeps use dense element rows)."""
+    Ke = np.ascontiguousarray(Ke, dtype=np.float64).reshape(-1)
+    c = np.zeros(8)
+    st = _lib.gputo_fine_op_constants(_p(Ke), _p(c))
+    return c if st == GPUTO_OK else None
 
 
 def cantilever(nelx, nely, nelz):

@@ -84,6 +84,11 @@ typedef struct {
     int tc_xchunk;       /* node planes per CTA of the tensor-core smoother
                             (0 = 16)                                              */
     int coarse;          /* gputo_coarse                                          */
+    int fine_op;         /* fine-level sweeps: 0 = the element matrix in its
+                            Hadamard basis when Ke has the structure of an
+                            isotropic cube element and nely <= 256 (fewer
+                            operations, same results to rounding), else dense
+                            element rows; 1 = always dense element rows       */
 } gputo_options;
 
 void gputo_default_options(gputo_options *opt);
@@ -94,6 +99,14 @@ void gputo_default_options(gputo_options *opt);
  * (top3D125modCuda.m:50-77) and Kem3 (Cantilever/omp/mgcg1.c:1370).  Host
  * only; needs no GPU. */
 int gputo_hex8_stiffness(double nu, double h, double *Ke);
+
+/* The eight constants of Ke in the element's Hadamard basis (S = T Ke T', T
+ * the 2x2x2 Hadamard transform over the element's corners): a, b, c, d, e,
+ * f, g, h of the 45-entry pattern that the fine sweeps with fine_op = 0 use.
+ * Returns GPUTO_OK when Ke has that pattern to 1e-12 relative (every
+ * isotropic cube element does), GPUTO_ERR_ARG when it does not; such a Ke
+ * runs on the dense element-row sweeps.  Host only; no reference counterpart. */
+int gputo_fine_op_constants(const double *Ke, double *c8);
 
 /* ---------------------------------------------------------------------- */
 /* Drop-in MEX replacement                                                  */
