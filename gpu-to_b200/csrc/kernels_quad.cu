@@ -12,24 +12,45 @@
 //   2. one thread per node: the sum of its rows of y over the (up to) 8
 //      elements around it, followed by the same epilogues as the other sweeps
 //      (K u, f - K u, damped Jacobi, Dirichlet rows zeroed).
-// The strain-displacement values at the Gauss points are compile-time
-// constants, so pass 1 costs about 1250 FMAs per element with no table reads.
+// Pass 1 works in the Hadamard basis of the element's corners: with
+// V = T u, T[p][c] = (-1)^(p.c), the trilinear displacement is
+// u(xi) = (1/8) sum_p (-1)^|p| xi^p V_p.  A derivative along one axis needs
+// only the four modes with that axis' bit set and does not vary along that
+// axis, so the gradients at all 8 Gauss points cost 72 operations; the
+// adjoint sum_g B_g^T sigma_g comes back as y = (1/8) T W, W built from sums
+// of the stress over the Gauss points.  About 530 operations per element
+// instead of 1250 FMAs for the strain-displacement products.
 #include "gputo_internal.h"
 
 namespace gputo {
 
-// dN_a/dx_p at Gauss point (ix, iy, iz) of a cube of edge h = 2:
-// 0.25 * sgn_p(a) * (product of (1 + sgn_q(a) gp_q) over the other axes) / h.
-__host__ __device__ constexpr double gauss_coord(int i) { return i ? 0.57735026918962576451 : -0.57735026918962576451; }
-__host__ __device__ constexpr double sgn(int v) { return v ? 1.0 : -1.0; }
-__host__ __device__ constexpr double dN(int a, int p, int ix, int iy, int iz)
+// Hadamard transform of 8 values indexed by c = 4 x + 2 y + z:
+// x_p <- sum_c (-1)^(p.c) x_c.
+template <typename T>
+__device__ __forceinline__ void fwht8(T (&x)[8])
 {
-    const double fx = 1.0 + sgn(local_x(a)) * gauss_coord(ix);
-    const double fy = 1.0 + sgn(local_y(a)) * gauss_coord(iy);
-    const double fz = 1.0 + sgn(local_z(a)) * gauss_coord(iz);
-    return p == 0 ? 0.125 * sgn(local_x(a)) * fy * fz
-         : p == 1 ? 0.125 * sgn(local_y(a)) * fx * fz
-                  : 0.125 * sgn(local_z(a)) * fx * fy;
+#pragma unroll
+    for (int b = 1; b < 8; b <<= 1)
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+            if (!(i & b)) {
+                const T u = x[i], v = x[i | b];
+                x[i] = u + v;
+                x[i | b] = u - v;
+            }
+}
+
+// Signed sums of P[i][j] (sign of the i-th and j-th Gauss coordinate):
+// H = [sum P, sum s_i P, sum s_j P, sum s_i s_j P].
+template <typename T>
+__device__ __forceinline__ void h22(const T (&P)[2][2], T (&H)[4])
+{
+    const T r0 = P[0][0] + P[0][1], r1 = P[1][0] + P[1][1];
+    const T q0 = P[0][1] - P[0][0], q1 = P[1][1] - P[1][0];
+    H[0] = r0 + r1;
+    H[1] = r1 - r0;
+    H[2] = q0 + q1;
+    H[3] = q1 - q0;
 }
 
 template <typename T, bool PRE>
@@ -61,9 +82,43 @@ quad_element_kernel(Lay L, const T *__restrict__ CXp, ELay Ef,
             }
         }
     }
-    T ye[24];
+    // corner a -> index c = 4 x + 2 y + z; modes p use the same bits
+    T V[3][8];
 #pragma unroll
-    for (int m = 0; m < 24; ++m) ye[m] = T(0);
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) V[d][4 * local_x(a) + 2 * local_y(a) + local_z(a)] = ue[3 * a + d];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) fwht8(V[d]);
+    const T s = T(0.57735026918962576451);   // Gauss coordinate 1/sqrt(3)
+    // 8 x displacement gradient: Gx[d][iy][iz] = 8 du_d/dx at Gauss points
+    // (., iy, iz), Gy[d][ix][iz], Gz[d][ix][iy] likewise
+    T Gx[3][2][2], Gy[3][2][2], Gz[3][2][2];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const T si = i ? s : -s;
+            const T ax = fma(si, V[d][6], -V[d][4]), bx = fma(-si, V[d][7], V[d][5]);
+            const T ay = fma(si, V[d][6], -V[d][2]), by = fma(-si, V[d][7], V[d][3]);
+            const T az = fma(si, V[d][5], -V[d][1]), bz = fma(-si, V[d][7], V[d][3]);
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const T sj = j ? s : -s;
+                Gx[d][i][j] = fma(sj, bx, ax);
+                Gy[d][i][j] = fma(sj, by, ay);
+                Gz[d][i][j] = fma(sj, bz, az);
+            }
+        }
+    // stress at each Gauss point, summed over the axis its column does not
+    // depend on: Px[d][iy][iz] = sum_ix sigma[d][x], Py[d][ix][iz], Pz[d][ix][iy]
+    T Px[3][2][2], Py[3][2][2], Pz[3][2][2];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) Px[d][i][j] = Py[d][i][j] = Pz[d][i][j] = T(0);
 #pragma unroll
     for (int ix = 0; ix < 2; ++ix)
 #pragma unroll
@@ -71,38 +126,43 @@ quad_element_kernel(Lay L, const T *__restrict__ CXp, ELay Ef,
 #pragma unroll
             for (int iy = 0; iy < 2; ++iy) {
                 const T c = CXp[Ef.at(2 * i + ix, 2 * j + iy, 2 * k + iz)];
-                // displacement gradient G[d][p] = sum_a dN_a/dx_p u_{a,d}
-                T G[3][3];
-#pragma unroll
-                for (int d = 0; d < 3; ++d)
-#pragma unroll
-                    for (int p = 0; p < 3; ++p) {
-                        T s = T(0);
-#pragma unroll
-                        for (int a = 0; a < 8; ++a) s = fma(T(dN(a, p, ix, iy, iz)), ue[3 * a + d], s);
-                        G[d][p] = s;
-                    }
-                // sigma = CX (lam tr(eps) I + 2 mu eps), eps = sym(G)
-                const T tr = G[0][0] + G[1][1] + G[2][2];
-                const T cl = c * lam, cm = c * mu;
-                T S[3][3];
-                S[0][0] = fma(cl, tr, T(2) * cm * G[0][0]);
-                S[1][1] = fma(cl, tr, T(2) * cm * G[1][1]);
-                S[2][2] = fma(cl, tr, T(2) * cm * G[2][2]);
-                S[0][1] = S[1][0] = cm * (G[0][1] + G[1][0]);
-                S[1][2] = S[2][1] = cm * (G[1][2] + G[2][1]);
-                S[0][2] = S[2][0] = cm * (G[0][2] + G[2][0]);
-                // y_{a,d} += sum_p dN_a/dx_p sigma[d][p]
-#pragma unroll
-                for (int a = 0; a < 8; ++a)
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) {
-                        T s = ye[3 * a + d];
-#pragma unroll
-                        for (int p = 0; p < 3; ++p) s = fma(T(dN(a, p, ix, iy, iz)), S[d][p], s);
-                        ye[3 * a + d] = s;
-                    }
+                const T cl = c * lam, cm = c * mu, cm2 = cm + cm;   // lam, mu carry 1/64
+                const T g00 = Gx[0][iy][iz], g01 = Gy[0][ix][iz], g02 = Gz[0][ix][iy];
+                const T g10 = Gx[1][iy][iz], g11 = Gy[1][ix][iz], g12 = Gz[1][ix][iy];
+                const T g20 = Gx[2][iy][iz], g21 = Gy[2][ix][iz], g22 = Gz[2][ix][iy];
+                const T tr = g00 + g11 + g22;
+                const T s00 = fma(cl, tr, cm2 * g00), s11 = fma(cl, tr, cm2 * g11), s22 = fma(cl, tr, cm2 * g22);
+                const T s01 = cm * (g01 + g10), s02 = cm * (g02 + g20), s12 = cm * (g12 + g21);
+                Px[0][iy][iz] += s00;
+                Px[1][iy][iz] += s01;
+                Px[2][iy][iz] += s02;
+                Py[0][ix][iz] += s01;
+                Py[1][ix][iz] += s11;
+                Py[2][ix][iz] += s12;
+                Pz[0][ix][iy] += s02;
+                Pz[1][ix][iy] += s12;
+                Pz[2][ix][iy] += s22;
             }
+    T ye[24];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        T X[4], Y[4], Z[4];   // [00, 10, 01, 11]: sums weighted by the signs of the two Gauss coordinates
+        h22(Px[d], X);
+        h22(Py[d], Y);
+        h22(Pz[d], Z);
+        T W[8];
+        W[0] = T(0);
+        W[1] = -Z[0];
+        W[2] = -Y[0];
+        W[3] = s * (Y[2] + Z[2]);
+        W[4] = -X[0];
+        W[5] = s * (X[2] + Z[1]);
+        W[6] = s * (X[1] + Y[1]);
+        W[7] = -(s * s) * (X[3] + Y[3] + Z[3]);
+        fwht8(W);
+#pragma unroll
+        for (int a = 0; a < 8; ++a) ye[3 * a + d] = W[4 * local_x(a) + 2 * local_y(a) + local_z(a)];
+    }
 #pragma unroll
     for (int m = 0; m < 24; ++m) y[(long long)m * nel + e] = ye[m];
 }
@@ -171,8 +231,10 @@ int launch_quad_sweep(int mode, const Lay &L, const ELay &Ef, const T *CX, const
                       const T *diag, const uint8_t *mask, T *out, T omega, T prerelax, double nu,
                       T *yscratch, const int *done, int *, cudaStream_t st)
 {
-    const T lam = (T)(nu / ((1.0 + nu) * (1.0 - 2.0 * nu)));
-    const T mu = (T)(1.0 / (2.0 * (1.0 + nu)));
+    // Lame constants of the unit-modulus material, with the 1/64 of the two
+    // Hadamard transforms folded in
+    const T lam = (T)(nu / ((1.0 + nu) * (1.0 - 2.0 * nu)) / 64.0);
+    const T mu = (T)(1.0 / (2.0 * (1.0 + nu)) / 64.0);
     const int bs = 128;
     const unsigned eb = (unsigned)((L.g.nel() + bs - 1) / bs);
     const unsigned nb = (unsigned)((L.g.nnod() + bs - 1) / bs);
