@@ -237,12 +237,15 @@ void launch_recip(long long n, const double *in, T *out, cudaStream_t st);
 int reduce_partials_capacity();
 void launch_dot(long long n, const double *a, const double *b, double *partial, unsigned *ticket,
                 PcgScalars *sc, int which, const int *done, cudaStream_t st);
+// R32 (optional): also write float(R) there.
 void launch_pcg_update(long long n, double *U, double *R, const double *P, const double *Q,
-                       double *partial, unsigned *ticket, PcgScalars *sc, cudaStream_t st);
-void launch_p_update(long long n, const double *Z, double *P, double *Zold, const PcgScalars *sc,
-                     cudaStream_t st);
-void launch_dot2(long long n, const double *r, const double *z, const double *zold, double *partial,
-                 unsigned *ticket, PcgScalars *sc, const int *done, cudaStream_t st);
+                       double *partial, unsigned *ticket, PcgScalars *sc, cudaStream_t st, float *R32 = nullptr);
+// Z: double, or float for the FP32 V-cycle output read directly.
+template <typename Z>
+void launch_p_update(long long n, const Z *z, double *P, Z *Zold, const PcgScalars *sc, cudaStream_t st);
+template <typename Z>
+void launch_dot2(long long n, const double *r, const Z *z, const Z *zold, double *partial, unsigned *ticket,
+                 PcgScalars *sc, const int *done, cudaStream_t st);
 void launch_pcg_init(long long n, const double *F, double *U, double *R, double *partial,
                      unsigned *ticket, PcgScalars *sc, double tol, int maxit, int flexible,
                      cudaStream_t st);

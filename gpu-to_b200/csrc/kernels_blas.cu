@@ -129,10 +129,12 @@ void launch_dot(long long n, const double *a, const double *b, double *partial, 
     count_launches(1);
 }
 
-// r'z and r'z_old in one pass, for the flexible recurrence.
+// r'z and r'z_old in one pass, for the flexible recurrence.  Z is FP64, or
+// the FP32 V-cycle output itself (the FP64 z would be its exact widening).
+template <typename Z>
 __global__ void __launch_bounds__(kRedThreads)
-dot2_kernel(long long n, const double *__restrict__ r, const double *__restrict__ z,
-            const double *__restrict__ zold, double *__restrict__ partial, unsigned *ticket,
+dot2_kernel(long long n, const double *__restrict__ r, const Z *__restrict__ z,
+            const Z *__restrict__ zold, double *__restrict__ partial, unsigned *ticket,
             PcgScalars *sc, const int *done)
 {
     if (done && *done) return;
@@ -141,8 +143,8 @@ dot2_kernel(long long n, const double *__restrict__ r, const double *__restrict_
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
         const double ri = r[i];
-        v = fma(ri, z[i], v);
-        w = fma(ri, zold[i], w);
+        v = fma(ri, (double)z[i], v);
+        w = fma(ri, (double)zold[i], w);
     }
     v = block_sum(v, red);
     __syncthreads();
@@ -168,18 +170,24 @@ dot2_kernel(long long n, const double *__restrict__ r, const double *__restrict_
     }
 }
 
-void launch_dot2(long long n, const double *r, const double *z, const double *zold, double *partial,
-                 unsigned *ticket, PcgScalars *sc, const int *done, cudaStream_t st)
+template <typename Z>
+void launch_dot2(long long n, const double *r, const Z *z, const Z *zold, double *partial, unsigned *ticket,
+                 PcgScalars *sc, const int *done, cudaStream_t st)
 {
-    dot2_kernel<<<red_blocks(n), kRedThreads, 0, st>>>(n, r, z, zold, partial, ticket, sc, done);
+    dot2_kernel<Z><<<red_blocks(n), kRedThreads, 0, st>>>(n, r, z, zold, partial, ticket, sc, done);
     count_launches(1);
 }
+template void launch_dot2<double>(long long, const double *, const double *, const double *, double *, unsigned *,
+                                  PcgScalars *, const int *, cudaStream_t);
+template void launch_dot2<float>(long long, const double *, const float *, const float *, double *, unsigned *,
+                                 PcgScalars *, const int *, cudaStream_t);
 
-// U += alpha P, R -= alpha Q, and r'r (mgcg1.cu:258-259,269).
+// U += alpha P, R -= alpha Q, and r'r (mgcg1.cu:258-259,269); R32, when
+// given, receives float(R) for the mixed-precision V-cycle.
 __global__ void __launch_bounds__(kRedThreads)
 pcg_update_kernel(long long n, double *__restrict__ U, double *__restrict__ R,
                   const double *__restrict__ P, const double *__restrict__ Q,
-                  double *__restrict__ partial, unsigned *ticket, PcgScalars *sc)
+                  double *__restrict__ partial, unsigned *ticket, PcgScalars *sc, float *__restrict__ R32)
 {
     if (sc->done) return;
     __shared__ double red[kRedThreads / 32];
@@ -190,6 +198,7 @@ pcg_update_kernel(long long n, double *__restrict__ U, double *__restrict__ R,
         U[i] = fma(alpha, P[i], U[i]);
         const double r = fma(-alpha, Q[i], R[i]);
         R[i] = r;
+        if (R32) R32[i] = (float)r;
         v = fma(r, r, v);
     }
     v = block_sum(v, red);
@@ -204,32 +213,37 @@ pcg_update_kernel(long long n, double *__restrict__ U, double *__restrict__ R,
 }
 
 void launch_pcg_update(long long n, double *U, double *R, const double *P, const double *Q,
-                       double *partial, unsigned *ticket, PcgScalars *sc, cudaStream_t st)
+                       double *partial, unsigned *ticket, PcgScalars *sc, cudaStream_t st, float *R32)
 {
-    pcg_update_kernel<<<red_blocks(n), kRedThreads, 0, st>>>(n, U, R, P, Q, partial, ticket, sc);
+    pcg_update_kernel<<<red_blocks(n), kRedThreads, 0, st>>>(n, U, R, P, Q, partial, ticket, sc, R32);
     count_launches(1);
 }
 
 // P = Z + beta P (mgcg1.cu:265); the flexible variant also keeps Z as Z_old.
-__global__ void p_update_kernel(long long n, const double *__restrict__ Z, double *__restrict__ P,
-                                double *__restrict__ Zold, const PcgScalars *sc)
+template <typename Z>
+__global__ void p_update_kernel(long long n, const Z *__restrict__ z_in, double *__restrict__ P,
+                                Z *__restrict__ Zold, const PcgScalars *sc)
 {
     if (sc->done) return;
     const double beta = sc->beta;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
-        const double z = Z[i];
-        P[i] = fma(beta, P[i], z);
+        const Z z = z_in[i];
+        P[i] = fma(beta, P[i], (double)z);
         if (Zold) Zold[i] = z;
     }
 }
 
-void launch_p_update(long long n, const double *Z, double *P, double *Zold, const PcgScalars *sc,
-                     cudaStream_t st)
+template <typename Z>
+void launch_p_update(long long n, const Z *z, double *P, Z *Zold, const PcgScalars *sc, cudaStream_t st)
 {
-    p_update_kernel<<<red_blocks(n), kRedThreads, 0, st>>>(n, Z, P, Zold, sc);
+    p_update_kernel<Z><<<red_blocks(n), kRedThreads, 0, st>>>(n, z, P, Zold, sc);
     count_launches(1);
 }
+template void launch_p_update<double>(long long, const double *, double *, double *, const PcgScalars *,
+                                      cudaStream_t);
+template void launch_p_update<float>(long long, const float *, double *, float *, const PcgScalars *,
+                                     cudaStream_t);
 
 // U = 0, R = F, res0 = ||F|| and the scalar state (mgcg1.cu:235-238).
 __global__ void __launch_bounds__(kRedThreads)

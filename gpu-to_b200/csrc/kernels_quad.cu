@@ -182,26 +182,31 @@ quad_node_kernel(Lay L, const T *__restrict__ y, const T *__restrict__ u, const 
     const int i = (int)(t / (g.nz + 1));
     const int k = (int)(t - (long long)i * (g.nz + 1));
     const long long nel = g.nel();
-    T acc[3] = {T(0), T(0), T(0)};
+    // all 24 loads issue before any is used (predicated, no branches), so the
+    // gather waits for memory once instead of once per element
+    const bool vx[2] = {i >= 1, i < g.nx}, vz[2] = {k >= 1, k < g.nz}, vy[2] = {j >= 1, j < g.ny};
+    T v[2][2][2][3];
 #pragma unroll
-    for (int ex = 0; ex < 2; ++ex) {
-        const int ei = i - 1 + ex;
-        if (ei < 0 || ei >= g.nx) continue;
+    for (int ex = 0; ex < 2; ++ex)
 #pragma unroll
-        for (int ez = 0; ez < 2; ++ez) {
-            const int ek = k - 1 + ez;
-            if (ek < 0 || ek >= g.nz) continue;
+        for (int ez = 0; ez < 2; ++ez)
 #pragma unroll
             for (int ey = 0; ey < 2; ++ey) {
-                const int ej = j - 1 + ey;
-                if (ej < 0 || ej >= g.ny) continue;
-                const long long e = g.elem(ei, ej, ek);
+                const bool ok = vx[ex] && vz[ez] && vy[ey];
+                const long long e = ok ? g.elem(i - 1 + ex, j - 1 + ey, k - 1 + ez) : 0;
                 const int a = local_index(1 - ex, 1 - ey, 1 - ez);
 #pragma unroll
-                for (int d = 0; d < 3; ++d) acc[d] += y[(long long)(3 * a + d) * nel + e];
+                for (int d = 0; d < 3; ++d) v[ex][ez][ey][d] = ok ? __ldg(y + (long long)(3 * a + d) * nel + e) : T(0);
             }
-        }
-    }
+    T acc[3] = {T(0), T(0), T(0)};
+#pragma unroll
+    for (int ex = 0; ex < 2; ++ex)
+#pragma unroll
+        for (int ez = 0; ez < 2; ++ez)
+#pragma unroll
+            for (int ey = 0; ey < 2; ++ey)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) acc[d] += v[ex][ez][ey][d];
     const unsigned m = mask[n];
     const long long base = L.at(i, j, k);
 #pragma unroll

@@ -141,7 +141,10 @@ int Solver::create(int nelx, int nely, int nelz, int nl_, const gputo_options *o
     ALLOC(Uw, nv);
     ALLOC(Fw, nv);
     ALLOC(Dn, g[0].ndof());
-    if (opt.precision == GPUTO_PREC_MIXED) ALLOC(Zold, nv);
+    if (opt.precision == GPUTO_PREC_MIXED) {
+        ALLOC(Zold, nv);
+        ALLOC(Zold32, nv);
+    }
     if (redisc())
         for (int l = 1; l < nl; ++l) {
             elayr[l] = ELay::of(g[l]);
@@ -515,14 +518,23 @@ void Solver::iteration(cudaStream_t st)
     const int *done = &sc->done;
     apply(P, Q, partial, done, st);
     launch_finish_apply_dot(apply_blocks(), partial, ticket, sc, st);
+    if (opt.precision == GPUTO_PREC_MIXED && !net_on) {
+        // float(r) comes from the residual update and z stays the FP32
+        // V-cycle output: no precision-conversion passes
+        launch_pcg_update(nv, Uw, R, P, Q, partial, ticket, sc, st, Lf[0].f);
+        vcycle_impl<float>(Lf, CXpf, Lf[0].f, Lf[0].u1, done, st);
+        launch_dot2<float>(nv, R, Lf[0].u1, Zold32, partial, ticket, sc, done, st);
+        launch_p_update<float>(nv, Lf[0].u1, P, Zold32, sc, st);
+        return;
+    }
     launch_pcg_update(nv, Uw, R, P, Q, partial, ticket, sc, st);
     vcycle(R, Z, done, st);
     if (Zold) {
-        launch_dot2(nv, R, Z, Zold, partial, ticket, sc, done, st);
-        launch_p_update(nv, Z, P, Zold, sc, st);
+        launch_dot2<double>(nv, R, Z, Zold, partial, ticket, sc, done, st);
+        launch_p_update<double>(nv, Z, P, Zold, sc, st);
     } else {
         launch_dot(nv, R, Z, partial, ticket, sc, 2 /*DOT_RZ*/, done, st);
-        launch_p_update(nv, Z, P, nullptr, sc, st);
+        launch_p_update<double>(nv, Z, P, nullptr, sc, st);
     }
 }
 
@@ -559,6 +571,8 @@ int Solver::solve_begin(const double *Fp, double tol, int maxit, cudaStream_t st
     vcycle(R, P, done, st);
     launch_dot(nv, R, P, partial, ticket, sc, 1 /*DOT_RHO0*/, done, st);
     if (Zold) launch_copy(nv, P, Zold, done, st);
+    if (Zold32 && !net_on)   // the FP32 V-cycle output of the first step, for the fast iteration
+        GPUTO_CUDA(cudaMemcpyAsync(Zold32, Lf[0].u1, sizeof(float) * nv, cudaMemcpyDeviceToDevice, st));
     return launch_status;
 }
 

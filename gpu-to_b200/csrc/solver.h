@@ -25,6 +25,7 @@ struct Solver {
 
     // fine-level PCG vectors (FP64, padded layout)
     double *R = nullptr, *P = nullptr, *Q = nullptr, *Z = nullptr, *Zold = nullptr;
+    float *Zold32 = nullptr;   // mixed precision: z_old as the FP32 V-cycle output it is
     double *Uw = nullptr, *Fw = nullptr;
     // staging in the reference's dense layout (MEX / device API boundary)
     double *Dn = nullptr;
