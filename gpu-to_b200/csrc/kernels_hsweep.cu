@@ -107,77 +107,144 @@ struct HSmem {
                   "TMA shared-memory destinations must be 128-byte aligned");
 };
 
-// (y, z) butterflies of one face: x[(cy 2 + cz) 3 + d] -> x[(py 2 + pz) 3 + d];
-// applied twice it multiplies by 4.
+// Face values are stored at [c 4 + d]: corner (or mode) c = 2 cy + cz (2 py +
+// pz), component d < 3; slot 3 of each group is unused.  The x and y
+// components of a group sit in an aligned register pair, so FP32 code works
+// on them with paired instructions.
+constexpr int HF = 16;
+
+// (y, z) butterflies of one face: corners -> modes; applied twice it
+// multiplies by 4.
 template <typename T>
-__device__ __forceinline__ void face_h(T (&x)[12])
+__device__ __forceinline__ void face_h(T (&x)[HF])
 {
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        const T u00 = x[d], u01 = x[3 + d], u10 = x[6 + d], u11 = x[9 + d];
+        const T u00 = x[d], u01 = x[4 + d], u10 = x[8 + d], u11 = x[12 + d];
         const T s0 = u00 + u10, d0 = u00 - u10, s1 = u01 + u11, d1 = u01 - u11;
         x[d] = s0 + s1;
-        x[3 + d] = s0 - s1;
-        x[6 + d] = d0 + d1;
-        x[9 + d] = d0 - d1;
+        x[4 + d] = s0 - s1;
+        x[8 + d] = d0 + d1;
+        x[12 + d] = d0 - d1;
     }
+}
+
+__device__ __forceinline__ float2 f2(const float (&x)[HF], int i) { return make_float2(x[i], x[i + 1]); }
+__device__ __forceinline__ void f2set(float (&x)[HF], int i, float2 v)
+{
+    x[i] = v.x;
+    x[i + 1] = v.y;
+}
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(make_float2(-1.f, -1.f), b, a); }
+
+// FP32: components x, y of each group with paired adds, z alone.
+template <>
+__device__ __forceinline__ void face_h<float>(float (&x)[HF])
+{
+    const float2 u00 = f2(x, 0), u01 = f2(x, 4), u10 = f2(x, 8), u11 = f2(x, 12);
+    const float2 s0 = __fadd2_rn(u00, u10), d0 = sub2(u00, u10), s1 = __fadd2_rn(u01, u11), d1 = sub2(u01, u11);
+    f2set(x, 0, __fadd2_rn(s0, s1));
+    f2set(x, 4, sub2(s0, s1));
+    f2set(x, 8, __fadd2_rn(d0, d1));
+    f2set(x, 12, sub2(d0, d1));
+    const float z00 = x[2], z01 = x[6], z10 = x[10], z11 = x[14];
+    const float zs0 = z00 + z10, zd0 = z00 - z10, zs1 = z01 + z11, zd1 = z01 - z11;
+    x[2] = zs0 + zs1;
+    x[6] = zs0 - zs1;
+    x[10] = zd0 + zd1;
+    x[14] = zd0 - zd1;
 }
 
 // One element in the Hadamard basis.  Fp, Fn: transformed front (x = 0) and
 // back (x = 1) faces.  Adds the element's front-face output (still in face
 // modes) to A and sets An to its back-face output.  Mode m = 4 px + 2 py + pz
-// with px selecting v0 / v1 and (py, pz, d) the index (py 2 + pz) 3 + d.
+// with px selecting v0 / v1 and (py, pz, d) the index (2 py + pz) 4 + d.
+// The S step: v -> w (the mode-(0,0,0) rows are zero).
 template <typename T>
-__device__ __forceinline__ void element_h(const T (&Fp)[12], const T (&Fn)[12], T cx, const HC<T> &k, T (&A)[12],
-                                          T (&An)[12])
+__device__ __forceinline__ void element_s(const T (&v0)[HF], const T (&v1)[HF], T cx, const HC<T> &k, T (&w0)[HF],
+                                          T (&w1)[HF])
 {
-    T v0[12], v1[12], w0[12], w1[12];
-#pragma unroll
-    for (int q = 0; q < 12; ++q) {
-        v0[q] = Fp[q] + Fn[q];
-        v1[q] = Fp[q] - Fn[q];
-    }
     const T ka = k.a * cx, kbc = k.bc * cx, kc = k.c * cx, kde = k.de * cx, ke = k.e * cx, kf = k.f * cx,
             kg = k.g * cx, kh = k.h * cx;
     T t;
     w0[0] = w0[1] = w0[2] = T(0);   // mode (0,0,0): rigid translation
     // a [1 1; 1 1]: {(m1,x),(m4,z)}, {(m1,y),(m2,z)}, {(m2,x),(m4,y)}
-    t = ka * (v0[3] + v1[2]);
-    w0[3] = t, w1[2] = t;
-    t = ka * (v0[4] + v0[8]);
-    w0[4] = t, w0[8] = t;
-    t = ka * (v0[6] + v1[1]);
-    w0[6] = t, w1[1] = t;
+    t = ka * (v0[4] + v1[2]);
+    w0[4] = t, w1[2] = t;
+    t = ka * (v0[5] + v0[10]);
+    w0[5] = t, w0[10] = t;
+    t = ka * (v0[8] + v1[1]);
+    w0[8] = t, w1[1] = t;
     // (b - c) I + c 11': {(m1,z),(m2,y),(m4,x)}
-    t = kc * (v0[5] + v0[7] + v1[0]);
-    w0[5] = fma(kbc, v0[5], t);
-    w0[7] = fma(kbc, v0[7], t);
+    t = kc * (v0[6] + v0[9] + v1[0]);
+    w0[6] = fma(kbc, v0[6], t);
+    w0[9] = fma(kbc, v0[9], t);
     w1[0] = fma(kbc, v1[0], t);
     // (d - e) I + e 11': {(m3,x),(m5,y),(m6,z)}
-    t = ke * (v0[9] + v1[4] + v1[8]);
-    w0[9] = fma(kde, v0[9], t);
-    w1[4] = fma(kde, v1[4], t);
-    w1[8] = fma(kde, v1[8], t);
+    t = ke * (v0[12] + v1[5] + v1[10]);
+    w0[12] = fma(kde, v0[12], t);
+    w1[5] = fma(kde, v1[5], t);
+    w1[10] = fma(kde, v1[10], t);
     // [f g; g f]: {(m3,y),(m5,x)}, {(m3,z),(m6,x)}, {(m5,z),(m6,y)}
-    w0[10] = fma(kf, v0[10], kg * v1[3]);
-    w1[3] = fma(kf, v1[3], kg * v0[10]);
-    w0[11] = fma(kf, v0[11], kg * v1[6]);
-    w1[6] = fma(kf, v1[6], kg * v0[11]);
-    w1[5] = fma(kf, v1[5], kg * v1[7]);
-    w1[7] = fma(kf, v1[7], kg * v1[5]);
+    w0[13] = fma(kf, v0[13], kg * v1[4]);
+    w1[4] = fma(kf, v1[4], kg * v0[13]);
+    w0[14] = fma(kf, v0[14], kg * v1[8]);
+    w1[8] = fma(kf, v1[8], kg * v0[14]);
+    w1[6] = fma(kf, v1[6], kg * v1[9]);
+    w1[9] = fma(kf, v1[9], kg * v1[6]);
     // h I on mode (1,1,1)
-    w1[9] = kh * v1[9];
-    w1[10] = kh * v1[10];
-    w1[11] = kh * v1[11];
+    w1[12] = kh * v1[12];
+    w1[13] = kh * v1[13];
+    w1[14] = kh * v1[14];
+}
+
+template <typename T>
+__device__ __forceinline__ void element_h(const T (&Fp)[HF], const T (&Fn)[HF], T cx, const HC<T> &k, T (&A)[HF],
+                                          T (&An)[HF])
+{
+    T v0[HF], v1[HF], w0[HF], w1[HF];
 #pragma unroll
-    for (int q = 0; q < 12; ++q) {
-        A[q] += w0[q] + w1[q];
-        An[q] = w0[q] - w1[q];
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            v0[4 * c + d] = Fp[4 * c + d] + Fn[4 * c + d];
+            v1[4 * c + d] = Fp[4 * c + d] - Fn[4 * c + d];
+        }
+    element_s(v0, v1, cx, k, w0, w1);
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            A[4 * c + d] += w0[4 * c + d] + w1[4 * c + d];
+            An[4 * c + d] = w0[4 * c + d] - w1[4 * c + d];
+        }
+}
+
+// FP32: the sums and differences of faces and outputs on (x, y) pairs.
+template <>
+__device__ __forceinline__ void element_h<float>(const float (&Fp)[HF], const float (&Fn)[HF], float cx,
+                                                 const HC<float> &k, float (&A)[HF], float (&An)[HF])
+{
+    float v0[HF], v1[HF], w0[HF], w1[HF];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const float2 p = f2(Fp, 4 * c), n = f2(Fn, 4 * c);
+        f2set(v0, 4 * c, __fadd2_rn(p, n));
+        f2set(v1, 4 * c, sub2(p, n));
+        v0[4 * c + 2] = Fp[4 * c + 2] + Fn[4 * c + 2];
+        v1[4 * c + 2] = Fp[4 * c + 2] - Fn[4 * c + 2];
+    }
+    element_s(v0, v1, cx, k, w0, w1);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const float2 a = f2(w0, 4 * c), b = f2(w1, 4 * c);
+        f2set(A, 4 * c, __fadd2_rn(f2(A, 4 * c), __fadd2_rn(a, b)));
+        f2set(An, 4 * c, sub2(a, b));
+        A[4 * c + 2] += w0[4 * c + 2] + w1[4 * c + 2];
+        An[4 * c + 2] = w0[4 * c + 2] - w1[4 * c + 2];
     }
 }
 
-// One node's result from K u (ku), u, f, 1/diag and its Dirichlet bits m; fv
-// and rv point at that node's three f and 1/diag values (shared or global).
 template <typename T, int MODE>
 __device__ __forceinline__ void h_store(long long base, unsigned m, const T (&ku)[3], const T (&u)[3], const T *fv,
                                         const T *rv, T *__restrict__ out, T omega, double &dsum)
@@ -277,7 +344,7 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
     auto wait_stage = [&](int s) {
         if (!bad && !mbar_wait_bounded(&bar[s % HRING], (uint32_t)((s / HRING) & 1), kHWaitPolls)) bad = true;
     };
-    auto load_face = [&](int s, T (&U)[12]) {
+    auto load_face = [&](int s, T (&U)[HF]) {
         const unsigned char *sb = smem + (s % HRING) * S::slot;
         const T *su = reinterpret_cast<const T *>(sb);
         const T *sd = reinterpret_cast<const T *>(sb + S::d_off);
@@ -290,25 +357,25 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
                     const int idx = (w + cz) * HUW + 3 * (l + cy) + d;
                     T v = su[idx];
                     if (N::PRE) v = prerelax * v * sd[idx];   // 1/diag is 0 outside the grid
-                    U[(cy * 2 + cz) * 3 + d] = v;
+                    U[(cy * 2 + cz) * 4 + d] = v;
                 }
     };
     double dsum = 0.0;
     // Corner partials P of node plane p -> y sums through the warp, z partner
     // values into the exchange buffer (read after the next barrier).
-    auto reduce_y = [&](int p, T (&P)[12], T (&q0)[3]) {
+    auto reduce_y = [&](int p, T (&P)[HF], T (&q0)[3]) {
         T *z = zb + (p & 1) * (WZ * S::ZROW * 3);
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            const T a0 = __shfl_up_sync(0xffffffffu, P[6 + d], 1);
-            const T a1 = __shfl_up_sync(0xffffffffu, P[9 + d], 1);
+            const T a0 = __shfl_up_sync(0xffffffffu, P[8 + d], 1);
+            const T a1 = __shfl_up_sync(0xffffffffu, P[12 + d], 1);
             q0[d] = P[d] + (l > 0 ? a0 : T(0));
-            z[(w * S::ZROW + l) * 3 + d] = P[3 + d] + (l > 0 ? a1 : T(0));
-            if (l == HY - 1) z[(w * S::ZROW + HY) * 3 + d] = P[9 + d];
+            z[(w * S::ZROW + l) * 3 + d] = P[4 + d] + (l > 0 ? a1 : T(0));
+            if (l == HY - 1) z[(w * S::ZROW + HY) * 3 + d] = P[12 + d];
         }
     };
     // Finish node plane p with the epilogue tiles of ring stage s.
-    auto emit = [&](int p, int s, const T (&P)[12], const T (&q0)[3], const T (&Uu)[12]) {
+    auto emit = [&](int p, int s, const T (&P)[HF], const T (&q0)[3], const T (&Uu)[HF]) {
         if (!zok) return;
         const unsigned char *sb = smem + (s % HRING) * S::slot;
         const T *ef = reinterpret_cast<const T *>(sb + S::ef_off) + w * HUW;
@@ -332,13 +399,13 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
         if (l == HY - 1) {   // this CTA's part of node column jc0 + HY
             T Sd[3];
 #pragma unroll
-            for (int d = 0; d < 3; ++d) Sd[d] = P[6 + d] + (w > 0 ? z[((w - 1) * S::ZROW + HY) * 3 + d] : T(0));
+            for (int d = 0; d < 3; ++d) Sd[d] = P[8 + d] + (w > 0 ? z[((w - 1) * S::ZROW + HY) * 3 + d] : T(0));
             if (r + 1 < CY) {
                 T *rem = cluster.map_shared_rank(s_recv, r + 1);
 #pragma unroll
                 for (int d = 0; d < 3; ++d) rem[at + d] = Sd[d];
             } else if (tail_owner) {
-                const T uu[3] = {Uu[6], Uu[7], Uu[8]};
+                const T uu[3] = {Uu[8], Uu[9], Uu[10]};
                 h_store<T, MODE>(L.at(p, g.ny, k), em[HY], Sd, uu, ef + 3 * HY, ed + 3 * HY, out, omega, dsum);
             }
         }
@@ -350,12 +417,13 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
     // are copied.
     int cur = 0;   // the stage being consumed
     bool fail = false;
-    auto step = [&](int t, T (&Uc)[12], T (&Fc)[12], T (&Ac)[12], T (&Un)[12], T (&Fn)[12], T (&An)[12]) {
+    auto step = [&](int t, T (&Uc)[HF], T (&Fc)[HF], T (&Ac)[HF], T (&Un)[HF], T (&Fn)[HF], T (&An)[HF]) {
         cur = t;
         wait_stage(t);
         load_face(t, Un);
 #pragma unroll
-        for (int q = 0; q < 12; ++q) Fn[q] = Un[q];
+        for (int q = 0; q < HF; ++q)
+            if ((q & 3) != 3) Fn[q] = Un[q];
         face_h(Fn);
         const T cx = reinterpret_cast<const T *>(smem + (t % HRING) * S::slot + S::c_off)[w * HY + l];
         element_h(Fc, Fn, cx, hc, Ac, An);
@@ -370,7 +438,7 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
         if (!fail && tid == 0 && t - 1 + HRING < nst) issue(t - 1 + HRING);
         if (!fail && out_plane) emit(p, t, Ac, q0, Uc);
     };
-    auto finish_last = [&](T (&Uc)[12], T (&Ac)[12]) {   // plane nx: only element nx - 1 touches it
+    auto finish_last = [&](T (&Uc)[HF], T (&Ac)[HF]) {   // plane nx: only element nx - 1 touches it
         cur = nE + 1;
         wait_stage(nE + 1);
         T q0[3];
@@ -380,12 +448,12 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
         if (!fail) emit(E1, nE + 1, Ac, q0, Uc);
     };
 
-    T U0[12], F0[12], A0[12], U1[12], F1[12], A1[12];
+    T U0[HF], F0[HF], A0[HF], U1[HF], F1[HF], A1[HF];
     wait_stage(0);
     load_face(0, U0);
 #pragma unroll
-    for (int q = 0; q < 12; ++q) {
-        F0[q] = U0[q];
+    for (int q = 0; q < HF; ++q) {
+        F0[q] = (q & 3) != 3 ? U0[q] : T(0);
         A0[q] = T(0);
     }
     face_h(F0);

@@ -208,52 +208,64 @@ packed_sweep_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u,
     }
 }
 
-// Small levels: one warp per node.  Lane l takes element l/4 of the 8 around
-// the node and a quarter (6 columns) of its 24, i.e. 18 products, and the
-// warp sums the three rows with shuffles -- 32x the parallelism of a thread
-// per node, for levels with too few nodes to fill the GPU.
+// Small coarse levels: a CTA finishes 32 consecutive nodes.  Warp w takes
+// element slot w (the element at offset (ex, ey, ez) = bits of w from each
+// node) and lane l node n0 + l, so every load of a matrix entry
+// A[row, col] reads 32 neighbouring elements (the [300][nel] layout is
+// element-fastest): four 32-byte sectors per warp instead of 32.  The eight
+// slot partials are summed in a fixed order through shared memory.
 template <typename T, int MODE>
-__global__ void __launch_bounds__(128)
-packed_sweep_warp_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u,
-                         const T *__restrict__ f, const T *__restrict__ diag,
-                         const uint8_t *__restrict__ mask, T *__restrict__ out, T omega, T prerelax,
-                         const int *__restrict__ done)
+__global__ void __launch_bounds__(256)
+packed_sweep_slot_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u, const T *__restrict__ f,
+                         const T *__restrict__ diag, const uint8_t *__restrict__ mask, T *__restrict__ out,
+                         T omega, T prerelax, const int *__restrict__ done)
 {
     if (done && *done) return;
+    __shared__ T part[8][32][3];
     const Grid &g = L.g;
-    const long long n = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (n >= g.nnod()) return;
-    int i, j, k;
-    node_ijk(g, n, i, j, k);
-    const int eidx = lane >> 2, quarter = lane & 3;
-    const int ex = (eidx >> 2) & 1, ez = (eidx >> 1) & 1, ey = eidx & 1;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const long long n = (long long)blockIdx.x * 32 + lane;
+    const bool have = n < g.nnod();
+    int i = 0, j = 0, k = 0;
+    if (have) node_ijk(g, n, i, j, k);
+    const int ex = (w >> 2) & 1, ez = (w >> 1) & 1, ey = w & 1;
     const int ei = i - 1 + ex, ej = j - 1 + ey, ek = k - 1 + ez;
     T acc[3] = {T(0), T(0), T(0)};
-    if (ei >= 0 && ei < g.nx && ej >= 0 && ej < g.ny && ek >= 0 && ek < g.nz) {
+    if (have && ei >= 0 && ei < g.nx && ej >= 0 && ej < g.ny && ek >= 0 && ek < g.nz) {
         const long long nel = g.nel();
         const long long e = g.elem(ei, ej, ek);
         const int a = local_index(1 - ex, 1 - ey, 1 - ez);
+        T ub[24];
 #pragma unroll
-        for (int c = 0; c < 6; ++c) {
-            const int col = quarter * 6 + c, b = col / 3, q = col - 3 * b;
-            const long long dof = L.at(ei + local_x(b), ej + local_y(b), ek + local_z(b)) + q;
-            T ub;
-            if (MODE == MODE_JACOBI_PRE) {
-                const T dv = diag[dof];
-                ub = dv != T(0) ? prerelax * f[dof] / dv : T(0);
-            } else {
-                ub = u[dof];
+        for (int b = 0; b < 8; ++b) {
+            const long long nb = L.at(ei + local_x(b), ej + local_y(b), ek + local_z(b));
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                if (MODE == MODE_JACOBI_PRE) {
+                    const T dv = diag[nb + q];
+                    ub[3 * b + q] = dv != T(0) ? prerelax * f[nb + q] / dv : T(0);
+                } else {
+                    ub[3 * b + q] = u[nb + q];
+                }
             }
-#pragma unroll
-            for (int d = 0; d < 3; ++d)
-                acc[d] = fma(A[(long long)packed_index(3 * a + d, col) * nel + e], ub, acc[d]);
         }
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+#pragma unroll
+            for (int col = 0; col < 24; ++col)
+                acc[d] = fma(A[(long long)packed_index(3 * a + d, col) * nel + e], ub[col], acc[d]);
     }
 #pragma unroll
-    for (int d = 0; d < 3; ++d)
-        for (int o = 16; o > 0; o >>= 1) acc[d] += __shfl_xor_sync(0xffffffffu, acc[d], o);
-    if (lane != 0) return;
+    for (int d = 0; d < 3; ++d) part[w][lane][d] = acc[d];
+    __syncthreads();
+    if (w != 0 || !have) return;
+    T s[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        s[d] = part[0][lane][d];
+#pragma unroll
+        for (int q = 1; q < 8; ++q) s[d] += part[q][lane][d];
+    }
     const unsigned m = mask[n];
     const long long base = L.at(i, j, k);
 #pragma unroll
@@ -261,11 +273,11 @@ packed_sweep_warp_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u
         const long long dof = base + d;
         const bool fixed = (m >> d) & 1u;
         if (MODE == MODE_APPLY) {
-            out[dof] = fixed ? T(0) : acc[d];
+            out[dof] = fixed ? T(0) : s[d];
         } else if (MODE == MODE_DEFECT) {
-            out[dof] = fixed ? T(0) : f[dof] - acc[d];
+            out[dof] = fixed ? T(0) : f[dof] - s[d];
         } else {
-            const T r = fixed ? T(0) : f[dof] - acc[d];
+            const T r = fixed ? T(0) : f[dof] - s[d];
             T us;
             if (MODE == MODE_JACOBI_PRE) {
                 const T dv = diag[dof];
@@ -285,19 +297,19 @@ void launch_packed_sweep(int mode, const Lay &L, const T *Apk, const T *u, const
 {
     const int bs = 128;
     if (L.g.nnod() < 65536) {
-        const unsigned wb = (unsigned)((L.g.nnod() * 32 + bs - 1) / bs);
+        const unsigned sb = (unsigned)((L.g.nnod() + 31) / 32);
         switch (mode) {
         case MODE_APPLY:
-            packed_sweep_warp_kernel<T, MODE_APPLY><<<wb, bs, 0, st>>>(L, Apk, u, f, diag, mask, out, omega, prerelax, done);
+            packed_sweep_slot_kernel<T, MODE_APPLY><<<sb, 256, 0, st>>>(L, Apk, u, f, diag, mask, out, omega, prerelax, done);
             break;
         case MODE_DEFECT:
-            packed_sweep_warp_kernel<T, MODE_DEFECT><<<wb, bs, 0, st>>>(L, Apk, u, f, diag, mask, out, omega, prerelax, done);
+            packed_sweep_slot_kernel<T, MODE_DEFECT><<<sb, 256, 0, st>>>(L, Apk, u, f, diag, mask, out, omega, prerelax, done);
             break;
         case MODE_JACOBI:
-            packed_sweep_warp_kernel<T, MODE_JACOBI><<<wb, bs, 0, st>>>(L, Apk, u, f, diag, mask, out, omega, prerelax, done);
+            packed_sweep_slot_kernel<T, MODE_JACOBI><<<sb, 256, 0, st>>>(L, Apk, u, f, diag, mask, out, omega, prerelax, done);
             break;
         default:
-            packed_sweep_warp_kernel<T, MODE_JACOBI_PRE><<<wb, bs, 0, st>>>(L, Apk, u, f, diag, mask, out, omega, prerelax, done);
+            packed_sweep_slot_kernel<T, MODE_JACOBI_PRE><<<sb, 256, 0, st>>>(L, Apk, u, f, diag, mask, out, omega, prerelax, done);
         }
         count_launches(1);
         return;
