@@ -140,11 +140,21 @@ dot2_kernel(long long n, const double *__restrict__ r, const Z *__restrict__ z,
     if (done && *done) return;
     __shared__ double red[kRedThreads / 32];
     double v = 0.0, w = 0.0;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+    // two neighbouring entries per trip (16-byte loads); n odd leaves a tail
+    const long long n2 = n >> 1;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n2;
          i += (long long)gridDim.x * blockDim.x) {
-        const double ri = r[i];
-        v = fma(ri, (double)z[i], v);
-        w = fma(ri, (double)zold[i], w);
+        const double2 ri = reinterpret_cast<const double2 *>(r)[i];
+        const double z0 = (double)z[2 * i], z1 = (double)z[2 * i + 1];
+        const double o0 = (double)zold[2 * i], o1 = (double)zold[2 * i + 1];
+        v = fma(ri.x, z0, v);
+        w = fma(ri.x, o0, w);
+        v = fma(ri.y, z1, v);
+        w = fma(ri.y, o1, w);
+    }
+    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+        v = fma(r[n - 1], (double)z[n - 1], v);
+        w = fma(r[n - 1], (double)zold[n - 1], w);
     }
     v = block_sum(v, red);
     __syncthreads();
@@ -193,8 +203,24 @@ pcg_update_kernel(long long n, double *__restrict__ U, double *__restrict__ R,
     __shared__ double red[kRedThreads / 32];
     const double alpha = sc->alpha;
     double v = 0.0;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+    // two neighbouring entries per trip (16-byte loads and stores)
+    const long long n2 = n >> 1;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n2;
          i += (long long)gridDim.x * blockDim.x) {
+        const double2 p = reinterpret_cast<const double2 *>(P)[i], q = reinterpret_cast<const double2 *>(Q)[i];
+        double2 u = reinterpret_cast<double2 *>(U)[i], r = reinterpret_cast<double2 *>(R)[i];
+        u.x = fma(alpha, p.x, u.x);
+        u.y = fma(alpha, p.y, u.y);
+        r.x = fma(-alpha, q.x, r.x);
+        r.y = fma(-alpha, q.y, r.y);
+        reinterpret_cast<double2 *>(U)[i] = u;
+        reinterpret_cast<double2 *>(R)[i] = r;
+        if (R32) reinterpret_cast<float2 *>(R32)[i] = make_float2((float)r.x, (float)r.y);
+        v = fma(r.x, r.x, v);
+        v = fma(r.y, r.y, v);
+    }
+    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+        const long long i = n - 1;
         U[i] = fma(alpha, P[i], U[i]);
         const double r = fma(-alpha, Q[i], R[i]);
         R[i] = r;
@@ -226,11 +252,23 @@ __global__ void p_update_kernel(long long n, const Z *__restrict__ z_in, double 
 {
     if (sc->done) return;
     const double beta = sc->beta;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+    const long long n2 = n >> 1;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n2;
          i += (long long)gridDim.x * blockDim.x) {
-        const Z z = z_in[i];
-        P[i] = fma(beta, P[i], (double)z);
-        if (Zold) Zold[i] = z;
+        const Z z0 = z_in[2 * i], z1 = z_in[2 * i + 1];
+        double2 p = reinterpret_cast<double2 *>(P)[i];
+        p.x = fma(beta, p.x, (double)z0);
+        p.y = fma(beta, p.y, (double)z1);
+        reinterpret_cast<double2 *>(P)[i] = p;
+        if (Zold) {
+            Zold[2 * i] = z0;
+            Zold[2 * i + 1] = z1;
+        }
+    }
+    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+        const Z z = z_in[n - 1];
+        P[n - 1] = fma(beta, P[n - 1], (double)z);
+        if (Zold) Zold[n - 1] = z;
     }
 }
 

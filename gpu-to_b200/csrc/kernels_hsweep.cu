@@ -271,8 +271,15 @@ __device__ __forceinline__ void h_store(long long base, unsigned m, const T (&ku
 // z = x chunk (node planes [c htx, (c + 1) htx), the last one up to nx;
 // htx <= HTX).  The Dirichlet bits come by TMA from a copy with rows padded
 // to 16 bytes (tm_m); rdiag = 1/diag.
+// CTAs per SM the compiler budgets registers for: 2 where two fit in shared
+// memory (FP64 apply and defect measured 10 % faster at 2, with a few spills,
+// than at 1); the FP64 Jacobi instances hold 129 and 158 KB, so only one fits.
+template <typename T, int MODE> struct HMinBlocks {
+    static constexpr int value = (sizeof(T) == 4 || MODE == MODE_APPLY || MODE == MODE_DEFECT) ? 2 : 1;
+};
+
 template <typename T, int MODE, int WZ>
-__global__ void __launch_bounds__(32 * WZ, 2)   // 2 CTAs per SM (FP64 measured 10 % faster than 1 despite spills)
+__global__ void __launch_bounds__(32 * WZ, HMinBlocks<T, MODE>::value)
 hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ CUtensorMap tm_d,
               const __grid_constant__ CUtensorMap tm_f, const __grid_constant__ CUtensorMap tm_c,
               const __grid_constant__ CUtensorMap tm_m, Lay L, HC<T> hc, int htx, const T *__restrict__ f,

@@ -278,52 +278,80 @@ template int launch_quad_sweep<float>(int, const Lay &, const ELay &, const floa
 namespace gputo {
 
 // Element-centric sweep for a level with stored (packed) element matrices:
-// one thread per element reads its 300 matrix entries once (coalesced,
-// structure of arrays) and writes y_E = A_E u_E; the node pass is the same
-// deterministic gather as for level 1.  Used for the large coarse levels,
+// y_E = A_E u_E into the 24-per-element scratch, then the node pass (the same
+// deterministic gather as for level 1).  Used for the large coarse levels,
 // where the node-centred form re-reads every entry from the 8 nodes around it.
-template <typename T, bool PRE>
-__global__ void __launch_bounds__(128)
-packed_element_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u, const T *__restrict__ f,
-                      const T *__restrict__ diag, T prerelax, T *__restrict__ y, const int *__restrict__ done)
+// A CTA of 4 warps takes 32 elements (lane = element, so every entry load is
+// coalesced over the [300][nel] layout); warp g multiplies the packed rows
+// [M0, M1) of its share (78, 75, 78 and 69 of the 300 entries), using each
+// off-diagonal entry for both of its products, into a partial 24-vector; the
+// four partials are summed in a fixed order through shared memory.
+template <typename T, int M0, int M1>
+__device__ __forceinline__ void packed_rows(const T *__restrict__ A, long long nel, long long e, const T (&ue)[24],
+                                            T (&ye)[24])
 {
-    if (done && *done) return;
-    const Grid &g = L.g;
-    const long long nel = g.nel();
-    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= nel) return;
-    const long long t = e / g.ny;
-    const int j = (int)(e - t * g.ny);
-    const int i = (int)(t / g.nz);
-    const int k = (int)(t - (long long)i * g.nz);
-    T ue[24];
 #pragma unroll
-    for (int a = 0; a < 8; ++a) {
-        const long long nb = L.at(i + local_x(a), j + local_y(a), k + local_z(a));
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-            if (PRE) {
-                const T dv = diag[nb + q];
-                ue[3 * a + q] = dv != T(0) ? prerelax * f[nb + q] / dv : T(0);
-            } else {
-                ue[3 * a + q] = u[nb + q];
-            }
-        }
-    }
-    T ye[24];
-#pragma unroll
-    for (int m = 0; m < 24; ++m) ye[m] = T(0);
-#pragma unroll
-    for (int m = 0; m < 24; ++m) {
+    for (int m = M0; m < M1; ++m)
 #pragma unroll
         for (int n = 0; n <= m; ++n) {
             const T amn = A[(long long)packed_index(m, n) * nel + e];
             ye[m] = fma(amn, ue[n], ye[m]);
             if (n != m) ye[n] = fma(amn, ue[m], ye[n]);
         }
+}
+
+template <typename T, bool PRE>
+__global__ void __launch_bounds__(128)
+packed_element_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u, const T *__restrict__ f,
+                      const T *__restrict__ diag, T prerelax, T *__restrict__ y, const int *__restrict__ done)
+{
+    if (done && *done) return;
+    __shared__ T part[4][24][32];
+    const Grid &g = L.g;
+    const long long nel = g.nel();
+    const int lane = threadIdx.x & 31, wg = threadIdx.x >> 5;
+    const long long e = (long long)blockIdx.x * 32 + lane;
+    const bool have = e < nel;
+    T ye[24];
+#pragma unroll
+    for (int m = 0; m < 24; ++m) ye[m] = T(0);
+    if (have) {
+        const long long t = e / g.ny;
+        const int j = (int)(e - t * g.ny);
+        const int i = (int)(t / g.nz);
+        const int k = (int)(t - (long long)i * g.nz);
+        T ue[24];
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+            const long long nb = L.at(i + local_x(a), j + local_y(a), k + local_z(a));
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                if (PRE) {
+                    const T dv = diag[nb + q];
+                    ue[3 * a + q] = dv != T(0) ? prerelax * f[nb + q] / dv : T(0);
+                } else {
+                    ue[3 * a + q] = u[nb + q];
+                }
+            }
+        }
+        switch (wg) {
+        case 0: packed_rows<T, 0, 12>(A, nel, e, ue, ye); break;
+        case 1: packed_rows<T, 12, 17>(A, nel, e, ue, ye); break;
+        case 2: packed_rows<T, 17, 21>(A, nel, e, ue, ye); break;
+        default: packed_rows<T, 21, 24>(A, nel, e, ue, ye);
+        }
     }
 #pragma unroll
-    for (int m = 0; m < 24; ++m) y[(long long)m * nel + e] = ye[m];
+    for (int m = 0; m < 24; ++m) part[wg][m][lane] = ye[m];
+    __syncthreads();
+    if (!have) return;
+    // warp wg writes rows 6 wg .. 6 wg + 5
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+        const int m = 6 * wg + r;
+        const T s = ((part[0][m][lane] + part[1][m][lane]) + part[2][m][lane]) + part[3][m][lane];
+        y[(long long)m * nel + e] = s;
+    }
 }
 
 template <typename T>
@@ -332,7 +360,7 @@ void launch_packed_sweep_ec(int mode, const Lay &L, const T *Apk, const T *u, co
                             const int *done, cudaStream_t st)
 {
     const int bs = 128;
-    const unsigned eb = (unsigned)((L.g.nel() + bs - 1) / bs);
+    const unsigned eb = (unsigned)((L.g.nel() + 31) / 32);   // 32 elements per CTA of 4 warps
     const unsigned nb = (unsigned)((L.g.nnod() + bs - 1) / bs);
     if (mode == MODE_JACOBI_PRE)
         packed_element_kernel<T, true><<<eb, bs, 0, st>>>(L, Apk, u, f, diag, prerelax, yscratch, done);
