@@ -358,19 +358,24 @@ __global__ void restrict_kernel(Lay Lc, Lay Lf, const T *__restrict__ rf,
     node_ijk(gc, n, i, j, k);
     const Grid &gf = Lf.g;
     T acc[3] = {T(0), T(0), T(0)};
+    // all 27 taps unrolled with predicated loads (a tap outside the grid
+    // adds an exact zero), so the loads of a plane issue together
+#pragma unroll
     for (int di = -1; di <= 1; ++di) {
         const int fi = 2 * i + di;
-        if (fi < 0 || fi > gf.nx) continue;
+        const bool oki = fi >= 0 && fi <= gf.nx;
+#pragma unroll
         for (int dk = -1; dk <= 1; ++dk) {
             const int fk = 2 * k + dk;
-            if (fk < 0 || fk > gf.nz) continue;
+            const bool okk = oki && fk >= 0 && fk <= gf.nz;
+#pragma unroll
             for (int dj = -1; dj <= 1; ++dj) {
                 const int fj = 2 * j + dj;
-                if (fj < 0 || fj > gf.ny) continue;
-                const T w = T(1) / T(1 << (abs(di) + abs(dj) + abs(dk)));
-                const long long nf = Lf.at(fi, fj, fk);
+                const bool ok = okk && fj >= 0 && fj <= gf.ny;
+                const T w = T(1.0 / (1 << ((di != 0) + (dj != 0) + (dk != 0))));
+                const long long nf = ok ? Lf.at(fi, fj, fk) : 0;
 #pragma unroll
-                for (int d = 0; d < 3; ++d) acc[d] = fma(w, rf[nf + d], acc[d]);
+                for (int d = 0; d < 3; ++d) acc[d] = fma(w, ok ? rf[nf + d] : T(0), acc[d]);
             }
         }
     }
@@ -408,12 +413,17 @@ __global__ void prolong_kernel(Lay Lf, Lay Lc, const T *__restrict__ uc,
     node_ijk(gf, n, i, j, k);
     const int ni = (i & 1) + 1, nj = (j & 1) + 1, nk = (k & 1) + 1;
     T acc[3] = {T(0), T(0), T(0)};
-    for (int a = 0; a < ni; ++a)
-        for (int c = 0; c < nk; ++c)
-            for (int b = 0; b < nj; ++b) {
-                const long long nc = Lc.at((i >> 1) + a, (j >> 1) + b, (k >> 1) + c);
+    // the up to 8 coarse nodes unrolled with predicated loads (same order)
 #pragma unroll
-                for (int d = 0; d < 3; ++d) acc[d] += uc[nc + d];
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+#pragma unroll
+            for (int b = 0; b < 2; ++b) {
+                const bool ok = a < ni && c < nk && b < nj;
+                const long long nc = ok ? Lc.at((i >> 1) + a, (j >> 1) + b, (k >> 1) + c) : 0;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) acc[d] += ok ? uc[nc + d] : T(0);
             }
     const T w = T(1) / T(ni * nj * nk);
     const unsigned m = maskf[n];
