@@ -444,21 +444,21 @@ int gputo_solver_time_kernel(gputo_solver *h, int which, int reps, double *ms, v
         case 2:
             if (s.quad_level1())
                 r = gputo::launch_quad_sweep<float>(gputo::MODE_JACOBI, s.lay[1], s.elay, s.CXpf, s.Lf[1].u0,
-                                                    s.Lf[1].f, s.Lf[1].diag, s.mask[1], s.Lf[1].u1, 0.48f,
+                                                    s.Lf[1].f, s.Lf[1].rdiag, s.mask[1], s.Lf[1].u1, 0.48f,
                                                     0.7f, s.opt.nu, s.Lf[1].yq, nullptr, s.err, st);
             else
                 gputo::launch_packed_sweep<float>(gputo::MODE_JACOBI, s.lay[1], s.Lf[1].Apk, s.Lf[1].u0,
-                                                  s.Lf[1].f, s.Lf[1].diag, s.mask[1], s.Lf[1].u1, 0.48f,
+                                                  s.Lf[1].f, s.Lf[1].rdiag, s.mask[1], s.Lf[1].u1, 0.48f,
                                                   0.7f, nullptr, st);
             break;
         default:
             if (s.quad_level1())
                 r = gputo::launch_quad_sweep<double>(gputo::MODE_JACOBI, s.lay[1], s.elay, s.CXp, s.L[1].u0,
-                                                     s.L[1].f, s.L[1].diag, s.mask[1], s.L[1].u1, 0.48,
+                                                     s.L[1].f, s.L[1].rdiag, s.mask[1], s.L[1].u1, 0.48,
                                                      0.7, s.opt.nu, s.L[1].yq, nullptr, s.err, st);
             else
                 gputo::launch_packed_sweep<double>(gputo::MODE_JACOBI, s.lay[1], s.L[1].Apk, s.L[1].u0,
-                                                   s.L[1].f, s.L[1].diag, s.mask[1], s.L[1].u1, 0.48,
+                                                   s.L[1].f, s.L[1].rdiag, s.mask[1], s.L[1].u1, 0.48,
                                                    0.7, nullptr, st);
         }
         if (r && !lst) lst = r;

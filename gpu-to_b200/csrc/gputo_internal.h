@@ -95,7 +95,7 @@ struct LevelBuf {
     T *f = nullptr;                  // right-hand side of this level
     T *r = nullptr;                  // defect after pre-smoothing (restriction input)
     T *diag = nullptr;               // operator diagonal
-    T *rdiag = nullptr;              // 1 / diag (0 where diag is 0), levels with fine sweeps
+    T *rdiag = nullptr;              // 1 / diag (0 where diag is 0): the sweeps multiply by it
     T *Apk = nullptr;                // packed element matrices, [300][nel] (levels >= 1)
     T *yq = nullptr;                 // level-1 element outputs, [24][nel] (matrix-free level 1)
     uint8_t *mask = nullptr;         // fixed-dof bits per node (bit d = dof d fixed)
@@ -148,7 +148,7 @@ int launch_tc_sweep(int parts, int mode, const Lay &L, const ELay &E, const floa
 
 template <typename T>
 int launch_quad_sweep(int mode, const Lay &L, const ELay &Ef, const T *CX, const T *u, const T *f,
-                      const T *diag, const uint8_t *mask, T *out, T omega, T prerelax, double nu,
+                      const T *rdiag, const uint8_t *mask, T *out, T omega, T prerelax, double nu,
                       T *yscratch, const int *done, int *err, cudaStream_t st);
 void launch_diag_quad(const Lay &L, const double *CXf, double *diag, cudaStream_t st);
 int upload_quadrature_fine(const double *kg_packed, cudaStream_t st);
@@ -180,13 +180,14 @@ int init_fine_kernels();
 int fine_sweep_blocks(const Grid &g);
 // Coarse level (packed element matrices, natural element order).
 template <typename T>
+// The coarse-level sweeps take rdiag = 1/diag (LevelBuf::rdiag).
 void launch_packed_sweep(int mode, const Lay &L, const T *Apk, const T *u, const T *f,
-                         const T *diag, const uint8_t *mask, T *out, T omega, T prerelax,
+                         const T *rdiag, const uint8_t *mask, T *out, T omega, T prerelax,
                          const int *done, cudaStream_t st);
 
 // Element-centric form of the same sweep (yscratch: 24 values per element).
 template <typename T>
-void launch_packed_sweep_ec(int mode, const Lay &L, const T *Apk, const T *u, const T *f, const T *diag,
+void launch_packed_sweep_ec(int mode, const Lay &L, const T *Apk, const T *u, const T *f, const T *rdiag,
                             const uint8_t *mask, T *out, T omega, T prerelax, T *yscratch,
                             const int *done, cudaStream_t st);
 // Levels at least this many elements use the element-centric sweep.

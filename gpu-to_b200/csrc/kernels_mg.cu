@@ -146,7 +146,7 @@ __device__ __forceinline__ void node_ijk(const Grid &g, long long n, int &i, int
 template <typename T, int MODE>
 __global__ void __launch_bounds__(128)
 packed_sweep_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u,
-                    const T *__restrict__ f, const T *__restrict__ diag,
+                    const T *__restrict__ f, const T *__restrict__ rdiag,
                     const uint8_t *__restrict__ mask, T *__restrict__ out, T omega, T prerelax,
                     const int *__restrict__ done)
 {
@@ -179,7 +179,7 @@ packed_sweep_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u,
 #pragma unroll
                     for (int q = 0; q < 3; ++q) {
                         const long long dof = nb + q;
-                        ub[q] = (MODE == MODE_JACOBI_PRE) ? prerelax * f[dof] / diag[dof] : u[dof];
+                        ub[q] = (MODE == MODE_JACOBI_PRE) ? prerelax * f[dof] * rdiag[dof] : u[dof];
                     }
 #pragma unroll
                     for (int d = 0; d < 3; ++d)
@@ -202,8 +202,8 @@ packed_sweep_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u,
             out[dof] = fixed ? T(0) : f[dof] - acc[d];
         } else {
             const T r = fixed ? T(0) : f[dof] - acc[d];
-            const T us = (MODE == MODE_JACOBI_PRE) ? prerelax * f[dof] / diag[dof] : u[dof];
-            out[dof] = us + omega * r / diag[dof];
+            const T us = (MODE == MODE_JACOBI_PRE) ? prerelax * f[dof] * rdiag[dof] : u[dof];
+            out[dof] = us + omega * r * rdiag[dof];
         }
     }
 }
@@ -217,7 +217,7 @@ packed_sweep_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u,
 template <typename T, int MODE>
 __global__ void __launch_bounds__(256)
 packed_sweep_slot_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u, const T *__restrict__ f,
-                         const T *__restrict__ diag, const uint8_t *__restrict__ mask, T *__restrict__ out,
+                         const T *__restrict__ rdiag, const uint8_t *__restrict__ mask, T *__restrict__ out,
                          T omega, T prerelax, const int *__restrict__ done)
 {
     if (done && *done) return;
@@ -242,8 +242,7 @@ packed_sweep_slot_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u
 #pragma unroll
             for (int q = 0; q < 3; ++q) {
                 if (MODE == MODE_JACOBI_PRE) {
-                    const T dv = diag[nb + q];
-                    ub[3 * b + q] = dv != T(0) ? prerelax * f[nb + q] / dv : T(0);
+                    ub[3 * b + q] = prerelax * f[nb + q] * rdiag[nb + q];
                 } else {
                     ub[3 * b + q] = u[nb + q];
                 }
@@ -280,19 +279,18 @@ packed_sweep_slot_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u
             const T r = fixed ? T(0) : f[dof] - s[d];
             T us;
             if (MODE == MODE_JACOBI_PRE) {
-                const T dv = diag[dof];
-                us = dv != T(0) ? prerelax * f[dof] / dv : T(0);
+                us = prerelax * f[dof] * rdiag[dof];
             } else {
                 us = u[dof];
             }
-            out[dof] = us + omega * r / diag[dof];
+            out[dof] = us + omega * r * rdiag[dof];
         }
     }
 }
 
 template <typename T>
 void launch_packed_sweep(int mode, const Lay &L, const T *Apk, const T *u, const T *f,
-                         const T *diag, const uint8_t *mask, T *out, T omega, T prerelax,
+                         const T *rdiag, const uint8_t *mask, T *out, T omega, T prerelax,
                          const int *done, cudaStream_t st)
 {
     const int bs = 128;
@@ -300,16 +298,16 @@ void launch_packed_sweep(int mode, const Lay &L, const T *Apk, const T *u, const
         const unsigned sb = (unsigned)((L.g.nnod() + 31) / 32);
         switch (mode) {
         case MODE_APPLY:
-            packed_sweep_slot_kernel<T, MODE_APPLY><<<sb, 256, 0, st>>>(L, Apk, u, f, diag, mask, out, omega, prerelax, done);
+            packed_sweep_slot_kernel<T, MODE_APPLY><<<sb, 256, 0, st>>>(L, Apk, u, f, rdiag, mask, out, omega, prerelax, done);
             break;
         case MODE_DEFECT:
-            packed_sweep_slot_kernel<T, MODE_DEFECT><<<sb, 256, 0, st>>>(L, Apk, u, f, diag, mask, out, omega, prerelax, done);
+            packed_sweep_slot_kernel<T, MODE_DEFECT><<<sb, 256, 0, st>>>(L, Apk, u, f, rdiag, mask, out, omega, prerelax, done);
             break;
         case MODE_JACOBI:
-            packed_sweep_slot_kernel<T, MODE_JACOBI><<<sb, 256, 0, st>>>(L, Apk, u, f, diag, mask, out, omega, prerelax, done);
+            packed_sweep_slot_kernel<T, MODE_JACOBI><<<sb, 256, 0, st>>>(L, Apk, u, f, rdiag, mask, out, omega, prerelax, done);
             break;
         default:
-            packed_sweep_slot_kernel<T, MODE_JACOBI_PRE><<<sb, 256, 0, st>>>(L, Apk, u, f, diag, mask, out, omega, prerelax, done);
+            packed_sweep_slot_kernel<T, MODE_JACOBI_PRE><<<sb, 256, 0, st>>>(L, Apk, u, f, rdiag, mask, out, omega, prerelax, done);
         }
         count_launches(1);
         return;
@@ -317,16 +315,16 @@ void launch_packed_sweep(int mode, const Lay &L, const T *Apk, const T *u, const
     const unsigned nb = (unsigned)((L.g.nnod() + bs - 1) / bs);
     switch (mode) {
     case MODE_APPLY:
-        packed_sweep_kernel<T, MODE_APPLY><<<nb, bs, 0, st>>>(L, Apk, u, f, diag, mask, out, omega, prerelax, done);
+        packed_sweep_kernel<T, MODE_APPLY><<<nb, bs, 0, st>>>(L, Apk, u, f, rdiag, mask, out, omega, prerelax, done);
         break;
     case MODE_DEFECT:
-        packed_sweep_kernel<T, MODE_DEFECT><<<nb, bs, 0, st>>>(L, Apk, u, f, diag, mask, out, omega, prerelax, done);
+        packed_sweep_kernel<T, MODE_DEFECT><<<nb, bs, 0, st>>>(L, Apk, u, f, rdiag, mask, out, omega, prerelax, done);
         break;
     case MODE_JACOBI:
-        packed_sweep_kernel<T, MODE_JACOBI><<<nb, bs, 0, st>>>(L, Apk, u, f, diag, mask, out, omega, prerelax, done);
+        packed_sweep_kernel<T, MODE_JACOBI><<<nb, bs, 0, st>>>(L, Apk, u, f, rdiag, mask, out, omega, prerelax, done);
         break;
     default:
-        packed_sweep_kernel<T, MODE_JACOBI_PRE><<<nb, bs, 0, st>>>(L, Apk, u, f, diag, mask, out, omega, prerelax, done);
+        packed_sweep_kernel<T, MODE_JACOBI_PRE><<<nb, bs, 0, st>>>(L, Apk, u, f, rdiag, mask, out, omega, prerelax, done);
     }
     count_launches(1);
 }

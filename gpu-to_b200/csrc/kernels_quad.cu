@@ -56,7 +56,7 @@ __device__ __forceinline__ void h22(const T (&P)[2][2], T (&H)[4])
 template <typename T, bool PRE>
 __global__ void __launch_bounds__(128)
 quad_element_kernel(Lay L, const T *__restrict__ CXp, ELay Ef,
-                    const T *__restrict__ u, const T *__restrict__ f, const T *__restrict__ diag,
+                    const T *__restrict__ u, const T *__restrict__ f, const T *__restrict__ rdiag,
                     T prerelax, T lam, T mu, T *__restrict__ y, const int *__restrict__ done)
 {
     if (done && *done) return;
@@ -75,8 +75,7 @@ quad_element_kernel(Lay L, const T *__restrict__ CXp, ELay Ef,
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
             if (PRE) {
-                const T dv = diag[nb + q];
-                ue[3 * a + q] = dv != T(0) ? prerelax * f[nb + q] / dv : T(0);
+                ue[3 * a + q] = prerelax * f[nb + q] * rdiag[nb + q];
             } else {
                 ue[3 * a + q] = u[nb + q];
             }
@@ -170,7 +169,7 @@ quad_element_kernel(Lay L, const T *__restrict__ CXp, ELay Ef,
 template <typename T, int MODE>
 __global__ void __launch_bounds__(128)
 quad_node_kernel(Lay L, const T *__restrict__ y, const T *__restrict__ u, const T *__restrict__ f,
-                 const T *__restrict__ diag, const uint8_t *__restrict__ mask, T *__restrict__ out,
+                 const T *__restrict__ rdiag, const uint8_t *__restrict__ mask, T *__restrict__ out,
                  T omega, T prerelax, const int *__restrict__ done)
 {
     if (done && *done) return;
@@ -221,19 +220,18 @@ quad_node_kernel(Lay L, const T *__restrict__ y, const T *__restrict__ u, const 
             const T r = fixed ? T(0) : f[dof] - acc[d];
             T us;
             if (MODE == MODE_JACOBI_PRE) {
-                const T dv = diag[dof];
-                us = dv != T(0) ? prerelax * f[dof] / dv : T(0);
+                us = prerelax * f[dof] * rdiag[dof];
             } else {
                 us = u[dof];
             }
-            out[dof] = us + omega * r / diag[dof];
+            out[dof] = us + omega * r * rdiag[dof];
         }
     }
 }
 
 template <typename T>
 int launch_quad_sweep(int mode, const Lay &L, const ELay &Ef, const T *CX, const T *u, const T *f,
-                      const T *diag, const uint8_t *mask, T *out, T omega, T prerelax, double nu,
+                      const T *rdiag, const uint8_t *mask, T *out, T omega, T prerelax, double nu,
                       T *yscratch, const int *done, int *, cudaStream_t st)
 {
     // Lame constants of the unit-modulus material, with the 1/64 of the two
@@ -244,23 +242,23 @@ int launch_quad_sweep(int mode, const Lay &L, const ELay &Ef, const T *CX, const
     const unsigned eb = (unsigned)((L.g.nel() + bs - 1) / bs);
     const unsigned nb = (unsigned)((L.g.nnod() + bs - 1) / bs);
     if (mode == MODE_JACOBI_PRE)
-        quad_element_kernel<T, true><<<eb, bs, 0, st>>>(L, CX, Ef, u, f, diag, prerelax, lam, mu,
+        quad_element_kernel<T, true><<<eb, bs, 0, st>>>(L, CX, Ef, u, f, rdiag, prerelax, lam, mu,
                                                         yscratch, done);
     else
-        quad_element_kernel<T, false><<<eb, bs, 0, st>>>(L, CX, Ef, u, f, diag, prerelax, lam, mu,
+        quad_element_kernel<T, false><<<eb, bs, 0, st>>>(L, CX, Ef, u, f, rdiag, prerelax, lam, mu,
                                                          yscratch, done);
     switch (mode) {
     case MODE_APPLY:
-        quad_node_kernel<T, MODE_APPLY><<<nb, bs, 0, st>>>(L, yscratch, u, f, diag, mask, out, omega, prerelax, done);
+        quad_node_kernel<T, MODE_APPLY><<<nb, bs, 0, st>>>(L, yscratch, u, f, rdiag, mask, out, omega, prerelax, done);
         break;
     case MODE_DEFECT:
-        quad_node_kernel<T, MODE_DEFECT><<<nb, bs, 0, st>>>(L, yscratch, u, f, diag, mask, out, omega, prerelax, done);
+        quad_node_kernel<T, MODE_DEFECT><<<nb, bs, 0, st>>>(L, yscratch, u, f, rdiag, mask, out, omega, prerelax, done);
         break;
     case MODE_JACOBI:
-        quad_node_kernel<T, MODE_JACOBI><<<nb, bs, 0, st>>>(L, yscratch, u, f, diag, mask, out, omega, prerelax, done);
+        quad_node_kernel<T, MODE_JACOBI><<<nb, bs, 0, st>>>(L, yscratch, u, f, rdiag, mask, out, omega, prerelax, done);
         break;
     default:
-        quad_node_kernel<T, MODE_JACOBI_PRE><<<nb, bs, 0, st>>>(L, yscratch, u, f, diag, mask, out, omega, prerelax, done);
+        quad_node_kernel<T, MODE_JACOBI_PRE><<<nb, bs, 0, st>>>(L, yscratch, u, f, rdiag, mask, out, omega, prerelax, done);
     }
     count_launches(2);
     return GPUTO_OK;
@@ -303,7 +301,7 @@ __device__ __forceinline__ void packed_rows(const T *__restrict__ A, long long n
 template <typename T, bool PRE>
 __global__ void __launch_bounds__(128)
 packed_element_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u, const T *__restrict__ f,
-                      const T *__restrict__ diag, T prerelax, T *__restrict__ y, const int *__restrict__ done)
+                      const T *__restrict__ rdiag, T prerelax, T *__restrict__ y, const int *__restrict__ done)
 {
     if (done && *done) return;
     __shared__ T part[4][24][32];
@@ -327,8 +325,7 @@ packed_element_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u, c
 #pragma unroll
             for (int q = 0; q < 3; ++q) {
                 if (PRE) {
-                    const T dv = diag[nb + q];
-                    ue[3 * a + q] = dv != T(0) ? prerelax * f[nb + q] / dv : T(0);
+                    ue[3 * a + q] = prerelax * f[nb + q] * rdiag[nb + q];
                 } else {
                     ue[3 * a + q] = u[nb + q];
                 }
@@ -355,7 +352,7 @@ packed_element_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u, c
 }
 
 template <typename T>
-void launch_packed_sweep_ec(int mode, const Lay &L, const T *Apk, const T *u, const T *f, const T *diag,
+void launch_packed_sweep_ec(int mode, const Lay &L, const T *Apk, const T *u, const T *f, const T *rdiag,
                             const uint8_t *mask, T *out, T omega, T prerelax, T *yscratch,
                             const int *done, cudaStream_t st)
 {
@@ -363,21 +360,21 @@ void launch_packed_sweep_ec(int mode, const Lay &L, const T *Apk, const T *u, co
     const unsigned eb = (unsigned)((L.g.nel() + 31) / 32);   // 32 elements per CTA of 4 warps
     const unsigned nb = (unsigned)((L.g.nnod() + bs - 1) / bs);
     if (mode == MODE_JACOBI_PRE)
-        packed_element_kernel<T, true><<<eb, bs, 0, st>>>(L, Apk, u, f, diag, prerelax, yscratch, done);
+        packed_element_kernel<T, true><<<eb, bs, 0, st>>>(L, Apk, u, f, rdiag, prerelax, yscratch, done);
     else
-        packed_element_kernel<T, false><<<eb, bs, 0, st>>>(L, Apk, u, f, diag, prerelax, yscratch, done);
+        packed_element_kernel<T, false><<<eb, bs, 0, st>>>(L, Apk, u, f, rdiag, prerelax, yscratch, done);
     switch (mode) {
     case MODE_APPLY:
-        quad_node_kernel<T, MODE_APPLY><<<nb, bs, 0, st>>>(L, yscratch, u, f, diag, mask, out, omega, prerelax, done);
+        quad_node_kernel<T, MODE_APPLY><<<nb, bs, 0, st>>>(L, yscratch, u, f, rdiag, mask, out, omega, prerelax, done);
         break;
     case MODE_DEFECT:
-        quad_node_kernel<T, MODE_DEFECT><<<nb, bs, 0, st>>>(L, yscratch, u, f, diag, mask, out, omega, prerelax, done);
+        quad_node_kernel<T, MODE_DEFECT><<<nb, bs, 0, st>>>(L, yscratch, u, f, rdiag, mask, out, omega, prerelax, done);
         break;
     case MODE_JACOBI:
-        quad_node_kernel<T, MODE_JACOBI><<<nb, bs, 0, st>>>(L, yscratch, u, f, diag, mask, out, omega, prerelax, done);
+        quad_node_kernel<T, MODE_JACOBI><<<nb, bs, 0, st>>>(L, yscratch, u, f, rdiag, mask, out, omega, prerelax, done);
         break;
     default:
-        quad_node_kernel<T, MODE_JACOBI_PRE><<<nb, bs, 0, st>>>(L, yscratch, u, f, diag, mask, out, omega, prerelax, done);
+        quad_node_kernel<T, MODE_JACOBI_PRE><<<nb, bs, 0, st>>>(L, yscratch, u, f, rdiag, mask, out, omega, prerelax, done);
     }
     count_launches(2);
 }

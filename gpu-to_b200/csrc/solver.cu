@@ -71,7 +71,7 @@ int Solver::alloc_levels(LevelBuf<T> *Lv, bool with_matrices)
         ALLOC(b.u0, nv);
         ALLOC(b.r, nv);
         ALLOC(b.diag, nv);
-        if (l == 0 || (redisc() && l < nl - 1)) ALLOC(b.rdiag, nv);   // levels with fine sweeps
+        ALLOC(b.rdiag, nv);
         ALLOC(b.u1, nv);
         ALLOC(b.f, nv);
         // level 1 is applied matrix-free unless it is the coarsest level; the
@@ -350,13 +350,13 @@ void Solver::vcycle_impl(LevelBuf<T> *Lv, const T *CXl, const T *r0, T *z0, cons
             else cxl = CXrp[l];
             note(fine_sweep<T>(l, mode, lay[l], elayr[l], cxl, u, f, Lv[l], out, w, pr, nullptr, done, st));
         } else if (l == 1 && quad_level1())
-            note(launch_quad_sweep<T>(mode, lay[1], elay, CXl, u, f, Lv[1].diag, mask[1], out, w, pr,
+            note(launch_quad_sweep<T>(mode, lay[1], elay, CXl, u, f, Lv[1].rdiag, mask[1], out, w, pr,
                                       opt.nu, Lv[1].yq, done, err, st));
         else if (Lv[l].yq)
-            launch_packed_sweep_ec<T>(mode, lay[l], Lv[l].Apk, u, f, Lv[l].diag, mask[l], out, w, pr,
+            launch_packed_sweep_ec<T>(mode, lay[l], Lv[l].Apk, u, f, Lv[l].rdiag, mask[l], out, w, pr,
                                       Lv[l].yq, done, st);
         else
-            launch_packed_sweep<T>(mode, lay[l], Lv[l].Apk, u, f, Lv[l].diag, mask[l], out, w, pr, done,
+            launch_packed_sweep<T>(mode, lay[l], Lv[l].Apk, u, f, Lv[l].rdiag, mask[l], out, w, pr, done,
                                    st);
     };
     auto bufs = [&](int l, int which) -> T * {
@@ -426,10 +426,10 @@ void Solver::learned_correction(double *z, const int *done, cudaStream_t st)
 void Solver::apply_level_f32(int l, const float *u, float *out, cudaStream_t st)
 {
     if (Lf[l].yq)
-        launch_packed_sweep_ec<float>(MODE_APPLY, lay[l], Lf[l].Apk, u, nullptr, Lf[l].diag, mask[l], out, 1.f, 0.f,
+        launch_packed_sweep_ec<float>(MODE_APPLY, lay[l], Lf[l].Apk, u, nullptr, Lf[l].rdiag, mask[l], out, 1.f, 0.f,
                                       Lf[l].yq, nullptr, st);
     else
-        launch_packed_sweep<float>(MODE_APPLY, lay[l], Lf[l].Apk, u, nullptr, Lf[l].diag, mask[l], out, 1.f, 0.f,
+        launch_packed_sweep<float>(MODE_APPLY, lay[l], Lf[l].Apk, u, nullptr, Lf[l].rdiag, mask[l], out, 1.f, 0.f,
                                    nullptr, st);
 }
 
