@@ -589,16 +589,25 @@ static int mex_solve(const char *log_name, int cg_lines, const double *Ke0, cons
         return st;
     }
     const long long nd = s.g[0].ndof(), ne = s.g[0].nel();
-    GPUTO_CUDA(cudaMemcpyAsync(s.Dn, F, sizeof(double) * nd, cudaMemcpyHostToDevice, strm));
-    gputo::launch_pack(s.lay[0], s.Dn, s.Fw, 0, strm);
-    GPUTO_CUDA(cudaMemcpyAsync(s.CX, CX, sizeof(double) * ne, cudaMemcpyHostToDevice, strm));
+    std::unique_lock<std::mutex> io(gputo::host_io_mutex());
+    GPUTO_CUDA(cudaStreamSynchronize(strm));   // set_problem's uploads have landed before Dn is reused
+    st = gputo::host_to_device(s.Dn, F, sizeof(double) * nd);
+    if (!st) gputo::launch_pack(s.lay[0], s.Dn, s.Fw, 0, strm);
+    if (!st) st = gputo::host_to_device(s.CX, CX, sizeof(double) * ne);
+    io.unlock();
+    if (st) {
+        if (log) std::fclose(log);
+        return st;
+    }
     st = s.setup(s.CX, strm);
     if (!st) st = s.solve(s.Fw, s.Uw, tol, maxit, relres, nit, strm, printLev >= cg_lines ? log : nullptr);
     if (!st || st == GPUTO_ERR_BREAKDOWN) {
         // solver frame -> MATLAB frame: y components negated (mgcg1.cu:282-283)
         gputo::launch_unpack(s.lay[0], s.Uw, s.Dn, 1, strm);
-        GPUTO_CUDA(cudaMemcpyAsync(U, s.Dn, sizeof(double) * nd, cudaMemcpyDeviceToHost, strm));
         GPUTO_CUDA(cudaStreamSynchronize(strm));
+        std::lock_guard<std::mutex> io2(gputo::host_io_mutex());
+        const int cs = gputo::device_to_host(U, s.Dn, sizeof(double) * nd);
+        if (cs && !st) st = cs;
     }
     if (log) {
         const double secs =
@@ -736,32 +745,24 @@ int gputo_compliance_sens(const double *Ke0, const double *U, const double *CX,
     if (st) return st;
     Grid g{nelx, nely, nelz};
     const size_t nd = (size_t)g.ndof(), ne = (size_t)g.nel();
-    double *dU = nullptr, *dCX = nullptr, *dS = nullptr, *dce = nullptr, *ddc = nullptr;
-    auto cleanup = [&]() {
-        cudaFree(dU);
-        cudaFree(dCX);
-        cudaFree(dS);
-        cudaFree(dce);
-        cudaFree(ddc);
-    };
-    if (cudaMalloc(&dU, nd * 8) || (CX && cudaMalloc(&dCX, ne * 8)) ||
-        (dsK && cudaMalloc(&dS, ne * 8)) || (ce && cudaMalloc(&dce, ne * 8)) ||
-        (dc && cudaMalloc(&ddc, ne * 8))) {
-        cudaGetLastError();
-        cleanup();
-        gputo::set_error("cudaMalloc failed in gputo_compliance_sens");
-        return GPUTO_ERR_OOM;
-    }
-    cudaMemcpy(dU, U, nd * 8, cudaMemcpyHostToDevice);
+    std::lock_guard<std::mutex> lock(gputo::host_io_mutex());
+    // device buffers kept between calls (slots 0-4 of the host-call workspace)
+    double *dU = gputo::host_call_buffer(0, nd, &st);
+    double *dCX = (!st && CX) ? gputo::host_call_buffer(1, ne, &st) : nullptr;
+    double *dS = (!st && dsK) ? gputo::host_call_buffer(2, ne, &st) : nullptr;
+    double *dce = (!st && ce) ? gputo::host_call_buffer(3, ne, &st) : nullptr;
+    double *ddc = (!st && dc) ? gputo::host_call_buffer(4, ne, &st) : nullptr;
+    if (st) return st;
+    if (!st) st = gputo::host_to_device(dU, U, nd * 8);
+    if (!st && CX) st = gputo::host_to_device(dCX, CX, ne * 8);
+    if (!st && dsK) st = gputo::host_to_device(dS, dsK, ne * 8);
+    if (st) return st;
     gputo::launch_flip_y(g.nnod(), dU, 0);  // MATLAB frame -> solver frame
-    if (CX) cudaMemcpy(dCX, CX, ne * 8, cudaMemcpyHostToDevice);
-    if (dsK) cudaMemcpy(dS, dsK, ne * 8, cudaMemcpyHostToDevice);
-    cudaDeviceSynchronize();
+    GPUTO_CUDA(cudaDeviceSynchronize());
     st = gputo_compliance_sens_dev(Ke0, dU, dCX, dS, nelx, nely, nelz, dce, ddc, compliance,
                                    nullptr);
-    if (!st && ce) cudaMemcpy(ce, dce, ne * 8, cudaMemcpyDeviceToHost);
-    if (!st && dc) cudaMemcpy(dc, ddc, ne * 8, cudaMemcpyDeviceToHost);
-    cleanup();
+    if (!st && ce) st = gputo::device_to_host(ce, dce, ne * 8);
+    if (!st && dc) st = gputo::device_to_host(dc, ddc, ne * 8);
     return st;
 }
 
@@ -794,23 +795,15 @@ int gputo_density_filter(const double *in, const double *divisor, double *out, i
     int st = gputo::check_device();
     if (st) return st;
     const size_t ne = (size_t)nelx * nely * nelz;
-    double *din = nullptr, *ddiv = nullptr, *dout = nullptr;
-    if (cudaMalloc(&din, ne * 8) || (divisor && cudaMalloc(&ddiv, ne * 8)) ||
-        cudaMalloc(&dout, ne * 8)) {
-        cudaGetLastError();
-        cudaFree(din);
-        cudaFree(ddiv);
-        cudaFree(dout);
-        gputo::set_error("cudaMalloc failed in gputo_density_filter");
-        return GPUTO_ERR_OOM;
-    }
-    cudaMemcpy(din, in, ne * 8, cudaMemcpyHostToDevice);
-    if (divisor) cudaMemcpy(ddiv, divisor, ne * 8, cudaMemcpyHostToDevice);
-    st = gputo_density_filter_dev(din, ddiv, dout, nelx, nely, nelz, rmin, normalize, nullptr);
-    if (!st) cudaMemcpy(out, dout, ne * 8, cudaMemcpyDeviceToHost);
-    cudaFree(din);
-    cudaFree(ddiv);
-    cudaFree(dout);
+    std::lock_guard<std::mutex> lock(gputo::host_io_mutex());
+    double *din = gputo::host_call_buffer(0, ne, &st);
+    double *ddiv = (!st && divisor) ? gputo::host_call_buffer(1, ne, &st) : nullptr;
+    double *dout = !st ? gputo::host_call_buffer(2, ne, &st) : nullptr;
+    if (st) return st;
+    st = gputo::host_to_device(din, in, ne * 8);
+    if (!st && divisor) st = gputo::host_to_device(ddiv, divisor, ne * 8);
+    if (!st) st = gputo_density_filter_dev(din, ddiv, dout, nelx, nely, nelz, rmin, normalize, nullptr);
+    if (!st) st = gputo::device_to_host(out, dout, ne * 8);
     return st;
 }
 
@@ -922,18 +915,14 @@ int gputo_oc_update(const double *x, const double *dc, const double *dV0, long l
     if (!x || !dc || !dV0 || !xnew || n <= 0) return GPUTO_ERR_ARG;
     int st = gputo::check_device();
     if (st) return st;
-    double *d = nullptr;
-    if (cudaMalloc(&d, sizeof(double) * 4 * (size_t)n) != cudaSuccess) {
-        cudaGetLastError();
-        gputo::set_error("cudaMalloc failed in gputo_oc_update");
-        return GPUTO_ERR_OOM;
-    }
-    cudaMemcpy(d, x, sizeof(double) * n, cudaMemcpyHostToDevice);
-    cudaMemcpy(d + n, dc, sizeof(double) * n, cudaMemcpyHostToDevice);
-    cudaMemcpy(d + 2 * n, dV0, sizeof(double) * n, cudaMemcpyHostToDevice);
-    st = gputo_oc_update_dev(d, d + n, d + 2 * n, n, volfrac, move, d + 3 * n, lmid, nullptr);
-    if (!st) cudaMemcpy(xnew, d + 3 * n, sizeof(double) * n, cudaMemcpyDeviceToHost);
-    cudaFree(d);
+    std::lock_guard<std::mutex> lock(gputo::host_io_mutex());
+    double *d = gputo::host_call_buffer(0, 4 * (size_t)n, &st);
+    if (st) return st;
+    st = gputo::host_to_device(d, x, sizeof(double) * n);
+    if (!st) st = gputo::host_to_device(d + n, dc, sizeof(double) * n);
+    if (!st) st = gputo::host_to_device(d + 2 * n, dV0, sizeof(double) * n);
+    if (!st) st = gputo_oc_update_dev(d, d + n, d + 2 * n, n, volfrac, move, d + 3 * n, lmid, nullptr);
+    if (!st) st = gputo::device_to_host(xnew, d + 3 * n, sizeof(double) * n);
     return st;
 }
 

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstddef>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -109,6 +110,17 @@ int cuda_status(cudaError_t e, const char *what);
         cudaError_t _e = (call);                                             \
         if (_e != cudaSuccess) return ::gputo::cuda_status(_e, #call);       \
     } while (0)
+
+// ---- host arrays (hostio.cpp) ----------------------------------------------
+// Copies between a caller's (pageable) host array and the device through
+// pinned chunks, host side split over a few threads; both return once the
+// data has arrived.  host_call_buffer: a device buffer of at least 'count'
+// doubles for slot 'slot' of the current device, kept between calls.  Hold
+// host_io_mutex() around all three.
+std::mutex &host_io_mutex();
+int host_to_device(void *dst, const void *src, size_t bytes);
+int device_to_host(void *dst, const void *src, size_t bytes);
+double *host_call_buffer(int slot, size_t count, int *status);
 
 // ---- kernel launchers (kernels_*.cu) --------------------------------------
 // Level-0 element matrix in constant memory (FP64 and FP32 copies).
