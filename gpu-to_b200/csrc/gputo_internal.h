@@ -6,6 +6,7 @@
 #include <cstddef>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "gputo.h"
@@ -297,6 +298,33 @@ void launch_oc_update(long long n, const double *x, const double *dc, const doub
 
 // Counter of kernel launches issued by this library (per process).
 void count_launches(long long n);
+
+// Programmatic dependent launch.  A kernel started with launch_pdl may begin
+// while its predecessor in the stream is still finishing (its launch latency
+// overlaps the predecessor's tail); it calls pdl_wait() before it touches
+// memory, which returns once the predecessor has completed and its writes
+// are visible.  A kernel that calls pdl_wait() but is launched normally is
+// unaffected.
+#if defined(__CUDACC__)
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args &&...args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+#endif
 long long launches_issued();
 
 // ---------------------------------------------------------------------------

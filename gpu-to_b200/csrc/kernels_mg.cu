@@ -150,6 +150,7 @@ packed_sweep_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u,
                     const uint8_t *__restrict__ mask, T *__restrict__ out, T omega, T prerelax,
                     const int *__restrict__ done)
 {
+    pdl_wait();
     if (done && *done) return;
     const Grid &g = L.g;
     const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -220,6 +221,7 @@ packed_sweep_slot_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u
                          const T *__restrict__ rdiag, const uint8_t *__restrict__ mask, T *__restrict__ out,
                          T omega, T prerelax, const int *__restrict__ done)
 {
+    pdl_wait();
     if (done && *done) return;
     __shared__ T part[8][32][3];
     const Grid &g = L.g;
@@ -298,16 +300,16 @@ void launch_packed_sweep(int mode, const Lay &L, const T *Apk, const T *u, const
         const unsigned sb = (unsigned)((L.g.nnod() + 31) / 32);
         switch (mode) {
         case MODE_APPLY:
-            packed_sweep_slot_kernel<T, MODE_APPLY><<<sb, 256, 0, st>>>(L, Apk, u, f, rdiag, mask, out, omega, prerelax, done);
+            launch_pdl(packed_sweep_slot_kernel<T, MODE_APPLY>, dim3(sb), dim3(256), 0, st, L, Apk, u, f, rdiag, mask, out, omega, prerelax, done);
             break;
         case MODE_DEFECT:
-            packed_sweep_slot_kernel<T, MODE_DEFECT><<<sb, 256, 0, st>>>(L, Apk, u, f, rdiag, mask, out, omega, prerelax, done);
+            launch_pdl(packed_sweep_slot_kernel<T, MODE_DEFECT>, dim3(sb), dim3(256), 0, st, L, Apk, u, f, rdiag, mask, out, omega, prerelax, done);
             break;
         case MODE_JACOBI:
-            packed_sweep_slot_kernel<T, MODE_JACOBI><<<sb, 256, 0, st>>>(L, Apk, u, f, rdiag, mask, out, omega, prerelax, done);
+            launch_pdl(packed_sweep_slot_kernel<T, MODE_JACOBI>, dim3(sb), dim3(256), 0, st, L, Apk, u, f, rdiag, mask, out, omega, prerelax, done);
             break;
         default:
-            packed_sweep_slot_kernel<T, MODE_JACOBI_PRE><<<sb, 256, 0, st>>>(L, Apk, u, f, rdiag, mask, out, omega, prerelax, done);
+            launch_pdl(packed_sweep_slot_kernel<T, MODE_JACOBI_PRE>, dim3(sb), dim3(256), 0, st, L, Apk, u, f, rdiag, mask, out, omega, prerelax, done);
         }
         count_launches(1);
         return;
@@ -315,16 +317,16 @@ void launch_packed_sweep(int mode, const Lay &L, const T *Apk, const T *u, const
     const unsigned nb = (unsigned)((L.g.nnod() + bs - 1) / bs);
     switch (mode) {
     case MODE_APPLY:
-        packed_sweep_kernel<T, MODE_APPLY><<<nb, bs, 0, st>>>(L, Apk, u, f, rdiag, mask, out, omega, prerelax, done);
+        launch_pdl(packed_sweep_kernel<T, MODE_APPLY>, dim3(nb), dim3(bs), 0, st, L, Apk, u, f, rdiag, mask, out, omega, prerelax, done);
         break;
     case MODE_DEFECT:
-        packed_sweep_kernel<T, MODE_DEFECT><<<nb, bs, 0, st>>>(L, Apk, u, f, rdiag, mask, out, omega, prerelax, done);
+        launch_pdl(packed_sweep_kernel<T, MODE_DEFECT>, dim3(nb), dim3(bs), 0, st, L, Apk, u, f, rdiag, mask, out, omega, prerelax, done);
         break;
     case MODE_JACOBI:
-        packed_sweep_kernel<T, MODE_JACOBI><<<nb, bs, 0, st>>>(L, Apk, u, f, rdiag, mask, out, omega, prerelax, done);
+        launch_pdl(packed_sweep_kernel<T, MODE_JACOBI>, dim3(nb), dim3(bs), 0, st, L, Apk, u, f, rdiag, mask, out, omega, prerelax, done);
         break;
     default:
-        packed_sweep_kernel<T, MODE_JACOBI_PRE><<<nb, bs, 0, st>>>(L, Apk, u, f, rdiag, mask, out, omega, prerelax, done);
+        launch_pdl(packed_sweep_kernel<T, MODE_JACOBI_PRE>, dim3(nb), dim3(bs), 0, st, L, Apk, u, f, rdiag, mask, out, omega, prerelax, done);
     }
     count_launches(1);
 }
@@ -348,6 +350,7 @@ __global__ void restrict_kernel(Lay Lc, Lay Lf, const T *__restrict__ rf,
                                 const uint8_t *__restrict__ maskc, T *__restrict__ fc,
                                 const int *__restrict__ done)
 {
+    pdl_wait();
     if (done && *done) return;
     const Grid &gc = Lc.g;
     const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -388,7 +391,7 @@ void launch_restrict(const Lay &Lc, const Lay &Lf, const T *rf, const uint8_t *m
                      const int *done, cudaStream_t st)
 {
     const int bs = 128;
-    restrict_kernel<T><<<(unsigned)((Lc.g.nnod() + bs - 1) / bs), bs, 0, st>>>(Lc, Lf, rf, maskc, fc, done);
+    launch_pdl(restrict_kernel<T>, dim3((unsigned)((Lc.g.nnod() + bs - 1) / bs)), dim3(bs), 0, st, Lc, Lf, rf, maskc, fc, done);
     count_launches(1);
 }
 template void launch_restrict<double>(const Lay &, const Lay &, const double *, const uint8_t *,
@@ -403,6 +406,7 @@ __global__ void prolong_kernel(Lay Lf, Lay Lc, const T *__restrict__ uc,
                                const uint8_t *__restrict__ maskf, T *__restrict__ uf,
                                const int *__restrict__ done)
 {
+    pdl_wait();
     if (done && *done) return;
     const Grid &gf = Lf.g;
     const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -438,7 +442,7 @@ void launch_prolong_add(const Lay &Lf, const Lay &Lc, const T *uc, const uint8_t
                         const int *done, cudaStream_t st)
 {
     const int bs = 128;
-    prolong_kernel<T><<<(unsigned)((Lf.g.nnod() + bs - 1) / bs), bs, 0, st>>>(Lf, Lc, uc, maskf, uf, done);
+    launch_pdl(prolong_kernel<T>, dim3((unsigned)((Lf.g.nnod() + bs - 1) / bs)), dim3(bs), 0, st, Lf, Lc, uc, maskf, uf, done);
     count_launches(1);
 }
 template void launch_prolong_add<double>(const Lay &, const Lay &, const double *, const uint8_t *,
@@ -943,6 +947,7 @@ __global__ void gemv_warp_kernel(Lay L, const double *__restrict__ M, const Tin 
                                  Tout *__restrict__ y, int lower, int in_padded, int out_padded,
                                  const int *__restrict__ done)
 {
+    pdl_wait();
     if (done && *done) return;
     const int n = (int)L.g.ndof();
     const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -966,8 +971,8 @@ void launch_coarse_solve(const Lay &L, const double *Linv, const double *LinvT, 
     const int n = (int)L.g.ndof();
     const int bs = 256;
     const unsigned nb = (unsigned)((n * 32 + bs - 1) / bs);
-    gemv_warp_kernel<T, double><<<nb, bs, 0, st>>>(L, Linv, b, tmp, 1, 1, 0, done);
-    gemv_warp_kernel<double, T><<<nb, bs, 0, st>>>(L, LinvT, tmp, x, 0, 0, 1, done);
+    launch_pdl(gemv_warp_kernel<T, double>, dim3(nb), dim3(bs), 0, st, L, Linv, b, tmp, 1, 1, 0, done);
+    launch_pdl(gemv_warp_kernel<double, T>, dim3(nb), dim3(bs), 0, st, L, LinvT, tmp, x, 0, 0, 1, done);
     count_launches(2);
 }
 template void launch_coarse_solve<double>(const Lay &, const double *, const double *, const double *,

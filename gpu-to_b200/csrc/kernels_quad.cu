@@ -59,6 +59,7 @@ quad_element_kernel(Lay L, const T *__restrict__ CXp, ELay Ef,
                     const T *__restrict__ u, const T *__restrict__ f, const T *__restrict__ rdiag,
                     T prerelax, T lam, T mu, T *__restrict__ y, const int *__restrict__ done)
 {
+    pdl_wait();
     if (done && *done) return;
     const Grid &g = L.g;
     const long long nel = g.nel();
@@ -172,6 +173,7 @@ quad_node_kernel(Lay L, const T *__restrict__ y, const T *__restrict__ u, const 
                  const T *__restrict__ rdiag, const uint8_t *__restrict__ mask, T *__restrict__ out,
                  T omega, T prerelax, const int *__restrict__ done)
 {
+    pdl_wait();
     if (done && *done) return;
     const Grid &g = L.g;
     const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -242,23 +244,23 @@ int launch_quad_sweep(int mode, const Lay &L, const ELay &Ef, const T *CX, const
     const unsigned eb = (unsigned)((L.g.nel() + bs - 1) / bs);
     const unsigned nb = (unsigned)((L.g.nnod() + bs - 1) / bs);
     if (mode == MODE_JACOBI_PRE)
-        quad_element_kernel<T, true><<<eb, bs, 0, st>>>(L, CX, Ef, u, f, rdiag, prerelax, lam, mu,
+        launch_pdl(quad_element_kernel<T, true>, dim3(eb), dim3(bs), 0, st, L, CX, Ef, u, f, rdiag, prerelax, lam, mu,
                                                         yscratch, done);
     else
-        quad_element_kernel<T, false><<<eb, bs, 0, st>>>(L, CX, Ef, u, f, rdiag, prerelax, lam, mu,
+        launch_pdl(quad_element_kernel<T, false>, dim3(eb), dim3(bs), 0, st, L, CX, Ef, u, f, rdiag, prerelax, lam, mu,
                                                          yscratch, done);
     switch (mode) {
     case MODE_APPLY:
-        quad_node_kernel<T, MODE_APPLY><<<nb, bs, 0, st>>>(L, yscratch, u, f, rdiag, mask, out, omega, prerelax, done);
+        launch_pdl(quad_node_kernel<T, MODE_APPLY>, dim3(nb), dim3(bs), 0, st, L, yscratch, u, f, rdiag, mask, out, omega, prerelax, done);
         break;
     case MODE_DEFECT:
-        quad_node_kernel<T, MODE_DEFECT><<<nb, bs, 0, st>>>(L, yscratch, u, f, rdiag, mask, out, omega, prerelax, done);
+        launch_pdl(quad_node_kernel<T, MODE_DEFECT>, dim3(nb), dim3(bs), 0, st, L, yscratch, u, f, rdiag, mask, out, omega, prerelax, done);
         break;
     case MODE_JACOBI:
-        quad_node_kernel<T, MODE_JACOBI><<<nb, bs, 0, st>>>(L, yscratch, u, f, rdiag, mask, out, omega, prerelax, done);
+        launch_pdl(quad_node_kernel<T, MODE_JACOBI>, dim3(nb), dim3(bs), 0, st, L, yscratch, u, f, rdiag, mask, out, omega, prerelax, done);
         break;
     default:
-        quad_node_kernel<T, MODE_JACOBI_PRE><<<nb, bs, 0, st>>>(L, yscratch, u, f, rdiag, mask, out, omega, prerelax, done);
+        launch_pdl(quad_node_kernel<T, MODE_JACOBI_PRE>, dim3(nb), dim3(bs), 0, st, L, yscratch, u, f, rdiag, mask, out, omega, prerelax, done);
     }
     count_launches(2);
     return GPUTO_OK;
@@ -303,6 +305,7 @@ __global__ void __launch_bounds__(128)
 packed_element_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u, const T *__restrict__ f,
                       const T *__restrict__ rdiag, T prerelax, T *__restrict__ y, const int *__restrict__ done)
 {
+    pdl_wait();
     if (done && *done) return;
     __shared__ T part[4][24][32];
     const Grid &g = L.g;
@@ -360,21 +363,21 @@ void launch_packed_sweep_ec(int mode, const Lay &L, const T *Apk, const T *u, co
     const unsigned eb = (unsigned)((L.g.nel() + 31) / 32);   // 32 elements per CTA of 4 warps
     const unsigned nb = (unsigned)((L.g.nnod() + bs - 1) / bs);
     if (mode == MODE_JACOBI_PRE)
-        packed_element_kernel<T, true><<<eb, bs, 0, st>>>(L, Apk, u, f, rdiag, prerelax, yscratch, done);
+        launch_pdl(packed_element_kernel<T, true>, dim3(eb), dim3(bs), 0, st, L, Apk, u, f, rdiag, prerelax, yscratch, done);
     else
-        packed_element_kernel<T, false><<<eb, bs, 0, st>>>(L, Apk, u, f, rdiag, prerelax, yscratch, done);
+        launch_pdl(packed_element_kernel<T, false>, dim3(eb), dim3(bs), 0, st, L, Apk, u, f, rdiag, prerelax, yscratch, done);
     switch (mode) {
     case MODE_APPLY:
-        quad_node_kernel<T, MODE_APPLY><<<nb, bs, 0, st>>>(L, yscratch, u, f, rdiag, mask, out, omega, prerelax, done);
+        launch_pdl(quad_node_kernel<T, MODE_APPLY>, dim3(nb), dim3(bs), 0, st, L, yscratch, u, f, rdiag, mask, out, omega, prerelax, done);
         break;
     case MODE_DEFECT:
-        quad_node_kernel<T, MODE_DEFECT><<<nb, bs, 0, st>>>(L, yscratch, u, f, rdiag, mask, out, omega, prerelax, done);
+        launch_pdl(quad_node_kernel<T, MODE_DEFECT>, dim3(nb), dim3(bs), 0, st, L, yscratch, u, f, rdiag, mask, out, omega, prerelax, done);
         break;
     case MODE_JACOBI:
-        quad_node_kernel<T, MODE_JACOBI><<<nb, bs, 0, st>>>(L, yscratch, u, f, rdiag, mask, out, omega, prerelax, done);
+        launch_pdl(quad_node_kernel<T, MODE_JACOBI>, dim3(nb), dim3(bs), 0, st, L, yscratch, u, f, rdiag, mask, out, omega, prerelax, done);
         break;
     default:
-        quad_node_kernel<T, MODE_JACOBI_PRE><<<nb, bs, 0, st>>>(L, yscratch, u, f, rdiag, mask, out, omega, prerelax, done);
+        launch_pdl(quad_node_kernel<T, MODE_JACOBI_PRE>, dim3(nb), dim3(bs), 0, st, L, yscratch, u, f, rdiag, mask, out, omega, prerelax, done);
     }
     count_launches(2);
 }
