@@ -299,7 +299,7 @@ def run_ours(args):
                 "achieved": round(dom["gbs"], 1), "peak": hbm_peak, "unit": "GB/s",
                 "frac": round(dom["gbs"] / hbm_peak, 4), "peak_source": peak_src,
                 "traffic": HSWEEP32_DRAM_BYTES,
-                "note": "issue-bound, not HBM-bound: ~420 instructions per element at 60% issue activity"}
+                "note": "issue-bound, not HBM-bound: ~380 instructions per element at 57% issue activity"}
 
     result = {
         "metric": METRIC, "value": round(s_mixed, 5), "unit": "s/design-iter",
