@@ -272,3 +272,31 @@ def test_design_loop_64x32x32_matches_golden(oracle, gputo, torch):
     assert np.abs(xphys - d["xPhys"].astype(np.float64)).max() <= 1e-4
     np.testing.assert_allclose(cs, d["c"], rtol=1e-6)
     assert max(abs(a - b) for a, b in zip(nits, d["nit"])) <= 1
+
+
+def test_host_calls_reuse_their_workspace(oracle, gputo):
+    """The host-array entry points keep device buffers and pinned staging
+    between calls: a large call, a smaller one, then the large one again
+    (sizes above one 8 MB staging chunk, so several chunks are in flight)
+    each match the oracle."""
+    rng = np.random.default_rng(11)
+    for shape in [(128, 64, 64), (16, 8, 8), (128, 64, 64)]:
+        nelx, nely, nelz = shape
+        nel = nelx * nely * nelz
+        x = rng.uniform(0.05, 1.0, nel)
+        out = gputo.density_filter(x, nelx, nely, nelz, 3 ** 0.5)
+        ref, hs = oracle.filter3d(x, nelx, nely, nelz, 3 ** 0.5)
+        assert np.abs(out - ref / hs).max() <= 1e-12
+        p = oracle.cantilever(*shape)
+        U = rng.standard_normal(p.ndof)
+        CX, dsK = oracle.simp(x)
+        ce, dc, c = gputo.compliance_sens(p.Ke0, U, CX, dsK, nelx, nely, nelz)
+        Uc = U.copy()
+        Uc[1::3] *= -1
+        ce_ref = oracle.element_energy(p, Uc)
+        assert np.abs(ce - ce_ref).max() <= 1e-12 * np.abs(ce_ref).max()
+        assert abs(c - CX @ ce_ref) <= 1e-12 * abs(CX @ ce_ref)
+        dv = np.full(nel, 1.0 / nel)
+        xn, lm = gputo.oc_update(x, -np.abs(dc), dv, 0.3, 0.2)
+        xr, lr = oracle.oc_update(x, -np.abs(dc), dv, 0.3, 0.2)
+        assert abs(lm - lr) <= 1e-12 * abs(lr) and np.abs(xn - xr).max() <= 1e-12
