@@ -631,6 +631,26 @@ int gputo_mgcg1(const double *Ke0, const double *F, double *U, const double *CX,
 // design-loop steps
 // ---------------------------------------------------------------------------
 
+int gputo_simp(const double *xPhys, long long n, double penal, double E0, double Emin, double *CX, double *dsK)
+{
+    if (!xPhys || !CX || n <= 0) return GPUTO_ERR_ARG;
+    int st = gputo::check_device();
+    if (st) return st;
+    std::lock_guard<std::mutex> lock(gputo::host_io_mutex());
+    double *dx = gputo::host_call_buffer(0, (size_t)n, &st);
+    double *dcx = !st ? gputo::host_call_buffer(1, (size_t)n, &st) : nullptr;
+    double *dds = (!st && dsK) ? gputo::host_call_buffer(2, (size_t)n, &st) : nullptr;
+    if (st) return st;
+    st = gputo::host_to_device(dx, xPhys, sizeof(double) * n);
+    if (st) return st;
+    gputo::launch_simp(n, dx, penal, E0, Emin, dcx, dds, nullptr);
+    GPUTO_CUDA(cudaDeviceSynchronize());
+    GPUTO_CUDA(cudaGetLastError());
+    st = gputo::device_to_host(CX, dcx, sizeof(double) * n);
+    if (!st && dsK) st = gputo::device_to_host(dsK, dds, sizeof(double) * n);
+    return st;
+}
+
 namespace {
 struct Scratch {
     double *partial = nullptr;

@@ -108,6 +108,7 @@ SIGNATURES = {
     "gputo_density_filter_dev": (_i, [_vp, _vp, _vp, _i, _i, _i, _d, _i, _vp]),
     "gputo_density_filter": (_i, [_dp, _dp, _dp, _i, _i, _i, _d, _i]),
     "gputo_simp_dev": (_i, [_vp, ctypes.c_longlong, _d, _d, _d, _vp, _vp, _vp]),
+    "gputo_simp": (_i, [_dp, ctypes.c_longlong, _d, _d, _d, _dp, _dp]),
     "gputo_oc_update_dev": (_i, [_vp, _vp, _vp, ctypes.c_longlong, _d, _d, _vp, _dp, _vp]),
     "gputo_oc_update": (_i, [_dp, _dp, _dp, ctypes.c_longlong, _d, _d, _dp, _dp]),
 }
@@ -601,6 +602,15 @@ def density_filter_dev(x, out, nelx, nely, nelz, rmin, divisor=None, normalize=T
 def simp_dev(xphys, CX, dsK=None, penal=3.0, E0=1.0, Emin=1e-9, stream=None):
     _check(_lib.gputo_simp_dev(_ptr(xphys), xphys.numel(), float(penal), float(E0), float(Emin),
                                _ptr(CX), _ptr(dsK), _ptr_stream(stream)), "gputo_simp_dev")
+
+
+def simp(xphys, penal=3.0, E0=1.0, Emin=1e-9):
+    """Host-array SIMP (top3D125modCuda.m:124,130): returns (CX, dsK)."""
+    xphys = np.ascontiguousarray(xphys, dtype=np.float64).reshape(-1)
+    CX, dsK = np.empty_like(xphys), np.empty_like(xphys)
+    _check(_lib.gputo_simp(_p(xphys), xphys.size, float(penal), float(E0), float(Emin), _p(CX), _p(dsK)),
+           "gputo_simp")
+    return CX, dsK
 
 
 def oc_update_dev(x, dc, dv0, xnew, volfrac, move, stream=None):

@@ -381,6 +381,9 @@ int gputo_density_filter(const double *in, const double *divisor, double *out, i
  * dsK may be NULL. */
 int gputo_simp_dev(const double *xPhys, long long n, double penal, double E0, double Emin,
                    double *CX, double *dsK, void *stream);
+/* The same on host arrays (the MATLAB lines themselves): xPhys in, CX and
+ * dsK out (dsK may be NULL). */
+int gputo_simp(const double *xPhys, long long n, double penal, double E0, double Emin, double *CX, double *dsK);
 
 /* Optimality-criteria update with bisection on the Lagrange multiplier
  * (top3D125modCuda.m:143-151), all elements active:

@@ -300,3 +300,10 @@ def test_host_calls_reuse_their_workspace(oracle, gputo):
         xn, lm = gputo.oc_update(x, -np.abs(dc), dv, 0.3, 0.2)
         xr, lr = oracle.oc_update(x, -np.abs(dc), dv, 0.3, 0.2)
         assert abs(lm - lr) <= 1e-12 * abs(lr) and np.abs(xn - xr).max() <= 1e-12
+
+
+def test_host_simp_matches_oracle(oracle, gputo):
+    x = np.random.default_rng(12).uniform(0.0, 1.0, 3 * 10 ** 6 + 7)   # several staging chunks
+    CX, dsK = gputo.simp(x, 3.0, 1.0, 1e-9)
+    CXr, dsr = oracle.simp(x)
+    assert np.abs(CX - CXr).max() <= 1e-15 and np.abs(dsK - dsr).max() <= 1e-14
