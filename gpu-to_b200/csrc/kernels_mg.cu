@@ -921,15 +921,55 @@ __global__ void tri_inverse_kernel(int n, const double *__restrict__ L, double *
     }
 }
 
+// The same with the column being built kept in shared memory: each step of a
+// column's forward substitution reads its earlier entries from there instead
+// of from global memory (stride n), which shortens the serial chain per row.
+// One warp (CTA) per column; x_r for r >= c lives at xs[r - c].
+__global__ void __launch_bounds__(32) tri_inverse_col_kernel(int n, const double *__restrict__ L,
+                                                             double *__restrict__ Linv, double *__restrict__ LinvT)
+{
+    extern __shared__ double xs[];
+    const int c = blockIdx.x, lane = threadIdx.x;
+    for (int r = lane; r < c; r += 32) {
+        Linv[(long long)r * n + c] = 0.0;
+        LinvT[(long long)c * n + r] = 0.0;
+    }
+    for (int r = c; r < n; ++r) {
+        const double *Lr = L + (long long)r * n;
+        double s = 0.0;
+        for (int kk = c + lane; kk < r; kk += 32) s = fma(Lr[kk], xs[kk - c], s);
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        const double x = ((r == c ? 1.0 : 0.0) - s) / Lr[r];
+        if (lane == 0) {
+            xs[r - c] = x;
+            Linv[(long long)r * n + c] = x;
+            LinvT[(long long)c * n + r] = x;
+        }
+        __syncwarp();
+    }
+}
+
+constexpr int kTriInvMaxSmem = 200 * 1024;
+
 void launch_tri_inverse(int n, const double *L, double *Linv, double *LinvT, cudaStream_t st)
 {
-    const int bs = 128;  // 4 columns per CTA
-    tri_inverse_kernel<<<(unsigned)((n * 32 + bs - 1) / bs), bs, 0, st>>>(n, L, Linv, LinvT);
+    const size_t smem = sizeof(double) * (size_t)n;
+    static bool attr_set[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (smem <= (size_t)kTriInvMaxSmem && dev < 64) {
+        if (!attr_set[dev]) {   // setup runs outside stream capture
+            cudaFuncSetAttribute(tri_inverse_col_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTriInvMaxSmem);
+            attr_set[dev] = true;
+        }
+        tri_inverse_col_kernel<<<(unsigned)n, 32, smem, st>>>(n, L, Linv, LinvT);
+    } else {
+        const int bs = 128;  // 4 columns per CTA
+        tri_inverse_kernel<<<(unsigned)((n * 32 + bs - 1) / bs), bs, 0, st>>>(n, L, Linv, LinvT);
+    }
     count_launches(1);
 }
 
-// y = M x for a dense row-major n x n matrix, one warp per row, FP64
-// accumulation; the input and output may be FP32 or FP64.
 // Position of dense (reference-order) dof r in the padded layout.
 __device__ __forceinline__ long long padded_pos(const Lay &L, long long r)
 {
