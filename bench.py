@@ -600,6 +600,70 @@ def run_batch(args):
     print(json.dumps(line))
 
 
+BRIDGE = (512, 256, 256, 7)   # nelx, nely, nelz, levels (coarsest grid 8x4x4)
+
+
+def run_bridge(args):
+    """The 512x256x256 bridge (101.6M dofs): supports on the two bottom corner
+    strips, unit uniform top load, volume fraction 0.15 from a uniform start.
+    Seconds per design iteration for the mixed and the FP64 solver; the
+    reference cannot run this size (its int workspace counter overflows)."""
+    import torch
+
+    import gputo
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    nelx, nely, nelz, nl = BRIDGE
+    F, fixed = gputo.bridge(nelx, nely, nelz)
+    Ke0 = gputo.hex8_stiffness(0.3)
+    out = {}
+    with torch.cuda.stream(stream):
+        clocks = ClockSampler(0)
+        for name, prec, steps in (("mixed", gputo.PREC_MIXED, args.steps),
+                                  ("fp64", gputo.PREC_FP64, max(1, args.steps // 2))):
+            dl = gputo.DesignLoop(nelx, nely, nelz, nl, F, fixed, Ke0, volfrac=0.15, penal=PENAL, rmin=RMIN,
+                                  move=MOVE, tol=TOL, maxit=MAXIT, options=gputo.default_options(precision=prec),
+                                  stream=stream)
+            x0 = dl.x.clone()
+            infos = []
+
+            def one():
+                dl.x.copy_(x0)
+                return dl.step()
+
+            for _ in range(args.warmup):
+                one()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ctx = clocks if name == "mixed" else _Null()
+            with ctx:
+                e0.record(stream)
+                for _ in range(steps):
+                    infos.append(one())
+                e1.record(stream)
+                torch.cuda.synchronize()
+            out[name] = {"s": e0.elapsed_time(e1) / steps / 1000.0, "nit": infos[-1]["nit"],
+                         "relres": infos[-1]["relres"], "c": infos[-1]["c"], "steps": steps,
+                         "solver_bytes": dl.solver.device_bytes}
+            del dl, x0
+            torch.cuda.empty_cache()
+    ndof = 3 * (nelx + 1) * (nely + 1) * (nelz + 1)
+    m = out["mixed"]
+    line = {"metric": "s per design iteration, 512x256x256 bridge, tol 1e-6", "value": round(m["s"], 4),
+            "unit": "s", "higher_is_better": False, "n_gpus": 1, "steps": m["steps"], "warmup": args.warmup,
+            "fp64_s": round(out["fp64"]["s"], 4), "mixed_vs_fp64": round(out["fp64"]["s"] / m["s"], 3),
+            "dtype": "f64 outer / f32 V-cycle", "data": "synthetic",
+            "clocks": clocks.summary(),
+            "config": {"workload": "bridge design iteration (filter, SIMP, MGCG solve to 1e-6, ce, OC)",
+                       "nelx": nelx, "nely": nely, "nelz": nelz, "nl": nl, "ndof": ndof, "volfrac": 0.15,
+                       "nit": {k: v["nit"] for k, v in out.items()},
+                       "relres": {k: v["relres"] for k, v in out.items()},
+                       "compliance": {k: v["c"] for k, v in out.items()},
+                       "solver_gb": {k: round(v["solver_bytes"] / 1e9, 2) for k, v in out.items()},
+                       "inputs_vs_l2": "inputs larger than L2"}}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -612,13 +676,16 @@ def main():
     ap.add_argument("--nl", type=int, default=NL)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--one-step", choices=["mixed", "fp64"], help="profiling aid: one design iteration")
-    ap.add_argument("--workload", default="cantilever", choices=["cantilever", "batch"],
-                    help="batch: the uneven multi-design batch instead of the headline design loop")
+    ap.add_argument("--workload", default="cantilever", choices=["cantilever", "batch", "bridge"],
+                    help="batch: the uneven multi-design batch; bridge: the 512x256x256 bridge "
+                         "(instead of the headline design loop)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.workload == "batch":
         run_batch(args)
+    elif args.workload == "bridge":
+        run_bridge(args)
     elif args.micro:
         run_micro(args)
     elif args.one_step:

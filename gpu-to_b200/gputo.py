@@ -191,6 +191,31 @@ def cantilever(nelx, nely, nelz):
     return F, fixed
 
 
+def bridge(nelx, nely, nelz):
+    """Supports and load of the bridge workload (the ArchBridge drivers'
+    layout, ArchBridge/1/top3D125modCudaBridge1.m:79-99, widened from its four
+    corner nodes to the two bottom corner strips): every node of the bottom
+    (k = 0) edge lines at x = 0 and x = nelx fixed in all three directions,
+    and a uniform downward pressure of unit total on the top face (k = nelz),
+    each top element giving a quarter of its share to the z dof of each of its
+    four top nodes.  Returns (F, fixed) in the MEX's layout."""
+    nd = 3 * (nelx + 1) * (nely + 1) * (nelz + 1)
+    F = np.zeros(nd)
+    js = np.arange(nely + 1)
+    plane = (nely + 1) * (nelz + 1)
+    # nodal weight of the top face: 1, 2 or 4 elements touch a node
+    wy = np.full(nely + 1, 2.0)
+    wy[[0, -1]] = 1.0
+    wx = np.full(nelx + 1, 2.0)
+    wx[[0, -1]] = 1.0
+    top = (np.arange(nelx + 1)[:, None] * plane + (nely + 1) * nelz + js[None, :]).reshape(-1)
+    F[3 * top + 2] = -0.25 / (nelx * nely) * (wx[:, None] * wy[None, :]).reshape(-1)
+    ends = np.concatenate([js, nelx * plane + js])   # k = 0 lines at i = 0 and i = nelx
+    fixed = np.sort((3 * ends[:, None] + np.arange(3)[None, :]).reshape(-1)) + 1.0
+    F[fixed.astype(np.int64) - 1] = 0.0
+    return F, fixed
+
+
 def version() -> str:
     return _lib.gputo_version().decode()
 

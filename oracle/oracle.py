@@ -179,6 +179,31 @@ def simp(xphys, penal=3.0, E0=1.0, Emin=1e-9):
 # solver restatement and the compiled reference
 # --------------------------------------------------------------------------
 
+def bridge(nelx, nely, nelz):
+    """Bridge supports and load, restated from ArchBridge/1/top3D125modCudaBridge1.m:79-99
+    (fixed corner nodes at the bottom of both x ends, widened here to the two
+    bottom edge lines; top-face pressure as -0.25 per element on each top
+    node's z dof, :90-98), scaled to a unit total load.  Written as the
+    per-element loop of the driver so it checks the vectorised product
+    version independently."""
+    n = ndof(nelx, nely, nelz)
+    F = np.zeros(n)
+    for i in range(nelx):
+        for j in range(nely):
+            for di in (0, 1):
+                for dj in (0, 1):
+                    nod = node_id(nelx, nely, nelz, i + di, j + dj, nelz)
+                    F[3 * nod + 2] -= 0.25 / (nelx * nely)
+    fixed = []
+    for i in (0, nelx):
+        for j in range(nely + 1):
+            nod = node_id(nelx, nely, nelz, i, j, 0)
+            fixed += [3 * nod + 1, 3 * nod + 2, 3 * nod + 3]
+    fixed = np.array(sorted(fixed), dtype=np.float64)
+    F[fixed.astype(np.int64) - 1] = 0.0
+    return Problem(nelx, nely, nelz, F, fixed)
+
+
 def mgcg1(p: Problem, CX, nl, tol, maxit, nswp=3, omega=0.48, prerelax=0.7, nu=0.3,
           history=False, coarse=0):
     """Restatement of the MEX: returns (U, relres, nit[, res_history]).
