@@ -34,7 +34,7 @@ SOURCES = ["kernels_fine.cu", "kernels_mg.cu", "kernels_blas.cu", "kernels_desig
            "capi.cpp", "noalloc.cu", "kernels_quad.cu", "kernels_tc.cu", "kernels_tcsweep.cu",
            "kernels_learned.cu", "batch.cpp", "design_io.cpp",
            "kernels_hsweep.cu", "hostio.cpp"]
-HEADERS = ["gputo_internal.h", "solver.h", "tma.h"]
+HEADERS = ["gputo_internal.h", "solver.h", "tma.h", "hadamard.h"]
 
 
 def _newer(target: str, deps: list[str]) -> bool:

@@ -1,6 +1,7 @@
 // Design-loop steps that the MATLAB driver runs around the solve
 // (Cantilever/TOP3D125MGCGCUDA/top3D125modCuda.m:95-96,109,139-141,163).
 #include "gputo_internal.h"
+#include "hadamard.h"
 
 #include <cmath>
 #include <vector>
@@ -9,11 +10,17 @@ namespace gputo {
 
 // Element matrix for the energy kernel.  Constant memory is per translation
 // unit without relocatable device code, so this file keeps its own copy,
-// written by upload_fine_ke() together with the solver's.
+// written by upload_fine_ke() together with the solver's.  When Ke has the
+// cube element's Hadamard pattern, its eight constants (per device) select
+// the Hadamard-basis energy pass.
 __constant__ double cKeD[576];
+HadamardKe g_design_hk[64];
 
 int upload_design_ke(const double *Ke_host, cudaStream_t st)
 {
+    int dev = 0;
+    GPUTO_CUDA(cudaGetDevice(&dev));
+    (void)hadamard_ke(Ke_host, &g_design_hk[dev < 64 ? dev : 63]);   // sets ok = false without the pattern
     GPUTO_CUDA(cudaMemcpyToSymbolAsync(cKeD, Ke_host, sizeof(double) * 576, 0,
                                        cudaMemcpyHostToDevice, st));
     return GPUTO_OK;
@@ -24,12 +31,15 @@ constexpr int kFilterW = 2 * kMaxFilterRadius + 1;
 __constant__ double cFilterH[kFilterW * kFilterW * kFilterW];
 
 // ce_e = u_e^T Ke u_e, dc_e = dsK_e ce_e, and sum_e CX_e ce_e.  Thread per
-// element; Ke from constant memory.  U is in the solver frame: the driver's
-// U(cMat) gather (top3D125modCuda.m:39-41,139) lists element nodes in an order
-// mirrored in y, which matches the y-negated U the MEX hands back, so both
-// give the same ce.
+// element.  U is in the solver frame: the driver's U(cMat) gather
+// (top3D125modCuda.m:39-41,139) lists element nodes in an order mirrored in y,
+// which matches the y-negated U the MEX hands back, so both give the same ce.
+// HAD: u_e' Ke u_e as (T u_e)' (S / 64) (T u_e) in the element's Hadamard
+// basis (about 140 FP64 operations, so the pass is bound by memory); else
+// the dense 24x24 product with Ke from constant memory (1152 FLOP).
+template <bool HAD>
 __global__ void __launch_bounds__(256)
-element_energy_kernel(Grid g, const double *__restrict__ U, const double *__restrict__ CX,
+element_energy_kernel(Grid g, HC<double> hc, const double *__restrict__ U, const double *__restrict__ CX,
                       const double *__restrict__ dsK, double *__restrict__ ce,
                       double *__restrict__ dc, double *__restrict__ partial, unsigned *ticket,
                       double *compliance)
@@ -44,20 +54,39 @@ element_energy_kernel(Grid g, const double *__restrict__ U, const double *__rest
         const int j = (int)(e - t * g.ny);
         const int i = (int)(t / g.nz);
         const int k = (int)(t - (long long)i * g.nz);
-        double ue[24];
-#pragma unroll
-        for (int a = 0; a < 8; ++a) {
-            const long long n = g.node(i + local_x(a), j + local_y(a), k + local_z(a));
-#pragma unroll
-            for (int d = 0; d < 3; ++d) ue[3 * a + d] = U[3 * n + d];
-        }
         double s = 0.0;
-#pragma unroll 4
-        for (int m = 0; m < 24; ++m) {
-            double tm = 0.0;
+        if constexpr (HAD) {
+            // corners (cx, cy, cz) into the two x faces, [(2 cy + cz) 4 + d]
+            double Fp[HF], Fn[HF];
 #pragma unroll
-            for (int q = 0; q < 24; ++q) tm = fma(cKeD[m * 24 + q], ue[q], tm);
-            s = fma(ue[m], tm, s);
+            for (int cy = 0; cy < 2; ++cy)
+#pragma unroll
+                for (int cz = 0; cz < 2; ++cz) {
+                    const long long n0 = g.node(i, j + cy, k + cz), n1 = g.node(i + 1, j + cy, k + cz);
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        Fp[(2 * cy + cz) * 4 + d] = U[3 * n0 + d];
+                        Fn[(2 * cy + cz) * 4 + d] = U[3 * n1 + d];
+                    }
+                }
+            face_h(Fp);
+            face_h(Fn);
+            s = element_energy_h(Fp, Fn, hc);
+        } else {
+            double ue[24];
+#pragma unroll
+            for (int a = 0; a < 8; ++a) {
+                const long long n = g.node(i + local_x(a), j + local_y(a), k + local_z(a));
+#pragma unroll
+                for (int d = 0; d < 3; ++d) ue[3 * a + d] = U[3 * n + d];
+            }
+#pragma unroll 4
+            for (int m = 0; m < 24; ++m) {
+                double tm = 0.0;
+#pragma unroll
+                for (int q = 0; q < 24; ++q) tm = fma(cKeD[m * 24 + q], ue[q], tm);
+                s = fma(ue[m], tm, s);
+            }
         }
         if (ce) ce[e] = s;
         if (dc) dc[e] = dsK[e] * s;
@@ -84,6 +113,24 @@ element_energy_kernel(Grid g, const double *__restrict__ U, const double *__rest
     }
 }
 
+// Same kernel with an explicit number of CTAs (one partial slot per CTA).
+void launch_element_energy_blocks(const Grid &g, const double *U, const double *CX,
+                                  const double *dsK, double *ce, double *dc, double *partial,
+                                  unsigned *ticket, double *compliance, int nblocks,
+                                  cudaStream_t st)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const HadamardKe &hk = g_design_hk[dev < 64 ? dev : 63];
+    if (hk.ok)
+        element_energy_kernel<true><<<(unsigned)nblocks, 256, 0, st>>>(g, make_hc<double>(hk), U, CX, dsK, ce, dc,
+                                                                       partial, ticket, compliance);
+    else
+        element_energy_kernel<false><<<(unsigned)nblocks, 256, 0, st>>>(g, HC<double>{}, U, CX, dsK, ce, dc,
+                                                                        partial, ticket, compliance);
+    count_launches(1);
+}
+
 void launch_element_energy(const Grid &g, const double *U, const double *CX, const double *dsK,
                            double *ce, double *dc, double *partial, unsigned *ticket,
                            double *compliance, cudaStream_t st)
@@ -91,20 +138,7 @@ void launch_element_energy(const Grid &g, const double *U, const double *CX, con
     long long nb = (g.nel() + 255) / 256;
     if (nb > 1184) nb = 1184;
     if (nb < 1) nb = 1;
-    element_energy_kernel<<<(unsigned)nb, 256, 0, st>>>(g, U, CX, dsK, ce, dc, partial, ticket,
-                                                         compliance);
-    count_launches(1);
-}
-
-// Same kernel with an explicit number of CTAs (one partial slot per CTA).
-void launch_element_energy_blocks(const Grid &g, const double *U, const double *CX,
-                                  const double *dsK, double *ce, double *dc, double *partial,
-                                  unsigned *ticket, double *compliance, int nblocks,
-                                  cudaStream_t st)
-{
-    element_energy_kernel<<<(unsigned)nblocks, 256, 0, st>>>(g, U, CX, dsK, ce, dc, partial, ticket,
-                                                              compliance);
-    count_launches(1);
+    launch_element_energy_blocks(g, U, CX, dsK, ce, dc, partial, ticket, compliance, (int)nb, st);
 }
 
 // MATLAB 'symmetric' padding: mirror including the edge sample.

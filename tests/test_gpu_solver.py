@@ -178,6 +178,31 @@ def test_compliance_sensitivity_matches_oracle(oracle, gputo):
     assert abs(c - CX @ ce_ref) <= 1e-12 * abs(CX @ ce_ref)
 
 
+@pytest.mark.parametrize("ke", ["cube", "perturbed"])
+def test_element_energy_both_element_paths(oracle, gputo, torch, ke):
+    """The cube element's Ke runs the energy pass in its Hadamard basis; a Ke
+    without that pattern (a symmetric perturbation) runs the dense 24x24
+    product.  Both against the oracle with the same Ke, on a grid with
+    several CTAs per x plane and ragged ends."""
+    nelx, nely, nelz = 20, 37, 11
+    p = oracle.cantilever(nelx, nely, nelz)
+    rng = np.random.default_rng(31)
+    if ke == "perturbed":
+        E = rng.standard_normal((24, 24)) * 1e-3
+        p.Ke0 = p.Ke0 + E + E.T
+    U = rng.standard_normal(p.ndof)
+    CX, dsK = oracle.simp(rng.uniform(0.05, 1.0, p.nel))
+    ce, dc = torch.empty(p.nel, dtype=torch.float64, device="cuda"), \
+        torch.empty(p.nel, dtype=torch.float64, device="cuda")
+    c = gputo.compliance_sens_dev(p.Ke0, _dev(torch, U), _dev(torch, CX), _dev(torch, dsK), nelx, nely, nelz,
+                                  ce, dc)
+    ce_ref = oracle.element_energy(p, U)
+    ce, dc = ce.cpu().numpy(), dc.cpu().numpy()
+    assert np.abs(ce - ce_ref).max() <= 1e-12 * np.abs(ce_ref).max()
+    assert np.abs(dc - dsK * ce_ref).max() <= 1e-12 * np.abs(dsK * ce_ref).max()
+    assert abs(c - CX @ ce_ref) <= 1e-12 * abs(CX @ ce_ref)
+
+
 @pytest.mark.parametrize("rmin", [3 ** 0.5, 2 * 3 ** 0.5, 1.2])
 def test_density_filter_matches_oracle(oracle, gputo, rmin):
     nelx, nely, nelz = 20, 12, 10
