@@ -135,6 +135,24 @@ int upload_quadrature_parts(double nu, cudaStream_t st)
 // coarse-level sweep: packed element matrices [300][nel]
 // ---------------------------------------------------------------------------
 
+// Grid of thread-per-node kernels, one row of CTAs per x node plane
+// (blockIdx.y = i), so a thread finds (j, k) with one 32-bit division.
+inline dim3 plane_grid(const Grid &g, int bs)
+{
+    const int per_plane = (g.ny + 1) * (g.nz + 1);
+    return dim3((unsigned)((per_plane + bs - 1) / bs), (unsigned)(g.nx + 1));
+}
+__device__ __forceinline__ bool plane_ijk(const Grid &g, int &i, int &j, int &k)
+{
+    const unsigned m = blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned ny1 = (unsigned)g.ny + 1u;
+    if (m >= ny1 * ((unsigned)g.nz + 1u)) return false;
+    i = (int)blockIdx.y;
+    k = (int)(m / ny1);
+    j = (int)(m - (unsigned)k * ny1);
+    return true;
+}
+
 __device__ __forceinline__ void node_ijk(const Grid &g, long long n, int &i, int &j, int &k)
 {
     const long long t = n / (g.ny + 1);
@@ -353,10 +371,9 @@ __global__ void restrict_kernel(Lay Lc, Lay Lf, const T *__restrict__ rf,
     pdl_wait();
     if (done && *done) return;
     const Grid &gc = Lc.g;
-    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= gc.nnod()) return;
     int i, j, k;
-    node_ijk(gc, n, i, j, k);
+    if (!plane_ijk(gc, i, j, k)) return;
+    const long long n = gc.node(i, j, k);
     const Grid &gf = Lf.g;
     T acc[3] = {T(0), T(0), T(0)};
     // all 27 taps unrolled with predicated loads (a tap outside the grid
@@ -391,7 +408,7 @@ void launch_restrict(const Lay &Lc, const Lay &Lf, const T *rf, const uint8_t *m
                      const int *done, cudaStream_t st)
 {
     const int bs = 128;
-    launch_pdl(restrict_kernel<T>, dim3((unsigned)((Lc.g.nnod() + bs - 1) / bs)), dim3(bs), 0, st, Lc, Lf, rf, maskc, fc, done);
+    launch_pdl(restrict_kernel<T>, plane_grid(Lc.g, bs), dim3(bs), 0, st, Lc, Lf, rf, maskc, fc, done);
     count_launches(1);
 }
 template void launch_restrict<double>(const Lay &, const Lay &, const double *, const uint8_t *,
@@ -409,24 +426,29 @@ __global__ void prolong_kernel(Lay Lf, Lay Lc, const T *__restrict__ uc,
     pdl_wait();
     if (done && *done) return;
     const Grid &gf = Lf.g;
-    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= gf.nnod()) return;
     int i, j, k;
-    node_ijk(gf, n, i, j, k);
+    if (!plane_ijk(gf, i, j, k)) return;
+    const long long n = gf.node(i, j, k);
     const int ni = (i & 1) + 1, nj = (j & 1) + 1, nk = (k & 1) + 1;
     T acc[3] = {T(0), T(0), T(0)};
-    // the up to 8 coarse nodes unrolled with predicated loads (same order)
+    // the up to 8 coarse nodes unrolled with predicated loads (same order),
+    // from one base pointer and the coarse plane and row strides; a tap that
+    // is not taken points at the base node, so no address leaves the array
+    const T *c0 = uc + Lc.at(i >> 1, j >> 1, k >> 1);
+    const long long si = (long long)(Lc.g.nz + 1) * Lc.pitch, sk = Lc.pitch;
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
-        for (int c = 0; c < 2; ++c)
+        for (int c = 0; c < 2; ++c) {
+            const T *cr = c0 + ((a && a < ni) ? si : 0) + ((c && c < nk) ? sk : 0);
 #pragma unroll
             for (int b = 0; b < 2; ++b) {
                 const bool ok = a < ni && c < nk && b < nj;
-                const long long nc = ok ? Lc.at((i >> 1) + a, (j >> 1) + b, (k >> 1) + c) : 0;
+                const int off = (b < nj) ? 3 * b : 0;
 #pragma unroll
-                for (int d = 0; d < 3; ++d) acc[d] += ok ? uc[nc + d] : T(0);
+                for (int d = 0; d < 3; ++d) acc[d] += ok ? cr[off + d] : T(0);
             }
+        }
     const T w = T(1) / T(ni * nj * nk);
     const unsigned m = maskf[n];
     const long long base = Lf.at(i, j, k);
@@ -442,7 +464,7 @@ void launch_prolong_add(const Lay &Lf, const Lay &Lc, const T *uc, const uint8_t
                         const int *done, cudaStream_t st)
 {
     const int bs = 128;
-    launch_pdl(prolong_kernel<T>, dim3((unsigned)((Lf.g.nnod() + bs - 1) / bs)), dim3(bs), 0, st, Lf, Lc, uc, maskf, uf, done);
+    launch_pdl(prolong_kernel<T>, plane_grid(Lf.g, bs), dim3(bs), 0, st, Lf, Lc, uc, maskf, uf, done);
     count_launches(1);
 }
 template void launch_prolong_add<double>(const Lay &, const Lay &, const double *, const uint8_t *,

@@ -97,6 +97,10 @@ int Solver::create(int nelx, int nely, int nelz, int nl_, const gputo_options *o
         set_error("grid sizes must be positive and 1 <= nl <= 12");
         return GPUTO_ERR_ARG;
     }
+    if (nelx > 65534) {   // the transfer kernels take one row of CTAs per x node plane
+        set_error("nelx must be at most 65534");
+        return GPUTO_ERR_ARG;
+    }
     const int m = 1 << (nl_ - 1);
     if (nelx % m || nely % m || nelz % m) {
         set_error("nelx, nely, nelz must be divisible by 2^(nl-1)");
