@@ -135,6 +135,10 @@ void gauss_part(double nu, double h, int ix, int iy, int iz, double K[24][24]);
 int upload_quadrature_parts(double nu, cudaStream_t st);
 
 enum SweepMode { MODE_APPLY = 0, MODE_DEFECT = 1, MODE_JACOBI = 2, MODE_JACOBI_PRE = 3 };
+// A Jacobi sweep of the FP32 fine level that also sums r'z and r'z_old (r the
+// FP64 PCG residual, z its output, z_old the previous one) into per-CTA
+// partial pairs: the mixed PCG's last smoothing sweep (Hadamard-basis kernel only).
+constexpr int MODE_JACOBI_DOT = 4;
 
 // Fine level (K = sum CX_e Ke), FP64 and FP32 instantiations; CX padded (ELay),
 // vectors padded (Lay).  'err' receives GPUTO_ERR_TIMEOUT if a bounded wait
@@ -178,13 +182,14 @@ struct HadamardKe {
 bool hadamard_ke(const double *Ke, HadamardKe *hk);
 int init_hsweep_kernels();
 template <typename T> bool hsweep_fits(const Grid &g);
-template <typename T> int hsweep_blocks(const Grid &g);
+template <typename T> int hsweep_blocks(const Grid &g, int mode = MODE_APPLY);   // CTAs (= partials) of a sweep
 // rdiag: 1/diag (launch_recip); maskp: the Dirichlet bytes with rows padded
 // to 16 bytes (launch_pad_mask; hsweep_mask_bytes of storage).
 template <typename T>
 int launch_hsweep(int mode, const Lay &L, const ELay &E, const HadamardKe &hk, const T *CX, const T *u, const T *f,
                   const T *rdiag, const uint8_t *mask, const uint8_t *maskp, T *out, T omega, T prerelax,
-                  double *dot_partial, const int *done, int *err, cudaStream_t st);
+                  double *dot_partial, const int *done, int *err, cudaStream_t st, const double *Rd = nullptr,
+                  const T *zo = nullptr);
 long long hsweep_mask_bytes(const Grid &g);
 void launch_pad_mask(const Grid &g, const uint8_t *mask, uint8_t *maskp, cudaStream_t st);
 // Opt the tile kernels into their dynamic shared memory (call once per device).
@@ -265,6 +270,9 @@ void launch_pcg_init(long long n, const double *F, double *U, double *R, double 
                      cudaStream_t st);
 void launch_finish_apply_dot(int nblocks, double *partial, unsigned *ticket, PcgScalars *sc,
                              cudaStream_t st);
+// r'z and r'z_old from the partial pairs of a MODE_JACOBI_DOT sweep, then the
+// end-of-iteration scalars (beta, relres, convergence) as the two-dot kernel.
+void launch_finish_dot2(int nblocks, const double *partial, PcgScalars *sc, cudaStream_t st);
 void launch_copy(long long n, const double *a, double *b, const int *done, cudaStream_t st);
 void launch_flip_y(long long nnod, double *U, cudaStream_t st);
 

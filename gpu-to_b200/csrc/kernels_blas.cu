@@ -358,6 +358,28 @@ void launch_finish_apply_dot(int nblocks, double *partial, unsigned *, PcgScalar
     count_launches(1);
 }
 
+__global__ void __launch_bounds__(kRedThreads)
+finish_dot2_kernel(int nb, const double *__restrict__ partial, PcgScalars *sc)
+{
+    if (sc->done) return;
+    __shared__ double red[kRedThreads / 32];
+    double a = 0.0, b = 0.0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+        a += partial[2 * i];
+        b += partial[2 * i + 1];
+    }
+    a = block_sum(a, red);
+    __syncthreads();
+    b = block_sum(b, red);
+    if (threadIdx.x == 0) finalize_dot(sc, DOT_RZ, a, b);
+}
+
+void launch_finish_dot2(int nblocks, const double *partial, PcgScalars *sc, cudaStream_t st)
+{
+    finish_dot2_kernel<<<1, kRedThreads, 0, st>>>(nblocks, partial, sc);
+    count_launches(1);
+}
+
 __global__ void copy_kernel(long long n, const double *__restrict__ a, double *__restrict__ b,
                             const int *done)
 {

@@ -71,13 +71,15 @@ __host__ __device__ constexpr size_t al128(size_t x) { return (x + 127) & ~size_
 template <int MODE> struct HNeeds {
     static constexpr bool PRE = MODE == MODE_JACOBI_PRE;
     static constexpr bool F = MODE != MODE_APPLY;
-    static constexpr bool D = MODE == MODE_JACOBI || MODE == MODE_JACOBI_PRE;
+    static constexpr bool D = MODE == MODE_JACOBI || MODE == MODE_JACOBI_PRE || MODE == MODE_JACOBI_DOT;
+    static constexpr bool DOT = MODE == MODE_JACOBI_DOT;   // also the FP64 residual and z_old tiles
 };
 
 // Shared memory of one CTA.  Ring slot s holds: the face tile of node plane
 // E0 + s (u; f and diag for pre-relaxation), the CX tile of element plane
 // E0 + s - 1, and the epilogue tiles of node plane E0 + s - 1 (f, diag, the
-// Dirichlet mask), which that stage finishes.
+// Dirichlet mask; with MODE_JACOBI_DOT also the FP64 residual and z_old),
+// which that stage finishes.
 template <typename T, int WZ, int MODE>
 struct HSmem {
     using N = HNeeds<MODE>;
@@ -89,7 +91,10 @@ struct HSmem {
     static constexpr size_t d_off = ua;                               // face 1/diag (pre-relaxation)
     static constexpr size_t ef_off = d_off + (N::PRE ? ua : 0);       // epilogue f
     static constexpr size_t ed_off = ef_off + (N::F ? ua : 0);        // epilogue 1/diag
-    static constexpr size_t c_off = ed_off + (N::D ? ua : 0);
+    static constexpr size_t r_bytes = sizeof(double) * (WZ + 1) * HUW;   // FP64 residual tile
+    static constexpr size_t er_off = ed_off + (N::D ? ua : 0);        // epilogue residual (MODE_JACOBI_DOT)
+    static constexpr size_t ez_off = er_off + (N::DOT ? al128(r_bytes) : 0);   // epilogue z_old
+    static constexpr size_t c_off = ez_off + (N::DOT ? ua : 0);
     static constexpr size_t m_off = c_off + al128(c_bytes);
     static constexpr size_t slot = al128(m_off + m_bytes);
     static constexpr int ZROW = HY + 1;                               // lanes + the seam column
@@ -99,11 +104,16 @@ struct HSmem {
     static constexpr size_t s_off = al128(z_off + z_bytes);
     static constexpr size_t s_bytes = sizeof(T) * 3 * SEAM;         // own, own u, received
     static constexpr size_t bar_off = al128(s_off + s_bytes);
-    static constexpr size_t red_off = bar_off + 8 * HRING;            // per-warp dot partials
-    static constexpr size_t bytes = red_off + 8 * WZ;
-    static_assert(ua % 128 == 0 && c_off % 128 == 0 && m_off % 128 == 0 && slot % 128 == 0,
+    static constexpr size_t red_off = bar_off + 8 * HRING;            // per-warp dot partials (two per warp)
+    static constexpr size_t bytes = red_off + 16 * WZ;
+    static_assert(ua % 128 == 0 && c_off % 128 == 0 && m_off % 128 == 0 && slot % 128 == 0 && er_off % 128 == 0 &&
+                      ez_off % 128 == 0,
                   "TMA shared-memory destinations must be 128-byte aligned");
 };
+// Two CTAs of the FP32 Jacobi sweep with the PCG dots share an SM (228 KB,
+// 1 KB of it reserved per CTA).
+static_assert(2 * (HSmem<float, 8, MODE_JACOBI_DOT>::bytes + 1024) <= 228 * 1024,
+              "the FP32 sweep with dots must fit two CTAs per SM");
 
 // One element in the Hadamard basis.  Fp, Fn: transformed front (x = 0) and
 // back (x = 1) faces.  Adds the element's front-face output (still in face
@@ -157,7 +167,8 @@ __device__ __forceinline__ void element_h<float>(const float (&Fp)[HF], const fl
 
 template <typename T, int MODE>
 __device__ __forceinline__ void h_store(long long base, unsigned m, const T (&ku)[3], const T (&u)[3], const T *fv,
-                                        const T *rv, T *__restrict__ out, T omega, double &dsum)
+                                        const T *rv, T *__restrict__ out, T omega, double &dsum, const double *rdv,
+                                        const T *zov, double &dsum2)
 {
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -170,7 +181,13 @@ __device__ __forceinline__ void h_store(long long base, unsigned m, const T (&ku
             out[base + d] = fixed ? T(0) : fv[d] - ku[d];
         } else {
             const T r = fixed ? T(0) : fv[d] - ku[d];
-            out[base + d] = u[d] + omega * r * rv[d];
+            const T z = u[d] + omega * r * rv[d];
+            out[base + d] = z;
+            if (MODE == MODE_JACOBI_DOT) {   // r'z and r'z_old with the FP64 residual
+                const double rd = rdv[d];
+                dsum = fma(rd, (double)z, dsum);
+                dsum2 = fma(rd, (double)zov[d], dsum2);
+            }
         }
     }
 }
@@ -191,9 +208,11 @@ template <typename T, int MODE, int WZ>
 __global__ void __launch_bounds__(32 * WZ, HMinBlocks<T, MODE>::value)
 hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ CUtensorMap tm_d,
               const __grid_constant__ CUtensorMap tm_f, const __grid_constant__ CUtensorMap tm_c,
-              const __grid_constant__ CUtensorMap tm_m, Lay L, HC<T> hc, int htx, const T *__restrict__ f,
+              const __grid_constant__ CUtensorMap tm_m, const __grid_constant__ CUtensorMap tm_r,
+              const __grid_constant__ CUtensorMap tm_z, Lay L, HC<T> hc, int htx, const T *__restrict__ f,
               const T *__restrict__ rdiag, const uint8_t *__restrict__ mask, T *__restrict__ out, T omega,
-              T prerelax, double *__restrict__ dot_partial, const int *__restrict__ done, int *__restrict__ err)
+              T prerelax, double *__restrict__ dot_partial, const int *__restrict__ done, int *__restrict__ err,
+              const double *__restrict__ Rd, const T *__restrict__ zo)
 {
     if (done && *done) return;   // the same value for every CTA of the cluster
     using N = HNeeds<MODE>;
@@ -239,7 +258,8 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
         uint32_t bytes = 0;
         if (face) bytes += (uint32_t)(S::u_bytes * (N::PRE ? 2 : 1));
         if (cxp) bytes += (uint32_t)S::c_bytes;
-        if (epi) bytes += (uint32_t)(S::u_bytes * ((N::F ? 1 : 0) + (N::D ? 1 : 0)) + S::m_bytes);
+        if (epi) bytes += (uint32_t)(S::u_bytes * ((N::F ? 1 : 0) + (N::D ? 1 : 0) + (N::DOT ? 1 : 0)) + S::m_bytes +
+                                     (N::DOT ? S::r_bytes : 0));
         mbar_arrive_expect_tx(b, bytes);
         if (face) {
             tma_load_3d(sb, &tm_u, 3 * jc0, kc0, E0 + s, b);
@@ -249,6 +269,10 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
         if (epi) {
             if (N::F) tma_load_3d(sb + S::ef_off, &tm_f, 3 * jc0, kc0, E0 + s - 1, b);
             if (N::D) tma_load_3d(sb + S::ed_off, &tm_d, 3 * jc0, kc0, E0 + s - 1, b);
+            if (N::DOT) {
+                tma_load_3d(sb + S::er_off, &tm_r, 3 * jc0, kc0, E0 + s - 1, b);
+                tma_load_3d(sb + S::ez_off, &tm_z, 3 * jc0, kc0, E0 + s - 1, b);
+            }
             tma_load_3d(sb + S::m_off, &tm_m, jc0, kc0, E0 + s - 1, b);
         }
         issued = s + 1;
@@ -277,7 +301,7 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
                     U[(cy * 2 + cz) * 4 + d] = v;
                 }
     };
-    double dsum = 0.0;
+    double dsum = 0.0, dsum2 = 0.0;
     // Corner partials P of node plane p -> y sums through the warp, z partner
     // values into the exchange buffer (read after the next barrier).
     auto reduce_y = [&](int p, T (&P)[HF], T (&q0)[3]) {
@@ -297,6 +321,8 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
         const unsigned char *sb = smem + (s % HRING) * S::slot;
         const T *ef = reinterpret_cast<const T *>(sb + S::ef_off) + w * HUW;
         const T *ed = reinterpret_cast<const T *>(sb + S::ed_off) + w * HUW;
+        const double *er = reinterpret_cast<const double *>(sb + S::er_off) + w * HUW;   // MODE_JACOBI_DOT only
+        const T *ez = reinterpret_cast<const T *>(sb + S::ez_off) + w * HUW;
         const uint8_t *em = sb + S::m_off + w * HM;
         const T *z = zb + (p & 1) * (WZ * S::ZROW * 3);
         const int k = kc0 + w, j = jc0 + l, at = ((p - P0) * WZ + w) * 3;
@@ -311,7 +337,8 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
             }
         } else if (j <= g.ny) {
             const T uu[3] = {Uu[0], Uu[1], Uu[2]};
-            h_store<T, MODE>(L.at(p, j, k), em[l], R, uu, ef + 3 * l, ed + 3 * l, out, omega, dsum);
+            h_store<T, MODE>(L.at(p, j, k), em[l], R, uu, ef + 3 * l, ed + 3 * l, out, omega, dsum, er + 3 * l,
+                             ez + 3 * l, dsum2);
         }
         if (l == HY - 1) {   // this CTA's part of node column jc0 + HY
             T Sd[3];
@@ -323,7 +350,8 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
                 for (int d = 0; d < 3; ++d) rem[at + d] = Sd[d];
             } else if (tail_owner) {
                 const T uu[3] = {Uu[8], Uu[9], Uu[10]};
-                h_store<T, MODE>(L.at(p, g.ny, k), em[HY], Sd, uu, ef + 3 * HY, ed + 3 * HY, out, omega, dsum);
+                h_store<T, MODE>(L.at(p, g.ny, k), em[HY], Sd, uu, ef + 3 * HY, ed + 3 * HY, out, omega, dsum,
+                                 er + 3 * HY, ez + 3 * HY, dsum2);
             }
         }
     };
@@ -421,18 +449,34 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
                 uu[d] = s_ownu[at + d];
             }
             const long long base = L.at(p, jc0, k);
-            h_store<T, MODE>(base, mask[g.node(p, jc0, k)], v, uu, f + base, rdiag + base, out, omega, dsum);
+            h_store<T, MODE>(base, mask[g.node(p, jc0, k)], v, uu, f + base, rdiag + base, out, omega, dsum,
+                             Rd + base, zo + base, dsum2);
         }
     }
-    if (MODE == MODE_APPLY && dot_partial) {
+    if ((MODE == MODE_APPLY || MODE == MODE_JACOBI_DOT) && dot_partial) {
         double *red = reinterpret_cast<double *>(smem + S::red_off);
-        for (int o = 16; o > 0; o >>= 1) dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
-        if (l == 0) red[w] = dsum;
+        for (int o = 16; o > 0; o >>= 1) {
+            dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
+            if (MODE == MODE_JACOBI_DOT) dsum2 += __shfl_xor_sync(0xffffffffu, dsum2, o);
+        }
+        if (l == 0) {
+            red[w] = dsum;
+            red[WZ + w] = dsum2;
+        }
         __syncthreads();
         if (tid == 0) {
-            double v = 0.0;
-            for (int q = 0; q < WZ; ++q) v += red[q];
-            dot_partial[blockIdx.x + gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z)] = v;
+            double v = 0.0, v2 = 0.0;
+            for (int q = 0; q < WZ; ++q) {
+                v += red[q];
+                v2 += red[WZ + q];
+            }
+            const long long cta = blockIdx.x + gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
+            if (MODE == MODE_APPLY) {
+                dot_partial[cta] = v;
+            } else {
+                dot_partial[2 * cta] = v;
+                dot_partial[2 * cta + 1] = v2;
+            }
         }
     }
 }
@@ -452,7 +496,7 @@ int hztiles(const Grid &g)
 
 struct HState {
     bool init = false, ok = false;
-    int resident[2][4][HMAXCY + 1] = {};   // [FP64?][mode][cluster size]: clusters resident on the device
+    int resident[2][5][HMAXCY + 1] = {};   // [FP64?][mode][cluster size]: clusters resident on the device
 };
 
 HState &hstate(int dev)
@@ -469,7 +513,7 @@ int hchunk(const Grid &g, int mode)
     int dev = 0;
     cudaGetDevice(&dev);
     const int cy = (g.ny + HY - 1) / HY;
-    const int res = cy <= HMAXCY ? hstate(dev).resident[sizeof(T) == 8][mode & 3][cy] : 0;
+    const int res = cy <= HMAXCY ? hstate(dev).resident[sizeof(T) == 8][mode][cy] : 0;
     if (res <= 0 || g.nx <= HTX) return g.nx <= HTX ? (g.nx > 0 ? g.nx : 1) : HTX;
     const long long nzt = hztiles<T>(g);
     long long best = -1;
@@ -499,7 +543,7 @@ dim3 hgrid(const Grid &g, int htx)
 template <typename T, int MODE>
 int hlaunch(const Lay &L, const ELay &E, const HadamardKe &hk, const T *CX, const T *u, const T *f, const T *rdiag,
             const uint8_t *mask, const uint8_t *maskp, T *out, T omega, T prerelax, double *dot_partial,
-            const int *done, int *err, cudaStream_t st)
+            const int *done, int *err, cudaStream_t st, const double *Rd = nullptr, const T *zo = nullptr)
 {
     constexpr int WZ = hwz<T>();
     using N = HNeeds<MODE>;
@@ -511,8 +555,13 @@ int hlaunch(const Lay &L, const ELay &E, const HadamardKe &hk, const T *CX, cons
         return make_tmap_3d(m, base, (int)es, (uint64_t)L.pitch, (uint64_t)g.nz + 1, (uint64_t)g.nx + 1,
                             L.pitch * es, L.pitch * es * (g.nz + 1), HUW, WZ + 1, 1);
     };
-    CUtensorMap mu, md, mf, mc, mm;
+    CUtensorMap mu, md, mf, mc, mm, mr, mz;
     int s = node_map(&mu, N::PRE ? f : u);
+    if (!s && N::DOT) {   // the FP64 residual and z_old, same boxes as the node planes
+        s = make_tmap_3d(&mr, Rd, 8, (uint64_t)L.pitch, (uint64_t)g.nz + 1, (uint64_t)g.nx + 1, L.pitch * 8,
+                         L.pitch * 8 * (g.nz + 1), HUW, WZ + 1, 1);
+        if (!s) s = node_map(&mz, zo);
+    }
     if (!s && N::D) s = node_map(&md, rdiag);
     if (!s && N::F) s = node_map(&mf, f);
     if (!s)
@@ -524,6 +573,7 @@ int hlaunch(const Lay &L, const ELay &E, const HadamardKe &hk, const T *CX, cons
     if (s) return s;
     if (!N::D) md = mu;
     if (!N::F) mf = mu;
+    if (!N::DOT) mr = mz = mu;
     const HC<T> hc = make_hc<T>(hk);
     const int htx = hchunk<T>(g, MODE);
     const dim3 grid = hgrid<T>(g, htx);
@@ -539,8 +589,8 @@ int hlaunch(const Lay &L, const ELay &E, const HadamardKe &hk, const T *CX, cons
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    GPUTO_CUDA(cudaLaunchKernelEx(&cfg, hsweep_kernel<T, MODE, WZ>, mu, md, mf, mc, mm, L, hc, htx, f, rdiag, mask,
-                                  out, omega, prerelax, dot_partial, done, err));
+    GPUTO_CUDA(cudaLaunchKernelEx(&cfg, hsweep_kernel<T, MODE, WZ>, mu, md, mf, mc, mm, mr, mz, L, hc, htx, f, rdiag, mask,
+                                  out, omega, prerelax, dot_partial, done, err, Rd, zo));
     count_launches(1);
     return GPUTO_OK;
 }
@@ -559,6 +609,8 @@ cudaError_t hset_attrs()
     if ((e = hset_attr<T, MODE_APPLY>()) != cudaSuccess) return e;
     if ((e = hset_attr<T, MODE_DEFECT>()) != cudaSuccess) return e;
     if ((e = hset_attr<T, MODE_JACOBI>()) != cudaSuccess) return e;
+    if constexpr (sizeof(T) == 4)
+        if ((e = hset_attr<T, MODE_JACOBI_DOT>()) != cudaSuccess) return e;
     return hset_attr<T, MODE_JACOBI_PRE>();
 }
 
@@ -592,6 +644,7 @@ void hresident_all(HState &s, int cy)
     s.resident[p][MODE_DEFECT][cy] = hresident<T, MODE_DEFECT>(cy);
     s.resident[p][MODE_JACOBI][cy] = hresident<T, MODE_JACOBI>(cy);
     s.resident[p][MODE_JACOBI_PRE][cy] = hresident<T, MODE_JACOBI_PRE>(cy);
+    if constexpr (sizeof(T) == 4) s.resident[p][MODE_JACOBI_DOT][cy] = hresident<T, MODE_JACOBI_DOT>(cy);
 }
 
 __global__ void pad_mask_kernel(Grid g, const uint8_t *__restrict__ mask, uint8_t *__restrict__ maskp, long long mp)
@@ -695,15 +748,15 @@ bool hsweep_fits(const Grid &g)
     const int cy = (g.ny + HY - 1) / HY;
     if (!s.ok || cy < 1 || cy > HMAXCY || g.nx < 1 || g.nz < 1) return false;
     const int p = sizeof(T) == 8;
-    for (int m = 0; m < 4; ++m)
+    for (int m = 0; m < (p ? 4 : 5); ++m)
         if (s.resident[p][m][cy] <= 0) return false;
     return true;
 }
 
 template <typename T>
-int hsweep_blocks(const Grid &g)
+int hsweep_blocks(const Grid &g, int mode)
 {
-    const dim3 gr = hgrid<T>(g, hchunk<T>(g, MODE_APPLY));
+    const dim3 gr = hgrid<T>(g, hchunk<T>(g, mode));
     return (int)(gr.x * gr.y * gr.z);
 }
 
@@ -718,9 +771,20 @@ void launch_pad_mask(const Grid &g, const uint8_t *mask, uint8_t *maskp, cudaStr
 template <typename T>
 int launch_hsweep(int mode, const Lay &L, const ELay &E, const HadamardKe &hk, const T *CX, const T *u, const T *f,
                   const T *rdiag, const uint8_t *mask, const uint8_t *maskp, T *out, T omega, T prerelax,
-                  double *dot_partial, const int *done, int *err, cudaStream_t st)
+                  double *dot_partial, const int *done, int *err, cudaStream_t st, const double *Rd, const T *zo)
 {
     switch (mode) {
+    case MODE_JACOBI_DOT:
+        if constexpr (sizeof(T) == 4) {
+            if (!Rd || !zo || !dot_partial) {
+                set_error("a Jacobi sweep with dots needs the residual, z_old and the partials");
+                return GPUTO_ERR_ARG;
+            }
+            return hlaunch<T, MODE_JACOBI_DOT>(L, E, hk, CX, u, f, rdiag, mask, maskp, out, omega, prerelax,
+                                               dot_partial, done, err, st, Rd, zo);
+        }
+        set_error("the Jacobi sweep with dots is FP32 only");
+        return GPUTO_ERR_ARG;
     case MODE_APPLY:
         return hlaunch<T, MODE_APPLY>(L, E, hk, CX, u, f, rdiag, mask, maskp, out, omega, prerelax, dot_partial, done,
                                       err, st);
@@ -738,14 +802,14 @@ int launch_hsweep(int mode, const Lay &L, const ELay &E, const HadamardKe &hk, c
 
 template bool hsweep_fits<float>(const Grid &);
 template bool hsweep_fits<double>(const Grid &);
-template int hsweep_blocks<float>(const Grid &);
-template int hsweep_blocks<double>(const Grid &);
+template int hsweep_blocks<float>(const Grid &, int);
+template int hsweep_blocks<double>(const Grid &, int);
 template int launch_hsweep<float>(int, const Lay &, const ELay &, const HadamardKe &, const float *, const float *,
                                   const float *, const float *, const uint8_t *, const uint8_t *, float *, float,
-                                  float, double *, const int *, int *, cudaStream_t);
+                                  float, double *, const int *, int *, cudaStream_t, const double *, const float *);
 template int launch_hsweep<double>(int, const Lay &, const ELay &, const HadamardKe &, const double *,
                                    const double *, const double *, const double *, const uint8_t *,
                                    const uint8_t *, double *, double, double, double *, const int *, int *,
-                                   cudaStream_t);
+                                   cudaStream_t, const double *, const double *);
 
 }  // namespace gputo

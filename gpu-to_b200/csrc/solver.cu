@@ -177,7 +177,8 @@ int Solver::create(int nelx, int nely, int nelz, int nl_, const gputo_options *o
     ALLOC(LinvT, (long long)nc * nc);
     ALLOC(ctmp, nc);
     if (nl == 1) ALLOC(Apk0, 300 * g[0].nel());
-    partial_cap = std::max({fine_sweep_blocks(g[0]), hsweep_blocks<double>(g[0]), 1 << 12});
+    partial_cap = std::max({fine_sweep_blocks(g[0]), hsweep_blocks<double>(g[0]),
+                            2 * hsweep_blocks<float>(g[0], MODE_JACOBI_DOT), 1 << 12});
     ALLOC(partial, partial_cap);
     ALLOC(ticket, 4);
     ALLOC(sc, 1);
@@ -333,7 +334,7 @@ int Solver::setup(const double *CX_in, cudaStream_t st)
 // in its second buffer (bufs[1]), which for level 0 is z itself.
 template <typename T>
 void Solver::vcycle_impl(LevelBuf<T> *Lv, const T *CXl, const T *r0, T *z0, const int *done,
-                         cudaStream_t st)
+                         cudaStream_t st, const double *dotR, const T *dotZold, double *dotPartial)
 {
     const int ns = opt.nswp;
     const T om = (T)opt.omega, pr = (T)opt.prerelax;
@@ -389,7 +390,11 @@ void Solver::vcycle_impl(LevelBuf<T> *Lv, const T *CXl, const T *r0, T *z0, cons
         int cur = (ns == 0) ? 1 : ((ns - 1) & 1);
         launch_prolong_add<T>(lay[l], lay[l + 1], bufs(l + 1, 1), mask[l], bufs(l, cur), done, st);
         for (int s = 0; s < ns; ++s) {
-            sweep(l, MODE_JACOBI, bufs(l, cur), f, bufs(l, cur ^ 1), om);
+            if (l == 0 && s == ns - 1 && dotR)   // the last sweep also sums r'z and r'z_old
+                note(fine_sweep<T>(0, MODE_JACOBI_DOT, lay[0], elay, CXl, bufs(0, cur), f, Lv[0], bufs(0, cur ^ 1), om,
+                                   pr, dotPartial, done, st, dotR, dotZold));
+            else
+                sweep(l, MODE_JACOBI, bufs(l, cur), f, bufs(l, cur ^ 1), om);
             cur ^= 1;
         }
     }
@@ -526,8 +531,13 @@ void Solver::iteration(cudaStream_t st)
         // float(r) comes from the residual update and z stays the FP32
         // V-cycle output: no precision-conversion passes
         launch_pcg_update(nv, Uw, R, P, Q, partial, ticket, sc, st, Lf[0].f);
-        vcycle_impl<float>(Lf, CXpf, Lf[0].f, Lf[0].u1, done, st);
-        launch_dot2<float>(nv, R, Lf[0].u1, Zold32, partial, ticket, sc, done, st);
+        if (fused_dot()) {
+            vcycle_impl<float>(Lf, CXpf, Lf[0].f, Lf[0].u1, done, st, R, Zold32, partial);
+            launch_finish_dot2(hsweep_blocks<float>(g[0], MODE_JACOBI_DOT), partial, sc, st);
+        } else {
+            vcycle_impl<float>(Lf, CXpf, Lf[0].f, Lf[0].u1, done, st);
+            launch_dot2<float>(nv, R, Lf[0].u1, Zold32, partial, ticket, sc, done, st);
+        }
         launch_p_update<float>(nv, Lf[0].u1, P, Zold32, sc, st);
         return;
     }

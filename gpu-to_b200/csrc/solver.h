@@ -97,11 +97,11 @@ struct Solver {
     template <typename T>
     int fine_sweep(int l, int mode, const Lay &Lo, const ELay &E, const T *CXl, const T *u, const T *f,
                    const LevelBuf<T> &B, T *out, T omega, T pr, double *dot_partial, const int *done,
-                   cudaStream_t st) const
+                   cudaStream_t st, const double *Rd = nullptr, const T *zo = nullptr) const
     {
         if (use_hsweep<T>(Lo.g) && B.rdiag)
             return launch_hsweep<T>(mode, Lo, E, hk, CXl, u, f, B.rdiag, mask[l], maskp[l], out, omega, pr,
-                                    dot_partial, done, err, st);
+                                    dot_partial, done, err, st, Rd, zo);
         return launch_fine_sweep<T>(mode, Lo, E, CXl, u, f, B.diag, mask[l], out, omega, pr, dot_partial, done, err,
                                     st);
     }
@@ -126,7 +126,11 @@ struct Solver {
     int alloc_levels(LevelBuf<T> *Lv, bool with_matrices);
     template <typename T>
     void vcycle_impl(LevelBuf<T> *Lv, const T *CXl, const T *r0, T *z0, const int *done,
-                     cudaStream_t st);
+                     cudaStream_t st, const double *dotR = nullptr, const T *dotZold = nullptr,
+                     double *dotPartial = nullptr);
+    // The mixed PCG's r'z and r'z_old come from its last fine smoothing sweep
+    // (MODE_JACOBI_DOT) when that sweep is the Hadamard-basis kernel.
+    bool fused_dot() const { return use_hsweep<float>(g[0]) && Lf[0].rdiag && opt.tc_parts == 0 && opt.nswp > 0; }
     int run_graph(int batch, cudaStream_t st);
     void note(int s)
     {
