@@ -2,9 +2,10 @@
 //
 // Same modes and results as tile_kernel (K u, f - K u, damped Jacobi with the
 // Dirichlet rows zeroed: mgcg1.cu:941-997,1199-1264,1326-1331), with far
-// fewer operations per element.
+// fewer operations per element; MODE_JACOBI_DOT is the FP32 Jacobi sweep that
+// also sums the mixed PCG's r'z and r'z_old (mgcg1.cu:263-265).
 //
-// The algebra.  Let H be the 2x2 Hadamard matrix and T = H (x) H (x) H act on
+// The algebra (its helpers are in hadamard.h).  Let H be the 2x2 Hadamard matrix and T = H (x) H (x) H act on
 // the eight corners of an element (corner (cx, cy, cz), mode (px, py, pz),
 // sign (-1)^(px cx + py cy + pz cz)).  For the trilinear hex8 of an isotropic
 // material on a cube, Ke is a sum of Kronecker products of the 1-D mass,
