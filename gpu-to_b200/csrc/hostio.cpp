@@ -5,13 +5,16 @@
 // A caller's arrays are ordinary (pageable) memory.  Each copy goes through
 // two pinned chunks of kChunk bytes: while the DMA engine moves one chunk,
 // host threads copy the next one between the caller's array and the other
-// pinned chunk.  The host-side copy is split over kCopyThreads threads, so
-// the copy is not limited by one core's memcpy bandwidth.
+// pinned chunk.  The host-side copy is split over copy_threads() threads, so
+// the copy is not limited by one core's memcpy bandwidth (environment
+// variable GPUTO_COPY_THREADS, 1-64, read once; default kCopyThreads, at most
+// the host's hardware threads).
 //
 // The device buffers are grown on demand and kept, so a design loop that calls
 // these entry points does not allocate and free device memory every time
 // (cudaFree also waits for the whole device).
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <mutex>
@@ -25,7 +28,7 @@ namespace gputo {
 namespace {
 
 constexpr size_t kChunk = size_t(8) << 20;   // bytes per pinned chunk
-constexpr int kCopyThreads = 8;              // host threads per chunk copy
+constexpr int kCopyThreads = 8;              // default host threads per chunk copy
 constexpr size_t kMinSplit = size_t(1) << 20;
 
 // Runs job(i) for i in [0, parts) on a few persistent threads plus the caller.
@@ -88,25 +91,40 @@ class CopyPool {
     std::vector<std::thread> workers_;
 };
 
+int copy_threads()
+{
+    static const int n = [] {
+        int v = kCopyThreads;
+        if (const char *e = std::getenv("GPUTO_COPY_THREADS")) {
+            const int a = std::atoi(e);
+            if (a >= 1 && a <= 64) v = a;
+        }
+        const int hw = (int)std::thread::hardware_concurrency();
+        return (hw > 0 && v > hw) ? hw : v;
+    }();
+    return n;
+}
+
 CopyPool &pool()
 {
     // never destroyed: its threads wait on the pool until the process ends
-    static CopyPool *p = new CopyPool(kCopyThreads - 1);
+    static CopyPool *p = new CopyPool(copy_threads() - 1);
     return *p;
 }
 
 void par_memcpy(void *dst, const void *src, size_t n)
 {
-    if (n < kMinSplit) {
+    const int nt = copy_threads();
+    if (n < kMinSplit || nt == 1) {
         std::memcpy(dst, src, n);
         return;
     }
-    const size_t part = (n + kCopyThreads - 1) / kCopyThreads;
+    const size_t part = (n + nt - 1) / nt;
     const std::function<void(int)> job = [&](int i) {
         const size_t off = (size_t)i * part;
         if (off < n) std::memcpy((char *)dst + off, (const char *)src + off, std::min(part, n - off));
     };
-    pool().run(kCopyThreads, job);
+    pool().run(nt, job);
 }
 
 struct Staging {
