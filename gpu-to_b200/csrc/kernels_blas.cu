@@ -199,6 +199,7 @@ pcg_update_kernel(long long n, double *__restrict__ U, double *__restrict__ R,
                   const double *__restrict__ P, const double *__restrict__ Q,
                   double *__restrict__ partial, unsigned *ticket, PcgScalars *sc, float *__restrict__ R32)
 {
+    pdl_wait();
     if (sc->done) return;
     __shared__ double red[kRedThreads / 32];
     const double alpha = sc->alpha;
@@ -241,7 +242,8 @@ pcg_update_kernel(long long n, double *__restrict__ U, double *__restrict__ R,
 void launch_pcg_update(long long n, double *U, double *R, const double *P, const double *Q,
                        double *partial, unsigned *ticket, PcgScalars *sc, cudaStream_t st, float *R32)
 {
-    pcg_update_kernel<<<red_blocks(n), kRedThreads, 0, st>>>(n, U, R, P, Q, partial, ticket, sc, R32);
+    launch_pdl(pcg_update_kernel, dim3(red_blocks(n)), dim3(kRedThreads), 0, st, n, U, R, P, Q, partial, ticket, sc,
+               R32);
     count_launches(1);
 }
 
@@ -250,6 +252,7 @@ template <typename Z>
 __global__ void p_update_kernel(long long n, const Z *__restrict__ z_in, double *__restrict__ P,
                                 Z *__restrict__ Zold, const PcgScalars *sc)
 {
+    pdl_wait();
     if (sc->done) return;
     const double beta = sc->beta;
     const long long n2 = n >> 1;
@@ -275,7 +278,7 @@ __global__ void p_update_kernel(long long n, const Z *__restrict__ z_in, double 
 template <typename Z>
 void launch_p_update(long long n, const Z *z, double *P, Z *Zold, const PcgScalars *sc, cudaStream_t st)
 {
-    p_update_kernel<Z><<<red_blocks(n), kRedThreads, 0, st>>>(n, z, P, Zold, sc);
+    launch_pdl(p_update_kernel<Z>, dim3(red_blocks(n)), dim3(kRedThreads), 0, st, n, z, P, Zold, sc);
     count_launches(1);
 }
 template void launch_p_update<double>(long long, const double *, double *, double *, const PcgScalars *,
@@ -336,6 +339,7 @@ void launch_pcg_init(long long n, const double *F, double *U, double *R, double 
 __global__ void __launch_bounds__(kRedThreads)
 finish_apply_dot_kernel(int nb, const double *__restrict__ partial, PcgScalars *sc)
 {
+    pdl_wait();
     if (sc->done) return;
     __shared__ double red[kRedThreads / 32];
     const double s = sum_partials(partial, nb, red);
@@ -354,13 +358,14 @@ finish_apply_dot_kernel(int nb, const double *__restrict__ partial, PcgScalars *
 void launch_finish_apply_dot(int nblocks, double *partial, unsigned *, PcgScalars *sc,
                              cudaStream_t st)
 {
-    finish_apply_dot_kernel<<<1, kRedThreads, 0, st>>>(nblocks, partial, sc);
+    launch_pdl(finish_apply_dot_kernel, dim3(1), dim3(kRedThreads), 0, st, nblocks, (const double *)partial, sc);
     count_launches(1);
 }
 
 __global__ void __launch_bounds__(kRedThreads)
 finish_dot2_kernel(int nb, const double *__restrict__ partial, PcgScalars *sc)
 {
+    pdl_wait();
     if (sc->done) return;
     __shared__ double red[kRedThreads / 32];
     double a = 0.0, b = 0.0;
@@ -376,7 +381,7 @@ finish_dot2_kernel(int nb, const double *__restrict__ partial, PcgScalars *sc)
 
 void launch_finish_dot2(int nblocks, const double *partial, PcgScalars *sc, cudaStream_t st)
 {
-    finish_dot2_kernel<<<1, kRedThreads, 0, st>>>(nblocks, partial, sc);
+    launch_pdl(finish_dot2_kernel, dim3(1), dim3(kRedThreads), 0, st, nblocks, partial, sc);
     count_launches(1);
 }
 
