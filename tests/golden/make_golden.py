@@ -8,7 +8,8 @@ Run here, where the reference tree is mounted:  python tests/golden/make_golden.
 * ``kem3_ref.npz``: Kem3 (Cantilever/omp/mgcg1.c:1370) from the compiled
   reference, h = 1 and 2.
 * ``solve_*.npz``: known-answer solves of the reference's own, unmodified
-  OpenMP MEX (Cantilever/omp/mgcg1.c), compiled into oracle/_ref.
+  OpenMP MEX (Cantilever/omp/mgcg1.c), compiled into oracle/_ref (cantilevers,
+  corner supports, and the bridge workload's supports and load).
 * ``design_c1.npz``: the 64x32x32 cantilever (~215k DOF) design loop,
   50 OC iterations, with every solve done by that compiled reference and the
   MATLAB-side steps by the oracle's numpy restatement.
@@ -84,27 +85,39 @@ def corner_supports(nelx, nely, nelz):
     return O.Problem(nelx, nely, nelz, F, np.array(sorted(set(fixed)), dtype=np.float64))
 
 
-def main(only_design=False):
-    O.build()
-    os.environ.setdefault("OMP_THREAD_LIMIT", str(os.cpu_count()))
-    if only_design:
-        return design()
-    np.save(os.path.join(HERE, "ke0_matlab.npy"), matlab_ke0())
-    np.savez(os.path.join(HERE, "kem3_ref.npz"), h1=kem3(1.0), h2=kem3(2.0))
-
-    cases = [
+def solve_cases():
+    return [
         ("solve_16x8x8_rand_nl3", O.cantilever(16, 8, 8), lambda: O.simp(O.random_density(16, 8, 8, 1))[0], 3, 1e-8, 200),
         ("solve_32x16x16_unif_nl4", O.cantilever(32, 16, 16), lambda: O.simp(np.full(32 * 16 * 16, 0.12))[0], 4, 1e-8, 200),
         ("solve_16x8x8_corner_nl3", corner_supports(16, 8, 8), lambda: O.simp(O.random_density(16, 8, 8, 7))[0], 3, 1e-8, 200),
         ("solve_16x8x8_maxit3_nl2", O.cantilever(16, 8, 8), lambda: O.simp(O.random_density(16, 8, 8, 3))[0], 2, 1e-12, 3),
+        # the bridge workload's supports and top-face load (oracle.bridge)
+        ("solve_16x8x8_bridge_nl3", O.bridge(16, 8, 8), lambda: O.simp(O.random_density(16, 8, 8, 11))[0], 3, 1e-8, 200),
     ]
-    for name, p, cxf, nl, tol, maxit in cases:
+
+
+def solves(only=None):
+    for name, p, cxf, nl, tol, maxit in solve_cases():
+        if only and name not in only:
+            continue
         CX = cxf()
         U, rr, nit = O.ref_mgcg1(p, CX, nl, tol, maxit)
         np.savez_compressed(os.path.join(HERE, name + ".npz"), nelx=p.nelx, nely=p.nely, nelz=p.nelz,
                             F=p.F, fixed=p.fixed, CX=CX, nl=nl, tol=tol, maxit=maxit, U=U,
                             relres=rr, nit=nit)
         print(name, "relres", rr, "nit", nit)
+
+
+def main(only_design=False, only=None):
+    O.build()
+    os.environ.setdefault("OMP_THREAD_LIMIT", str(os.cpu_count()))
+    if only_design:
+        return design()
+    if only:
+        return solves(only)
+    np.save(os.path.join(HERE, "ke0_matlab.npy"), matlab_ke0())
+    np.savez(os.path.join(HERE, "kem3_ref.npz"), h1=kem3(1.0), h2=kem3(2.0))
+    solves()
 
     # 64x32x32 cantilever: first solve (uniform 0.12) + the 50-iteration design
     p = O.cantilever(64, 32, 32)
@@ -132,4 +145,6 @@ def design():
 
 
 if __name__ == "__main__":
-    main(only_design="--design" in sys.argv)
+    # --design: only the design-loop history; --only NAME[,NAME]: only those solve fixtures
+    only = sys.argv[sys.argv.index("--only") + 1].split(",") if "--only" in sys.argv else None
+    main(only_design="--design" in sys.argv, only=only)

@@ -68,7 +68,7 @@ def test_vcycle_matches_oracle(oracle, gputo, torch, shape, nl):
 
 
 @pytest.mark.parametrize("name", ["solve_16x8x8_rand_nl3", "solve_32x16x16_unif_nl4",
-                                  "solve_16x8x8_maxit3_nl2"])
+                                  "solve_16x8x8_maxit3_nl2", "solve_16x8x8_bridge_nl3"])
 def test_mex_entry_matches_reference_golden(oracle, gputo, name):
     """gputo.mgcg1 (the MEX call layout, host buffers) vs the compiled reference."""
     d = load_golden(name)

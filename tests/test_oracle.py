@@ -74,7 +74,7 @@ def test_apply_matches_assembled_matrix(oracle):
 
 
 @pytest.mark.parametrize("name", ["solve_16x8x8_rand_nl3", "solve_32x16x16_unif_nl4",
-                                  "solve_16x8x8_maxit3_nl2"])
+                                  "solve_16x8x8_maxit3_nl2", "solve_16x8x8_bridge_nl3"])
 def test_oracle_solver_matches_reference_mex(oracle, name):
     d = load_golden(name)
     p = _problem(oracle, d)
