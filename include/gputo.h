@@ -122,7 +122,7 @@ int gputo_fine_op_constants(const double *Ke, double *c8);
  *         output (mgcg1.cu:282-283), as the MATLAB drivers expect
  * CX      nel element stiffness scale E(x)
  * fixed1b nfd 1-based indices of the fixed dofs (MATLAB's fixed')
- * nl      multigrid levels; nelx, nely, nelz divisible by 2^(nl-1)
+ * nl      multigrid levels; nelx, nely, nelz divisible by 2^(nl-1); nelx <= 65534
  * tol     relative residual tolerance on ||r||/||F||
  * maxit   PCG iteration limit
  * printLev  0: silent; >=1: append a summary to ./mgcg1.log as the MEX does
