@@ -9,9 +9,10 @@ Outputs (git-ignored, shipped with the tree):
                                     against libgputo.so.  It is compiled
                                     against MATLAB's mex.h when MATLAB_ROOT is
                                     set, else against the project's stand-in
-                                    declarations (oracle/shim/mex.h); the mx*
-                                    symbols stay undefined and resolve from
-                                    MATLAB's libmx (or the stand-in) at load.
+                                    declarations (gpu-to_b200/mex_api/mex.h);
+                                    the mx* symbols stay undefined and resolve
+                                    from MATLAB's libmx (or a harness's own
+                                    implementation) at load.
   gpu-to_b200/lib/libgputo_mex9.so  the same for the MEX mgcg9 (18 arguments)
 """
 from __future__ import annotations
@@ -70,7 +71,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         _run([NVCC, *ARCH, "-shared", "-o", so, *objs, "-cudart", "static", "-lpthread"])
     # MEX gateway
     mex_inc = os.path.join(os.environ["MATLAB_ROOT"], "extern", "include") if os.environ.get(
-        "MATLAB_ROOT") else os.path.join(ROOT, "oracle", "shim")
+        "MATLAB_ROOT") else os.path.join(HERE, "mex_api")
     for src, out in (("mex_gateway.cpp", "libgputo_mex.so"), ("mex_gateway9.cpp", "libgputo_mex9.so")):
         gw_src = os.path.join(CSRC, src)
         gw = os.path.join(LIB, out)

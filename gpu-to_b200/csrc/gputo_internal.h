@@ -126,6 +126,11 @@ double *host_call_buffer(int slot, size_t count, int *status);
 // ---- kernel launchers (kernels_*.cu) --------------------------------------
 // Level-0 element matrix in constant memory (FP64 and FP32 copies).
 int upload_fine_ke(const double *Ke_host, cudaStream_t st);
+// Unique id of the calling thread's current CUDA context (0 if none or the
+// driver lacks cuCtxGetId).  Per-device caches of device state (constant
+// memory contents, symbol addresses) key on it, so a cudaDeviceReset, which
+// replaces the primary context, invalidates them.
+unsigned long long current_context_id();
 int upload_design_ke(const double *Ke_host, cudaStream_t st);
 int upload_tc_ke(const double *Ke_host, cudaStream_t st);
 int upload_tcsweep_ke(const double *Ke_host, cudaStream_t st);

@@ -4,6 +4,7 @@
 #include "hadamard.h"
 
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 namespace gputo {
@@ -14,13 +15,19 @@ namespace gputo {
 // cube element's Hadamard pattern, its eight constants (per device) select
 // the Hadamard-basis energy pass.
 __constant__ double cKeD[576];
-HadamardKe g_design_hk[64];
+static HadamardKe g_design_hk[64];
+static std::mutex g_design_hk_mu;   // writers (upload) and readers (launch) on other threads
 
 int upload_design_ke(const double *Ke_host, cudaStream_t st)
 {
     int dev = 0;
     GPUTO_CUDA(cudaGetDevice(&dev));
-    (void)hadamard_ke(Ke_host, &g_design_hk[dev < 64 ? dev : 63]);   // sets ok = false without the pattern
+    HadamardKe hk;
+    (void)hadamard_ke(Ke_host, &hk);   // sets ok = false without the pattern
+    {
+        std::lock_guard<std::mutex> lock(g_design_hk_mu);
+        g_design_hk[dev < 64 ? dev : 63] = hk;
+    }
     GPUTO_CUDA(cudaMemcpyToSymbolAsync(cKeD, Ke_host, sizeof(double) * 576, 0,
                                        cudaMemcpyHostToDevice, st));
     return GPUTO_OK;
@@ -121,7 +128,11 @@ void launch_element_energy_blocks(const Grid &g, const double *U, const double *
 {
     int dev = 0;
     cudaGetDevice(&dev);
-    const HadamardKe &hk = g_design_hk[dev < 64 ? dev : 63];
+    HadamardKe hk;
+    {
+        std::lock_guard<std::mutex> lock(g_design_hk_mu);
+        hk = g_design_hk[dev < 64 ? dev : 63];
+    }
     if (hk.ok)
         element_energy_kernel<true><<<(unsigned)nblocks, 256, 0, st>>>(g, make_hc<double>(hk), U, CX, dsK, ce, dc,
                                                                        partial, ticket, compliance);

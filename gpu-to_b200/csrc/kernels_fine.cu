@@ -38,12 +38,15 @@ int upload_fine_ke(const double *Ke_host, cudaStream_t st)
     static std::mutex mu;
     static double last[64][576];
     static bool have[64] = {};
+    static unsigned long long ctx_of[64] = {};
     std::lock_guard<std::mutex> lock(mu);
     int dev = 0;
     GPUTO_CUDA(cudaGetDevice(&dev));
     const int slot = dev < 64 ? dev : 63;
-    // Ke0 is an argument of every MEX call; skip the copy when it repeats.
-    bool same = have[slot] && dev < 64;
+    // Ke0 is an argument of every MEX call; skip the copy when it repeats
+    // (in the same context: a device reset clears constant memory).
+    const unsigned long long ctx = current_context_id();
+    bool same = have[slot] && dev < 64 && ctx != 0 && ctx_of[slot] == ctx;
     for (int m = 0; same && m < 576; ++m) same = (last[slot][m] == Ke_host[m]);
     if (same) return GPUTO_OK;
     float kf[576];
@@ -52,6 +55,7 @@ int upload_fine_ke(const double *Ke_host, cudaStream_t st)
         kf[m] = (float)Ke_host[m];
     }
     have[slot] = true;
+    ctx_of[slot] = ctx;
     GPUTO_CUDA(cudaMemcpyToSymbolAsync(cKe64, last[slot], sizeof(double) * 576, 0, cudaMemcpyHostToDevice, st));
     GPUTO_CUDA(cudaMemcpyToSymbolAsync(cKe32, kf, sizeof(kf), 0, cudaMemcpyHostToDevice, st));
     GPUTO_CUDA(cudaMemcpyToSymbolAsync(cKe32p, kf, sizeof(kf), 0, cudaMemcpyHostToDevice, st));
@@ -656,6 +660,26 @@ static EncodeTiledFn encode_fn()
             fn = reinterpret_cast<EncodeTiledFn>(p);
     });
     return fn;
+}
+
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long *);
+
+unsigned long long current_context_id()
+{
+    static CtxGetIdFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, []() {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<CtxGetIdFn>(p);
+    });
+    if (!fn) return 0;
+    // 0 as well before the runtime has made its primary context current on
+    // this thread: callers then treat their cache as stale
+    unsigned long long id = 0;
+    return fn(nullptr, &id) == CUDA_SUCCESS ? id : 0;
 }
 
 int make_tmap_3d(CUtensorMap *m, const void *base, int elem_bytes, uint64_t d0, uint64_t d1,

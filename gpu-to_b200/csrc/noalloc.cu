@@ -3,13 +3,12 @@
 // gputo_compliance_sens_dev() creates its reduction scratch (per-CTA partial
 // sums, a completion ticket, the compliance scalar) and a stream with
 // cudaMalloc / cudaStreamCreate on its first call.  Some callers cannot let a
-// library do that: code running inside a CUDA stream capture (cudaMalloc is
-// not a stream operation and invalidates a global-mode capture), hosts whose
-// memory manager owns the whole device (a MATLAB gpuArray workspace or a
-// caching allocator that must see every byte), and real-time loops where the
-// implicit device synchronisation of cudaMalloc / cudaFree is not allowed.
-// This entry point computes the same result with its scratch in a file-scope
-// device array, so it allocates nothing at all.
+// library do that: hosts whose memory manager owns the whole device (a
+// MATLAB gpuArray workspace, or a caching allocator that has reserved the
+// free memory and must account for every byte), and real-time loops where
+// the implicit device synchronisation of cudaMalloc / cudaFree is not
+// allowed.  This entry point computes the same result with its scratch in a
+// file-scope device array, so it allocates nothing at all.
 #include "gputo_internal.h"
 
 #include <mutex>
@@ -31,12 +30,16 @@ struct NoAllocScratch {
 // the library until the process exits).
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
 
-// Device address of the scratch, looked up once per device (host code must not
-// use the symbol itself: on the host it only stands in for the device array).
+// Device address of the scratch, looked up once per device and context (host
+// code must not use the symbol itself: on the host it only stands in for the
+// device array).  A cudaDeviceReset replaces the device's primary context; the
+// context id tells the cached address of the old one apart, and the lookup
+// runs again.
 static NoAllocScratch *noalloc_scratch_for_current_device(int *status)
 {
     static std::mutex mu;
     static NoAllocScratch *addr[64] = {};
+    static unsigned long long ctx_of[64] = {};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess || dev < 0 || dev >= 64) {
@@ -44,7 +47,8 @@ static NoAllocScratch *noalloc_scratch_for_current_device(int *status)
         return nullptr;
     }
     std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev]) {
+    const unsigned long long ctx = current_context_id();
+    if (!addr[dev] || ctx == 0 || ctx != ctx_of[dev]) {
         void *p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) {
@@ -52,6 +56,7 @@ static NoAllocScratch *noalloc_scratch_for_current_device(int *status)
             return nullptr;
         }
         addr[dev] = static_cast<NoAllocScratch *>(p);
+        ctx_of[dev] = current_context_id();   // the lookup made the context current
     }
     *status = GPUTO_OK;
     return addr[dev];

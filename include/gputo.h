@@ -345,21 +345,26 @@ int gputo_compliance_sens_tc_dev(const double *Ke0, const double *U, const doubl
  * No counterpart in the reference: its sensitivity step is MATLAB code.
  *
  * gputo_compliance_sens_dev creates reduction scratch and a stream the first
- * time it runs.  Code inside a CUDA stream capture, hosts whose memory manager
- * owns the whole device (a MATLAB gpuArray workspace, a caching allocator) and
- * real-time loops that must not hit cudaMalloc's implicit synchronisation
- * cannot allow that.  This variant takes the same arguments and gives the same
- * results, but keeps its scratch in a fixed device array compiled into the
- * library (about 64 KB, held by every GPU that loads the library until the
- * process exits) and calls no allocator.
+ * time it runs.  Hosts whose memory manager owns the whole device (a MATLAB
+ * gpuArray workspace, a caching allocator that has reserved the free memory)
+ * and real-time loops that must not hit the implicit device synchronisation
+ * of cudaMalloc / cudaFree cannot allow that.  This variant takes the same
+ * arguments and gives the same results, but keeps its scratch in a fixed
+ * device array compiled into the library (about 64 KB, held by every GPU that
+ * loads the library until the process exits) and calls no allocator.
  *  - Grids above 16,777,216 elements are rejected with GPUTO_ERR_ARG.
- *  - The first call on a device looks up the array's device address; make that
- *    first call before any stream capture.
+ *  - The first call on a device (and the first after a cudaDeviceReset)
+ *    looks up the array's device address; make that first call before any
+ *    stream capture.
  *  - Every call shares the array: calls that overlap on the GPU (different
  *    streams, or different host threads on one device) race and must be
  *    serialised by the caller.
+ *  - A call whose Ke0 differs from the last one the device saw rewrites the
+ *    library's constant-memory copy of Ke, which every gputo kernel on that
+ *    device reads: serialise such a call against all other gputo work on the
+ *    device (solves, sensitivities) as well.
  * 'stream' may be NULL (the legacy default stream); the call returns after
- * the stream has finished the work. */
+ * the stream has finished the work, and 'compliance' is a host pointer. */
 int gputo_compliance_sens_noalloc_dev(const double *Ke0, const double *U, const double *CX,
                                       const double *dsK, int nelx, int nely, int nelz, double *ce,
                                       double *dc, double *compliance, void *stream);

@@ -30,7 +30,9 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 import oracle as O  # noqa: E402
 
-REFROOT = "/root/reference"
+# Root of the reference checkout (read-only).  Set GPUTO_REFERENCE_ROOT to
+# point at it; the fallback is where this build's recipe keeps it.
+REFROOT = os.environ.get("GPUTO_REFERENCE_ROOT", "/root/reference")
 
 
 def matlab_ke0():
