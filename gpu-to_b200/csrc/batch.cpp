@@ -102,6 +102,7 @@ int gputo_batch_solve_dev(gputo_batch *b, const double *const *F, double *const 
         Solver &s = b->members[i]->s;
         GPUTO_CUDA(cudaStreamWaitEvent(b->side[i], b->fork, 0));
         // the solver works in its row-padded layout (as gputo_solver_solve_dev)
+        s.have_solution = false;
         gputo::launch_pack(s.lay[0], F[i], s.Fw, 0, b->side[i]);
         int st = s.solve_begin(s.Fw, tol, maxit, b->side[i]);
         if (st) return st;
@@ -194,6 +195,7 @@ int gputo_autotune_dev(gputo_solver *h, const double *F, double *U, double tol, 
             }
     }
     cudaStream_t st = s.own_stream;
+    s.have_solution = false;
     gputo::launch_pack(s.lay[0], F, s.Fw, 0, st);   // the solver's row-padded layout
     cudaEvent_t e0, e1;
     GPUTO_CUDA(cudaEventCreate(&e0));

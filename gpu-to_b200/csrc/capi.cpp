@@ -173,12 +173,37 @@ int gputo_solver_solve_dev(gputo_solver *h, const double *F, double *U, double t
     if (!s.ready) return GPUTO_ERR_ARG;
     cudaStream_t st = s.stream(stream);
     gputo::launch_pack(s.lay[0], F, s.Fw, 0, st);
+    s.have_solution = false;
     int r = s.solve(s.Fw, s.Uw, tol, maxit, relres, nit, st, nullptr);
     if (r == GPUTO_OK || r == GPUTO_ERR_BREAKDOWN) {
         gputo::launch_unpack(s.lay[0], s.Uw, U, 0, st);
         GPUTO_CUDA(cudaStreamSynchronize(st));
+        s.have_solution = r == GPUTO_OK;
     }
     return r;
+}
+
+int gputo_solver_energy_dev(gputo_solver *h, const double *dsK, double *ce, double *dc, double *compliance,
+                            double *true_relres, void *stream)
+{
+    if (!h || !ce || (dc && !dsK)) return GPUTO_ERR_ARG;
+    Solver &s = h->s;
+    if (!s.ready || !s.have_solution) {
+        gputo::set_error("gputo_solver_energy_dev needs a successful gputo_solver_solve_dev before it");
+        return GPUTO_ERR_ARG;
+    }
+    cudaStream_t st = s.stream(stream);
+    int r = s.energy(dsK, ce, dc, s.e2, st);
+    if (r) return r;
+    double hv[2] = {0.0, 0.0};
+    GPUTO_CUDA(cudaMemcpyAsync(hv, s.e2, sizeof(hv), cudaMemcpyDeviceToHost, st));
+    GPUTO_CUDA(cudaStreamSynchronize(st));
+    GPUTO_CUDA(cudaGetLastError());
+    r = s.check_error_flags(st);
+    if (r) return r;
+    if (compliance) *compliance = hv[1];
+    if (true_relres) *true_relres = hv[0] < 0.0 ? -1.0 : (s.last_res0 > 0.0 ? std::sqrt(hv[0]) / s.last_res0 : 0.0);
+    return GPUTO_OK;
 }
 
 int gputo_solver_vcycle_dev(gputo_solver *h, const double *r, double *z, void *stream)
@@ -188,6 +213,7 @@ int gputo_solver_vcycle_dev(gputo_solver *h, const double *r, double *z, void *s
     if (!s.ready) return GPUTO_ERR_ARG;
     cudaStream_t st = s.stream(stream);
     s.launch_status = GPUTO_OK;
+    s.have_solution = false;   // Fw is reused
     gputo::launch_pack(s.lay[0], r, s.Fw, 0, st);
     s.vcycle(s.Fw, s.Z, nullptr, st);
     gputo::launch_unpack(s.lay[0], s.Z, z, 0, st);
@@ -412,6 +438,11 @@ int gputo_solver_level2_inject_dev(gputo_solver *h, const double *v, float *out,
 }
 
 long long gputo_solver_launch_count(const gputo_solver *) { return gputo::launches_issued(); }
+
+int gputo_debug_set_sweep_fault(int skip_stage, unsigned wait_us)
+{
+    return gputo::set_sweep_fault_hook(skip_stage, wait_us);
+}
 
 int gputo_solver_time_kernel(gputo_solver *h, int which, int reps, double *ms, void *stream)
 {

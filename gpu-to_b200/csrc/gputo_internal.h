@@ -144,6 +144,11 @@ enum SweepMode { MODE_APPLY = 0, MODE_DEFECT = 1, MODE_JACOBI = 2, MODE_JACOBI_P
 // FP64 PCG residual, z its output, z_old the previous one) into per-CTA
 // partial pairs: the mixed PCG's last smoothing sweep (Hadamard-basis kernel only).
 constexpr int MODE_JACOBI_DOT = 4;
+// The FP64 fine operator applied to a solution U, with the element energies
+// in the same pass (Hadamard-basis kernel only): per-CTA partial pairs of
+// |f - K u|^2 over the free dofs and sum CX_e u_e' Ke u_e, and ce_e (dc_e =
+// dsK_e ce_e) written once per element.
+constexpr int MODE_ENERGY = 5;
 
 // Fine level (K = sum CX_e Ke), FP64 and FP32 instantiations; CX padded (ELay),
 // vectors padded (Lay).  'err' receives GPUTO_ERR_TIMEOUT if a bounded wait
@@ -186,6 +191,9 @@ struct HadamardKe {
 };
 bool hadamard_ke(const double *Ke, HadamardKe *hk);
 int init_hsweep_kernels();
+// Test hook of the Hadamard-basis sweeps' bounded waits (see
+// gputo_debug_set_sweep_fault in gputo.h).
+int set_sweep_fault_hook(int skip_stage, unsigned wait_us);
 template <typename T> bool hsweep_fits(const Grid &g);
 template <typename T> int hsweep_blocks(const Grid &g, int mode = MODE_APPLY);   // CTAs (= partials) of a sweep
 // rdiag: 1/diag (launch_recip); maskp: the Dirichlet bytes with rows padded
@@ -195,6 +203,15 @@ int launch_hsweep(int mode, const Lay &L, const ELay &E, const HadamardKe &hk, c
                   const T *rdiag, const uint8_t *mask, const uint8_t *maskp, T *out, T omega, T prerelax,
                   double *dot_partial, const int *done, int *err, cudaStream_t st, const double *Rd = nullptr,
                   const T *zo = nullptr);
+// MODE_ENERGY sweep (FP64): out (optional) = f - K u with fixed rows zero,
+// ce / dc in natural element order, partial pairs (|r|^2, sum CX ce) per CTA.
+bool hsweep_energy_fits(const Grid &g);
+int launch_hsweep_energy(const Lay &L, const ELay &E, const HadamardKe &hk, const double *CX, const double *u,
+                         const double *f, const uint8_t *mask, const uint8_t *maskp, double *out, double *partial,
+                         double *ce, double *dc, const double *dsK, int *err, cudaStream_t st);
+// Sums the nb partial pairs in fixed order: out2[0] = sum of the first
+// members, out2[1] = sum of the second.
+void launch_sum_pairs(int nb, const double *partial, double *out2, cudaStream_t st);
 long long hsweep_mask_bytes(const Grid &g);
 void launch_pad_mask(const Grid &g, const uint8_t *mask, uint8_t *maskp, cudaStream_t st);
 // Opt the tile kernels into their dynamic shared memory (call once per device).

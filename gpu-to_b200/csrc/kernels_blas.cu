@@ -314,7 +314,13 @@ pcg_init_kernel(long long n, const double *__restrict__ F, double *__restrict__ 
             z.flexible = flexible;
             z.nit = maxit;
             z.done = (maxit <= 0) ? 1 : 0;
-            if (!(z.res0 > 0.0)) {
+            if (!isfinite(z.res0)) {
+                // a non-finite F: nothing to iterate on (the reference would
+                // run its loop on NaNs to maxit)
+                z.status = GPUTO_ERR_BREAKDOWN;
+                z.done = 1;
+                z.nit = 0;
+            } else if (!(z.res0 > 0.0)) {
                 // F = 0: U = 0 is the solution; the reference would divide 0/0.
                 z.done = 1;
                 z.nit = 0;

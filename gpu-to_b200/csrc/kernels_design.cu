@@ -3,6 +3,7 @@
 #include "gputo_internal.h"
 #include "hadamard.h"
 
+#include <algorithm>
 #include <cmath>
 #include <mutex>
 #include <vector>
@@ -162,38 +163,132 @@ __device__ __forceinline__ int mirror_index(int i, int n)
     return i;
 }
 
-// out = correlate(in ./ div, h) [/ sum h], elements in (y fastest) order.
-// Thread per element; the stencil weights live in constant memory.
+// out = correlate(in ./ div, h) [/ sum h], elements in (y fastest) order
+// (imfilter(..., 'symmetric'), top3D125modCuda.m:109,140-141).
+//
+// Shared-memory tiled: a CTA owns an output tile of 32 (y, one per lane) x 8
+// (z, one per warp) element columns and marches along x through a chunk of
+// planes.  Each input plane of the tile plus its R-wide halo, mirrored at the
+// grid faces, is loaded from global memory once (the quotient in ./ div is
+// taken at load time) into a ring of 2R + 2 plane slots; the loads of the
+// plane FPF steps ahead are in flight while the current output plane is
+// computed from shared memory, with one barrier per plane (the slot being
+// filled is never one being read).  The weights are in constant memory and
+// the same for every lane (broadcast).  The sum runs in the order x offset,
+// z offset, y offset, as a direct 3-D correlation would.
+constexpr int kFTY = 32, kFTZ = 8, kFPF = 2;
+
+template <int R> struct FiltTile {
+    static constexpr int W = 2 * R + 1;
+    static constexpr int TYH = kFTY + 2 * R, TZH = kFTZ + 2 * R;
+    static constexpr int PLANE = TYH * TZH;
+    static constexpr int NPOS = (PLANE + 255) / 256;   // halo-tile positions per thread
+    static constexpr int SLOTS = 2 * R + 2;
+    static constexpr size_t bytes = sizeof(double) * SLOTS * PLANE;
+};
+
 template <int R>
 __global__ void __launch_bounds__(256)
 filter_kernel(Grid g, const double *__restrict__ in, const double *__restrict__ div,
-              double *__restrict__ out, double scale)
+              double *__restrict__ out, double scale, int xc)
 {
-    const long long nel = g.nel();
-    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= nel) return;
-    const long long t = e / g.ny;
-    const int j = (int)(e - t * g.ny);
-    const int i = (int)(t / g.nz);
-    const int k = (int)(t - (long long)i * g.nz);
-    constexpr int W = 2 * R + 1;
-    double acc = 0.0;
+    using FT = FiltTile<R>;
+    constexpr int W = FT::W;
+    extern __shared__ double fs[];   // [SLOTS][PLANE]
+    const int tid = threadIdx.x, ly = tid & 31, lz = tid >> 5;
+    const int j0 = blockIdx.x * kFTY, k0 = blockIdx.y * kFTZ;
+    const int x0 = blockIdx.z * xc, x1 = min(x0 + xc, g.nx);
+    const long long ps = (long long)g.ny * g.nz;   // elements per x plane
+    // this thread's positions in a halo tile: offset inside an x plane (-1: none)
+    long long off[FT::NPOS];
 #pragma unroll
-    for (int a = -R; a <= R; ++a) {
-        const int ii = mirror_index(i + a, g.nx);
-#pragma unroll
-        for (int c = -R; c <= R; ++c) {
-            const int kk = mirror_index(k + c, g.nz);
-#pragma unroll
-            for (int b = -R; b <= R; ++b) {
-                const int jj = mirror_index(j + b, g.ny);
-                const long long s = g.elem(ii, jj, kk);
-                const double v = div ? in[s] / div[s] : in[s];
-                acc = fma(cFilterH[((a + R) * W + (b + R)) * W + (c + R)], v, acc);
-            }
+    for (int q = 0; q < FT::NPOS; ++q) {
+        const int p = tid + 256 * q;
+        off[q] = -1;
+        if (p < FT::PLANE) {
+            const int zz = p / FT::TYH, yy = p - zz * FT::TYH;
+            off[q] = (long long)mirror_index(k0 + zz - R, g.nz) * g.ny + mirror_index(j0 + yy - R, g.ny);
         }
     }
-    out[e] = acc * scale;
+    auto fetch = [&](int px, double (&v)[FT::NPOS]) {
+        const long long base = (long long)mirror_index(px, g.nx) * ps;
+#pragma unroll
+        for (int q = 0; q < FT::NPOS; ++q)
+            if (off[q] >= 0) {
+                const long long s = base + off[q];
+                v[q] = div ? in[s] / div[s] : in[s];
+            }
+    };
+    auto put = [&](int px, const double (&v)[FT::NPOS]) {
+        double *P = fs + ((px - x0 + R) % FT::SLOTS) * FT::PLANE;
+#pragma unroll
+        for (int q = 0; q < FT::NPOS; ++q)
+            if (off[q] >= 0) P[tid + 256 * q] = v[q];
+    };
+    // planes x0 - R .. x0 + R - 1 before the first output plane
+    for (int px = x0 - R; px < x0 + R; ++px) {
+        double v[FT::NPOS];
+        fetch(px, v);
+        put(px, v);
+    }
+    double pre[kFPF][FT::NPOS];
+#pragma unroll
+    for (int d = 0; d < kFPF; ++d)
+        if (x0 + d < x1) fetch(x0 + R + d, pre[d]);
+    const int j = j0 + ly, k = k0 + lz;
+    const bool mine = j < g.ny && k < g.nz;
+    for (int i0 = x0; i0 < x1; i0 += kFPF)
+#pragma unroll
+    for (int pf = 0; pf < kFPF; ++pf) {   // register sets by constant index
+        const int i = i0 + pf;
+        if (i >= x1) break;               // the same for the whole CTA
+        put(i + R, pre[pf]);
+        __syncthreads();
+        if (i + kFPF < x1) fetch(i + R + kFPF, pre[pf]);   // in flight while plane i is computed
+        if (mine) {
+            double acc = 0.0;
+#pragma unroll
+            for (int a = -R; a <= R; ++a) {
+                const double *P = fs + ((i + a - x0 + R) % FT::SLOTS) * FT::PLANE;
+#pragma unroll
+                for (int c = -R; c <= R; ++c) {
+                    const double *row = P + (lz + R + c) * FT::TYH + ly + R;
+#pragma unroll
+                    for (int b = -R; b <= R; ++b)
+                        acc = fma(cFilterH[((a + R) * W + (b + R)) * W + (c + R)], row[b], acc);
+                }
+            }
+            out[(long long)i * ps + (long long)k * g.ny + j] = acc * scale;
+        }
+    }
+}
+
+template <int R>
+int filter_launch(const Grid &g, const double *in, const double *div, double *out, double scale,
+                  cudaStream_t st)
+{
+    using FT = FiltTile<R>;
+    if (FT::bytes > 48 * 1024) {
+        static std::once_flag once[64];
+        int dev = 0;
+        GPUTO_CUDA(cudaGetDevice(&dev));
+        cudaError_t e = cudaSuccess;
+        std::call_once(once[dev < 64 ? dev : 63], [&]() {
+            e = cudaFuncSetAttribute(filter_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)FT::bytes);
+        });
+        GPUTO_CUDA(e);
+    }
+    const unsigned ty = (unsigned)((g.ny + kFTY - 1) / kFTY), tz = (unsigned)((g.nz + kFTZ - 1) / kFTZ);
+    // x chunks: about 1184 CTAs (8 per SM) in all, at least 16 planes each
+    const long long tiles = (long long)ty * tz;
+    const long long want = std::max(1LL, (1184 + tiles - 1) / tiles);
+    int xc = (int)std::max(16LL, ((long long)g.nx + want - 1) / want);
+    if (xc > g.nx) xc = g.nx;
+    const unsigned tx = (unsigned)((g.nx + xc - 1) / xc);
+    filter_kernel<R><<<dim3(ty, tz, tx), 256, FT::bytes, st>>>(g, in, div, out, scale, xc);
+    count_launches(1);
+    return GPUTO_OK;
 }
 
 int launch_filter(const Grid &g, const double *in, const double *div, double *out, double rmin,
@@ -225,19 +320,15 @@ int launch_filter(const Grid &g, const double *in, const double *div, double *ou
         have[slot] = true;
     }
     const double scale = normalize ? 1.0 / hs : 1.0;
-    const int bs = 256;
-    const unsigned nb = (unsigned)((g.nel() + bs - 1) / bs);
     switch (R) {
-    case 0: filter_kernel<0><<<nb, bs, 0, st>>>(g, in, div, out, scale); break;
-    case 1: filter_kernel<1><<<nb, bs, 0, st>>>(g, in, div, out, scale); break;
-    case 2: filter_kernel<2><<<nb, bs, 0, st>>>(g, in, div, out, scale); break;
-    case 3: filter_kernel<3><<<nb, bs, 0, st>>>(g, in, div, out, scale); break;
-    case 4: filter_kernel<4><<<nb, bs, 0, st>>>(g, in, div, out, scale); break;
-    case 5: filter_kernel<5><<<nb, bs, 0, st>>>(g, in, div, out, scale); break;
-    default: filter_kernel<6><<<nb, bs, 0, st>>>(g, in, div, out, scale); break;
+    case 0: return filter_launch<0>(g, in, div, out, scale, st);
+    case 1: return filter_launch<1>(g, in, div, out, scale, st);
+    case 2: return filter_launch<2>(g, in, div, out, scale, st);
+    case 3: return filter_launch<3>(g, in, div, out, scale, st);
+    case 4: return filter_launch<4>(g, in, div, out, scale, st);
+    case 5: return filter_launch<5>(g, in, div, out, scale, st);
+    default: return filter_launch<6>(g, in, div, out, scale, st);
     }
-    count_launches(1);
-    return GPUTO_OK;
 }
 
 }  // namespace gputo

@@ -63,7 +63,7 @@ constexpr int HM = 48;           // mask box width in bytes: HY + 1 = 33 nodes, 
 constexpr int HTX = 32;          // node planes per x chunk
 constexpr int HMAXP = HTX + 1;   // planes one chunk may finish (the last chunk also takes plane nx)
 constexpr int HMAXCY = 8;        // CTAs per cluster (portable limit): ny <= 256
-constexpr uint32_t kHWaitPolls = 1u << 22;
+constexpr uint32_t kHDrainNs = 1000000000u;   // wait for copies in flight before leaving after a failure
 
 __host__ __device__ constexpr size_t al128(size_t x) { return (x + 127) & ~size_t(127); }
 
@@ -71,7 +71,7 @@ __host__ __device__ constexpr size_t al128(size_t x) { return (x + 127) & ~size_
 // 1/diag (Jacobi, pre-relaxation) at the node plane being finished.
 template <int MODE> struct HNeeds {
     static constexpr bool PRE = MODE == MODE_JACOBI_PRE;
-    static constexpr bool F = MODE != MODE_APPLY;
+    static constexpr bool F = MODE != MODE_APPLY;   // MODE_ENERGY: the residual f - K u
     static constexpr bool D = MODE == MODE_JACOBI || MODE == MODE_JACOBI_PRE || MODE == MODE_JACOBI_DOT;
     static constexpr bool DOT = MODE == MODE_JACOBI_DOT;   // also the FP64 residual and z_old tiles
 };
@@ -180,6 +180,10 @@ __device__ __forceinline__ void h_store(long long base, unsigned m, const T (&ku
             dsum += (double)u[d] * (double)q;
         } else if (MODE == MODE_DEFECT) {
             out[base + d] = fixed ? T(0) : fv[d] - ku[d];
+        } else if (MODE == MODE_ENERGY) {
+            const T r = fixed ? T(0) : fv[d] - ku[d];
+            if (out) out[base + d] = r;
+            dsum = fma((double)r, (double)r, dsum);
         } else {
             const T r = fixed ? T(0) : fv[d] - ku[d];
             const T z = u[d] + omega * r * rv[d];
@@ -204,6 +208,8 @@ __device__ __forceinline__ void h_store(long long base, unsigned m, const T (&ku
 template <typename T, int MODE> struct HMinBlocks {
     static constexpr int value = (sizeof(T) == 4 || MODE == MODE_APPLY || MODE == MODE_DEFECT) ? 2 : 1;
 };
+// MODE_ENERGY (once per solve) keeps the element's modes for its energy as
+// well: one CTA per SM, no register cap.
 
 template <typename T, int MODE, int WZ>
 __global__ void __launch_bounds__(32 * WZ, HMinBlocks<T, MODE>::value)
@@ -213,7 +219,8 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
               const __grid_constant__ CUtensorMap tm_z, Lay L, HC<T> hc, int htx, const T *__restrict__ f,
               const T *__restrict__ rdiag, const uint8_t *__restrict__ mask, T *__restrict__ out, T omega,
               T prerelax, double *__restrict__ dot_partial, const int *__restrict__ done, int *__restrict__ err,
-              const double *__restrict__ Rd, const T *__restrict__ zo)
+              const double *__restrict__ Rd, const T *__restrict__ zo, uint32_t wait_ns, int skip_stage,
+              double *__restrict__ ce, double *__restrict__ dcv, const double *__restrict__ dsK)
 {
     if (done && *done) return;   // the same value for every CTA of the cluster
     using N = HNeeds<MODE>;
@@ -262,6 +269,10 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
         if (epi) bytes += (uint32_t)(S::u_bytes * ((N::F ? 1 : 0) + (N::D ? 1 : 0) + (N::DOT ? 1 : 0)) + S::m_bytes +
                                      (N::DOT ? S::r_bytes : 0));
         mbar_arrive_expect_tx(b, bytes);
+        if (s == skip_stage) {   // test hook: the stage stays armed with no copy in flight
+            issued = s + 1;
+            return;
+        }
         if (face) {
             tma_load_3d(sb, &tm_u, 3 * jc0, kc0, E0 + s, b);
             if (N::PRE) tma_load_3d(sb + S::d_off, &tm_d, 3 * jc0, kc0, E0 + s, b);
@@ -284,7 +295,7 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
 
     bool bad = false;
     auto wait_stage = [&](int s) {
-        if (!bad && !mbar_wait_bounded(&bar[s % HRING], (uint32_t)((s / HRING) & 1), kHWaitPolls)) bad = true;
+        if (!bad && !mbar_wait_for(&bar[s % HRING], (uint32_t)((s / HRING) & 1), wait_ns)) bad = true;
     };
     auto load_face = [&](int s, T (&U)[HF]) {
         const unsigned char *sb = smem + (s % HRING) * S::slot;
@@ -373,6 +384,18 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
         face_h(Fn);
         const T cx = reinterpret_cast<const T *>(smem + (t % HRING) * S::slot + S::c_off)[w * HY + l];
         element_h(Fc, Fn, cx, hc, Ac, An);
+        if constexpr (MODE == MODE_ENERGY) {
+            // element (E0 + t - 1, jc0 + l, kc0 + w): written by the one CTA that
+            // owns it (x chunks overlap by one element, z tiles by one row)
+            const int ei = E0 + t - 1, ej = jc0 + l, ek = kc0 + w;
+            if (ei >= P0 && (w < WZ - 1 || zt == (int)gridDim.y - 1) && ek < g.nz && ej < g.ny) {
+                const double en = element_energy_h(Fc, Fn, hc);
+                const long long e = g.elem(ei, ej, ek);
+                ce[e] = en;
+                if (dcv) dcv[e] = dsK[e] * en;
+                dsum2 = fma((double)cx, en, dsum2);
+            }
+        }
         const int p = E0 + t - 1;   // node plane finished by this element
         const bool out_plane = p >= P0;
         T q0[3];
@@ -431,9 +454,10 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
     }
     if (fail && tid == 0) {
         // let the loads still in flight (stages cur .. issued - 1, each the
-        // latest phase of its slot) land before the CTA ends (bounded)
+        // latest phase of its slot) land before the CTA ends (bounded); a
+        // stage the test hook left unissued has nothing in flight
         for (int s = cur; s < issued; ++s)
-            (void)mbar_wait_bounded(&bar[s % HRING], (uint32_t)((s / HRING) & 1), kHWaitPolls);
+            if (s != skip_stage) (void)mbar_wait_for(&bar[s % HRING], (uint32_t)((s / HRING) & 1), kHDrainNs);
         if (err) atomicExch(err, GPUTO_ERR_TIMEOUT);
     }
     cluster.sync();   // seam partials from the left neighbour have arrived
@@ -454,11 +478,12 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
                              Rd + base, zo + base, dsum2);
         }
     }
-    if ((MODE == MODE_APPLY || MODE == MODE_JACOBI_DOT) && dot_partial) {
+    if ((MODE == MODE_APPLY || MODE == MODE_JACOBI_DOT || MODE == MODE_ENERGY) && dot_partial) {
+        constexpr bool PAIR = MODE == MODE_JACOBI_DOT || MODE == MODE_ENERGY;
         double *red = reinterpret_cast<double *>(smem + S::red_off);
         for (int o = 16; o > 0; o >>= 1) {
             dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
-            if (MODE == MODE_JACOBI_DOT) dsum2 += __shfl_xor_sync(0xffffffffu, dsum2, o);
+            if (PAIR) dsum2 += __shfl_xor_sync(0xffffffffu, dsum2, o);
         }
         if (l == 0) {
             red[w] = dsum;
@@ -495,9 +520,25 @@ int hztiles(const Grid &g)
     return 1 + (rest > 0 ? (rest + WZ - 2) / (WZ - 1) : 0);
 }
 
+// Test hook for the bounded waits (gputo_debug_set_sweep_fault): the ring
+// stage whose copies a launch leaves unissued (-1: none) and how long each
+// wait of the march lasts before the CTA gives up (2 s by default).
+struct SweepFaultHook {
+    int skip_stage = -1;
+    uint32_t wait_ns = 2000000000u;
+};
+std::mutex g_hook_mu;
+SweepFaultHook g_hook;
+
+SweepFaultHook sweep_fault_hook()
+{
+    std::lock_guard<std::mutex> lock(g_hook_mu);
+    return g_hook;
+}
+
 struct HState {
     bool init = false, ok = false;
-    int resident[2][5][HMAXCY + 1] = {};   // [FP64?][mode][cluster size]: clusters resident on the device
+    int resident[2][6][HMAXCY + 1] = {};   // [FP64?][mode][cluster size]: clusters resident on the device
 };
 
 HState &hstate(int dev)
@@ -544,7 +585,8 @@ dim3 hgrid(const Grid &g, int htx)
 template <typename T, int MODE>
 int hlaunch(const Lay &L, const ELay &E, const HadamardKe &hk, const T *CX, const T *u, const T *f, const T *rdiag,
             const uint8_t *mask, const uint8_t *maskp, T *out, T omega, T prerelax, double *dot_partial,
-            const int *done, int *err, cudaStream_t st, const double *Rd = nullptr, const T *zo = nullptr)
+            const int *done, int *err, cudaStream_t st, const double *Rd = nullptr, const T *zo = nullptr,
+            double *ce = nullptr, double *dcv = nullptr, const double *dsK = nullptr)
 {
     constexpr int WZ = hwz<T>();
     using N = HNeeds<MODE>;
@@ -590,8 +632,10 @@ int hlaunch(const Lay &L, const ELay &E, const HadamardKe &hk, const T *CX, cons
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    const SweepFaultHook hook = sweep_fault_hook();
     GPUTO_CUDA(cudaLaunchKernelEx(&cfg, hsweep_kernel<T, MODE, WZ>, mu, md, mf, mc, mm, mr, mz, L, hc, htx, f, rdiag, mask,
-                                  out, omega, prerelax, dot_partial, done, err, Rd, zo));
+                                  out, omega, prerelax, dot_partial, done, err, Rd, zo, hook.wait_ns, hook.skip_stage,
+                                  ce, dcv, dsK));
     count_launches(1);
     return GPUTO_OK;
 }
@@ -612,6 +656,8 @@ cudaError_t hset_attrs()
     if ((e = hset_attr<T, MODE_JACOBI>()) != cudaSuccess) return e;
     if constexpr (sizeof(T) == 4)
         if ((e = hset_attr<T, MODE_JACOBI_DOT>()) != cudaSuccess) return e;
+    if constexpr (sizeof(T) == 8)
+        if ((e = hset_attr<T, MODE_ENERGY>()) != cudaSuccess) return e;
     return hset_attr<T, MODE_JACOBI_PRE>();
 }
 
@@ -646,6 +692,7 @@ void hresident_all(HState &s, int cy)
     s.resident[p][MODE_JACOBI][cy] = hresident<T, MODE_JACOBI>(cy);
     s.resident[p][MODE_JACOBI_PRE][cy] = hresident<T, MODE_JACOBI_PRE>(cy);
     if constexpr (sizeof(T) == 4) s.resident[p][MODE_JACOBI_DOT][cy] = hresident<T, MODE_JACOBI_DOT>(cy);
+    if constexpr (sizeof(T) == 8) s.resident[p][MODE_ENERGY][cy] = hresident<T, MODE_ENERGY>(cy);
 }
 
 __global__ void pad_mask_kernel(Grid g, const uint8_t *__restrict__ mask, uint8_t *__restrict__ maskp, long long mp)
@@ -718,6 +765,18 @@ bool hadamard_ke(const double *Ke, HadamardKe *hk)
     return true;
 }
 
+int set_sweep_fault_hook(int skip_stage, unsigned wait_us)
+{
+    if (skip_stage < -1 || wait_us > 4000000u) {
+        set_error("skip_stage must be >= -1 and wait_us at most 4,000,000");
+        return GPUTO_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lock(g_hook_mu);
+    g_hook.skip_stage = skip_stage;
+    g_hook.wait_ns = wait_us ? wait_us * 1000u : SweepFaultHook{}.wait_ns;
+    return GPUTO_OK;
+}
+
 int init_hsweep_kernels()
 {
     static std::mutex mu;
@@ -766,6 +825,60 @@ long long hsweep_mask_bytes(const Grid &g) { return hmask_pitch(g) * (g.nz + 1) 
 void launch_pad_mask(const Grid &g, const uint8_t *mask, uint8_t *maskp, cudaStream_t st)
 {
     pad_mask_kernel<<<(unsigned)((g.nnod() + 255) / 256), 256, 0, st>>>(g, mask, maskp, hmask_pitch(g));
+    count_launches(1);
+}
+
+bool hsweep_energy_fits(const Grid &g)
+{
+    int dev = 0;
+    if (!hsweep_fits<double>(g) || cudaGetDevice(&dev) != cudaSuccess) return false;
+    return hstate(dev).resident[1][MODE_ENERGY][(g.ny + HY - 1) / HY] > 0;
+}
+
+int launch_hsweep_energy(const Lay &L, const ELay &E, const HadamardKe &hk, const double *CX, const double *u,
+                         const double *f, const uint8_t *mask, const uint8_t *maskp, double *out, double *partial,
+                         double *ce, double *dc, const double *dsK, int *err, cudaStream_t st)
+{
+    if (!ce || !partial || (dc && !dsK)) {
+        set_error("the energy sweep needs ce, the partials, and dsK with dc");
+        return GPUTO_ERR_ARG;
+    }
+    return hlaunch<double, MODE_ENERGY>(L, E, hk, CX, u, f, nullptr, mask, maskp, out, 1.0, 0.0, partial, nullptr,
+                                        err, st, nullptr, nullptr, ce, dc, dsK);
+}
+
+__global__ void __launch_bounds__(256) sum_pairs_kernel(int nb, const double *__restrict__ partial,
+                                                        double *__restrict__ out2)
+{
+    __shared__ double red[2][8];
+    double a = 0.0, b = 0.0;
+    for (int i = threadIdx.x; i < nb; i += 256) {
+        a += partial[2 * i];
+        b += partial[2 * i + 1];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = a;
+        red[1][threadIdx.x >> 5] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double x = 0.0, y = 0.0;
+        for (int q = 0; q < 8; ++q) {
+            x += red[0][q];
+            y += red[1][q];
+        }
+        out2[0] = x;
+        out2[1] = y;
+    }
+}
+
+void launch_sum_pairs(int nb, const double *partial, double *out2, cudaStream_t st)
+{
+    sum_pairs_kernel<<<1, 256, 0, st>>>(nb, partial, out2);
     count_launches(1);
 }
 

@@ -57,10 +57,11 @@ extern "C" void mexFunction(int nlhs, mxArray *plhs[], int nrhs, const mxArray *
             mexPrintf("\nMGCG - Cuda device has not enough free memory: %s\n", gputo_last_error());
         else if (shapes_ok)
             mexPrintf("mgcg9: %s: %s\n", gputo_status_string(st), gputo_last_error());
-        if (st != GPUTO_ERR_BREAKDOWN) {
-            relres = 0.0;
-            nit = -1;
-        }
+        // every failure gives cgiters = -1, which the drivers test to stop
+        // their loop (top3D125modCuda.m:135); after a CG breakdown relres
+        // keeps the last residual and U the last iterate
+        if (st != GPUTO_ERR_BREAKDOWN) relres = 0.0;
+        nit = -1;
     }
     plhs[0] = mxCreateDoubleScalar(relres);
     plhs[1] = mxCreateDoubleScalar((double)nit);

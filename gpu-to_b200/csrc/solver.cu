@@ -178,10 +178,12 @@ int Solver::create(int nelx, int nely, int nelz, int nl_, const gputo_options *o
     ALLOC(ctmp, nc);
     if (nl == 1) ALLOC(Apk0, 300 * g[0].nel());
     partial_cap = std::max({fine_sweep_blocks(g[0]), hsweep_blocks<double>(g[0]),
-                            2 * hsweep_blocks<float>(g[0], MODE_JACOBI_DOT), 1 << 12});
+                            2 * hsweep_blocks<float>(g[0], MODE_JACOBI_DOT),
+                            2 * hsweep_blocks<double>(g[0], MODE_ENERGY), 1 << 12});
     ALLOC(partial, partial_cap);
     ALLOC(ticket, 4);
     ALLOC(sc, 1);
+    ALLOC(e2, 2);
     ALLOC(info, 4);
     ALLOC(err, 4);
     ALLOC(fixed_dev, 1);
@@ -270,6 +272,7 @@ int Solver::setup(const double *CX_in, cudaStream_t st)
         return GPUTO_ERR_ARG;
     }
     ready = false;
+    have_solution = false;
     const long long ne = g[0].nel();
     if (CX_in != CX)
         GPUTO_CUDA(cudaMemcpyAsync(CX, CX_in, sizeof(double) * ne, cudaMemcpyDeviceToDevice, st));
@@ -614,7 +617,10 @@ int Solver::solve_end(double *Up, double *relres, int *nit, cudaStream_t st)
         ++net_solves;
     }
     if (h_sc->status) {
-        set_error("PCG breakdown: p'q <= 0 or a non-finite scalar at iteration " + std::to_string(h_sc->nit));
+        if (!std::isfinite(h_sc->res0))
+            set_error("PCG breakdown: the right-hand side F has a non-finite entry");
+        else
+            set_error("PCG breakdown: p'q <= 0 or a non-finite scalar at iteration " + std::to_string(h_sc->nit));
         return h_sc->status;
     }
     return GPUTO_OK;
@@ -644,6 +650,38 @@ int Solver::solve(const double *Fp, double *Up, double tol, int maxit, double *r
         it += batch;
     }
     return solve_end(Up, relres, nit, st);
+}
+
+// The last solve's U: element energies ce (dc = dsK ce), the compliance
+// sum CX_e ce_e and |F - K U|^2 over the free dofs, from one FP64 operator
+// apply with the energies in its epilogue (Hadamard-basis kernel).  out2
+// (device, 2 doubles) receives (|F - K U|^2, compliance).  Without the
+// Hadamard-basis kernel: the separate energy pass, and out2[0] = -1.
+int Solver::energy(const double *dsK, double *ce, double *dc, double *out2, cudaStream_t st)
+{
+    if (!ready) {
+        set_error("solver setup has not succeeded");
+        return GPUTO_ERR_ARG;
+    }
+    if (!ce || (dc && !dsK) || !out2) {
+        set_error("energy needs ce, out2, and dsK with dc");
+        return GPUTO_ERR_ARG;
+    }
+    launch_status = GPUTO_OK;
+    if (use_hsweep<double>(g[0]) && hsweep_energy_fits(g[0])) {
+        const int nb = hsweep_blocks<double>(g[0], MODE_ENERGY);
+        note(launch_hsweep_energy(lay[0], elay, hk, CXp, Uw, Fw, mask[0], maskp[0], nullptr, partial, ce, dc, dsK,
+                                  err, st));
+        if (launch_status) return launch_status;
+        launch_sum_pairs(nb, partial, out2, st);
+    } else {
+        launch_unpack(lay[0], Uw, Dn, 0, st);
+        launch_element_energy(g[0], Dn, CX, dsK, ce, dc, partial, ticket, out2 + 1, st);
+        const double minus1 = -1.0;
+        GPUTO_CUDA(cudaMemcpyAsync(out2, &minus1, sizeof(double), cudaMemcpyHostToDevice, st));
+    }
+    GPUTO_CUDA(cudaGetLastError());
+    return GPUTO_OK;
 }
 
 // Options that change neither the hierarchy nor its buffers.

@@ -47,6 +47,8 @@ struct Solver {
     int partial_cap = 0;
     unsigned *ticket = nullptr;
     double last_res0 = 0.0;
+    bool have_solution = false;   // Uw and Fw hold the last solve's U and F
+    double *e2 = nullptr;         // (|F - K U|^2, compliance) of energy()
     int launch_status = GPUTO_OK;   // first failure seen while enqueuing kernels
 
     cudaGraphExec_t graph_exec = nullptr;
@@ -85,6 +87,8 @@ struct Solver {
     int solve_poll(cudaStream_t st, bool *finished);
     int solve_end(double *Up, double *relres, int *nit, cudaStream_t st);
     void iteration(cudaStream_t st);
+    // Element energies of the last solve's U, fused into an FP64 apply (see solver.cu).
+    int energy(const double *dsK, double *ce, double *dc, double *out2, cudaStream_t st);
     int set_tunables(const gputo_options &o);
     // Padded-layout preconditioner and operator.
     void vcycle(const double *r, double *z, const int *done, cudaStream_t st);

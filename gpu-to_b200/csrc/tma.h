@@ -76,6 +76,27 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
     return false;
 }
 
+__device__ __forceinline__ uint64_t globaltimer_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait on an mbarrier phase by elapsed time: gives up after about
+// 'limit_ns' nanoseconds of the device's global timer (and after 2^26 polls
+// in any case).  Returns true when the phase completed.
+__device__ __forceinline__ bool mbar_wait_for(uint64_t *bar, uint32_t parity, uint32_t limit_ns)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = globaltimer_ns();
+    for (uint32_t it = 0; it < (1u << 26); ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (globaltimer_ns() - t0 > (uint64_t)limit_ns) return false;
+    }
+    return false;
+}
+
 __device__ __forceinline__ void prefetch_tmap(const CUtensorMap *tm)
 {
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(tm)) : "memory");

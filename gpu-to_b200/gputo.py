@@ -101,6 +101,8 @@ SIGNATURES = {
     "gputo_solver_apply_dev": (_i, [_vp, _vp, _vp, _vp]),
     "gputo_solver_launch_count": (ctypes.c_longlong, [_vp]),
     "gputo_solver_time_kernel": (_i, [_vp, _i, _i, _dp, _vp]),
+    "gputo_debug_set_sweep_fault": (_i, [_i, ctypes.c_uint]),
+    "gputo_solver_energy_dev": (_i, [_vp, _vp, _vp, _vp, _dp, _dp, _vp]),
     "gputo_compliance_sens_dev": (_i, [_dp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _dp, _vp]),
     "gputo_compliance_sens": (_i, [_dp, _dp, _dp, _dp, _i, _i, _i, _dp, _dp, _dp]),
     "gputo_compliance_sens_tc_dev": (_i, [_dp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _dp, _vp]),
@@ -248,7 +250,9 @@ def mgcg1(Ke0, F1, U, CX, fixed, nfd, nelx, nely, nelz, nl, cgtol, cgmax, printL
                                  ctypes.byref(options), ctypes.byref(rr), ctypes.byref(nit))
     if st == GPUTO_ERR_OOM:
         return 0.0, -1
-    if st not in (GPUTO_OK, GPUTO_ERR_BREAKDOWN):
+    if st == GPUTO_ERR_BREAKDOWN:   # as the MEX: U holds the last iterate, cgiters = -1
+        return rr.value, -1
+    if st != GPUTO_OK:
         raise GputoError(st, "mgcg1")
     return rr.value, nit.value
 
@@ -273,7 +277,9 @@ def mgcg9(Ae, F, U, CX, FDofs, nFD, nelx, nely, nelz, nl, tol, maxit, nswp, prin
                           float(hy), float(hz), ctypes.byref(rr), ctypes.byref(nit))
     if st == GPUTO_ERR_OOM:
         return 0.0, -1
-    if st not in (GPUTO_OK, GPUTO_ERR_BREAKDOWN):
+    if st == GPUTO_ERR_BREAKDOWN:
+        return rr.value, -1
+    if st != GPUTO_OK:
         raise GputoError(st, "mgcg9")
     return rr.value, nit.value
 
@@ -330,6 +336,16 @@ class Solver:
                                          ctypes.byref(rr), ctypes.byref(nit), _ptr_stream(stream))
         _check(st, "gputo_solver_solve_dev")
         return rr.value, nit.value
+
+    def energy(self, dsK=None, ce=None, dc=None, stream=None):
+        """ce, dc = dsK ce, compliance and the true relative residual of the
+        last solve's U, from one fused FP64 apply (gputo_solver_energy_dev).
+        Returns (compliance, true_relres); true_relres is -1 when the dense
+        fallback ran."""
+        c, tr = ctypes.c_double(0.0), ctypes.c_double(0.0)
+        _check(_lib.gputo_solver_energy_dev(self._h, _ptr(dsK), _ptr(ce), _ptr(dc), ctypes.byref(c),
+                                            ctypes.byref(tr), _ptr_stream(stream)), "gputo_solver_energy_dev")
+        return c.value, tr.value
 
     def vcycle(self, r, z, stream=None):
         _check(_lib.gputo_solver_vcycle_dev(self._h, _ptr(r), _ptr(z), _ptr_stream(stream)),
@@ -569,6 +585,13 @@ def _ptr_stream(stream):
     return stream.cuda_stream  # torch.cuda.Stream
 
 
+def debug_set_sweep_fault(skip_stage=-1, wait_us=0):
+    """Test hook: Hadamard-basis sweeps launched afterwards leave ring stage
+    skip_stage unissued and give up each wait after wait_us microseconds
+    (gputo_debug_set_sweep_fault); (-1, 0) restores normal operation."""
+    _check(_lib.gputo_debug_set_sweep_fault(int(skip_stage), int(wait_us)), "gputo_debug_set_sweep_fault")
+
+
 def launch_count() -> int:
     return int(_lib.gputo_solver_launch_count(None))
 
@@ -707,7 +730,9 @@ class DesignLoop:
         xPhys = imfilter(x, h, 'symmetric') ./ Hs          density filter
         CX, dsK = SIMP(xPhys)                               stiffness
         [cgres, cgiters] = mgcg1(...)                       MGCG solve
-        dc = dsK .* ce;  c = sum(CX .* ce)                  sensitivity, compliance
+        dc = dsK .* ce;  c = sum(CX .* ce)                  sensitivity, compliance (one
+                                                            FP64 apply of U, which also
+                                                            gives the true residual)
         dc = imfilter(dc ./ Hs); dV0 = imfilter(dV ./ Hs)   filtered sensitivities
         x = OC(x, dc, dV0)                                  bisection update
 
@@ -786,8 +811,9 @@ class DesignLoop:
         simp_dev(self.xPhys, self.CX, self.dsK, self.penal, self.E0, self.Emin, stream=s)
         self.solver.setup(self.CX, stream=s)
         relres, nit = self.solver.solve(self.F, self.U, self.tol, self.maxit, stream=s)
-        c = compliance_sens_dev(self.Ke0, self.U, self.CX, self.dsK, nelx, nely, nelz,
-                                ce=self.ce, dc=self.dc, stream=s)
+        # ce, dc and the compliance from the FP64 apply of U that also gives
+        # the true residual of the solve (gputo_solver_energy_dev)
+        c, true_relres = self.solver.energy(self.dsK, self.ce, self.dc, stream=s)
         if self.ft == 3:
             # dc ./ dHs with dHs = Hs ./ dprj: filter(dc .* dprj) / Hs (top3D125modCuda.m:117,140-141)
             mul_dev(self.dc, self.dprj, self.dc, stream=s)
@@ -800,4 +826,4 @@ class DesignLoop:
         lmid = oc_update_dev(self.x, self.dcf, self.dV0, self.xnew, self.volfrac, self.move,
                              stream=s)
         self.x, self.xnew = self.xnew, self.x
-        return {"c": c, "nit": nit, "relres": relres, "lmid": lmid}
+        return {"c": c, "nit": nit, "relres": relres, "true_relres": true_relres, "lmid": lmid}

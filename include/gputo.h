@@ -199,6 +199,23 @@ int gputo_solver_setup_dev(gputo_solver *s, const double *CX, void *stream);
 int gputo_solver_solve_dev(gputo_solver *s, const double *F, double *U, double tol, int maxit,
                            double *relres, int *nit, void *stream);
 
+/* Element energies of the solution of the last gputo_solver_solve_dev call on
+ * this solver, from one FP64 operator apply of that U with the energies in
+ * its epilogue (the element loop of the driver's sensitivity line,
+ * top3D125modCuda.m:139, fused into the operator apply):
+ *   ce_e = u_e' Ke u_e,  dc = dsK .* ce  (dsK and dc may be NULL),
+ *   *compliance = sum_e CX_e ce_e,
+ *   *true_relres = |F - K U| / |F| over the free dofs (the solve itself stops
+ *   on the recursively updated residual, mgcg1.cu:254-275).
+ * ce, dc, dsK: device arrays of nel in element order; compliance and
+ * true_relres: host pointers, either may be NULL.  When the grid runs on the
+ * dense-row kernel (nely > 256 or a Ke without the cube element's pattern),
+ * ce comes from a separate pass and *true_relres is -1.  GPUTO_ERR_ARG
+ * without a successful solve since the last setup (a V-cycle call in between
+ * also discards the solve). */
+int gputo_solver_energy_dev(gputo_solver *s, const double *dsK, double *ce, double *dc,
+                            double *compliance, double *true_relres, void *stream);
+
 /* One V-cycle z = M r on device vectors (the preconditioner alone). */
 int gputo_solver_vcycle_dev(gputo_solver *s, const double *r, double *z, void *stream);
 
@@ -217,6 +234,17 @@ long long gputo_solver_launch_count(const gputo_solver *s);
  * solver's own work vectors; results are discarded.  Needs setup first. */
 int gputo_solver_time_kernel(gputo_solver *s, int which, int reps, double *ms_per_launch,
                              void *stream);
+
+/* Test hook of the failure handling; no counterpart in the reference, whose
+ * kernels have no bounded waits.  The Hadamard-basis fine sweeps launched
+ * after this call leave the tile copies of ring stage 'skip_stage' unissued
+ * (its mbarrier armed, nothing in flight), and every wait of their march
+ * gives up after 'wait_us' microseconds; the sweep then ends early and the
+ * call reports GPUTO_ERR_TIMEOUT, with the context still usable.
+ * gputo_debug_set_sweep_fault(-1, 0) restores normal operation (waits give up
+ * after 2 s).  Affects launches, not CUDA graphs captured earlier.  Not for
+ * production use. */
+int gputo_debug_set_sweep_fault(int skip_stage, unsigned wait_us);
 
 /* ---------------------------------------------------------------------- */
 /* Batched solves and the option autotuner (no reference counterpart)       */

@@ -112,3 +112,40 @@ def test_mixed_solve_matches_dense(oracle, gputo, torch):
         s.close()
     assert abs(res[0][1] - res[1][1]) <= 1 and res[0][2] < 1e-8
     assert np.linalg.norm(res[0][0] - res[1][0]) <= 1e-6 * np.linalg.norm(res[1][0])
+
+
+@pytest.mark.parametrize("shape,nl", SHAPES + [((70, 34, 18), 2)])
+def test_energy_fused_into_the_apply_matches_the_separate_pass(oracle, gputo, torch, shape, nl):
+    """gputo_solver_energy_dev: ce, dc and the compliance from one FP64 apply
+    of the solution (each element written by exactly one CTA, although x
+    chunks overlap by one element and z tiles by one row), against the
+    separate energy pass (gputo_compliance_sens_dev) to 1e-12, and its true
+    residual against |F - K U| from the plain apply.  nely = 264 runs the
+    dense fallback (true_relres -1)."""
+    p = oracle.cantilever(*shape)
+    rng = np.random.default_rng(11)
+    x = rng.uniform(0.05, 1.0, p.nel)
+    CX, dsK = oracle.simp(x)
+    s = _solver(gputo, p, CX, torch, nl=nl)
+    F = _dev(torch, p.F)
+    U = torch.zeros_like(F)
+    rr, nit = s.solve(F, U, 1e-8, 2000)
+    assert rr < 1e-8
+    dsKd = _dev(torch, dsK)
+    ce = torch.full((p.nel,), float("nan"), dtype=torch.float64, device="cuda")
+    dc = torch.full_like(ce, float("nan"))
+    c, tr = s.energy(dsKd, ce, dc)
+    ce_ref, dc_ref = torch.empty_like(ce), torch.empty_like(ce)
+    c_ref = gputo.compliance_sens_dev(p.Ke0, U, _dev(torch, CX), dsKd, *shape, ce=ce_ref, dc=dc_ref)
+    assert not torch.isnan(ce).any() and not torch.isnan(dc).any()
+    assert float((ce - ce_ref).abs().max()) <= 1e-12 * float(ce_ref.abs().max())
+    assert float((dc - dc_ref).abs().max()) <= 1e-12 * float(dc_ref.abs().max())
+    assert abs(c - c_ref) <= 1e-12 * abs(c_ref)
+    if p.nely > 256:
+        assert tr == -1.0
+        return
+    KU = torch.zeros_like(F)
+    s.apply(U, KU)
+    tr_ref = float(torch.linalg.norm(F - KU) / torch.linalg.norm(F))
+    assert abs(tr - tr_ref) <= 1e-6 * tr_ref, (tr, tr_ref)
+    assert tr < 1e-7

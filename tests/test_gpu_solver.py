@@ -4,8 +4,9 @@ solves, through the C ABI.  Needs a B200.
 Tolerances: FP64 operator / preconditioner applies agree with the oracle to
 1e-12 relative (only summation order differs); FP64 solves at the same
 tolerance agree to 1e-9 relative in U with the same iteration count;
-mixed-precision solves agree with the FP64 oracle to 1e-6 in compliance and
-relative displacement L2 at the tolerance the north-star metric uses.
+mixed-precision solves agree with an FP64 solve to 1e-10 within 1e-6 in
+compliance and relative displacement L2, at tol 1e-8 on a small grid and at
+tol 1e-6 (the benchmark's tolerance) on the 256x128x128 benchmark workload.
 """
 import numpy as np
 import pytest
@@ -150,8 +151,9 @@ def test_graph_and_eager_agree(oracle, gputo):
 
 
 def test_mixed_precision_matches_fp64_oracle(oracle, gputo):
-    """FP32 V-cycle + flexible FP64 outer PCG, tol 1e-6: compliance and
-    displacement within 1e-6 of the FP64 oracle solved to 1e-10."""
+    """FP32 V-cycle + flexible FP64 outer PCG, tol 1e-8 on a 32x16x16 random
+    design: compliance and displacement within 1e-6 of the FP64 oracle solved
+    to 1e-10."""
     p = oracle.cantilever(32, 16, 16)
     CX = oracle.simp(oracle.random_density(32, 16, 16, seed=9))[0]
     Uo, _, _ = oracle.mgcg1(p, CX, 4, 1e-10, 400)
@@ -332,3 +334,52 @@ def test_host_simp_matches_oracle(oracle, gputo):
     CX, dsK = gputo.simp(x, 3.0, 1.0, 1e-9)
     CXr, dsr = oracle.simp(x)
     assert np.abs(CX - CXr).max() <= 1e-15 and np.abs(dsK - dsr).max() <= 1e-14
+
+
+def _bench_design_cx(gputo, torch, nelx, nely, nelz):
+    """The benchmark's design (the 64x32x32 golden design after 50 OC
+    iterations, upsampled), filtered and through SIMP, on the device."""
+    d = load_golden("design_c1")
+    x = d["x"].astype(np.float64).reshape(64, 32, 32)   # (x, z, y) element order
+    f = nelx // 64
+    xb = np.repeat(np.repeat(np.repeat(x, f, 0), f, 1), f, 2).reshape(-1)
+    xd = _dev(torch, xb)
+    xp = torch.empty_like(xd)
+    gputo.density_filter_dev(xd, xp, nelx, nely, nelz, 3 ** 0.5)
+    CX = torch.empty_like(xd)
+    gputo.simp_dev(xp, CX)
+    return CX
+
+
+def test_mixed_precision_at_the_benchmark_configuration(gputo, torch):
+    """The headline workload: 256x128x128 cantilever (12.8M dofs), 6 levels,
+    the benchmark's mid-optimisation design.  The mixed-precision solve at
+    the benchmark tolerance 1e-6 against an FP64 solve to 1e-10: compliance
+    and relative displacement L2 within 1e-6, and the true residual of the
+    mixed U (an independent FP64 apply) within 2e-6 (the solve stops on the
+    recursively updated residual, mgcg1.cu:254-275)."""
+    nelx, nely, nelz, nl = 256, 128, 128, 6
+    CX = _bench_design_cx(gputo, torch, nelx, nely, nelz)
+    F, fixed = gputo.cantilever(nelx, nely, nelz)
+    Fd = _dev(torch, F)
+    s64 = gputo.Solver(nelx, nely, nelz, nl, gputo.default_options())
+    s64.set_problem(gputo.hex8_stiffness(), fixed)
+    s64.setup(CX)
+    U64 = torch.zeros_like(Fd)
+    rr64, nit64 = s64.solve(Fd, U64, 1e-10, 1000)
+    assert rr64 < 1e-10
+    sm = gputo.Solver(nelx, nely, nelz, nl, gputo.default_options(precision=gputo.PREC_MIXED))
+    sm.set_problem(gputo.hex8_stiffness(), fixed)
+    sm.setup(CX)
+    Um = torch.zeros_like(Fd)
+    rrm, nitm = sm.solve(Fd, Um, 1e-6, 500)
+    assert rrm < 1e-6 and 0 < nitm < 500
+    del sm
+    KU = torch.zeros_like(Fd)
+    s64.apply(Um, KU)
+    true_rr = float(torch.linalg.norm(Fd - KU) / torch.linalg.norm(Fd))
+    c64, cm = float(Fd @ U64), float(Fd @ Um)
+    u_err = float(torch.linalg.norm(Um - U64) / torch.linalg.norm(U64))
+    assert abs(cm - c64) <= 1e-6 * abs(c64), (cm, c64)
+    assert u_err <= 1e-6, u_err
+    assert true_rr <= 2e-6, true_rr
