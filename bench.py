@@ -205,6 +205,23 @@ class _Null:
         return False
 
 
+def time_filter(gputo, torch, inputs, reps, stream):
+    """Mean time of one density-filter launch (imfilter, normalised), CUDA
+    events on the launching stream.  The launches cycle through four inputs
+    and four outputs (268 MB, more than L2), so each one reads from HBM."""
+    outs = [torch.empty_like(inputs[0]) for _ in inputs]
+    for x, o in zip(inputs, outs):
+        gputo.density_filter_dev(x, o, NELX, NELY, NELZ, RMIN, stream=stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for r in range(reps):
+        q = r % len(inputs)
+        gputo.density_filter_dev(inputs[q], outs[q], NELX, NELY, NELZ, RMIN, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
 def mixed_parity(gputo, torch, dl, fixed, Ke0, stream):
     """Accuracy of the timed mixed-precision solve (the last step's U, at the
     benchmark tolerance): against an FP64 MGCG solve of the same design to
@@ -293,6 +310,8 @@ def run_ours(args):
         ms_apply64 = dl_m.solver.time_kernel(0, 20, stream)
         ms_jac32 = dl_m.solver.time_kernel(1, 20, stream)
         ms_lvl1_32 = dl_m.solver.time_kernel(2, 20, stream)
+        ms_energy = dl_m.solver.time_kernel(5, 20, stream)
+        ms_filter = time_filter(gputo, torch, [dl_m.x, dl_m.CX, dl_m.dsK, dl_m.dV], 20, stream)
         parity = mixed_parity(gputo, torch, dl_m, fixed, Ke0, stream)
         del dl_m
         torch.cuda.empty_cache()
@@ -338,6 +357,11 @@ def run_ours(args):
         # the element pass's per-element scratch is not algorithmic traffic
         "level1_jacobi_fp32": {"ms": ms_lvl1_32, "bytes": 16 * ndof1 + 4 * nel + nnod1},
         "level1_jacobi_fp64": {"ms": ms_lvl1_64, "bytes": 32 * ndof1 + 8 * nel + nnod1},
+        # the FP64 apply of the solution with ce, dc and |F - K U|^2 in its epilogue:
+        # U and F read, ce written, CX read, the mask byte per node
+        "energy_fused_fp64": {"ms": ms_energy, "bytes": 16 * ndof + 16 * nel + nnod},
+        # density filter (3^3 stencil): x read, xPhys written
+        "filter_fp64": {"ms": ms_filter, "bytes": 16 * nel},
     }
     for k in kernels.values():
         k["gbs"] = k["bytes"] / (k["ms"] * 1e-3) / 1e9
@@ -517,8 +541,8 @@ def run_reference(args):
     print(json.dumps(out))
 
 
-KERNELS = {"apply64": 0, "jacobi32": 1, "level1_32": 2, "level1_64": 3, "jacobi_tc": 4, "energy64": -1,
-           "energy_tc": -2}
+KERNELS = {"apply64": 0, "jacobi32": 1, "level1_32": 2, "level1_64": 3, "jacobi_tc": 4, "energy_fused": 5,
+           "energy64": -1, "energy_tc": -2, "filter": -3}
 
 
 def run_micro(args):
@@ -547,6 +571,18 @@ def run_micro(args):
     for k in kinds:
         if KERNELS[k] >= 0:
             out[k + "_ms"] = s.time_kernel(KERNELS[k], args.reps)
+            continue
+        if k == "filter":
+            xo = torch.empty_like(xd)
+            gputo.density_filter_dev(xd, xo, nelx, nely, nelz, RMIN)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(args.reps):
+                gputo.density_filter_dev(xd, xo, nelx, nely, nelz, RMIN)
+            e1.record()
+            torch.cuda.synchronize()
+            out[k + "_ms"] = e0.elapsed_time(e1) / args.reps
             continue
         # compliance sensitivity of a random displacement field: FP64 kernel or tensor cores
         U = torch.randn(3 * (nelx + 1) * (nely + 1) * (nelz + 1), dtype=torch.float64, device="cuda")
@@ -660,6 +696,54 @@ def run_batch(args):
     print(json.dumps(line))
 
 
+HOMOG = (128, 6)   # unit cell n^3, levels (coarsest grid 4^3)
+
+
+def run_homog(args):
+    """Batched periodic homogenization: a 128^3 unit cell whose density is a
+    seeded Gaussian random field (correlation length 8 voxels) through a
+    sigmoid to [1e-3, 1], SIMP moduli; the six unit-strain load cases solved
+    as six right-hand sides to tol 1e-6 (FP32 V-cycle, flexible FP64 PCG, one
+    graph launch per iteration of all six), then the 6x6 effective tensor.  A
+    step is one whole homogenization (hierarchy setup, solve, C_eff)."""
+    import torch
+
+    import gputo
+    torch.cuda.set_device(0)
+    n, nl = HOMOG
+    x = gputo.random_field_density(n, n, n, seed=2024, corr_len=8.0)
+    CX = torch.as_tensor(1e-9 + x ** 3 * (1 - 1e-9), dtype=torch.float64, device="cuda")
+    Ke = gputo.hex8_stiffness(0.3)
+    h = gputo.Homog(n, n, n, nl)
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            C, rr, nit = h.solve(Ke, CX, tol=TOL, maxit=MAXIT, stream=stream)
+        torch.cuda.synchronize()
+        clocks = ClockSampler(0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        launches0 = gputo.launch_count()
+        with clocks:
+            e0.record(stream)
+            for _ in range(args.steps):
+                C, rr, nit = h.solve(Ke, CX, tol=TOL, maxit=MAXIT, stream=stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+    s = e0.elapsed_time(e1) / args.steps / 1000.0
+    ndof = 3 * n ** 3
+    line = {"metric": "s per homogenization (6 load cases, 128^3 cell, tol 1e-6)", "value": round(s, 5),
+            "unit": "s", "higher_is_better": False, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "dtype": "f64 outer PCG / f32 V-cycle", "data": "synthetic: seeded Gaussian random field",
+            "gpu_launches": int((gputo.launch_count() - launches0) / max(1, args.steps)),
+            "dof_iters_per_s": round(6 * ndof * float(np.mean(nit)) / s, 1),
+            "clocks": clocks.summary(),
+            "config": {"workload": "periodic homogenization, 6 unit-strain load cases as 6 right-hand sides",
+                       "cell": [n, n, n], "nl": nl, "ndof_per_case": ndof, "tol": TOL, "nit": nit.tolist(),
+                       "relres": rr.tolist(), "Ceff": np.round(C, 8).tolist(),
+                       "device_gb": round(h.device_bytes / 1e9, 2)}}
+    print(json.dumps(line))
+
+
 BRIDGE = (512, 256, 256, 7)   # nelx, nely, nelz, levels (coarsest grid 8x4x4)
 
 
@@ -736,9 +820,9 @@ def main():
     ap.add_argument("--nl", type=int, default=NL)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--one-step", choices=["mixed", "fp64"], help="profiling aid: one design iteration")
-    ap.add_argument("--workload", default="cantilever", choices=["cantilever", "batch", "bridge"],
-                    help="batch: the uneven multi-design batch; bridge: the 512x256x256 bridge "
-                         "(instead of the headline design loop)")
+    ap.add_argument("--workload", default="cantilever", choices=["cantilever", "batch", "bridge", "homog"],
+                    help="batch: the uneven multi-design batch; bridge: the 512x256x256 bridge; homog: the "
+                         "128^3 periodic homogenization (instead of the headline design loop)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -746,6 +830,8 @@ def main():
         run_batch(args)
     elif args.workload == "bridge":
         run_bridge(args)
+    elif args.workload == "homog":
+        run_homog(args)
     elif args.micro:
         run_micro(args)
     elif args.one_step:

@@ -34,7 +34,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", f"-I{CSRC
 SOURCES = ["kernels_fine.cu", "kernels_mg.cu", "kernels_blas.cu", "kernels_design.cu", "solver.cu",
            "capi.cpp", "noalloc.cu", "kernels_quad.cu", "kernels_tc.cu", "kernels_tcsweep.cu",
            "kernels_learned.cu", "batch.cpp", "design_io.cpp",
-           "kernels_hsweep.cu", "hostio.cpp"]
+           "kernels_hsweep.cu", "hostio.cpp", "homog.cu"]
 HEADERS = ["gputo_internal.h", "solver.h", "tma.h", "hadamard.h"]
 
 

@@ -446,9 +446,10 @@ int gputo_debug_set_sweep_fault(int skip_stage, unsigned wait_us)
 
 int gputo_solver_time_kernel(gputo_solver *h, int which, int reps, double *ms, void *stream)
 {
-    if (!h || !ms || reps < 1 || which < 0 || which > 4) return GPUTO_ERR_ARG;
+    if (!h || !ms || reps < 1 || which < 0 || which > 5) return GPUTO_ERR_ARG;
     Solver &s = h->s;
     if (!s.ready) return GPUTO_ERR_ARG;
+    if (which == 5 && !(s.use_hsweep<double>(s.g[0]) && gputo::hsweep_energy_fits(s.g[0]))) return GPUTO_ERR_ARG;
     if ((which == 1 || which == 2 || which == 4) && s.opt.precision != GPUTO_PREC_MIXED) return GPUTO_ERR_ARG;
     if ((which == 2 || which == 3) && s.nl < 2) return GPUTO_ERR_ARG;
     cudaStream_t st = s.stream(stream);
@@ -466,6 +467,10 @@ int gputo_solver_time_kernel(gputo_solver *h, int which, int reps, double *ms, v
         case 1:
             r = s.fine_sweep<float>(0, gputo::MODE_JACOBI, s.lay[0], s.elay, s.CXpf, s.Lf[0].u0, s.Lf[0].f, s.Lf[0],
                                     s.Lf[0].u1, 0.48f, 0.7f, nullptr, nullptr, st);
+            break;
+        case 5:   // the fused energy apply on the solver's U and F; ce into the staging buffer
+            r = gputo::launch_hsweep_energy(s.lay[0], s.elay, s.hk, s.CXp, s.Uw, s.Fw, s.mask[0], s.maskp[0],
+                                            nullptr, s.partial, s.Dn, nullptr, nullptr, s.err, st);
             break;
         case 4:
             r = gputo::launch_tc_sweep(s.opt.tc_parts > 0 ? s.opt.tc_parts : 1, gputo::MODE_JACOBI, s.lay[0],

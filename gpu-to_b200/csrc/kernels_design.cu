@@ -263,6 +263,94 @@ filter_kernel(Grid g, const double *__restrict__ in, const double *__restrict__ 
     }
 }
 
+// The same correlation for 1 <= R <= 3, decomposed by x plane: h[a][b][c] =
+// h[-a][b][c], so plane q contributes P_|a|(q) = sum_{c,b} h[a][b][c] in(q, j+b,
+// k+c) (R + 1 two-dimensional sums over the same (2R + 1)^2 shared-memory
+// values) to the output at plane q - a, for every a in -R..R.  A thread keeps
+// the 2R + 1 outputs still open in registers (a ring indexed at compile time:
+// the march is unrolled by 2 (2R + 1)), so each input plane sits in shared
+// memory once (two slots, one barrier per plane) and costs (2R + 1)^2 shared
+// loads per output instead of (2R + 1)^3.  Output i sums P_R(i - R), ...,
+// P_0(i), ..., P_R(i + R) in plane order.
+template <int R>
+__global__ void __launch_bounds__(256)
+filter_plane_kernel(Grid g, const double *__restrict__ in, const double *__restrict__ div,
+                    double *__restrict__ out, double scale, int xc)
+{
+    using FT = FiltTile<R>;
+    constexpr int W = FT::W;
+    extern __shared__ double fs[];   // [2][PLANE]
+    const int tid = threadIdx.x, ly = tid & 31, lz = tid >> 5;
+    const int j0 = blockIdx.x * kFTY, k0 = blockIdx.y * kFTZ;
+    const int x0 = blockIdx.z * xc, x1 = min(x0 + xc, g.nx);
+    const long long ps = (long long)g.ny * g.nz;
+    long long off[FT::NPOS];
+#pragma unroll
+    for (int q = 0; q < FT::NPOS; ++q) {
+        const int p = tid + 256 * q;
+        off[q] = -1;
+        if (p < FT::PLANE) {
+            const int zz = p / FT::TYH, yy = p - zz * FT::TYH;
+            off[q] = (long long)mirror_index(k0 + zz - R, g.nz) * g.ny + mirror_index(j0 + yy - R, g.ny);
+        }
+    }
+    auto fetch = [&](int px, double (&v)[FT::NPOS]) {
+        const long long base = (long long)mirror_index(px, g.nx) * ps;
+#pragma unroll
+        for (int q = 0; q < FT::NPOS; ++q)
+            if (off[q] >= 0) {
+                const long long s = base + off[q];
+                v[q] = div ? in[s] / div[s] : in[s];
+            }
+    };
+    const int j = j0 + ly, k = k0 + lz;
+    const bool mine = j < g.ny && k < g.nz;
+    const long long obase = (long long)k * g.ny + j;
+    double acc[W];
+#pragma unroll
+    for (int s = 0; s < W; ++s) acc[s] = 0.0;
+    const int T = x1 - x0 + 2 * R;   // planes x0 - R .. x1 + R - 1
+    double pre[2][FT::NPOS];
+    fetch(x0 - R, pre[0]);
+    if (T > 1) fetch(x0 - R + 1, pre[1]);
+    for (int t0 = 0; t0 < T; t0 += 2 * W)
+#pragma unroll
+    for (int u = 0; u < 2 * W; ++u) {
+        const int t = t0 + u;
+        if (t >= T) break;                 // the same for the whole CTA
+        const int q = x0 - R + t;          // this plane
+        double *P = fs + (u & 1) * FT::PLANE;
+#pragma unroll
+        for (int v = 0; v < FT::NPOS; ++v)
+            if (off[v] >= 0) P[tid + 256 * v] = pre[u & 1][v];
+        __syncthreads();
+        if (t + 2 < T) fetch(q + 2, pre[u & 1]);   // in flight while this plane is used
+        double pa[R + 1];
+#pragma unroll
+        for (int a = 0; a <= R; ++a) pa[a] = 0.0;
+#pragma unroll
+        for (int c = -R; c <= R; ++c) {
+            const double *row = P + (lz + R + c) * FT::TYH + ly + R;
+#pragma unroll
+            for (int b = -R; b <= R; ++b) {
+                const double x = row[b];
+#pragma unroll
+                for (int a = 0; a <= R; ++a) pa[a] = fma(cFilterH[((a + R) * W + (b + R)) * W + (c + R)], x, pa[a]);
+            }
+        }
+        // output q + a (a = -R..R) sits in slot (t + a + R) mod W
+#pragma unroll
+        for (int a = -R; a <= R; ++a) {
+            const int sl = (u + a + R) % W;
+            acc[sl] += pa[a < 0 ? -a : a];
+        }
+        // output q - R is complete
+        const int i = q - R, sl = u % W;
+        if (i >= x0 && mine) out[(long long)i * ps + obase] = acc[sl] * scale;
+        acc[sl] = 0.0;
+    }
+}
+
 template <int R>
 int filter_launch(const Grid &g, const double *in, const double *div, double *out, double scale,
                   cudaStream_t st)
@@ -286,7 +374,11 @@ int filter_launch(const Grid &g, const double *in, const double *div, double *ou
     int xc = (int)std::max(16LL, ((long long)g.nx + want - 1) / want);
     if (xc > g.nx) xc = g.nx;
     const unsigned tx = (unsigned)((g.nx + xc - 1) / xc);
-    filter_kernel<R><<<dim3(ty, tz, tx), 256, FT::bytes, st>>>(g, in, div, out, scale, xc);
+    if constexpr (R >= 1 && R <= 3)
+        filter_plane_kernel<R><<<dim3(ty, tz, tx), 256, sizeof(double) * 2 * FT::PLANE, st>>>(g, in, div, out, scale,
+                                                                                              xc);
+    else
+        filter_kernel<R><<<dim3(ty, tz, tx), 256, FT::bytes, st>>>(g, in, div, out, scale, xc);
     count_launches(1);
     return GPUTO_OK;
 }

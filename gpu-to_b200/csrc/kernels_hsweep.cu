@@ -141,6 +141,35 @@ __device__ __forceinline__ void element_h(const T (&Fp)[HF], const T (&Fn)[HF], 
         }
 }
 
+// element_h that also returns v . w with w = S v / 64 (CX applied after the
+// S step), the element's energy u_e' Ke u_e: the FP64 apply with the element
+// energies.
+__device__ __forceinline__ double element_h_energy(const double (&Fp)[HF], const double (&Fn)[HF], double cx,
+                                                   const HC<double> &k, double (&A)[HF], double (&An)[HF])
+{
+    double v0[HF], v1[HF], w0[HF], w1[HF];
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            v0[4 * c + d] = Fp[4 * c + d] + Fn[4 * c + d];
+            v1[4 * c + d] = Fp[4 * c + d] - Fn[4 * c + d];
+        }
+    element_s(v0, v1, 1.0, k, w0, w1);
+    double en = 0.0;
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const int q = 4 * c + d;
+            en = fma(v0[q], w0[q], en);
+            en = fma(v1[q], w1[q], en);
+            A[q] = fma(cx, w0[q] + w1[q], A[q]);
+            An[q] = cx * (w0[q] - w1[q]);
+        }
+    return en;
+}
+
 // FP32: the sums and differences of faces and outputs on (x, y) pairs.
 template <>
 __device__ __forceinline__ void element_h<float>(const float (&Fp)[HF], const float (&Fn)[HF], float cx,
@@ -206,10 +235,9 @@ __device__ __forceinline__ void h_store(long long base, unsigned m, const T (&ku
 // memory (FP64 apply and defect measured 10 % faster at 2, with a few spills,
 // than at 1); the FP64 Jacobi instances hold 129 and 158 KB, so only one fits.
 template <typename T, int MODE> struct HMinBlocks {
-    static constexpr int value = (sizeof(T) == 4 || MODE == MODE_APPLY || MODE == MODE_DEFECT) ? 2 : 1;
+    static constexpr int value =
+        (sizeof(T) == 4 || MODE == MODE_APPLY || MODE == MODE_DEFECT || MODE == MODE_ENERGY) ? 2 : 1;
 };
-// MODE_ENERGY (once per solve) keeps the element's modes for its energy as
-// well: one CTA per SM, no register cap.
 
 template <typename T, int MODE, int WZ>
 __global__ void __launch_bounds__(32 * WZ, HMinBlocks<T, MODE>::value)
@@ -383,18 +411,19 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
             if ((q & 3) != 3) Fn[q] = Un[q];
         face_h(Fn);
         const T cx = reinterpret_cast<const T *>(smem + (t % HRING) * S::slot + S::c_off)[w * HY + l];
-        element_h(Fc, Fn, cx, hc, Ac, An);
         if constexpr (MODE == MODE_ENERGY) {
+            const double en = element_h_energy(Fc, Fn, cx, hc, Ac, An);
             // element (E0 + t - 1, jc0 + l, kc0 + w): written by the one CTA that
             // owns it (x chunks overlap by one element, z tiles by one row)
             const int ei = E0 + t - 1, ej = jc0 + l, ek = kc0 + w;
             if (ei >= P0 && (w < WZ - 1 || zt == (int)gridDim.y - 1) && ek < g.nz && ej < g.ny) {
-                const double en = element_energy_h(Fc, Fn, hc);
                 const long long e = g.elem(ei, ej, ek);
                 ce[e] = en;
                 if (dcv) dcv[e] = dsK[e] * en;
                 dsum2 = fma((double)cx, en, dsum2);
             }
+        } else {
+            element_h(Fc, Fn, cx, hc, Ac, An);
         }
         const int p = E0 + t - 1;   // node plane finished by this element
         const bool out_plane = p >= P0;

@@ -103,6 +103,10 @@ SIGNATURES = {
     "gputo_solver_time_kernel": (_i, [_vp, _i, _i, _dp, _vp]),
     "gputo_debug_set_sweep_fault": (_i, [_i, ctypes.c_uint]),
     "gputo_solver_energy_dev": (_i, [_vp, _vp, _vp, _vp, _dp, _dp, _vp]),
+    "gputo_homog_create": (_i, [ctypes.POINTER(_vp), _i, _i, _i, _i, ctypes.POINTER(Options)]),
+    "gputo_homog_destroy": (None, [_vp]),
+    "gputo_homog_device_bytes": (ctypes.c_size_t, [_vp]),
+    "gputo_homog_solve_dev": (_i, [_vp, _dp, _vp, _d, _i, _dp, _dp, ctypes.POINTER(_i), _vp, _vp]),
     "gputo_compliance_sens_dev": (_i, [_dp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _dp, _vp]),
     "gputo_compliance_sens": (_i, [_dp, _dp, _dp, _dp, _i, _i, _i, _dp, _dp, _dp]),
     "gputo_compliance_sens_tc_dev": (_i, [_dp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _dp, _vp]),
@@ -411,6 +415,45 @@ class Solver:
         """The mixed V-cycle's FP32 fine operator (0: CUDA cores, 1-3: tensor cores)."""
         _check(_lib.gputo_solver_apply_fp32_dev(self._h, _ptr(u), _ptr(r), int(tc_parts), _ptr_stream(stream)),
                "gputo_solver_apply_fp32_dev")
+
+
+class Homog:
+    """Periodic homogenization of a voxel unit cell (gputo_homog_*): the six
+    unit-strain load cases as six right-hand sides of one MGCG solve."""
+
+    def __init__(self, nx, ny, nz, nl, options: Options | None = None):
+        self._h = ctypes.c_void_p()
+        self.shape = (int(nx), int(ny), int(nz))
+        self.options = options or default_options(precision=PREC_MIXED)
+        _check(_lib.gputo_homog_create(ctypes.byref(self._h), *self.shape, int(nl), ctypes.byref(self.options)),
+               "gputo_homog_create")
+
+    def close(self):
+        if self._h:
+            _lib.gputo_homog_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def device_bytes(self) -> int:
+        return int(_lib.gputo_homog_device_bytes(self._h))
+
+    def solve(self, Ke0, CX, tol=1e-6, maxit=500, chi=None, stream=None):
+        """Returns (Ceff [6, 6], relres [6], nit [6]); CX a device tensor of the
+        element moduli; chi (optional device tensor of 18 N doubles) receives the
+        fluctuations as [3 node + d][r]."""
+        Ke0 = np.ascontiguousarray(Ke0, dtype=np.float64).reshape(-1)
+        C = np.zeros(36)
+        rr = np.zeros(6)
+        nit = (ctypes.c_int * 6)()
+        _check(_lib.gputo_homog_solve_dev(self._h, _p(Ke0), _ptr(CX), float(tol), int(maxit), _p(C), _p(rr), nit,
+                                          _ptr(chi), _ptr_stream(stream)), "gputo_homog_solve_dev")
+        return C.reshape(6, 6), rr, np.array(list(nit))
 
 
 class Batch:

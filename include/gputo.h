@@ -230,8 +230,10 @@ long long gputo_solver_launch_count(const gputo_solver *s);
  * hierarchy with CUDA events on 'stream' and return the mean launch time in
  * milliseconds.  which: 0 fine-level FP64 apply (p -> K p), 1 fine-level FP32
  * Jacobi sweep, 2 level-1 FP32 sweep, 3 level-1 FP64 sweep, 4 fine-level
- * tensor-core Jacobi sweep (tc_parts of the options, 1 if 0).  Inputs are the
- * solver's own work vectors; results are discarded.  Needs setup first. */
+ * tensor-core Jacobi sweep (tc_parts of the options, 1 if 0), 5 the FP64
+ * apply with the element energies (gputo_solver_energy_dev's pass; Hadamard-
+ * basis grids only).  Inputs are the solver's own work vectors; results are
+ * discarded.  Needs setup first. */
 int gputo_solver_time_kernel(gputo_solver *s, int which, int reps, double *ms_per_launch,
                              void *stream);
 
@@ -245,6 +247,34 @@ int gputo_solver_time_kernel(gputo_solver *s, int which, int reps, double *ms_pe
  * after 2 s).  Affects launches, not CUDA graphs captured earlier.  Not for
  * production use. */
 int gputo_debug_set_sweep_fault(int skip_stage, unsigned wait_us);
+
+/* ---------------------------------------------------------------------- */
+/* Periodic homogenization (no reference counterpart)                      */
+/* ---------------------------------------------------------------------- */
+
+/* Effective elasticity of a periodic voxel unit cell of nx x ny x nz unit
+ * elements (element (i, j, k) at (nz ny) i + ny k + j, as the solver's).  The
+ * six unit-strain load cases (Voigt order xx, yy, zz, yz, xz, xy, engineering
+ * shear strains) are solved together as six right-hand sides: each operator,
+ * smoother and transfer launch serves all six, and one CUDA graph launch runs
+ * a PCG iteration of all six.  Method: the MGCG of gputo_mgcg1 on a periodic
+ * grid (node 0 held against the rigid translations), coarse levels
+ * re-discretised as gputo_mgcg9's (CX_l = 2 mean of the children), FP32
+ * V-cycle, flexible FP64 PCG per load case.  nx, ny, nz divisible by
+ * 2^(nl-1) with at least 2 coarsest elements per direction; the options'
+ * nswp, omega, prerelax, check_every, use_graph and max_coarse_dofs apply. */
+typedef struct gputo_homog gputo_homog;
+int gputo_homog_create(gputo_homog **out, int nx, int ny, int nz, int nl, const gputo_options *opt);
+void gputo_homog_destroy(gputo_homog *h);
+size_t gputo_homog_device_bytes(const gputo_homog *h);
+/* Ke0: the 24x24 element matrix (host, as for gputo_mgcg1); CX: device array
+ * of the element moduli.  Ceff: host 6x6 (row-major, symmetric)
+ * C_rs = mean_e CX_e (u0_r + chi_r)_e' Ke0 (u0_s + chi_s)_e, with u0_r the
+ * affine field of unit strain r and chi_r its periodic fluctuation; relres[6],
+ * nit[6]: per load case (either may be NULL); chi (optional, device,
+ * 18 nx ny nz doubles): the fluctuations as [3 node + d][r]. */
+int gputo_homog_solve_dev(gputo_homog *h, const double *Ke0, const double *CX, double tol, int maxit,
+                          double *Ceff, double *relres, int *nit, double *chi, void *stream);
 
 /* ---------------------------------------------------------------------- */
 /* Batched solves and the option autotuner (no reference counterpart)       */

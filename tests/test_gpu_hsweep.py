@@ -114,7 +114,7 @@ def test_mixed_solve_matches_dense(oracle, gputo, torch):
     assert np.linalg.norm(res[0][0] - res[1][0]) <= 1e-6 * np.linalg.norm(res[1][0])
 
 
-@pytest.mark.parametrize("shape,nl", SHAPES + [((70, 34, 18), 2)])
+@pytest.mark.parametrize("shape,nl", SHAPES + [((72, 36, 20), 3)])
 def test_energy_fused_into_the_apply_matches_the_separate_pass(oracle, gputo, torch, shape, nl):
     """gputo_solver_energy_dev: ce, dc and the compliance from one FP64 apply
     of the solution (each element written by exactly one CTA, although x
