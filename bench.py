@@ -691,7 +691,7 @@ def run_batch(args):
             "dtype": "f64 outer / f32 V-cycle", "data": "synthetic",
             "config": {"workload": "uneven multi-design batch", "designs": [list(m[2]) for m in members],
                        "total_dofs": dofs, "nit": nits,
-                       "tuned": {"x".join(map(str, k)): {"nswp": v.nswp, "tc_parts": v.tc_parts,
+                       "tuned": {"x".join(map(str, k)): {"nswp": v.nswp, "nswp_fine": v.nswp_fine, "tc_parts": v.tc_parts,
                                                          "tc_xchunk": v.tc_xchunk} for k, v in tuned.items()}}}
     print(json.dumps(line))
 

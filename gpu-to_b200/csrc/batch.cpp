@@ -96,6 +96,18 @@ int gputo_batch_solve_dev(gputo_batch *b, const double *const *F, double *const 
     const int n = (int)b->members.size();
     for (int i = 0; i < n; ++i)
         if (!F[i] || !U[i]) return GPUTO_ERR_ARG;
+    // members run on concurrent streams: no persistent (grid-barrier) kernels
+    struct TailOff {
+        gputo_batch *b;
+        explicit TailOff(gputo_batch *bb) : b(bb)
+        {
+            for (gputo_solver *m : b->members) m->s.tail_ok = false;
+        }
+        ~TailOff()
+        {
+            for (gputo_solver *m : b->members) m->s.tail_ok = true;
+        }
+    } tail_off(b);
     // initial residuals and V-cycles, each member on its own stream
     GPUTO_CUDA(cudaEventRecord(b->fork, b->main));
     for (int i = 0; i < n; ++i) {
@@ -183,10 +195,16 @@ int gputo_autotune_dev(gputo_solver *h, const double *F, double *U, double tol, 
     for (int nswp : {2, 3, 4}) {
         gputo_options o = base;
         o.nswp = nswp;
+        o.nswp_fine = 0;
         o.use_graph = 1;
         o.check_every = 8;
         o.tc_parts = 0;
         cand.push_back(o);
+        for (int nf = 1; nf < nswp; ++nf) {   // fewer sweeps on the finest level, where they cost most
+            o.nswp_fine = nf;
+            cand.push_back(o);
+        }
+        o.nswp_fine = 0;
         if (s.opt.precision == GPUTO_PREC_MIXED)
             for (int xc : {8, 16}) {
                 o.tc_parts = 2;

@@ -118,6 +118,8 @@ void gputo_default_options(gputo_options *o)
     o->tc_xchunk = 0;
     o->coarse = GPUTO_COARSE_GALERKIN;
     o->fine_op = 0;
+    o->nswp_fine = 0;
+    o->coarse_tail = 1;
 }
 
 int gputo_fine_op_constants(const double *Ke, double *c8)

@@ -490,7 +490,8 @@ __global__ void __launch_bounds__(256) pfinish_kernel(int nb, const double *__re
                                                       const double *__restrict__ partial_rr, HScal *sc, int which)
 {
     if (which >= PF_ALPHA && sc->done) return;
-    const int K = which == PF_END ? 2 * NR : NR;
+    // pdot2 writes 2 NR partials per block (INIT: pinit, ALPHA: the apply, NR each)
+    const int K = (which == PF_END || which == PF_RHO0) ? 2 * NR : NR;
     __shared__ double tot[2 * NR], tot_rr[NR];
     // thread q sums column q (fixed order: deterministic)
     if (threadIdx.x < K) {

@@ -8,7 +8,10 @@
 // (:1199-1206) and Dirichlet zeroing (ZeroBCc, :1326-1331) are fused into the
 // epilogue.  Vectors use the padded row layout (Lay); element arrays keep the
 // reference's element order.
+#include <algorithm>
+
 #include "gputo_internal.h"
+#include "tma.h"
 
 namespace gputo {
 
@@ -233,18 +236,18 @@ packed_sweep_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u,
 // A[row, col] reads 32 neighbouring elements (the [300][nel] layout is
 // element-fastest): four 32-byte sectors per warp instead of 32.  The eight
 // slot partials are summed in a fixed order through shared memory.
+// One CTA of the slot sweep (CTA index vb): 32 nodes, warp w = element slot
+// (ex, ez, ey) of the 8 around each node.  Shared by the kernel below and the
+// persistent coarse-level kernel; ends with a barrier so 'part' can be reused.
 template <typename T, int MODE>
-__global__ void __launch_bounds__(256)
-packed_sweep_slot_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u, const T *__restrict__ f,
-                         const T *__restrict__ rdiag, const uint8_t *__restrict__ mask, T *__restrict__ out,
-                         T omega, T prerelax, const int *__restrict__ done)
+__device__ __forceinline__ void slot_sweep_block(const Lay &L, const T *__restrict__ A, const T *__restrict__ u,
+                                                 const T *__restrict__ f, const T *__restrict__ rdiag,
+                                                 const uint8_t *__restrict__ mask, T *__restrict__ out, T omega,
+                                                 T prerelax, long long vb, T (&part)[8][32][3])
 {
-    pdl_wait();
-    if (done && *done) return;
-    __shared__ T part[8][32][3];
     const Grid &g = L.g;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const long long n = (long long)blockIdx.x * 32 + lane;
+    const long long n = vb * 32 + lane;
     const bool have = n < g.nnod();
     int i = 0, j = 0, k = 0;
     if (have) node_ijk(g, n, i, j, k);
@@ -277,35 +280,49 @@ packed_sweep_slot_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u
 #pragma unroll
     for (int d = 0; d < 3; ++d) part[w][lane][d] = acc[d];
     __syncthreads();
-    if (w != 0 || !have) return;
-    T s[3];
+    if (w == 0 && have) {
+        T s[3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        s[d] = part[0][lane][d];
+        for (int d = 0; d < 3; ++d) {
+            s[d] = part[0][lane][d];
 #pragma unroll
-        for (int q = 1; q < 8; ++q) s[d] += part[q][lane][d];
-    }
-    const unsigned m = mask[n];
-    const long long base = L.at(i, j, k);
+            for (int q = 1; q < 8; ++q) s[d] += part[q][lane][d];
+        }
+        const unsigned m = mask[n];
+        const long long base = L.at(i, j, k);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        const long long dof = base + d;
-        const bool fixed = (m >> d) & 1u;
-        if (MODE == MODE_APPLY) {
-            out[dof] = fixed ? T(0) : s[d];
-        } else if (MODE == MODE_DEFECT) {
-            out[dof] = fixed ? T(0) : f[dof] - s[d];
-        } else {
-            const T r = fixed ? T(0) : f[dof] - s[d];
-            T us;
-            if (MODE == MODE_JACOBI_PRE) {
-                us = prerelax * f[dof] * rdiag[dof];
+        for (int d = 0; d < 3; ++d) {
+            const long long dof = base + d;
+            const bool fixed = (m >> d) & 1u;
+            if (MODE == MODE_APPLY) {
+                out[dof] = fixed ? T(0) : s[d];
+            } else if (MODE == MODE_DEFECT) {
+                out[dof] = fixed ? T(0) : f[dof] - s[d];
             } else {
-                us = u[dof];
+                const T r = fixed ? T(0) : f[dof] - s[d];
+                T us;
+                if (MODE == MODE_JACOBI_PRE) {
+                    us = prerelax * f[dof] * rdiag[dof];
+                } else {
+                    us = u[dof];
+                }
+                out[dof] = us + omega * r * rdiag[dof];
             }
-            out[dof] = us + omega * r * rdiag[dof];
         }
     }
+    __syncthreads();
+}
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256)
+packed_sweep_slot_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u, const T *__restrict__ f,
+                         const T *__restrict__ rdiag, const uint8_t *__restrict__ mask, T *__restrict__ out,
+                         T omega, T prerelax, const int *__restrict__ done)
+{
+    pdl_wait();
+    if (done && *done) return;
+    __shared__ T part[8][32][3];
+    slot_sweep_block<T, MODE>(L, A, u, f, rdiag, mask, out, omega, prerelax, blockIdx.x, part);
 }
 
 template <typename T>
@@ -364,15 +381,11 @@ template void launch_packed_sweep<float>(int, const Lay &, const float *, const 
 // fine neighbours of each coarse node (mgcg1.cu:792-831 rstrFc), then the
 // coarse Dirichlet rows are zeroed (ZeroBCc after rstrFc, mgcg1.cu:537).
 template <typename T>
-__global__ void restrict_kernel(Lay Lc, Lay Lf, const T *__restrict__ rf,
-                                const uint8_t *__restrict__ maskc, T *__restrict__ fc,
-                                const int *__restrict__ done)
+__device__ __forceinline__ void restrict_node(const Lay &Lc, const Lay &Lf, const T *__restrict__ rf,
+                                              const uint8_t *__restrict__ maskc, T *__restrict__ fc, int i, int j,
+                                              int k)
 {
-    pdl_wait();
-    if (done && *done) return;
     const Grid &gc = Lc.g;
-    int i, j, k;
-    if (!plane_ijk(gc, i, j, k)) return;
     const long long n = gc.node(i, j, k);
     const Grid &gf = Lf.g;
     T acc[3] = {T(0), T(0), T(0)};
@@ -404,6 +417,18 @@ __global__ void restrict_kernel(Lay Lc, Lay Lf, const T *__restrict__ rf,
 }
 
 template <typename T>
+__global__ void restrict_kernel(Lay Lc, Lay Lf, const T *__restrict__ rf,
+                                const uint8_t *__restrict__ maskc, T *__restrict__ fc,
+                                const int *__restrict__ done)
+{
+    pdl_wait();
+    if (done && *done) return;
+    int i, j, k;
+    if (!plane_ijk(Lc.g, i, j, k)) return;
+    restrict_node<T>(Lc, Lf, rf, maskc, fc, i, j, k);
+}
+
+template <typename T>
 void launch_restrict(const Lay &Lc, const Lay &Lf, const T *rf, const uint8_t *maskc, T *fc,
                      const int *done, cudaStream_t st)
 {
@@ -419,15 +444,11 @@ template void launch_restrict<float>(const Lay &, const Lay &, const float *, co
 // u_f += P u_c, trilinear (mgcg1.cu:1587-1641 interpc), then the fine
 // Dirichlet dofs are zeroed (ZeroBCc after interpc, mgcg1.cu:631).
 template <typename T>
-__global__ void prolong_kernel(Lay Lf, Lay Lc, const T *__restrict__ uc,
-                               const uint8_t *__restrict__ maskf, T *__restrict__ uf,
-                               const int *__restrict__ done)
+__device__ __forceinline__ void prolong_node(const Lay &Lf, const Lay &Lc, const T *__restrict__ uc,
+                                             const uint8_t *__restrict__ maskf, T *__restrict__ uf, int i, int j,
+                                             int k)
 {
-    pdl_wait();
-    if (done && *done) return;
     const Grid &gf = Lf.g;
-    int i, j, k;
-    if (!plane_ijk(gf, i, j, k)) return;
     const long long n = gf.node(i, j, k);
     const int ni = (i & 1) + 1, nj = (j & 1) + 1, nk = (k & 1) + 1;
     T acc[3] = {T(0), T(0), T(0)};
@@ -457,6 +478,18 @@ __global__ void prolong_kernel(Lay Lf, Lay Lc, const T *__restrict__ uc,
         const long long dof = base + d;
         uf[dof] = ((m >> d) & 1u) ? T(0) : fma(w, acc[d], uf[dof]);
     }
+}
+
+template <typename T>
+__global__ void prolong_kernel(Lay Lf, Lay Lc, const T *__restrict__ uc,
+                               const uint8_t *__restrict__ maskf, T *__restrict__ uf,
+                               const int *__restrict__ done)
+{
+    pdl_wait();
+    if (done && *done) return;
+    int i, j, k;
+    if (!plane_ijk(Lf.g, i, j, k)) return;
+    prolong_node<T>(Lf, Lc, uc, maskf, uf, i, j, k);
 }
 
 template <typename T>
@@ -1005,16 +1038,11 @@ __device__ __forceinline__ long long padded_pos(const Lay &L, long long r)
 // FP64 accumulation.  in_padded / out_padded: x / y live in the level's padded
 // layout (otherwise dense vectors of n).
 template <typename Tin, typename Tout>
-__global__ void gemv_warp_kernel(Lay L, const double *__restrict__ M, const Tin *__restrict__ x,
-                                 Tout *__restrict__ y, int lower, int in_padded, int out_padded,
-                                 const int *__restrict__ done)
+__device__ __forceinline__ void gemv_row(const Lay &L, const double *__restrict__ M, const Tin *__restrict__ x,
+                                         Tout *__restrict__ y, int lower, int in_padded, int out_padded, int row,
+                                         int lane)
 {
-    pdl_wait();
-    if (done && *done) return;
     const int n = (int)L.g.ndof();
-    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (row >= n) return;
     const int lo = lower ? 0 : row, hi = lower ? row + 1 : n;
     const double *mr = M + (long long)row * n;
     double s = 0.0;
@@ -1022,6 +1050,18 @@ __global__ void gemv_warp_kernel(Lay L, const double *__restrict__ M, const Tin 
         s = fma(mr[c], (double)x[in_padded ? padded_pos(L, c) : c], s);
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0) y[out_padded ? padded_pos(L, row) : row] = (Tout)s;
+}
+
+template <typename Tin, typename Tout>
+__global__ void gemv_warp_kernel(Lay L, const double *__restrict__ M, const Tin *__restrict__ x,
+                                 Tout *__restrict__ y, int lower, int in_padded, int out_padded,
+                                 const int *__restrict__ done)
+{
+    pdl_wait();
+    if (done && *done) return;
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (row >= (int)L.g.ndof()) return;
+    gemv_row<Tin, Tout>(L, M, x, y, lower, in_padded, out_padded, row, threadIdx.x & 31);
 }
 
 // Coarsest solve x = A^-1 b = Linv^T (Linv b) with the explicit inverse of the
@@ -1085,5 +1125,155 @@ void launch_mask_restrict(const Grid &gc, const uint8_t *maskf, uint8_t *maskc, 
     mask_restrict_kernel<<<(unsigned)((gc.nnod() + bs - 1) / bs), bs, 0, st>>>(gc, maskf, maskc);
     count_launches(1);
 }
+
+
+// ---------------------------------------------------------------------------
+// persistent coarse-level V-cycle
+// ---------------------------------------------------------------------------
+
+// Grid-wide barrier of a kernel whose CTAs are all resident (a cooperative
+// launch): arrival count and generation in bar[0], bar[1].  The wait is
+// bounded (1 s of the global timer); on timeout it sets err and goes on, so
+// the kernel ends and the host reads GPUTO_ERR_TIMEOUT.
+__device__ __forceinline__ void tail_barrier(unsigned *bar, unsigned nblocks, int *err)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *gen = bar + 1;
+        const unsigned g0 = *gen;
+        __threadfence();   // this CTA's results before its arrival
+        if (atomicAdd(bar, 1u) == nblocks - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            const uint64_t t0 = globaltimer_ns();
+            while (*gen == g0) {
+                __nanosleep(64);
+                if (globaltimer_ns() - t0 > 1000000000ull) {
+                    atomicExch(err, GPUTO_ERR_TIMEOUT);
+                    break;
+                }
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+// The levels lt .. nl-1 of a V-cycle in one launch: every restriction,
+// slot sweep, the coarsest solve's two products and every prolongation is
+// a phase over all CTAs, phases separated by the grid barrier.  Each phase
+// runs the same device code as the separate kernels (slot_sweep_block,
+// restrict_node, prolong_node, gemv_row), so results are bit for bit those
+// of the launch-per-step schedule; what goes is about 20 launches and their
+// gaps per V-cycle on levels of a few thousand nodes.
+template <typename T>
+__global__ void __launch_bounds__(256, 2)
+coarse_tail_kernel(TailLevels tl, const TailPhase *__restrict__ ph, int nph, T omega, T prerelax,
+                   const double *__restrict__ Linv, const double *__restrict__ LinvT, double *__restrict__ ctmp,
+                   unsigned *bar, int *err, const int *__restrict__ done)
+{
+    if (done && *done) return;   // written before this launch: the same for every CTA
+    __shared__ T part[8][32][3];
+    const unsigned nblocks = gridDim.x;
+    const int lane = threadIdx.x & 31;
+    for (int p = 0; p < nph; ++p) {
+        const TailPhase P = ph[p];
+        const Lay L = tl.lay[P.l];
+        if (P.kind == TAIL_RESTRICT) {
+            const Lay Lf = tl.lay[P.l - 1];
+            for (long long n = blockIdx.x * 256LL + threadIdx.x; n < L.g.nnod(); n += 256LL * nblocks) {
+                int i, j, k;
+                node_ijk(L.g, n, i, j, k);
+                restrict_node<T>(L, Lf, (const T *)P.in, tl.mask[P.l], (T *)P.out, i, j, k);
+            }
+        } else if (P.kind == TAIL_PROLONG) {
+            const Lay Lc = tl.lay[P.l + 1];
+            for (long long n = blockIdx.x * 256LL + threadIdx.x; n < L.g.nnod(); n += 256LL * nblocks) {
+                int i, j, k;
+                node_ijk(L.g, n, i, j, k);
+                prolong_node<T>(L, Lc, (const T *)P.in, tl.mask[P.l], (T *)P.out, i, j, k);
+            }
+        } else if (P.kind == TAIL_SWEEP) {
+            const long long nvb = (L.g.nnod() + 31) / 32;
+            const T *A = (const T *)tl.A[P.l], *rd = (const T *)tl.rdiag[P.l];
+            const T *u = (const T *)P.in, *f = (const T *)P.f;
+            T *out = (T *)P.out;
+            for (long long vb = blockIdx.x; vb < nvb; vb += nblocks) {
+                switch (P.mode) {
+                case MODE_APPLY:
+                    slot_sweep_block<T, MODE_APPLY>(L, A, u, f, rd, tl.mask[P.l], out, omega, prerelax, vb, part);
+                    break;
+                case MODE_DEFECT:
+                    slot_sweep_block<T, MODE_DEFECT>(L, A, u, f, rd, tl.mask[P.l], out, omega, prerelax, vb, part);
+                    break;
+                case MODE_JACOBI:
+                    slot_sweep_block<T, MODE_JACOBI>(L, A, u, f, rd, tl.mask[P.l], out, omega, prerelax, vb, part);
+                    break;
+                default:
+                    slot_sweep_block<T, MODE_JACOBI_PRE>(L, A, u, f, rd, tl.mask[P.l], out, omega, prerelax, vb,
+                                                         part);
+                }
+            }
+        } else {   // the coarsest solve: tmp = Linv f, then u = Linv' tmp (warp per row)
+            const int n = (int)L.g.ndof();
+            for (int row = blockIdx.x * 8 + (threadIdx.x >> 5); row < n; row += nblocks * 8) {
+                if (P.kind == TAIL_GEMV_LOWER)
+                    gemv_row<T, double>(L, Linv, (const T *)P.in, ctmp, 1, 1, 0, row, lane);
+                else
+                    gemv_row<double, T>(L, LinvT, ctmp, (T *)P.out, 0, 0, 1, row, lane);
+            }
+        }
+        if (p + 1 < nph) tail_barrier(bar, nblocks, err);
+    }
+}
+
+template <typename T>
+int tail_blocks()
+{
+    static int cache[2][64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int &c = cache[sizeof(T) == 8][dev < 64 ? dev : 63];
+    if (c == 0) {
+        int per_sm = 0, sms = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, coarse_tail_kernel<T>, 256, 0) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
+        c = std::min(per_sm, 2) * sms;
+    }
+    return c;
+}
+
+template <typename T>
+int launch_coarse_tail(const TailLevels &tl, const TailPhase *ph, int nph, T omega, T prerelax, const double *Linv,
+                       const double *LinvT, double *ctmp, unsigned *bar, int *err, const int *done, cudaStream_t st)
+{
+    const int nb = tail_blocks<T>();
+    if (nb <= 0) {
+        set_error("the persistent coarse-level kernel has no resident CTAs");
+        return GPUTO_ERR_CUDA;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)nb);
+    cfg.blockDim = dim3(256);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;   // all CTAs resident: the grid barrier is safe
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    GPUTO_CUDA(cudaLaunchKernelEx(&cfg, coarse_tail_kernel<T>, tl, ph, nph, omega, prerelax, Linv, LinvT, ctmp, bar,
+                                  err, done));
+    count_launches(1);
+    return GPUTO_OK;
+}
+template int launch_coarse_tail<float>(const TailLevels &, const TailPhase *, int, float, float, const double *,
+                                       const double *, double *, unsigned *, int *, const int *, cudaStream_t);
+template int launch_coarse_tail<double>(const TailLevels &, const TailPhase *, int, double, double, const double *,
+                                        const double *, double *, unsigned *, int *, const int *, cudaStream_t);
 
 }  // namespace gputo

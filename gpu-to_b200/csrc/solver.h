@@ -51,6 +51,18 @@ struct Solver {
     double *e2 = nullptr;         // (|F - K U|^2, compliance) of energy()
     int launch_status = GPUTO_OK;   // first failure seen while enqueuing kernels
 
+    // persistent coarse-level V-cycle, per hierarchy (0: FP32, 1: FP64)
+    TailPhase *tail_ph[2]{};
+    int tail_n[2]{}, tail_lt[2]{kMaxLevels, kMaxLevels};
+    TailLevels tail_lv[2]{};
+    unsigned *tail_bar = nullptr;
+    // false while a batch runs this solver beside others on concurrent
+    // streams: a grid barrier needs all of its CTAs resident at once
+    bool tail_ok = true;
+    template <typename T>
+    int build_tail(LevelBuf<T> *Lv, int which);
+    int build_tails();
+
     cudaGraphExec_t graph_exec = nullptr;
     cudaStream_t graph_stream = nullptr;
 
@@ -134,7 +146,9 @@ struct Solver {
                      double *dotPartial = nullptr);
     // The mixed PCG's r'z and r'z_old come from its last fine smoothing sweep
     // (MODE_JACOBI_DOT) when that sweep is the Hadamard-basis kernel.
-    bool fused_dot() const { return use_hsweep<float>(g[0]) && Lf[0].rdiag && opt.tc_parts == 0 && opt.nswp > 0; }
+    bool fused_dot() const { return use_hsweep<float>(g[0]) && Lf[0].rdiag && opt.tc_parts == 0 && sweeps(0) > 0; }
+    // Jacobi sweeps per smoothing step on level l
+    int sweeps(int l) const { return (l == 0 && opt.nswp_fine > 0) ? opt.nswp_fine : opt.nswp; }
     int run_graph(int batch, cudaStream_t st);
     void note(int s)
     {

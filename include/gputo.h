@@ -89,6 +89,13 @@ typedef struct {
                             isotropic cube element and nely <= 256 (fewer
                             operations, same results to rounding), else dense
                             element rows; 1 = always dense element rows       */
+    int nswp_fine;       /* Jacobi sweeps per smoothing step on the finest level
+                            only (0 = nswp, the reference's schedule); the
+                            autotuner may pick fewer there, where a sweep costs
+                            most                                                  */
+    int coarse_tail;     /* 1: the levels below 65,536 nodes (and the coarsest
+                            solve) run as one persistent kernel per V-cycle,
+                            same results bit for bit; 0: one launch per step  */
 } gputo_options;
 
 void gputo_default_options(gputo_options *opt);
