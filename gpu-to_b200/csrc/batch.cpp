@@ -96,18 +96,6 @@ int gputo_batch_solve_dev(gputo_batch *b, const double *const *F, double *const 
     const int n = (int)b->members.size();
     for (int i = 0; i < n; ++i)
         if (!F[i] || !U[i]) return GPUTO_ERR_ARG;
-    // members run on concurrent streams: no persistent (grid-barrier) kernels
-    struct TailOff {
-        gputo_batch *b;
-        explicit TailOff(gputo_batch *bb) : b(bb)
-        {
-            for (gputo_solver *m : b->members) m->s.tail_ok = false;
-        }
-        ~TailOff()
-        {
-            for (gputo_solver *m : b->members) m->s.tail_ok = true;
-        }
-    } tail_off(b);
     // initial residuals and V-cycles, each member on its own stream
     GPUTO_CUDA(cudaEventRecord(b->fork, b->main));
     for (int i = 0; i < n; ++i) {

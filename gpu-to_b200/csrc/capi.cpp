@@ -119,7 +119,6 @@ void gputo_default_options(gputo_options *o)
     o->coarse = GPUTO_COARSE_GALERKIN;
     o->fine_op = 0;
     o->nswp_fine = 0;
-    o->coarse_tail = 1;
 }
 
 int gputo_fine_op_constants(const double *Ke, double *c8)

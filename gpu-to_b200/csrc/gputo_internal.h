@@ -218,26 +218,6 @@ void launch_pad_mask(const Grid &g, const uint8_t *mask, uint8_t *maskp, cudaStr
 int init_fine_kernels();
 // Number of per-CTA partials a MODE_APPLY fine sweep writes.
 int fine_sweep_blocks(const Grid &g);
-// Persistent coarse-level V-cycle (kernels_mg.cu): the levels from lt down to
-// the coarsest and back in one cooperative launch, one phase per step.
-enum TailKind { TAIL_RESTRICT = 0, TAIL_SWEEP = 1, TAIL_GEMV_LOWER = 2, TAIL_GEMV_UPPER = 3, TAIL_PROLONG = 4 };
-struct TailPhase {
-    int kind, mode, l, pad;   // l: the level written
-    const void *in;           // restrict: level l-1 defect; sweep: u; gemv: f; prolong: level l+1 result
-    const void *f;            // sweep: the level's right-hand side
-    void *out;
-};
-struct TailLevels {
-    Lay lay[kMaxLevels];
-    const void *A[kMaxLevels];
-    const void *rdiag[kMaxLevels];
-    const uint8_t *mask[kMaxLevels];
-};
-constexpr int kMaxTailPhases = 512;
-template <typename T>
-int launch_coarse_tail(const TailLevels &tl, const TailPhase *ph, int nph, T omega, T prerelax, const double *Linv,
-                       const double *LinvT, double *ctmp, unsigned *bar, int *err, const int *done, cudaStream_t st);
-
 // Coarse level (packed element matrices, natural element order).
 template <typename T>
 // The coarse-level sweeps take rdiag = 1/diag (LevelBuf::rdiag).

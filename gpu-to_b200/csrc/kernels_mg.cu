@@ -11,7 +11,6 @@
 #include <algorithm>
 
 #include "gputo_internal.h"
-#include "tma.h"
 
 namespace gputo {
 
@@ -1126,154 +1125,5 @@ void launch_mask_restrict(const Grid &gc, const uint8_t *maskf, uint8_t *maskc, 
     count_launches(1);
 }
 
-
-// ---------------------------------------------------------------------------
-// persistent coarse-level V-cycle
-// ---------------------------------------------------------------------------
-
-// Grid-wide barrier of a kernel whose CTAs are all resident (a cooperative
-// launch): arrival count and generation in bar[0], bar[1].  The wait is
-// bounded (1 s of the global timer); on timeout it sets err and goes on, so
-// the kernel ends and the host reads GPUTO_ERR_TIMEOUT.
-__device__ __forceinline__ void tail_barrier(unsigned *bar, unsigned nblocks, int *err)
-{
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned *gen = bar + 1;
-        const unsigned g0 = *gen;
-        __threadfence();   // this CTA's results before its arrival
-        if (atomicAdd(bar, 1u) == nblocks - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            const uint64_t t0 = globaltimer_ns();
-            while (*gen == g0) {
-                __nanosleep(64);
-                if (globaltimer_ns() - t0 > 1000000000ull) {
-                    atomicExch(err, GPUTO_ERR_TIMEOUT);
-                    break;
-                }
-            }
-        }
-        __threadfence();
-    }
-    __syncthreads();
-}
-
-// The levels lt .. nl-1 of a V-cycle in one launch: every restriction,
-// slot sweep, the coarsest solve's two products and every prolongation is
-// a phase over all CTAs, phases separated by the grid barrier.  Each phase
-// runs the same device code as the separate kernels (slot_sweep_block,
-// restrict_node, prolong_node, gemv_row), so results are bit for bit those
-// of the launch-per-step schedule; what goes is about 20 launches and their
-// gaps per V-cycle on levels of a few thousand nodes.
-template <typename T>
-__global__ void __launch_bounds__(256, 2)
-coarse_tail_kernel(TailLevels tl, const TailPhase *__restrict__ ph, int nph, T omega, T prerelax,
-                   const double *__restrict__ Linv, const double *__restrict__ LinvT, double *__restrict__ ctmp,
-                   unsigned *bar, int *err, const int *__restrict__ done)
-{
-    if (done && *done) return;   // written before this launch: the same for every CTA
-    __shared__ T part[8][32][3];
-    const unsigned nblocks = gridDim.x;
-    const int lane = threadIdx.x & 31;
-    for (int p = 0; p < nph; ++p) {
-        const TailPhase P = ph[p];
-        const Lay L = tl.lay[P.l];
-        if (P.kind == TAIL_RESTRICT) {
-            const Lay Lf = tl.lay[P.l - 1];
-            for (long long n = blockIdx.x * 256LL + threadIdx.x; n < L.g.nnod(); n += 256LL * nblocks) {
-                int i, j, k;
-                node_ijk(L.g, n, i, j, k);
-                restrict_node<T>(L, Lf, (const T *)P.in, tl.mask[P.l], (T *)P.out, i, j, k);
-            }
-        } else if (P.kind == TAIL_PROLONG) {
-            const Lay Lc = tl.lay[P.l + 1];
-            for (long long n = blockIdx.x * 256LL + threadIdx.x; n < L.g.nnod(); n += 256LL * nblocks) {
-                int i, j, k;
-                node_ijk(L.g, n, i, j, k);
-                prolong_node<T>(L, Lc, (const T *)P.in, tl.mask[P.l], (T *)P.out, i, j, k);
-            }
-        } else if (P.kind == TAIL_SWEEP) {
-            const long long nvb = (L.g.nnod() + 31) / 32;
-            const T *A = (const T *)tl.A[P.l], *rd = (const T *)tl.rdiag[P.l];
-            const T *u = (const T *)P.in, *f = (const T *)P.f;
-            T *out = (T *)P.out;
-            for (long long vb = blockIdx.x; vb < nvb; vb += nblocks) {
-                switch (P.mode) {
-                case MODE_APPLY:
-                    slot_sweep_block<T, MODE_APPLY>(L, A, u, f, rd, tl.mask[P.l], out, omega, prerelax, vb, part);
-                    break;
-                case MODE_DEFECT:
-                    slot_sweep_block<T, MODE_DEFECT>(L, A, u, f, rd, tl.mask[P.l], out, omega, prerelax, vb, part);
-                    break;
-                case MODE_JACOBI:
-                    slot_sweep_block<T, MODE_JACOBI>(L, A, u, f, rd, tl.mask[P.l], out, omega, prerelax, vb, part);
-                    break;
-                default:
-                    slot_sweep_block<T, MODE_JACOBI_PRE>(L, A, u, f, rd, tl.mask[P.l], out, omega, prerelax, vb,
-                                                         part);
-                }
-            }
-        } else {   // the coarsest solve: tmp = Linv f, then u = Linv' tmp (warp per row)
-            const int n = (int)L.g.ndof();
-            for (int row = blockIdx.x * 8 + (threadIdx.x >> 5); row < n; row += nblocks * 8) {
-                if (P.kind == TAIL_GEMV_LOWER)
-                    gemv_row<T, double>(L, Linv, (const T *)P.in, ctmp, 1, 1, 0, row, lane);
-                else
-                    gemv_row<double, T>(L, LinvT, ctmp, (T *)P.out, 0, 0, 1, row, lane);
-            }
-        }
-        if (p + 1 < nph) tail_barrier(bar, nblocks, err);
-    }
-}
-
-template <typename T>
-int tail_blocks()
-{
-    static int cache[2][64] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    int &c = cache[sizeof(T) == 8][dev < 64 ? dev : 63];
-    if (c == 0) {
-        int per_sm = 0, sms = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, coarse_tail_kernel<T>, 256, 0) != cudaSuccess ||
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
-            cudaGetLastError();
-            return 0;
-        }
-        c = std::min(per_sm, 2) * sms;
-    }
-    return c;
-}
-
-template <typename T>
-int launch_coarse_tail(const TailLevels &tl, const TailPhase *ph, int nph, T omega, T prerelax, const double *Linv,
-                       const double *LinvT, double *ctmp, unsigned *bar, int *err, const int *done, cudaStream_t st)
-{
-    const int nb = tail_blocks<T>();
-    if (nb <= 0) {
-        set_error("the persistent coarse-level kernel has no resident CTAs");
-        return GPUTO_ERR_CUDA;
-    }
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)nb);
-    cfg.blockDim = dim3(256);
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeCooperative;   // all CTAs resident: the grid barrier is safe
-    attr[0].val.cooperative = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    GPUTO_CUDA(cudaLaunchKernelEx(&cfg, coarse_tail_kernel<T>, tl, ph, nph, omega, prerelax, Linv, LinvT, ctmp, bar,
-                                  err, done));
-    count_launches(1);
-    return GPUTO_OK;
-}
-template int launch_coarse_tail<float>(const TailLevels &, const TailPhase *, int, float, float, const double *,
-                                       const double *, double *, unsigned *, int *, const int *, cudaStream_t);
-template int launch_coarse_tail<double>(const TailLevels &, const TailPhase *, int, double, double, const double *,
-                                        const double *, double *, unsigned *, int *, const int *, cudaStream_t);
 
 }  // namespace gputo

@@ -185,90 +185,12 @@ int Solver::create(int nelx, int nely, int nelz, int nl_, const gputo_options *o
     ALLOC(ticket, 4);
     ALLOC(sc, 1);
     ALLOC(e2, 2);
-    ALLOC(tail_bar, 2);
-    ALLOC(tail_ph[0], kMaxTailPhases);
-    ALLOC(tail_ph[1], kMaxTailPhases);
     ALLOC(info, 4);
     ALLOC(err, 4);
     ALLOC(fixed_dev, 1);
     GPUTO_CUDA(cudaMallocHost((void **)&h_sc, sizeof(PcgScalars)));
     GPUTO_CUDA(cudaStreamSynchronize(own_stream));
-    return build_tails();
-}
-
-// Phases of the persistent coarse-level kernel: the schedule of vcycle_impl
-// for the levels lt .. nl-1, lt the first level on the slot sweeps (below
-// 65,536 nodes, packed Galerkin matrices, not the matrix-free level 1).
-template <typename T>
-int Solver::build_tail(LevelBuf<T> *Lv, int which)
-{
-    tail_n[which] = 0;
-    tail_lt[which] = nl;
-    if (redisc() || !opt.coarse_tail || nl < 2) return GPUTO_OK;
-    int lt = -1;
-    for (int l = nl - 1; l >= 1; --l) {
-        const bool slot = l == nl - 1 ||
-                          (!(l == 1 && quad_level1()) && !Lv[l].yq && Lv[l].Apk && g[l].nnod() < 65536);
-        if (!slot) break;
-        lt = l;
-    }
-    if (lt < 1) return GPUTO_OK;
-    auto bufs = [&](int l, int w) -> T * { return w ? Lv[l].u1 : Lv[l].u0; };
-    std::vector<TailPhase> ph;
-    auto add = [&](int kind, int mode, int l, const void *in, const void *f, void *out) {
-        TailPhase p{};
-        p.kind = kind;
-        p.mode = mode;
-        p.l = l;
-        p.in = in;
-        p.f = f;
-        p.out = out;
-        ph.push_back(p);
-    };
-    for (int l = lt; l < nl - 1; ++l) {
-        const int ns = sweeps(l);
-        add(TAIL_RESTRICT, 0, l, Lv[l - 1].r, nullptr, Lv[l].f);
-        if (ns == 0) {
-            add(TAIL_SWEEP, MODE_JACOBI_PRE, l, nullptr, Lv[l].f, bufs(l, 1));
-        } else {
-            for (int s2 = 0; s2 < ns; ++s2)
-                add(TAIL_SWEEP, s2 == 0 ? MODE_JACOBI_PRE : MODE_JACOBI, l, s2 == 0 ? nullptr : bufs(l, (s2 - 1) & 1),
-                    Lv[l].f, bufs(l, s2 & 1));
-        }
-        add(TAIL_SWEEP, MODE_DEFECT, l, ns == 0 ? bufs(l, 1) : bufs(l, (ns - 1) & 1), Lv[l].f, Lv[l].r);
-    }
-    const int c = nl - 1;
-    add(TAIL_RESTRICT, 0, c, Lv[c - 1].r, nullptr, Lv[c].f);
-    add(TAIL_GEMV_LOWER, 0, c, Lv[c].f, nullptr, nullptr);
-    add(TAIL_GEMV_UPPER, 0, c, nullptr, nullptr, bufs(c, 1));
-    for (int l = nl - 2; l >= lt; --l) {
-        const int ns = sweeps(l);
-        int cur = (ns == 0) ? 1 : ((ns - 1) & 1);
-        add(TAIL_PROLONG, 0, l, bufs(l + 1, 1), nullptr, bufs(l, cur));
-        for (int s2 = 0; s2 < ns; ++s2) {
-            add(TAIL_SWEEP, MODE_JACOBI, l, bufs(l, cur), Lv[l].f, bufs(l, cur ^ 1));
-            cur ^= 1;
-        }
-    }
-    if ((int)ph.size() > kMaxTailPhases) return GPUTO_OK;   // launch per step instead
-    TailLevels &tl = tail_lv[which];
-    for (int l = 0; l < nl; ++l) {
-        tl.lay[l] = lay[l];
-        tl.A[l] = Lv[l].Apk;
-        tl.rdiag[l] = Lv[l].rdiag;
-        tl.mask[l] = mask[l];
-    }
-    GPUTO_CUDA(cudaMemcpy(tail_ph[which], ph.data(), sizeof(TailPhase) * ph.size(), cudaMemcpyHostToDevice));
-    tail_n[which] = (int)ph.size();
-    tail_lt[which] = lt;
     return GPUTO_OK;
-}
-
-int Solver::build_tails()
-{
-    int s = build_tail<double>(L, 1);
-    if (!s && opt.precision == GPUTO_PREC_MIXED) s = build_tail<float>(Lf, 0);
-    return s;
 }
 
 int Solver::set_problem(const double *Ke0, const double *fixed1b, int nfd, cudaStream_t st)
@@ -336,10 +258,9 @@ int Solver::check_error_flags(cudaStream_t st)
     GPUTO_CUDA(cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st));
     GPUTO_CUDA(cudaStreamSynchronize(st));
     if (h_err) {
-        set_error(h_err == GPUTO_ERR_TIMEOUT ? "a bounded device wait (a TMA tile load or a grid barrier) gave up"
+        set_error(h_err == GPUTO_ERR_TIMEOUT ? "a bounded wait for a TMA tile load gave up"
                                              : "a fine sweep found its shared memory misaligned for TMA");
         cudaMemsetAsync(err, 0, sizeof(int), st);
-        if (tail_bar) cudaMemsetAsync(tail_bar, 0, 2 * sizeof(unsigned), st);
         return h_err;
     }
     return GPUTO_OK;
@@ -450,14 +371,7 @@ void Solver::vcycle_impl(LevelBuf<T> *Lv, const T *CXl, const T *r0, T *z0, cons
         if (l == 0) return which ? z0 : Lv[0].u0;
         return which ? Lv[l].u1 : Lv[l].u0;
     };
-    const int which = std::is_same<T, float>::value ? 0 : 1;
-    const int lt = (tail_ok && tail_n[which] > 0) ? tail_lt[which] : nl;   // levels >= lt: one persistent launch
     for (int l = 0; l < nl; ++l) {
-        if (l == lt) {
-            note(launch_coarse_tail<T>(tail_lv[which], tail_ph[which], tail_n[which], om, pr, Linv, LinvT, ctmp,
-                                       tail_bar, err, done, st));
-            break;
-        }
         const int ns = sweeps(l);
         const T *f = (l == 0) ? r0 : Lv[l].f;
         if (l > 0) launch_restrict<T>(lay[l], lay[l - 1], Lv[l - 1].r, mask[l], Lv[l].f, done, st);
@@ -475,7 +389,7 @@ void Solver::vcycle_impl(LevelBuf<T> *Lv, const T *CXl, const T *r0, T *z0, cons
             launch_coarse_solve<T>(lay[l], Linv, LinvT, f, bufs(l, 1), ctmp, done, st);
         }
     }
-    for (int l = std::min(nl - 2, lt - 1); l >= 0; --l) {
+    for (int l = nl - 2; l >= 0; --l) {
         const int ns = sweeps(l);
         const T *f = (l == 0) ? r0 : Lv[l].f;
         int cur = (ns == 0) ? 1 : ((ns - 1) & 1);
@@ -791,13 +705,11 @@ int Solver::set_tunables(const gputo_options &o)
     opt.tc_parts = o.tc_parts;
     opt.tc_xchunk = o.tc_xchunk;
     opt.fine_op = o.fine_op;
-    opt.coarse_tail = o.coarse_tail;
     if (graph_exec) {
         cudaGraphExecDestroy(graph_exec);
         graph_exec = nullptr;
     }
-    cudaStreamSynchronize(own_stream);
-    return build_tails();
+    return GPUTO_OK;
 }
 
 // The PCG iteration captured once into a CUDA graph (all pointers are

@@ -51,18 +51,6 @@ struct Solver {
     double *e2 = nullptr;         // (|F - K U|^2, compliance) of energy()
     int launch_status = GPUTO_OK;   // first failure seen while enqueuing kernels
 
-    // persistent coarse-level V-cycle, per hierarchy (0: FP32, 1: FP64)
-    TailPhase *tail_ph[2]{};
-    int tail_n[2]{}, tail_lt[2]{kMaxLevels, kMaxLevels};
-    TailLevels tail_lv[2]{};
-    unsigned *tail_bar = nullptr;
-    // false while a batch runs this solver beside others on concurrent
-    // streams: a grid barrier needs all of its CTAs resident at once
-    bool tail_ok = true;
-    template <typename T>
-    int build_tail(LevelBuf<T> *Lv, int which);
-    int build_tails();
-
     cudaGraphExec_t graph_exec = nullptr;
     cudaStream_t graph_stream = nullptr;
 

@@ -93,9 +93,6 @@ typedef struct {
                             only (0 = nswp, the reference's schedule); the
                             autotuner may pick fewer there, where a sweep costs
                             most                                                  */
-    int coarse_tail;     /* 1: the levels below 65,536 nodes (and the coarsest
-                            solve) run as one persistent kernel per V-cycle,
-                            same results bit for bit; 0: one launch per step  */
 } gputo_options;
 
 void gputo_default_options(gputo_options *opt);
