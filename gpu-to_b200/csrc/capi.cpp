@@ -119,6 +119,7 @@ void gputo_default_options(gputo_options *o)
     o->coarse = GPUTO_COARSE_GALERKIN;
     o->fine_op = 0;
     o->nswp_fine = 0;
+    o->fuse_prolong = 0;
 }
 
 int gputo_fine_op_constants(const double *Ke, double *c8)

@@ -149,6 +149,11 @@ constexpr int MODE_JACOBI_DOT = 4;
 // |f - K u|^2 over the free dofs and sum CX_e u_e' Ke u_e, and ce_e (dc_e =
 // dsK_e ce_e) written once per element.
 constexpr int MODE_ENERGY = 5;
+// The first damped-Jacobi sweep after a coarse-grid correction: u = u_pre +
+// P e_c (trilinear prolongation, fixed dofs zeroed) is formed in the sweep's
+// own node-plane tiles, so the prolongation pass and its write and re-read
+// of u disappear (Hadamard-basis kernel only; same results bit for bit).
+constexpr int MODE_JACOBI_PRO = 6;
 
 // Fine level (K = sum CX_e Ke), FP64 and FP32 instantiations; CX padded (ELay),
 // vectors padded (Lay).  'err' receives GPUTO_ERR_TIMEOUT if a bounded wait
@@ -198,11 +203,13 @@ template <typename T> bool hsweep_fits(const Grid &g);
 template <typename T> int hsweep_blocks(const Grid &g, int mode = MODE_APPLY);   // CTAs (= partials) of a sweep
 // rdiag: 1/diag (launch_recip); maskp: the Dirichlet bytes with rows padded
 // to 16 bytes (launch_pad_mask; hsweep_mask_bytes of storage).
+// MODE_JACOBI_PRO: uc is the coarse correction in the layout Lc (level 1).
 template <typename T>
 int launch_hsweep(int mode, const Lay &L, const ELay &E, const HadamardKe &hk, const T *CX, const T *u, const T *f,
                   const T *rdiag, const uint8_t *mask, const uint8_t *maskp, T *out, T omega, T prerelax,
                   double *dot_partial, const int *done, int *err, cudaStream_t st, const double *Rd = nullptr,
-                  const T *zo = nullptr);
+                  const T *zo = nullptr, const T *uc = nullptr, const Lay *Lc = nullptr);
+template <typename T> bool hsweep_pro_fits(const Grid &g);
 // MODE_ENERGY sweep (FP64): out (optional) = f - K u with fixed rows zero,
 // ce / dc in natural element order, partial pairs (|r|^2, sum CX ce) per CTA.
 bool hsweep_energy_fits(const Grid &g);

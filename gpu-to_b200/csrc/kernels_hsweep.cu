@@ -71,8 +71,9 @@ __host__ __device__ constexpr size_t al128(size_t x) { return (x + 127) & ~size_
 // 1/diag (Jacobi, pre-relaxation) at the node plane being finished.
 template <int MODE> struct HNeeds {
     static constexpr bool PRE = MODE == MODE_JACOBI_PRE;
+    static constexpr bool PRO = MODE == MODE_JACOBI_PRO;   // u = u_pre + P e_c formed in the face tiles
     static constexpr bool F = MODE != MODE_APPLY;   // MODE_ENERGY: the residual f - K u
-    static constexpr bool D = MODE == MODE_JACOBI || MODE == MODE_JACOBI_PRE || MODE == MODE_JACOBI_DOT;
+    static constexpr bool D = MODE == MODE_JACOBI || MODE == MODE_JACOBI_PRE || MODE == MODE_JACOBI_DOT || PRO;
     static constexpr bool DOT = MODE == MODE_JACOBI_DOT;   // also the FP64 residual and z_old tiles
 };
 
@@ -248,7 +249,8 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
               const T *__restrict__ rdiag, const uint8_t *__restrict__ mask, T *__restrict__ out, T omega,
               T prerelax, double *__restrict__ dot_partial, const int *__restrict__ done, int *__restrict__ err,
               const double *__restrict__ Rd, const T *__restrict__ zo, uint32_t wait_ns, int skip_stage,
-              double *__restrict__ ce, double *__restrict__ dcv, const double *__restrict__ dsK)
+              double *__restrict__ ce, double *__restrict__ dcv, const double *__restrict__ dsK,
+              const T *__restrict__ ucoarse, Lay Lc)
 {
     if (done && *done) return;   // the same value for every CTA of the cluster
     using N = HNeeds<MODE>;
@@ -341,6 +343,42 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
                     U[(cy * 2 + cz) * 4 + d] = v;
                 }
     };
+    // MODE_JACOBI_PRO: add the prolonged coarse correction to the u tile of
+    // ring stage s (node plane E0 + s) in place, as prolong_node does it
+    // (same taps, same order), with the fixed dofs zeroed; a barrier follows.
+    auto prolong_tile = [&](int s) {
+        T *su = reinterpret_cast<T *>(smem + (s % HRING) * S::slot);
+        const int p = E0 + s;
+        const T *c0p = ucoarse + Lc.row(p >> 1, 0);
+        const long long si = (long long)(Lc.g.nz + 1) * Lc.pitch, sk = Lc.pitch;
+        const int ni = (p & 1) + 1;
+        for (int idx = tid; idx < (WZ + 1) * (HY + 1); idx += NT) {
+            const int zz = idx / (HY + 1), jj = idx - zz * (HY + 1);
+            const int j = jc0 + jj, k = kc0 + zz;
+            if (j > g.ny || k > g.nz) continue;
+            const int nj = (j & 1) + 1, nk = (k & 1) + 1;
+            T acc[3] = {T(0), T(0), T(0)};
+            const T *c0 = c0p + (long long)(k >> 1) * sk + 3 * (j >> 1);
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    const T *cr = c0 + ((a && a < ni) ? si : 0) + ((c && c < nk) ? sk : 0);
+#pragma unroll
+                    for (int b = 0; b < 2; ++b) {
+                        const bool ok = a < ni && c < nk && b < nj;
+                        const int off = (b < nj) ? 3 * b : 0;
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) acc[d] += ok ? cr[off + d] : T(0);
+                    }
+                }
+            const T wgt = T(1) / T(ni * nj * nk);
+            const unsigned m = mask[g.node(p, j, k)];
+            T *v = su + zz * HUW + 3 * jj;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) v[d] = ((m >> d) & 1u) ? T(0) : fma(wgt, acc[d], v[d]);
+        }
+    };
     double dsum = 0.0, dsum2 = 0.0;
     // Corner partials P of node plane p -> y sums through the warp, z partner
     // values into the exchange buffer (read after the next barrier).
@@ -405,6 +443,10 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
     auto step = [&](int t, T (&Uc)[HF], T (&Fc)[HF], T (&Ac)[HF], T (&Un)[HF], T (&Fn)[HF], T (&An)[HF]) {
         cur = t;
         wait_stage(t);
+        if constexpr (N::PRO) {
+            if (!bad) prolong_tile(t);
+            __syncthreads();
+        }
         load_face(t, Un);
 #pragma unroll
         for (int q = 0; q < HF; ++q)
@@ -448,6 +490,10 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
 
     T U0[HF], F0[HF], A0[HF], U1[HF], F1[HF], A1[HF];
     wait_stage(0);
+    if constexpr (N::PRO) {
+        if (!bad) prolong_tile(0);
+        __syncthreads();
+    }
     load_face(0, U0);
 #pragma unroll
     for (int q = 0; q < HF; ++q) {
@@ -567,7 +613,7 @@ SweepFaultHook sweep_fault_hook()
 
 struct HState {
     bool init = false, ok = false;
-    int resident[2][6][HMAXCY + 1] = {};   // [FP64?][mode][cluster size]: clusters resident on the device
+    int resident[2][7][HMAXCY + 1] = {};   // [FP64?][mode][cluster size]: clusters resident on the device
 };
 
 HState &hstate(int dev)
@@ -615,7 +661,8 @@ template <typename T, int MODE>
 int hlaunch(const Lay &L, const ELay &E, const HadamardKe &hk, const T *CX, const T *u, const T *f, const T *rdiag,
             const uint8_t *mask, const uint8_t *maskp, T *out, T omega, T prerelax, double *dot_partial,
             const int *done, int *err, cudaStream_t st, const double *Rd = nullptr, const T *zo = nullptr,
-            double *ce = nullptr, double *dcv = nullptr, const double *dsK = nullptr)
+            double *ce = nullptr, double *dcv = nullptr, const double *dsK = nullptr, const T *uc = nullptr,
+            const Lay *Lc = nullptr)
 {
     constexpr int WZ = hwz<T>();
     using N = HNeeds<MODE>;
@@ -664,7 +711,7 @@ int hlaunch(const Lay &L, const ELay &E, const HadamardKe &hk, const T *CX, cons
     const SweepFaultHook hook = sweep_fault_hook();
     GPUTO_CUDA(cudaLaunchKernelEx(&cfg, hsweep_kernel<T, MODE, WZ>, mu, md, mf, mc, mm, mr, mz, L, hc, htx, f, rdiag, mask,
                                   out, omega, prerelax, dot_partial, done, err, Rd, zo, hook.wait_ns, hook.skip_stage,
-                                  ce, dcv, dsK));
+                                  ce, dcv, dsK, uc, Lc ? *Lc : L));
     count_launches(1);
     return GPUTO_OK;
 }
@@ -687,6 +734,7 @@ cudaError_t hset_attrs()
         if ((e = hset_attr<T, MODE_JACOBI_DOT>()) != cudaSuccess) return e;
     if constexpr (sizeof(T) == 8)
         if ((e = hset_attr<T, MODE_ENERGY>()) != cudaSuccess) return e;
+    if ((e = hset_attr<T, MODE_JACOBI_PRO>()) != cudaSuccess) return e;
     return hset_attr<T, MODE_JACOBI_PRE>();
 }
 
@@ -722,6 +770,7 @@ void hresident_all(HState &s, int cy)
     s.resident[p][MODE_JACOBI_PRE][cy] = hresident<T, MODE_JACOBI_PRE>(cy);
     if constexpr (sizeof(T) == 4) s.resident[p][MODE_JACOBI_DOT][cy] = hresident<T, MODE_JACOBI_DOT>(cy);
     if constexpr (sizeof(T) == 8) s.resident[p][MODE_ENERGY][cy] = hresident<T, MODE_ENERGY>(cy);
+    s.resident[p][MODE_JACOBI_PRO][cy] = hresident<T, MODE_JACOBI_PRO>(cy);
 }
 
 __global__ void pad_mask_kernel(Grid g, const uint8_t *__restrict__ mask, uint8_t *__restrict__ maskp, long long mp)
@@ -857,6 +906,16 @@ void launch_pad_mask(const Grid &g, const uint8_t *mask, uint8_t *maskp, cudaStr
     count_launches(1);
 }
 
+template <typename T>
+bool hsweep_pro_fits(const Grid &g)
+{
+    int dev = 0;
+    if (!hsweep_fits<T>(g) || cudaGetDevice(&dev) != cudaSuccess) return false;
+    return hstate(dev).resident[sizeof(T) == 8][MODE_JACOBI_PRO][(g.ny + HY - 1) / HY] > 0;
+}
+template bool hsweep_pro_fits<float>(const Grid &);
+template bool hsweep_pro_fits<double>(const Grid &);
+
 bool hsweep_energy_fits(const Grid &g)
 {
     int dev = 0;
@@ -914,9 +973,17 @@ void launch_sum_pairs(int nb, const double *partial, double *out2, cudaStream_t 
 template <typename T>
 int launch_hsweep(int mode, const Lay &L, const ELay &E, const HadamardKe &hk, const T *CX, const T *u, const T *f,
                   const T *rdiag, const uint8_t *mask, const uint8_t *maskp, T *out, T omega, T prerelax,
-                  double *dot_partial, const int *done, int *err, cudaStream_t st, const double *Rd, const T *zo)
+                  double *dot_partial, const int *done, int *err, cudaStream_t st, const double *Rd, const T *zo,
+                  const T *uc, const Lay *Lc)
 {
     switch (mode) {
+    case MODE_JACOBI_PRO:
+        if (!uc || !Lc || Lc->g.nx * 2 != L.g.nx || Lc->g.ny * 2 != L.g.ny || Lc->g.nz * 2 != L.g.nz) {
+            set_error("a Jacobi sweep with the prolongation needs the coarse correction and its layout");
+            return GPUTO_ERR_ARG;
+        }
+        return hlaunch<T, MODE_JACOBI_PRO>(L, E, hk, CX, u, f, rdiag, mask, maskp, out, omega, prerelax, nullptr,
+                                           done, err, st, nullptr, nullptr, nullptr, nullptr, nullptr, uc, Lc);
     case MODE_JACOBI_DOT:
         if constexpr (sizeof(T) == 4) {
             if (!Rd || !zo || !dot_partial) {
@@ -949,10 +1016,11 @@ template int hsweep_blocks<float>(const Grid &, int);
 template int hsweep_blocks<double>(const Grid &, int);
 template int launch_hsweep<float>(int, const Lay &, const ELay &, const HadamardKe &, const float *, const float *,
                                   const float *, const float *, const uint8_t *, const uint8_t *, float *, float,
-                                  float, double *, const int *, int *, cudaStream_t, const double *, const float *);
+                                  float, double *, const int *, int *, cudaStream_t, const double *, const float *,
+                                  const float *, const Lay *);
 template int launch_hsweep<double>(int, const Lay &, const ELay &, const HadamardKe &, const double *,
                                    const double *, const double *, const double *, const uint8_t *,
                                    const uint8_t *, double *, double, double, double *, const int *, int *,
-                                   cudaStream_t, const double *, const double *);
+                                   cudaStream_t, const double *, const double *, const double *, const Lay *);
 
 }  // namespace gputo

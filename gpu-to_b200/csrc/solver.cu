@@ -393,11 +393,18 @@ void Solver::vcycle_impl(LevelBuf<T> *Lv, const T *CXl, const T *r0, T *z0, cons
         const int ns = sweeps(l);
         const T *f = (l == 0) ? r0 : Lv[l].f;
         int cur = (ns == 0) ? 1 : ((ns - 1) & 1);
-        launch_prolong_add<T>(lay[l], lay[l + 1], bufs(l + 1, 1), mask[l], bufs(l, cur), done, st);
+        // the fine level's first post-smoothing sweep forms u + P e_c itself
+        bool pro = opt.fuse_prolong && l == 0 && ns >= 1 && !(ns == 1 && dotR) && use_hsweep<T>(g[0]) &&
+                   Lv[0].rdiag && hsweep_pro_fits<T>(g[0]);
+        if constexpr (std::is_same<T, float>::value) pro = pro && opt.tc_parts == 0;
+        if (!pro) launch_prolong_add<T>(lay[l], lay[l + 1], bufs(l + 1, 1), mask[l], bufs(l, cur), done, st);
         for (int s = 0; s < ns; ++s) {
             if (l == 0 && s == ns - 1 && dotR)   // the last sweep also sums r'z and r'z_old
                 note(fine_sweep<T>(0, MODE_JACOBI_DOT, lay[0], elay, CXl, bufs(0, cur), f, Lv[0], bufs(0, cur ^ 1), om,
                                    pr, dotPartial, done, st, dotR, dotZold));
+            else if (pro && s == 0)
+                note(fine_sweep<T>(0, MODE_JACOBI_PRO, lay[0], elay, CXl, bufs(0, cur), f, Lv[0], bufs(0, cur ^ 1), om,
+                                   pr, nullptr, done, st, nullptr, nullptr, bufs(1, 1), &lay[1]));
             else
                 sweep(l, MODE_JACOBI, bufs(l, cur), f, bufs(l, cur ^ 1), om);
             cur ^= 1;
@@ -698,6 +705,7 @@ int Solver::set_tunables(const gputo_options &o)
     }
     opt.nswp = o.nswp;
     opt.nswp_fine = o.nswp_fine;
+    opt.fuse_prolong = o.fuse_prolong;
     opt.omega = o.omega;
     opt.prerelax = o.prerelax;
     opt.check_every = o.check_every;

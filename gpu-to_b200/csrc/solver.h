@@ -101,11 +101,12 @@ struct Solver {
     template <typename T>
     int fine_sweep(int l, int mode, const Lay &Lo, const ELay &E, const T *CXl, const T *u, const T *f,
                    const LevelBuf<T> &B, T *out, T omega, T pr, double *dot_partial, const int *done,
-                   cudaStream_t st, const double *Rd = nullptr, const T *zo = nullptr) const
+                   cudaStream_t st, const double *Rd = nullptr, const T *zo = nullptr, const T *uc = nullptr,
+                   const Lay *Lc = nullptr) const
     {
         if (use_hsweep<T>(Lo.g) && B.rdiag)
             return launch_hsweep<T>(mode, Lo, E, hk, CXl, u, f, B.rdiag, mask[l], maskp[l], out, omega, pr,
-                                    dot_partial, done, err, st, Rd, zo);
+                                    dot_partial, done, err, st, Rd, zo, uc, Lc);
         return launch_fine_sweep<T>(mode, Lo, E, CXl, u, f, B.diag, mask[l], out, omega, pr, dot_partial, done, err,
                                     st);
     }

@@ -93,6 +93,11 @@ typedef struct {
                             only (0 = nswp, the reference's schedule); the
                             autotuner may pick fewer there, where a sweep costs
                             most                                                  */
+    int fuse_prolong;    /* 1: the finest level's first post-smoothing sweep
+                            adds the prolonged coarse correction in its own
+                            tiles (Hadamard-basis sweep; same results bit for
+                            bit); 0 (default): a separate prolongation pass,
+                            measured faster                                      */
 } gputo_options;
 
 void gputo_default_options(gputo_options *opt);

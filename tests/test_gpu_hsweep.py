@@ -149,3 +149,24 @@ def test_energy_fused_into_the_apply_matches_the_separate_pass(oracle, gputo, to
     tr_ref = float(torch.linalg.norm(F - KU) / torch.linalg.norm(F))
     assert abs(tr - tr_ref) <= 1e-6 * tr_ref, (tr, tr_ref)
     assert tr < 1e-7
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("shape,nl", [((68, 64, 20), 3), ((16, 8, 8), 2)])
+def test_prolongation_fused_into_the_first_post_sweep_is_bit_identical(oracle, gputo, torch, prec, shape, nl):
+    """fuse_prolong = 1: the finest level's first post-smoothing sweep adds
+    P e_c to its own node-plane tiles; the V-cycle must equal the one with the
+    separate prolongation pass bit for bit (same taps, same order)."""
+    p = oracle.cantilever(*shape)
+    rng = np.random.default_rng(8)
+    CX = oracle.simp(oracle.random_density(*shape, seed=5))[0]
+    r = rng.standard_normal(p.ndof)
+    r[p.fixed.astype(np.int64) - 1] = 0.0
+    precision = gputo.PREC_MIXED if prec == "mixed" else gputo.PREC_FP64
+    out = []
+    for fp in (0, 1):
+        s = _solver(gputo, p, CX, torch, nl=nl, precision=precision, fuse_prolong=fp)
+        z = torch.zeros(p.ndof, dtype=torch.float64, device="cuda")
+        s.vcycle(_dev(torch, r), z)
+        out.append(z)
+    assert torch.equal(out[0], out[1])
