@@ -63,6 +63,8 @@ constexpr int HM = 48;           // mask box width in bytes: HY + 1 = 33 nodes, 
 constexpr int HTX = 32;          // node planes per x chunk
 constexpr int HMAXP = HTX + 1;   // planes one chunk may finish (the last chunk also takes plane nx)
 constexpr int HMAXCY = 8;        // CTAs per cluster (portable limit): ny <= 256
+constexpr int HCZ = 6;           // MODE_JACOBI_PRO: coarse rows of a tile (fine rows kc0 .. kc0 + 8)
+constexpr int HCW = 52;          // ... and coarse values per row: 3 (HY / 2 + 1) = 51, rounded to 16 bytes
 constexpr uint32_t kHDrainNs = 1000000000u;   // wait for copies in flight before leaving after a failure
 
 __host__ __device__ constexpr size_t al128(size_t x) { return (x + 127) & ~size_t(127); }
@@ -98,9 +100,16 @@ struct HSmem {
     static constexpr size_t ez_off = er_off + (N::DOT ? al128(r_bytes) : 0);   // epilogue z_old
     static constexpr size_t c_off = ez_off + (N::DOT ? ua : 0);
     static constexpr size_t m_off = c_off + al128(c_bytes);
-    static constexpr size_t slot = al128(m_off + m_bytes);
+    // MODE_JACOBI_PRO: the coarse correction's node plane (E0 + s + 1) / 2 and
+    // the Dirichlet bits of face plane E0 + s (WZ + 1 rows)
+    static constexpr size_t co_bytes = sizeof(T) * HCZ * HCW;
+    static constexpr size_t mf_bytes = (size_t)(WZ + 1) * HM;
+    static constexpr size_t co_off = al128(m_off + m_bytes);
+    static constexpr size_t mf_off = co_off + (N::PRO ? al128(co_bytes) : 0);
+    static constexpr size_t slot = al128(mf_off + (N::PRO ? mf_bytes : 0));
     static constexpr int ZROW = HY + 1;                               // lanes + the seam column
-    static constexpr size_t z_off = HRING * slot;
+    static constexpr size_t x0_off = HRING * slot;                    // PRO: coarse plane E0 / 2 (odd E0)
+    static constexpr size_t z_off = x0_off + (N::PRO ? al128(co_bytes) : 0);
     static constexpr size_t z_bytes = sizeof(T) * 2 * WZ * ZROW * 3;
     static constexpr int SEAM = HMAXP * WZ * 3;
     static constexpr size_t s_off = al128(z_off + z_bytes);
@@ -109,7 +118,7 @@ struct HSmem {
     static constexpr size_t red_off = bar_off + 8 * HRING;            // per-warp dot partials (two per warp)
     static constexpr size_t bytes = red_off + 16 * WZ;
     static_assert(ua % 128 == 0 && c_off % 128 == 0 && m_off % 128 == 0 && slot % 128 == 0 && er_off % 128 == 0 &&
-                      ez_off % 128 == 0,
+                      ez_off % 128 == 0 && co_off % 128 == 0 && mf_off % 128 == 0 && x0_off % 128 == 0,
                   "TMA shared-memory destinations must be 128-byte aligned");
 };
 // Two CTAs of the FP32 Jacobi sweep with the PCG dots share an SM (228 KB,
@@ -295,6 +304,8 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
         const bool face = s <= nE, cxp = s >= 1 && s <= nE, epi = s >= 1 && E0 + s - 1 >= P0;
         uint32_t bytes = 0;
         if (face) bytes += (uint32_t)(S::u_bytes * (N::PRE ? 2 : 1));
+        if (face && N::PRO)
+            bytes += (uint32_t)(S::co_bytes * ((s == 0 && (E0 & 1)) ? 2 : 1) + S::mf_bytes);
         if (cxp) bytes += (uint32_t)S::c_bytes;
         if (epi) bytes += (uint32_t)(S::u_bytes * ((N::F ? 1 : 0) + (N::D ? 1 : 0) + (N::DOT ? 1 : 0)) + S::m_bytes +
                                      (N::DOT ? S::r_bytes : 0));
@@ -306,6 +317,11 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
         if (face) {
             tma_load_3d(sb, &tm_u, 3 * jc0, kc0, E0 + s, b);
             if (N::PRE) tma_load_3d(sb + S::d_off, &tm_d, 3 * jc0, kc0, E0 + s, b);
+            if (N::PRO) {   // tm_r: the coarse correction, tm_z: the Dirichlet bits, WZ + 1 rows
+                tma_load_3d(sb + S::co_off, &tm_r, 3 * (jc0 >> 1), kc0 >> 1, (E0 + s + 1) >> 1, b);
+                tma_load_3d(sb + S::mf_off, &tm_z, jc0, kc0, E0 + s, b);
+                if (s == 0 && (E0 & 1)) tma_load_3d(smem + S::x0_off, &tm_r, 3 * (jc0 >> 1), kc0 >> 1, E0 >> 1, b);
+            }
         }
         if (cxp) tma_load_3d(sb + S::c_off, &tm_c, jc0, kc0, E0 + s - 1, b);
         if (epi) {
@@ -344,26 +360,35 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
                 }
     };
     // MODE_JACOBI_PRO: add the prolonged coarse correction to the u tile of
-    // ring stage s (node plane E0 + s) in place, as prolong_node does it
-    // (same taps, same order), with the fixed dofs zeroed; a barrier follows.
+    // ring stage s (node plane p = E0 + s) in place, from the coarse tiles
+    // that came by TMA with the stage (plane p / 2 in slot s, for odd p plane
+    // (p - 1) / 2 in slot s - 1 or, at s = 0, the extra tile), with the same
+    // taps in the same order as prolong_node, the fixed dofs zeroed from the
+    // stage's own Dirichlet tile.  Tile t + 1 is corrected during step t,
+    // before the barrier that ends it, so no barrier of its own is needed
+    // (tile 0 before the first one).
     auto prolong_tile = [&](int s) {
-        T *su = reinterpret_cast<T *>(smem + (s % HRING) * S::slot);
-        const int p = E0 + s;
-        const T *c0p = ucoarse + Lc.row(p >> 1, 0);
-        const long long si = (long long)(Lc.g.nz + 1) * Lc.pitch, sk = Lc.pitch;
-        const int ni = (p & 1) + 1;
+        unsigned char *sb = smem + (s % HRING) * S::slot;
+        T *su = reinterpret_cast<T *>(sb);
+        const int p = E0 + s, ni = (p & 1) + 1;
+        const T *tb = reinterpret_cast<const T *>(sb + S::co_off);   // plane (p + 1) / 2
+        const T *ta = (p & 1) ? reinterpret_cast<const T *>(s == 0 ? smem + S::x0_off
+                                                                   : smem + ((s - 1) % HRING) * S::slot + S::co_off)
+                              : tb;                                     // plane p / 2
+        const uint8_t *mf = sb + S::mf_off;
+        const int K0 = kc0 >> 1, J0 = jc0 >> 1;
         for (int idx = tid; idx < (WZ + 1) * (HY + 1); idx += NT) {
             const int zz = idx / (HY + 1), jj = idx - zz * (HY + 1);
             const int j = jc0 + jj, k = kc0 + zz;
             if (j > g.ny || k > g.nz) continue;
             const int nj = (j & 1) + 1, nk = (k & 1) + 1;
             T acc[3] = {T(0), T(0), T(0)};
-            const T *c0 = c0p + (long long)(k >> 1) * sk + 3 * (j >> 1);
 #pragma unroll
             for (int a = 0; a < 2; ++a)
 #pragma unroll
                 for (int c = 0; c < 2; ++c) {
-                    const T *cr = c0 + ((a && a < ni) ? si : 0) + ((c && c < nk) ? sk : 0);
+                    const T *cr = (a && a < ni ? tb : ta) + ((k >> 1) - K0 + ((c && c < nk) ? 1 : 0)) * HCW +
+                                  3 * ((j >> 1) - J0);
 #pragma unroll
                     for (int b = 0; b < 2; ++b) {
                         const bool ok = a < ni && c < nk && b < nj;
@@ -373,7 +398,7 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
                     }
                 }
             const T wgt = T(1) / T(ni * nj * nk);
-            const unsigned m = mask[g.node(p, j, k)];
+            const unsigned m = mf[zz * HM + jj];
             T *v = su + zz * HUW + 3 * jj;
 #pragma unroll
             for (int d = 0; d < 3; ++d) v[d] = ((m >> d) & 1u) ? T(0) : fma(wgt, acc[d], v[d]);
@@ -443,11 +468,7 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
     auto step = [&](int t, T (&Uc)[HF], T (&Fc)[HF], T (&Ac)[HF], T (&Un)[HF], T (&Fn)[HF], T (&An)[HF]) {
         cur = t;
         wait_stage(t);
-        if constexpr (N::PRO) {
-            if (!bad) prolong_tile(t);
-            __syncthreads();
-        }
-        load_face(t, Un);
+        load_face(t, Un);   // MODE_JACOBI_PRO: tile t got its correction in step t - 1
 #pragma unroll
         for (int q = 0; q < HF; ++q)
             if ((q & 3) != 3) Fn[q] = Un[q];
@@ -473,6 +494,12 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
         if (out_plane) {
             face_h(Ac);   // node partials of plane p
             reduce_y(p, Ac, q0);
+        }
+        if constexpr (N::PRO) {   // the next face tile, before the barrier that publishes it
+            if (t + 1 <= nE) {
+                wait_stage(t + 1);
+                if (!bad) prolong_tile(t + 1);
+            }
         }
         fail = __syncthreads_or(bad);   // z partners visible; ring slot t - 1 free
         if (!fail && tid == 0 && t - 1 + HRING < nst) issue(t - 1 + HRING);
@@ -501,6 +528,12 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
         A0[q] = T(0);
     }
     face_h(F0);
+    if constexpr (N::PRO) {
+        if (1 <= nE) {
+            wait_stage(1);
+            if (!bad) prolong_tile(1);
+        }
+    }
     fail = __syncthreads_or(bad);
     if constexpr (sizeof(T) == 8) {   // FP64: one step per trip, the state copied back
         for (int t = 1; !fail && t <= nE; ++t) {
@@ -689,10 +722,20 @@ int hlaunch(const Lay &L, const ELay &E, const HadamardKe &hk, const T *CX, cons
     const uint64_t mp = hmask_pitch(g);
     if (!s)
         s = make_tmap_3d(&mm, maskp, 1, mp, (uint64_t)g.nz + 1, (uint64_t)g.nx + 1, mp, mp * (g.nz + 1), HM, WZ, 1);
+    // MODE_JACOBI_PRO: mr carries the coarse correction (level-1 layout, boxes
+    // of HCZ rows x HCW values) and mz the Dirichlet bits with WZ + 1 rows
+    if (!s && N::PRO) {
+        const uint64_t ces = sizeof(T);
+        s = make_tmap_3d(&mr, uc, (int)es, (uint64_t)Lc->pitch, (uint64_t)Lc->g.nz + 1, (uint64_t)Lc->g.nx + 1,
+                         Lc->pitch * ces, Lc->pitch * ces * (Lc->g.nz + 1), HCW, HCZ, 1);
+        if (!s)
+            s = make_tmap_3d(&mz, maskp, 1, mp, (uint64_t)g.nz + 1, (uint64_t)g.nx + 1, mp, mp * (g.nz + 1), HM,
+                             WZ + 1, 1);
+    }
     if (s) return s;
     if (!N::D) md = mu;
     if (!N::F) mf = mu;
-    if (!N::DOT) mr = mz = mu;
+    if (!N::DOT && !N::PRO) mr = mz = mu;
     const HC<T> hc = make_hc<T>(hk);
     const int htx = hchunk<T>(g, MODE);
     const dim3 grid = hgrid<T>(g, htx);
