@@ -187,12 +187,21 @@ int gputo_autotune_dev(gputo_solver *h, const double *F, double *U, double tol, 
         o.use_graph = 1;
         o.check_every = 8;
         o.tc_parts = 0;
+        o.sweep_xchunk = 0;
         cand.push_back(o);
         for (int nf = 1; nf < nswp; ++nf) {   // fewer sweeps on the finest level, where they cost most
             o.nswp_fine = nf;
             cand.push_back(o);
         }
+        if (nswp == 3)   // the fine sweeps' tile: node planes per CTA along x
+            for (int nf : {0, 1})
+                for (int xc : {16, 24}) {
+                    o.nswp_fine = nf;
+                    o.sweep_xchunk = xc;
+                    cand.push_back(o);
+                }
         o.nswp_fine = 0;
+        o.sweep_xchunk = 0;
         if (s.opt.precision == GPUTO_PREC_MIXED)
             for (int xc : {8, 16}) {
                 o.tc_parts = 2;

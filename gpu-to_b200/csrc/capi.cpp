@@ -120,6 +120,7 @@ void gputo_default_options(gputo_options *o)
     o->fine_op = 0;
     o->nswp_fine = 0;
     o->fuse_prolong = 0;
+    o->sweep_xchunk = 0;
 }
 
 int gputo_fine_op_constants(const double *Ke, double *c8)

@@ -682,6 +682,16 @@ int hchunk(const Grid &g, int mode)
     return bh;
 }
 
+// The x chunk of a launch: the caller's choice (an autotuned option, clamped
+// to 1 .. HTX planes) or the heuristic above.
+template <typename T>
+int hsweep_chunk(const Grid &g, int mode, int xchunk)
+{
+    if (xchunk <= 0) return hchunk<T>(g, mode);
+    int c = xchunk < HTX ? xchunk : HTX;
+    return c < g.nx ? c : (g.nx > 0 ? g.nx : 1);
+}
+
 template <typename T>
 dim3 hgrid(const Grid &g, int htx)
 {
@@ -695,7 +705,7 @@ int hlaunch(const Lay &L, const ELay &E, const HadamardKe &hk, const T *CX, cons
             const uint8_t *mask, const uint8_t *maskp, T *out, T omega, T prerelax, double *dot_partial,
             const int *done, int *err, cudaStream_t st, const double *Rd = nullptr, const T *zo = nullptr,
             double *ce = nullptr, double *dcv = nullptr, const double *dsK = nullptr, const T *uc = nullptr,
-            const Lay *Lc = nullptr)
+            const Lay *Lc = nullptr, int xchunk = 0)
 {
     constexpr int WZ = hwz<T>();
     using N = HNeeds<MODE>;
@@ -737,7 +747,7 @@ int hlaunch(const Lay &L, const ELay &E, const HadamardKe &hk, const T *CX, cons
     if (!N::F) mf = mu;
     if (!N::DOT && !N::PRO) mr = mz = mu;
     const HC<T> hc = make_hc<T>(hk);
-    const int htx = hchunk<T>(g, MODE);
+    const int htx = hsweep_chunk<T>(g, MODE, xchunk);
     const dim3 grid = hgrid<T>(g, htx);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
@@ -935,9 +945,9 @@ bool hsweep_fits(const Grid &g)
 }
 
 template <typename T>
-int hsweep_blocks(const Grid &g, int mode)
+int hsweep_blocks(const Grid &g, int mode, int xchunk)
 {
-    const dim3 gr = hgrid<T>(g, hchunk<T>(g, mode));
+    const dim3 gr = hgrid<T>(g, hsweep_chunk<T>(g, mode, xchunk));
     return (int)(gr.x * gr.y * gr.z);
 }
 
@@ -1017,7 +1027,7 @@ template <typename T>
 int launch_hsweep(int mode, const Lay &L, const ELay &E, const HadamardKe &hk, const T *CX, const T *u, const T *f,
                   const T *rdiag, const uint8_t *mask, const uint8_t *maskp, T *out, T omega, T prerelax,
                   double *dot_partial, const int *done, int *err, cudaStream_t st, const double *Rd, const T *zo,
-                  const T *uc, const Lay *Lc)
+                  const T *uc, const Lay *Lc, int xchunk)
 {
     switch (mode) {
     case MODE_JACOBI_PRO:
@@ -1026,7 +1036,7 @@ int launch_hsweep(int mode, const Lay &L, const ELay &E, const HadamardKe &hk, c
             return GPUTO_ERR_ARG;
         }
         return hlaunch<T, MODE_JACOBI_PRO>(L, E, hk, CX, u, f, rdiag, mask, maskp, out, omega, prerelax, nullptr,
-                                           done, err, st, nullptr, nullptr, nullptr, nullptr, nullptr, uc, Lc);
+                                           done, err, st, nullptr, nullptr, nullptr, nullptr, nullptr, uc, Lc, xchunk);
     case MODE_JACOBI_DOT:
         if constexpr (sizeof(T) == 4) {
             if (!Rd || !zo || !dot_partial) {
@@ -1034,36 +1044,38 @@ int launch_hsweep(int mode, const Lay &L, const ELay &E, const HadamardKe &hk, c
                 return GPUTO_ERR_ARG;
             }
             return hlaunch<T, MODE_JACOBI_DOT>(L, E, hk, CX, u, f, rdiag, mask, maskp, out, omega, prerelax,
-                                               dot_partial, done, err, st, Rd, zo);
+                                               dot_partial, done, err, st, Rd, zo, nullptr, nullptr, nullptr, nullptr,
+                                               nullptr, xchunk);
         }
         set_error("the Jacobi sweep with dots is FP32 only");
         return GPUTO_ERR_ARG;
     case MODE_APPLY:
         return hlaunch<T, MODE_APPLY>(L, E, hk, CX, u, f, rdiag, mask, maskp, out, omega, prerelax, dot_partial, done,
-                                      err, st);
+                                      err, st, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, xchunk);
     case MODE_DEFECT:
         return hlaunch<T, MODE_DEFECT>(L, E, hk, CX, u, f, rdiag, mask, maskp, out, omega, prerelax, nullptr, done,
-                                       err, st);
+                                       err, st, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, xchunk);
     case MODE_JACOBI:
         return hlaunch<T, MODE_JACOBI>(L, E, hk, CX, u, f, rdiag, mask, maskp, out, omega, prerelax, nullptr, done,
-                                       err, st);
+                                       err, st, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, xchunk);
     default:
         return hlaunch<T, MODE_JACOBI_PRE>(L, E, hk, CX, u, f, rdiag, mask, maskp, out, omega, prerelax, nullptr,
-                                           done, err, st);
+                                           done, err, st, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                           xchunk);
     }
 }
 
 template bool hsweep_fits<float>(const Grid &);
 template bool hsweep_fits<double>(const Grid &);
-template int hsweep_blocks<float>(const Grid &, int);
-template int hsweep_blocks<double>(const Grid &, int);
+template int hsweep_blocks<float>(const Grid &, int, int);
+template int hsweep_blocks<double>(const Grid &, int, int);
 template int launch_hsweep<float>(int, const Lay &, const ELay &, const HadamardKe &, const float *, const float *,
                                   const float *, const float *, const uint8_t *, const uint8_t *, float *, float,
                                   float, double *, const int *, int *, cudaStream_t, const double *, const float *,
-                                  const float *, const Lay *);
+                                  const float *, const Lay *, int);
 template int launch_hsweep<double>(int, const Lay &, const ELay &, const HadamardKe &, const double *,
                                    const double *, const double *, const double *, const uint8_t *,
                                    const uint8_t *, double *, double, double, double *, const int *, int *,
-                                   cudaStream_t, const double *, const double *, const double *, const Lay *);
+                                   cudaStream_t, const double *, const double *, const double *, const Lay *, int);
 
 }  // namespace gputo

@@ -106,14 +106,15 @@ struct Solver {
     {
         if (use_hsweep<T>(Lo.g) && B.rdiag)
             return launch_hsweep<T>(mode, Lo, E, hk, CXl, u, f, B.rdiag, mask[l], maskp[l], out, omega, pr,
-                                    dot_partial, done, err, st, Rd, zo, uc, Lc);
+                                    dot_partial, done, err, st, Rd, zo, uc, Lc, l == 0 ? opt.sweep_xchunk : 0);
         return launch_fine_sweep<T>(mode, Lo, E, CXl, u, f, B.diag, mask[l], out, omega, pr, dot_partial, done, err,
                                     st);
     }
     // Per-CTA partials written by the FP64 fine apply.
     int apply_blocks() const
     {
-        return use_hsweep<double>(g[0]) && L[0].rdiag ? hsweep_blocks<double>(g[0]) : fine_sweep_blocks(g[0]);
+        return use_hsweep<double>(g[0]) && L[0].rdiag ? hsweep_blocks<double>(g[0], MODE_APPLY, opt.sweep_xchunk)
+                                                      : fine_sweep_blocks(g[0]);
     }
     // Level 1 is applied matrix-free from the fine CX whenever it is not the
     // coarsest level (then it needs assembled matrices for the direct solve).

@@ -98,6 +98,10 @@ typedef struct {
                             tiles (Hadamard-basis sweep; same results bit for
                             bit); 0 (default): a separate prolongation pass,
                             measured faster                                      */
+    int sweep_xchunk;    /* node planes per CTA along x of the Hadamard-basis
+                            fine sweeps: 0 = chosen from the device's resident
+                            clusters, else 8 .. 32 (the autotuner's tile
+                            choice)                                               */
 } gputo_options;
 
 void gputo_default_options(gputo_options *opt);

@@ -170,3 +170,26 @@ def test_prolongation_fused_into_the_first_post_sweep_is_bit_identical(oracle, g
         s.vcycle(_dev(torch, r), z)
         out.append(z)
     assert torch.equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("xchunk", [8, 16, 24])
+def test_autotuned_x_chunk_gives_the_same_operator_and_solve(oracle, gputo, torch, xchunk):
+    """sweep_xchunk (the autotuner's tile choice): the fine sweeps with x chunks
+    of 8, 16 or 24 node planes agree with the default chunking to rounding, and
+    a mixed solve converges to the same U."""
+    p = oracle.cantilever(68, 64, 20)
+    CX = oracle.simp(oracle.random_density(68, 64, 20, seed=9))[0]
+    u = np.random.default_rng(10).standard_normal(p.ndof)
+    res = []
+    for xc in (0, xchunk):
+        s = _solver(gputo, p, CX, torch, nl=3, sweep_xchunk=xc)
+        r = torch.zeros(p.ndof, dtype=torch.float64, device="cuda")
+        s.apply(_dev(torch, u), r)
+        sm = _solver(gputo, p, CX, torch, nl=3, sweep_xchunk=xc, precision=gputo.PREC_MIXED)
+        F = _dev(torch, p.F)
+        U = torch.zeros_like(F)
+        rr, nit = sm.solve(F, U, 1e-8, 400)
+        assert rr < 1e-8
+        res.append((r, U))
+    assert float((res[0][0] - res[1][0]).abs().max()) <= 1e-13 * float(res[0][0].abs().max())
+    assert float(torch.linalg.norm(res[0][1] - res[1][1])) <= 1e-6 * float(torch.linalg.norm(res[0][1]))
