@@ -635,9 +635,11 @@ def run_one_step(args):
     import gputo
     prec = gputo.PREC_MIXED if args.one_step == "mixed" else gputo.PREC_FP64
     F, fixed = gputo.cantilever(NELX, NELY, NELZ)
+    opts = gputo.default_options(precision=prec, nswp_fine=args.nswp_fine,
+                                 check_every=8 if args.nswp_fine else 1)
     dl = gputo.DesignLoop(NELX, NELY, NELZ, NL, F, fixed, gputo.hex8_stiffness(), volfrac=VOLFRAC,
                           penal=PENAL, rmin=RMIN, move=MOVE, tol=TOL, maxit=MAXIT,
-                          options=gputo.default_options(precision=prec), x0=bench_design())
+                          options=opts, x0=bench_design())
     info = dl.step()
     torch.cuda.synchronize()
     print(json.dumps({"one_step": args.one_step, **info}))
@@ -846,6 +848,8 @@ def main():
     ap.add_argument("--nl", type=int, default=NL)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--one-step", choices=["mixed", "fp64"], help="profiling aid: one design iteration")
+    ap.add_argument("--nswp-fine", type=int, default=0,
+                    help="with --one-step: Jacobi sweeps on the finest level (the autotuner's choice)")
     ap.add_argument("--workload", default="cantilever", choices=["cantilever", "batch", "bridge", "homog"],
                     help="batch: the uneven multi-design batch; bridge: the 512x256x256 bridge; homog: the "
                          "128^3 periodic homogenization (instead of the headline design loop)")

@@ -137,24 +137,6 @@ int upload_quadrature_parts(double nu, cudaStream_t st)
 // coarse-level sweep: packed element matrices [300][nel]
 // ---------------------------------------------------------------------------
 
-// Grid of thread-per-node kernels, one row of CTAs per x node plane
-// (blockIdx.y = i), so a thread finds (j, k) with one 32-bit division.
-inline dim3 plane_grid(const Grid &g, int bs)
-{
-    const int per_plane = (g.ny + 1) * (g.nz + 1);
-    return dim3((unsigned)((per_plane + bs - 1) / bs), (unsigned)(g.nx + 1));
-}
-__device__ __forceinline__ bool plane_ijk(const Grid &g, int &i, int &j, int &k)
-{
-    const unsigned m = blockIdx.x * blockDim.x + threadIdx.x;
-    const unsigned ny1 = (unsigned)g.ny + 1u;
-    if (m >= ny1 * ((unsigned)g.nz + 1u)) return false;
-    i = (int)blockIdx.y;
-    k = (int)(m / ny1);
-    j = (int)(m - (unsigned)k * ny1);
-    return true;
-}
-
 __device__ __forceinline__ void node_ijk(const Grid &g, long long n, int &i, int &j, int &k)
 {
     const long long t = n / (g.ny + 1);

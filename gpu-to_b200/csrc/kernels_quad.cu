@@ -176,12 +176,9 @@ quad_node_kernel(Lay L, const T *__restrict__ y, const T *__restrict__ u, const 
     pdl_wait();
     if (done && *done) return;
     const Grid &g = L.g;
-    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= g.nnod()) return;
-    const long long t = n / (g.ny + 1);
-    const int j = (int)(n - t * (g.ny + 1));
-    const int i = (int)(t / (g.nz + 1));
-    const int k = (int)(t - (long long)i * (g.nz + 1));
+    int i, j, k;
+    if (!plane_ijk(g, i, j, k)) return;
+    const long long n = g.node(i, j, k);
     const long long nel = g.nel();
     // all 24 loads issue before any is used (predicated, no branches), so the
     // gather waits for memory once instead of once per element
@@ -242,7 +239,7 @@ int launch_quad_sweep(int mode, const Lay &L, const ELay &Ef, const T *CX, const
     const T mu = (T)(1.0 / (2.0 * (1.0 + nu)) / 64.0);
     const int bs = 128;
     const unsigned eb = (unsigned)((L.g.nel() + bs - 1) / bs);
-    const unsigned nb = (unsigned)((L.g.nnod() + bs - 1) / bs);
+    const dim3 nb = plane_grid(L.g, bs);   // quad_node_kernel: one row of CTAs per node plane
     if (mode == MODE_JACOBI_PRE)
         launch_pdl(quad_element_kernel<T, true>, dim3(eb), dim3(bs), 0, st, L, CX, Ef, u, f, rdiag, prerelax, lam, mu,
                                                         yscratch, done);
@@ -361,7 +358,7 @@ void launch_packed_sweep_ec(int mode, const Lay &L, const T *Apk, const T *u, co
 {
     const int bs = 128;
     const unsigned eb = (unsigned)((L.g.nel() + 31) / 32);   // 32 elements per CTA of 4 warps
-    const unsigned nb = (unsigned)((L.g.nnod() + bs - 1) / bs);
+    const dim3 nb = plane_grid(L.g, bs);   // quad_node_kernel: one row of CTAs per node plane
     if (mode == MODE_JACOBI_PRE)
         launch_pdl(packed_element_kernel<T, true>, dim3(eb), dim3(bs), 0, st, L, Apk, u, f, rdiag, prerelax, yscratch, done);
     else
