@@ -285,7 +285,10 @@ size_t gputo_homog_device_bytes(const gputo_homog *h);
  * C_rs = mean_e CX_e (u0_r + chi_r)_e' Ke0 (u0_s + chi_s)_e, with u0_r the
  * affine field of unit strain r and chi_r its periodic fluctuation; relres[6],
  * nit[6]: per load case (either may be NULL); chi (optional, device,
- * 18 nx ny nz doubles): the fluctuations as [3 node + d][r]. */
+ * 18 nx ny nz doubles): the fluctuations as [3 node + d][r].  Ke0 goes to
+ * constant memory shared by every gputo_homog on the device, so calls with
+ * different Ke0 must not overlap on one device.  The call synchronises its
+ * stream before it returns. */
 int gputo_homog_solve_dev(gputo_homog *h, const double *Ke0, const double *CX, double tol, int maxit,
                           double *Ceff, double *relres, int *nit, double *chi, void *stream);
 
