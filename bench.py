@@ -583,7 +583,7 @@ def run_micro(args):
     kinds = list(KERNELS) if args.micro == "all" else [args.micro]
     mixed = any(k in ("jacobi32", "level1_32", "jacobi_tc") for k in kinds)
     opts = gputo.default_options(precision=gputo.PREC_MIXED if mixed else gputo.PREC_FP64,
-                                 tc_parts=2 if "jacobi_tc" in kinds else 0)
+                                 tc_parts=2 if "jacobi_tc" in kinds else 0, sweep_pairs=args.sweep_pairs)
     s = gputo.Solver(nelx, nely, nelz, nl, opts)
     s.set_problem(gputo.hex8_stiffness(), fixed)
     xd = torch.as_tensor(x0, dtype=torch.float64, device="cuda")
@@ -636,7 +636,7 @@ def run_one_step(args):
     prec = gputo.PREC_MIXED if args.one_step == "mixed" else gputo.PREC_FP64
     F, fixed = gputo.cantilever(NELX, NELY, NELZ)
     opts = gputo.default_options(precision=prec, nswp_fine=args.nswp_fine,
-                                 check_every=8 if args.nswp_fine else 1)
+                                 check_every=8 if args.nswp_fine else 1, sweep_pairs=args.sweep_pairs)
     dl = gputo.DesignLoop(NELX, NELY, NELZ, NL, F, fixed, gputo.hex8_stiffness(), volfrac=VOLFRAC,
                           penal=PENAL, rmin=RMIN, move=MOVE, tol=TOL, maxit=MAXIT,
                           options=opts, x0=bench_design())
@@ -847,6 +847,8 @@ def main():
     ap.add_argument("--size", default=f"{NELX}x{NELY}x{NELZ}")
     ap.add_argument("--nl", type=int, default=NL)
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--sweep-pairs", type=int, default=1, choices=[0, 1],
+                    help="profiling aid: FP32 fine sweeps with two element columns per lane (1) or one (0)")
     ap.add_argument("--one-step", choices=["mixed", "fp64"], help="profiling aid: one design iteration")
     ap.add_argument("--nswp-fine", type=int, default=0,
                     help="with --one-step: Jacobi sweeps on the finest level (the autotuner's choice)")

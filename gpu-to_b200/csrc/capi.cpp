@@ -121,6 +121,7 @@ void gputo_default_options(gputo_options *o)
     o->nswp_fine = 0;
     o->fuse_prolong = 0;
     o->sweep_xchunk = 0;
+    o->sweep_pairs = 1;
 }
 
 int gputo_fine_op_constants(const double *Ke, double *c8)

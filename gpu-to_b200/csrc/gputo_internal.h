@@ -200,9 +200,13 @@ int init_hsweep_kernels();
 // gputo_debug_set_sweep_fault in gputo.h).
 int set_sweep_fault_hook(int skip_stage, unsigned wait_us);
 template <typename T> bool hsweep_fits(const Grid &g);
+// The paired FP32 sweep (two element columns per lane, ny <= 512) is built
+// and resident on this device for g.
+bool hsweep_pairs_fit(const Grid &g);
 // CTAs (= partials) of a sweep; xchunk: node planes per x chunk (0: chosen
-// from the device's resident clusters)
-template <typename T> int hsweep_blocks(const Grid &g, int mode = MODE_APPLY, int xchunk = 0);
+// from the device's resident clusters); pairs: the paired FP32 sweep where it
+// fits.
+template <typename T> int hsweep_blocks(const Grid &g, int mode = MODE_APPLY, int xchunk = 0, bool pairs = false);
 // rdiag: 1/diag (launch_recip); maskp: the Dirichlet bytes with rows padded
 // to 16 bytes (launch_pad_mask; hsweep_mask_bytes of storage).
 // MODE_JACOBI_PRO: uc is the coarse correction in the layout Lc (level 1).
@@ -210,7 +214,8 @@ template <typename T>
 int launch_hsweep(int mode, const Lay &L, const ELay &E, const HadamardKe &hk, const T *CX, const T *u, const T *f,
                   const T *rdiag, const uint8_t *mask, const uint8_t *maskp, T *out, T omega, T prerelax,
                   double *dot_partial, const int *done, int *err, cudaStream_t st, const double *Rd = nullptr,
-                  const T *zo = nullptr, const T *uc = nullptr, const Lay *Lc = nullptr, int xchunk = 0);
+                  const T *zo = nullptr, const T *uc = nullptr, const Lay *Lc = nullptr, int xchunk = 0,
+                  bool pairs = false);
 template <typename T> bool hsweep_pro_fits(const Grid &g);
 // MODE_ENERGY sweep (FP64): out (optional) = f - K u with fixed rows zero,
 // ce / dc in natural element order, partial pairs (|r|^2, sum CX ce) per CTA.

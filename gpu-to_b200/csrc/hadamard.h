@@ -18,6 +18,26 @@ template <typename T> struct HC {
     T a, bc, c, de, e, f, g, h;   // S constants / 64: a, b - c, c, d - e, e, f, g, h
 };
 
+// Arithmetic shared by the scalar kernels and the paired FP32 sweep, which
+// runs two elements per lane as float2 (element 2l in .x, 2l + 1 in .y):
+// each operation on a pair is one paired instruction with the same rounding
+// as the scalar one (a - b as fma(-1, b, a) is exact before rounding).
+__device__ __forceinline__ float hfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double hfma(double a, double b, double c) { return ::fma(a, b, c); }
+__device__ __forceinline__ float2 hfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 operator+(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 operator-(float2 a, float2 b) { return __ffma2_rn(make_float2(-1.f, -1.f), b, a); }
+__device__ __forceinline__ float2 operator*(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float hmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double hmul(double a, double b) { return __dmul_rn(a, b); }
+template <typename T> __device__ __forceinline__ T hzero() { return T(0); }
+template <> __device__ __forceinline__ float2 hzero<float2>() { return make_float2(0.f, 0.f); }
+inline HC<float2> pair_hc(const HC<float> &k)
+{
+    auto p = [](float v) { return make_float2(v, v); };
+    return HC<float2>{p(k.a), p(k.bc), p(k.c), p(k.de), p(k.e), p(k.f), p(k.g), p(k.h)};
+}
+
 // The eight constants as the kernels use them (divided by 64).
 template <typename T>
 inline HC<T> make_hc(const HadamardKe &hk)
@@ -75,11 +95,12 @@ __device__ __forceinline__ void face_h<float>(float (&x)[HF])
     f2set(x, 8, __fadd2_rn(d0, d1));
     f2set(x, 12, sub2(d0, d1));
     const float z00 = x[2], z01 = x[6], z10 = x[10], z11 = x[14];
-    const float zs0 = z00 + z10, zd0 = z00 - z10, zs1 = z01 + z11, zd1 = z01 - z11;
-    x[2] = zs0 + zs1;
-    x[6] = zs0 - zs1;
-    x[10] = zd0 + zd1;
-    x[14] = zd0 - zd1;
+    const float zs0 = __fadd_rn(z00, z10), zd0 = __fsub_rn(z00, z10), zs1 = __fadd_rn(z01, z11),
+                zd1 = __fsub_rn(z01, z11);
+    x[2] = __fadd_rn(zs0, zs1);
+    x[6] = __fsub_rn(zs0, zs1);
+    x[10] = __fadd_rn(zd0, zd1);
+    x[14] = __fsub_rn(zd0, zd1);
 }
 
 // The S step of one element, v -> w = cx S v / 64 (the mode-(0,0,0) rows
@@ -92,7 +113,7 @@ __device__ __forceinline__ void element_s(const T (&v0)[HF], const T (&v1)[HF], 
     const T ka = k.a * cx, kbc = k.bc * cx, kc = k.c * cx, kde = k.de * cx, ke = k.e * cx, kf = k.f * cx,
             kg = k.g * cx, kh = k.h * cx;
     T t;
-    w0[0] = w0[1] = w0[2] = T(0);   // mode (0,0,0): rigid translation
+    w0[0] = w0[1] = w0[2] = hzero<T>();   // mode (0,0,0): rigid translation
     // a [1 1; 1 1]: {(m1,x),(m4,z)}, {(m1,y),(m2,z)}, {(m2,x),(m4,y)}
     t = ka * (v0[4] + v1[2]);
     w0[4] = t, w1[2] = t;
@@ -102,21 +123,21 @@ __device__ __forceinline__ void element_s(const T (&v0)[HF], const T (&v1)[HF], 
     w0[8] = t, w1[1] = t;
     // (b - c) I + c 11': {(m1,z),(m2,y),(m4,x)}
     t = kc * (v0[6] + v0[9] + v1[0]);
-    w0[6] = fma(kbc, v0[6], t);
-    w0[9] = fma(kbc, v0[9], t);
-    w1[0] = fma(kbc, v1[0], t);
+    w0[6] = hfma(kbc, v0[6], t);
+    w0[9] = hfma(kbc, v0[9], t);
+    w1[0] = hfma(kbc, v1[0], t);
     // (d - e) I + e 11': {(m3,x),(m5,y),(m6,z)}
     t = ke * (v0[12] + v1[5] + v1[10]);
-    w0[12] = fma(kde, v0[12], t);
-    w1[5] = fma(kde, v1[5], t);
-    w1[10] = fma(kde, v1[10], t);
+    w0[12] = hfma(kde, v0[12], t);
+    w1[5] = hfma(kde, v1[5], t);
+    w1[10] = hfma(kde, v1[10], t);
     // [f g; g f]: {(m3,y),(m5,x)}, {(m3,z),(m6,x)}, {(m5,z),(m6,y)}
-    w0[13] = fma(kf, v0[13], kg * v1[4]);
-    w1[4] = fma(kf, v1[4], kg * v0[13]);
-    w0[14] = fma(kf, v0[14], kg * v1[8]);
-    w1[8] = fma(kf, v1[8], kg * v0[14]);
-    w1[6] = fma(kf, v1[6], kg * v1[9]);
-    w1[9] = fma(kf, v1[9], kg * v1[6]);
+    w0[13] = hfma(kf, v0[13], kg * v1[4]);
+    w1[4] = hfma(kf, v1[4], kg * v0[13]);
+    w0[14] = hfma(kf, v0[14], kg * v1[8]);
+    w1[8] = hfma(kf, v1[8], kg * v0[14]);
+    w1[6] = hfma(kf, v1[6], kg * v1[9]);
+    w1[9] = hfma(kf, v1[9], kg * v1[6]);
     // h I on mode (1,1,1)
     w1[12] = kh * v1[12];
     w1[13] = kh * v1[13];

@@ -113,7 +113,9 @@ struct HSmem {
     static constexpr size_t z_bytes = sizeof(T) * 2 * WZ * ZROW * 3;
     static constexpr int SEAM = HMAXP * WZ * 3;
     static constexpr size_t s_off = al128(z_off + z_bytes);
-    static constexpr size_t s_bytes = sizeof(T) * 3 * SEAM;         // own, own u, received
+    // seam node partials: own (row sums, z partners), received (the same from
+    // the left neighbour), and with MODE_JACOBI_PRO the tile's corrected u
+    static constexpr size_t s_bytes = sizeof(T) * (N::PRO ? 5 : 4) * SEAM;
     static constexpr size_t bar_off = al128(s_off + s_bytes);
     static constexpr size_t red_off = bar_off + 8 * HRING;            // per-warp dot partials (two per warp)
     static constexpr size_t bytes = red_off + 16 * WZ;
@@ -180,7 +182,9 @@ __device__ __forceinline__ double element_h_energy(const double (&Fp)[HF], const
     return en;
 }
 
-// FP32: the sums and differences of faces and outputs on (x, y) pairs.
+// FP32: the sums and differences of faces and outputs on (x, y) pairs.  All
+// FP32 steps are rounding intrinsics (never contracted into an FMA), so the
+// one- and two-column kernels give the same results bit for bit.
 template <>
 __device__ __forceinline__ void element_h<float>(const float (&Fp)[HF], const float (&Fn)[HF], float cx,
                                                  const HC<float> &k, float (&A)[HF], float (&An)[HF])
@@ -191,8 +195,8 @@ __device__ __forceinline__ void element_h<float>(const float (&Fp)[HF], const fl
         const float2 p = f2(Fp, 4 * c), n = f2(Fn, 4 * c);
         f2set(v0, 4 * c, __fadd2_rn(p, n));
         f2set(v1, 4 * c, sub2(p, n));
-        v0[4 * c + 2] = Fp[4 * c + 2] + Fn[4 * c + 2];
-        v1[4 * c + 2] = Fp[4 * c + 2] - Fn[4 * c + 2];
+        v0[4 * c + 2] = __fadd_rn(Fp[4 * c + 2], Fn[4 * c + 2]);
+        v1[4 * c + 2] = __fsub_rn(Fp[4 * c + 2], Fn[4 * c + 2]);
     }
     element_s(v0, v1, cx, k, w0, w1);
 #pragma unroll
@@ -200,8 +204,8 @@ __device__ __forceinline__ void element_h<float>(const float (&Fp)[HF], const fl
         const float2 a = f2(w0, 4 * c), b = f2(w1, 4 * c);
         f2set(A, 4 * c, __fadd2_rn(f2(A, 4 * c), __fadd2_rn(a, b)));
         f2set(An, 4 * c, sub2(a, b));
-        A[4 * c + 2] += w0[4 * c + 2] + w1[4 * c + 2];
-        An[4 * c + 2] = w0[4 * c + 2] - w1[4 * c + 2];
+        A[4 * c + 2] = __fadd_rn(A[4 * c + 2], __fadd_rn(w0[4 * c + 2], w1[4 * c + 2]));
+        An[4 * c + 2] = __fsub_rn(w0[4 * c + 2], w1[4 * c + 2]);
     }
 }
 
@@ -225,7 +229,7 @@ __device__ __forceinline__ void h_store(long long base, unsigned m, const T (&ku
             dsum = fma((double)r, (double)r, dsum);
         } else {
             const T r = fixed ? T(0) : fv[d] - ku[d];
-            const T z = u[d] + omega * r * rv[d];
+            const T z = hfma(hmul(omega, r), rv[d], u[d]);
             out[base + d] = z;
             if (MODE == MODE_JACOBI_DOT) {   // r'z and r'z_old with the FP64 residual
                 const double rd = rdv[d];
@@ -259,7 +263,7 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
               T prerelax, double *__restrict__ dot_partial, const int *__restrict__ done, int *__restrict__ err,
               const double *__restrict__ Rd, const T *__restrict__ zo, uint32_t wait_ns, int skip_stage,
               double *__restrict__ ce, double *__restrict__ dcv, const double *__restrict__ dsK,
-              const T *__restrict__ ucoarse, Lay Lc)
+              const T *__restrict__ ucoarse, Lay Lc, const T *__restrict__ ug)
 {
     if (done && *done) return;   // the same value for every CTA of the cluster
     using N = HNeeds<MODE>;
@@ -274,8 +278,10 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem + S::bar_off);
     T *zb = reinterpret_cast<T *>(smem + S::z_off);
     T *s_own = reinterpret_cast<T *>(smem + S::s_off);
-    T *s_ownu = s_own + S::SEAM;
+    T *s_ownz = s_own + S::SEAM;
     T *s_recv = s_own + 2 * S::SEAM;
+    T *s_recvz = s_own + 3 * S::SEAM;
+    T *s_ownu = s_own + 4 * S::SEAM;   // MODE_JACOBI_PRO only
 
     cg::cluster_group cluster = cg::this_cluster();
     const Grid &g = L.g;
@@ -355,7 +361,7 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
                 for (int d = 0; d < 3; ++d) {
                     const int idx = (w + cz) * HUW + 3 * (l + cy) + d;
                     T v = su[idx];
-                    if (N::PRE) v = prerelax * v * sd[idx];   // 1/diag is 0 outside the grid
+                    if (N::PRE) v = hmul(hmul(prerelax, v), sd[idx]);   // 1/diag is 0 outside the grid
                     U[(cy * 2 + cz) * 4 + d] = v;
                 }
     };
@@ -429,14 +435,18 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
         const uint8_t *em = sb + S::m_off + w * HM;
         const T *z = zb + (p & 1) * (WZ * S::ZROW * 3);
         const int k = kc0 + w, j = jc0 + l, at = ((p - P0) * WZ + w) * 3;
-        T R[3];
+        T R[3], Z[3];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) R[d] = q0[d] + (w > 0 ? z[((w - 1) * S::ZROW + l) * 3 + d] : T(0));
+        for (int d = 0; d < 3; ++d) {
+            Z[d] = w > 0 ? z[((w - 1) * S::ZROW + l) * 3 + d] : T(0);
+            R[d] = q0[d] + Z[d];
+        }
         if (l == 0 && r > 0) {   // seam node: finished after the cluster barrier
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
-                s_own[at + d] = R[d];
-                s_ownu[at + d] = Uu[d];
+                s_own[at + d] = q0[d];
+                s_ownz[at + d] = Z[d];
+                if (N::PRO) s_ownu[at + d] = Uu[d];
             }
         } else if (j <= g.ny) {
             const T uu[3] = {Uu[0], Uu[1], Uu[2]};
@@ -444,13 +454,21 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
                              ez + 3 * l, dsum2);
         }
         if (l == HY - 1) {   // this CTA's part of node column jc0 + HY
-            T Sd[3];
+            T Sq[3], Sz[3], Sd[3];
 #pragma unroll
-            for (int d = 0; d < 3; ++d) Sd[d] = P[8 + d] + (w > 0 ? z[((w - 1) * S::ZROW + HY) * 3 + d] : T(0));
+            for (int d = 0; d < 3; ++d) {
+                Sq[d] = P[8 + d];
+                Sz[d] = w > 0 ? z[((w - 1) * S::ZROW + HY) * 3 + d] : T(0);
+                Sd[d] = Sq[d] + Sz[d];
+            }
             if (r + 1 < CY) {
                 T *rem = cluster.map_shared_rank(s_recv, r + 1);
+                T *remz = cluster.map_shared_rank(s_recvz, r + 1);
 #pragma unroll
-                for (int d = 0; d < 3; ++d) rem[at + d] = Sd[d];
+                for (int d = 0; d < 3; ++d) {
+                    rem[at + d] = Sq[d];
+                    remz[at + d] = Sz[d];
+                }
             } else if (tail_owner) {
                 const T uu[3] = {Uu[8], Uu[9], Uu[10]};
                 h_store<T, MODE>(L.at(p, g.ny, k), em[HY], Sd, uu, ef + 3 * HY, ed + 3 * HY, out, omega, dsum,
@@ -575,13 +593,19 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
             const int pp = idx / WZ, ww = idx - pp * WZ;
             const int k = kc0 + ww, p = P0 + pp, at = idx * 3;
             if (!((ww >= 1 || zt == 0) && k <= g.nz)) continue;
+            // the interior nodes' order: (row sums) + (z partners), each own + left
+            const long long base = L.at(p, jc0, k);
             T v[3], uu[3];
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
-                v[d] = s_own[at + d] + s_recv[at + d];
-                uu[d] = s_ownu[at + d];
+                v[d] = (s_own[at + d] + s_recv[at + d]) + (s_ownz[at + d] + s_recvz[at + d]);
+                if (N::PRO)
+                    uu[d] = s_ownu[at + d];
+                else if (N::PRE)
+                    uu[d] = hmul(hmul(prerelax, f[base + d]), rdiag[base + d]);
+                else
+                    uu[d] = (MODE == MODE_APPLY || N::D) ? ug[base + d] : T(0);
             }
-            const long long base = L.at(p, jc0, k);
             h_store<T, MODE>(base, mask[g.node(p, jc0, k)], v, uu, f + base, rdiag + base, out, omega, dsum,
                              Rd + base, zo + base, dsum2);
         }
@@ -615,18 +639,518 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
     }
 }
 
+// ---------------------------------------------------------------------------
+// FP32 sweeps with two element columns per lane (hsweep2_kernel).
+//
+// The same sweeps as hsweep_kernel with the same results bit for bit (the
+// dot partials aside, which group their FP64 sums differently), but each lane
+// owns elements j = jc0 + 2l and 2l + 1, so a CTA covers 64 element columns
+// along y.  The two elements run one instruction stream: every arithmetic
+// step of the Hadamard form is a paired FP32 instruction on a float2 (element
+// 2l in .x, 2l + 1 in .y), the node column between the two is summed inside
+// the lane, and the per-step costs (the ring wait, the barrier, the shuffles,
+// the index arithmetic, the seam branches) are shared by two elements.  The
+// node pairs of the epilogue move as 8-byte words (f, 1/diag, the z
+// partners, the output).  About 40 % fewer instructions per element than
+// hsweep_kernel.  Twice the state per thread (about 200 registers): CTAs of
+// four warps, two per SM.  The per-step CTA barrier holds all of a CTA's
+// warps in the same phase (element arithmetic, then shuffles and shared
+// memory, then stores); a second CTA on the SM issues during the first one's
+// barrier and latency phases.
+constexpr int HY2 = 64;     // element columns per CTA along y (two per lane)
+constexpr int HUW2 = 196;   // u box width: 3 (HY2 + 1) = 195 values, rounded to 16 bytes
+constexpr int HM2 = 80;     // mask box width in bytes: HY2 + 1 = 65 nodes, rounded to 16
+constexpr int ZROW2 = 66;   // z exchange row: 65 node columns, even so node pairs are 8-byte aligned
+constexpr int HWZ2 = 4;     // warps (element rows along z) per CTA: two CTAs share an SM, so one CTA's
+                            // barrier leaves the other issuing (measured 79 us against 84 us for one
+                            // CTA of eight warps, despite the extra overlapping row)
+
+template <int MODE>
+struct HSmem2 {
+    using N = HNeeds<MODE>;
+    static constexpr int WZ = HWZ2;
+    static constexpr size_t u_bytes = sizeof(float) * (WZ + 1) * HUW2;   // one node plane tile
+    static constexpr size_t ua = al128(u_bytes);
+    static constexpr size_t c_bytes = sizeof(float) * WZ * HY2;          // one CX plane tile
+    static constexpr size_t m_bytes = (size_t)WZ * HM2;                  // one mask plane tile
+    static constexpr size_t r_bytes = sizeof(double) * (WZ + 1) * HUW2;   // FP64 residual tile
+    static constexpr size_t d_off = ua;
+    static constexpr size_t ef_off = d_off + (N::PRE ? ua : 0);
+    static constexpr size_t ed_off = ef_off + (N::F ? ua : 0);
+    static constexpr size_t er_off = ed_off + (N::D ? ua : 0);
+    static constexpr size_t ez_off = er_off + (N::DOT ? al128(r_bytes) : 0);
+    static constexpr size_t c_off = ez_off + (N::DOT ? ua : 0);
+    static constexpr size_t m_off = c_off + al128(c_bytes);
+    static constexpr size_t slot = al128(m_off + m_bytes);
+    static constexpr size_t z_off = HRING * slot;
+    static constexpr size_t z_bytes = sizeof(float) * 2 * WZ * ZROW2 * 3;
+    static constexpr int SEAM = HMAXP * WZ * 3;
+    static constexpr size_t s_off = al128(z_off + z_bytes);
+    static constexpr size_t s_bytes = sizeof(float) * 4 * SEAM;   // own and received row sums and z partners
+    static constexpr size_t bar_off = al128(s_off + s_bytes);
+    static constexpr size_t red_off = bar_off + 8 * HRING;
+    static constexpr size_t bytes = red_off + 16 * WZ;
+    static_assert(ua % 128 == 0 && c_off % 128 == 0 && m_off % 128 == 0 && slot % 128 == 0 && er_off % 128 == 0 &&
+                      ez_off % 128 == 0 && z_off % 128 == 0,
+                  "TMA shared-memory destinations must be 128-byte aligned");
+};
+static_assert(2 * (HSmem2<MODE_JACOBI_DOT>::bytes + 1024) <= 228 * 1024,
+              "two CTAs of the paired FP32 sweep with dots must share an SM");
+
+// Node columns 2l, 2l + 1, 2l + 2 of rows w, w + 1 (raw[cz][n][d]) -> the
+// face modes of elements 2l and 2l + 1, F[4 c + d] with mode c = 2 py + pz:
+// the y butterflies in scalar form (each node column 2l + 1 serves both
+// elements), the z butterflies paired.
+__device__ __forceinline__ void face_h2(const float (&raw)[2][3][3], float2 (&F)[HF])
+{
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        float2 s[2], df[2];
+#pragma unroll
+        for (int cz = 0; cz < 2; ++cz) {
+            const float a = raw[cz][0][d], b = raw[cz][1][d], c = raw[cz][2][d];
+            s[cz] = make_float2(__fadd_rn(a, b), __fadd_rn(b, c));
+            df[cz] = make_float2(__fsub_rn(a, b), __fsub_rn(b, c));
+        }
+        F[d] = s[0] + s[1];
+        F[4 + d] = s[0] - s[1];
+        F[8 + d] = df[0] + df[1];
+        F[12 + d] = df[0] - df[1];
+    }
+}
+
+// element_h on a pair of elements.
+__device__ __forceinline__ void element_h2(const float2 (&Fp)[HF], const float2 (&Fn)[HF], float2 cx,
+                                           const HC<float2> &k, float2 (&A)[HF], float2 (&An)[HF])
+{
+    float2 v0[HF], v1[HF], w0[HF], w1[HF];
+#pragma unroll
+    for (int q = 0; q < HF; ++q)
+        if ((q & 3) != 3) {
+            v0[q] = Fp[q] + Fn[q];
+            v1[q] = Fp[q] - Fn[q];
+        }
+    element_s(v0, v1, cx, k, w0, w1);
+#pragma unroll
+    for (int q = 0; q < HF; ++q)
+        if ((q & 3) != 3) {
+            A[q] = A[q] + (w0[q] + w1[q]);
+            An[q] = w0[q] - w1[q];
+        }
+}
+
+__device__ __forceinline__ void lds6(const float *p, float (&v)[6])
+{
+    const float2 *q = reinterpret_cast<const float2 *>(p);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float2 x = q[i];
+        v[2 * i] = x.x;
+        v[2 * i + 1] = x.y;
+    }
+}
+
+// The epilogue operands of a lane's node pair (f, 1/diag, the Dirichlet
+// bits; with the dots also the FP64 residual and z_old), read from the ring
+// slot before the step's barrier so that their latency overlaps it.
+struct Epi2 {
+    float fv[6], rv[6], zv[6];
+    double rd[6];
+    unsigned mm;
+};
+
+template <int MODE>
+__device__ __forceinline__ void load_epi2(const unsigned char *sb, int w, int l, Epi2 &e)
+{
+    using N = HNeeds<MODE>;
+    using S = HSmem2<MODE>;
+    const int o = w * HUW2 + 6 * l;
+    if (N::F) lds6(reinterpret_cast<const float *>(sb + S::ef_off) + o, e.fv);
+    if (N::D) lds6(reinterpret_cast<const float *>(sb + S::ed_off) + o, e.rv);
+    if (N::DOT) {
+        lds6(reinterpret_cast<const float *>(sb + S::ez_off) + o, e.zv);
+        const double2 *q = reinterpret_cast<const double2 *>(reinterpret_cast<const double *>(sb + S::er_off) + o);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const double2 x = q[i];
+            e.rd[2 * i] = x.x;
+            e.rd[2 * i + 1] = x.y;
+        }
+    }
+    e.mm = *reinterpret_cast<const uint16_t *>(sb + S::m_off + w * HM2 + 2 * l);
+}
+
+// Finish node columns j0 = jc0 + 2l and j0 + 1 of one row (h_store on a node
+// pair): 'base' is the dof of node j0, in1 whether node j0 + 1 is in the grid
+// (node j0 is), count0 whether node j0 enters the dot sums (not on a CTA
+// seam, where it is written here with this CTA's partial and rewritten after
+// the cluster barrier).  u comes from the face registers.
+template <int MODE>
+__device__ __forceinline__ void h_store2(long long base, bool in1, bool count0, const Epi2 &e, const float (&R)[6],
+                                         const float (&u)[9], float *__restrict__ out, float omega, double &dsum,
+                                         double &dsum2)
+{
+    float o[6];
+    const unsigned mm = e.mm;
+    const float(&fv)[6] = e.fv;
+    const float(&rv)[6] = e.rv;
+    const float(&zv)[6] = e.zv;
+    const double(&rd)[6] = e.rd;
+#pragma unroll
+    for (int n = 0; n < 2; ++n) {
+        const bool counted = n ? in1 : count0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const int i = 3 * n + d;
+            const bool fixed = (mm >> (8 * n + d)) & 1u;
+            if (MODE == MODE_APPLY) {
+                const float q = fixed ? 0.f : R[i];
+                o[i] = q;
+                if (counted) dsum += (double)u[i] * (double)q;
+            } else if (MODE == MODE_DEFECT) {
+                o[i] = fixed ? 0.f : fv[i] - R[i];
+            } else {
+                const float r = fixed ? 0.f : fv[i] - R[i];
+                const float z = hfma(hmul(omega, r), rv[i], u[i]);
+                o[i] = z;
+                if (MODE == MODE_JACOBI_DOT && counted) {
+                    dsum = fma(rd[i], (double)z, dsum);
+                    dsum2 = fma(rd[i], (double)zv[i], dsum2);
+                }
+            }
+        }
+    }
+    if (in1) {
+        float2 *o2 = reinterpret_cast<float2 *>(out + base);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) o2[i] = make_float2(o[2 * i], o[2 * i + 1]);
+    } else {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) out[base + d] = o[d];
+    }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(32 * HWZ2, 2)
+hsweep2_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ CUtensorMap tm_d,
+               const __grid_constant__ CUtensorMap tm_f, const __grid_constant__ CUtensorMap tm_c,
+               const __grid_constant__ CUtensorMap tm_m, const __grid_constant__ CUtensorMap tm_r,
+               const __grid_constant__ CUtensorMap tm_z, Lay L, HC<float2> hc, int htx, const float *__restrict__ f,
+               const float *__restrict__ rdiag, const uint8_t *__restrict__ mask, float *__restrict__ out,
+               float omega, float prerelax, double *__restrict__ dot_partial, const int *__restrict__ done,
+               int *__restrict__ err, const double *__restrict__ Rd, const float *__restrict__ zo, uint32_t wait_ns,
+               int skip_stage, const float *__restrict__ ug)
+{
+    static_assert(MODE != MODE_ENERGY && MODE != MODE_JACOBI_PRO, "FP64 energy and the fused prolongation use hsweep_kernel");
+    if (done && *done) return;   // the same value for every CTA of the cluster
+    using N = HNeeds<MODE>;
+    constexpr int WZ = HWZ2, NT = 32 * WZ;
+    using S = HSmem2<MODE>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    if (smem_u32(smem) & 127u) {
+        if (threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && err)
+            atomicExch(err, GPUTO_ERR_CUDA);
+        return;
+    }
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + S::bar_off);
+    float *zb = reinterpret_cast<float *>(smem + S::z_off);
+    float *s_own = reinterpret_cast<float *>(smem + S::s_off);
+    float *s_ownz = s_own + S::SEAM;
+    float *s_recv = s_own + 2 * S::SEAM;
+    float *s_recvz = s_own + 3 * S::SEAM;
+
+    cg::cluster_group cluster = cg::this_cluster();
+    const Grid &g = L.g;
+    const int tid = threadIdx.x, l = tid & 31, w = tid >> 5;
+    const int r = blockIdx.x, CY = gridDim.x;
+    const int jc0 = HY2 * r;
+    const int zt = blockIdx.y, kc0 = (WZ - 1) * zt;
+    const int P0 = blockIdx.z * htx;
+    const int P1 = (blockIdx.z == gridDim.z - 1) ? g.nx + 1 : P0 + htx;
+    const int E0 = P0 > 0 ? P0 - 1 : 0, E1 = P1 < g.nx ? P1 : g.nx;
+    const int nE = E1 - E0;
+    const bool last_plane = E1 == g.nx && E1 < P1;
+    const int nst = nE + 1 + (last_plane ? 1 : 0);
+    const bool tail_owner = (r == CY - 1) && (jc0 + HY2 == g.ny);
+    const bool zok = (w >= 1 || zt == 0) && kc0 + w <= g.nz;
+    const int j0 = jc0 + 2 * l;
+    const bool in0 = j0 <= g.ny, in1 = j0 + 1 <= g.ny, seam = l == 0 && r > 0;
+
+    if (tid == 0) {
+        for (int s = 0; s < HRING; ++s) mbar_init(&bar[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    int issued = 0;
+    auto issue = [&](int s) {
+        unsigned char *sb = smem + (s % HRING) * S::slot;
+        uint64_t *b = &bar[s % HRING];
+        const bool face = s <= nE, cxp = s >= 1 && s <= nE, epi = s >= 1 && E0 + s - 1 >= P0;
+        uint32_t bytes = 0;
+        if (face) bytes += (uint32_t)(S::u_bytes * (N::PRE ? 2 : 1));
+        if (cxp) bytes += (uint32_t)S::c_bytes;
+        if (epi) bytes += (uint32_t)(S::u_bytes * ((N::F ? 1 : 0) + (N::D ? 1 : 0) + (N::DOT ? 1 : 0)) + S::m_bytes +
+                                     (N::DOT ? S::r_bytes : 0));
+        mbar_arrive_expect_tx(b, bytes);
+        if (s == skip_stage) {   // test hook: the stage stays armed with no copy in flight
+            issued = s + 1;
+            return;
+        }
+        if (face) {
+            tma_load_3d(sb, &tm_u, 3 * jc0, kc0, E0 + s, b);
+            if (N::PRE) tma_load_3d(sb + S::d_off, &tm_d, 3 * jc0, kc0, E0 + s, b);
+        }
+        if (cxp) tma_load_3d(sb + S::c_off, &tm_c, jc0, kc0, E0 + s - 1, b);
+        if (epi) {
+            if (N::F) tma_load_3d(sb + S::ef_off, &tm_f, 3 * jc0, kc0, E0 + s - 1, b);
+            if (N::D) tma_load_3d(sb + S::ed_off, &tm_d, 3 * jc0, kc0, E0 + s - 1, b);
+            if (N::DOT) {
+                tma_load_3d(sb + S::er_off, &tm_r, 3 * jc0, kc0, E0 + s - 1, b);
+                tma_load_3d(sb + S::ez_off, &tm_z, 3 * jc0, kc0, E0 + s - 1, b);
+            }
+            tma_load_3d(sb + S::m_off, &tm_m, jc0, kc0, E0 + s - 1, b);
+        }
+        issued = s + 1;
+    };
+    if (tid == 0)
+        for (int s = 0; s < HRING && s < nst; ++s) issue(s);
+    cluster.sync();   // every CTA of the cluster is running before any remote store
+
+    bool bad = false;
+    auto wait_stage = [&](int s) {
+        if (!bad && !mbar_wait_for(&bar[s % HRING], (uint32_t)((s / HRING) & 1), wait_ns)) bad = true;
+    };
+    // Face of ring stage s: raw node values (u, or the pre-relaxed f / diag)
+    // and the element pair's CX, read a step ahead (before the barrier of the
+    // step that precedes their use).
+    auto load_face = [&](int s, float (&raw)[2][3][3], float2 &cx) {
+        const unsigned char *sb = smem + (s % HRING) * S::slot;
+        const float *su = reinterpret_cast<const float *>(sb) + w * HUW2 + 6 * l;
+        const float *sd = reinterpret_cast<const float *>(sb + S::d_off) + w * HUW2 + 6 * l;
+#pragma unroll
+        for (int cz = 0; cz < 2; ++cz)
+#pragma unroll
+            for (int n = 0; n < 3; ++n)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const int idx = cz * HUW2 + 3 * n + d;
+                    float v = su[idx];
+                    if (N::PRE) v = hmul(hmul(prerelax, v), sd[idx]);   // 1/diag is 0 outside the grid
+                    raw[cz][n][d] = v;
+                }
+        if (s >= 1)
+            cx = *reinterpret_cast<const float2 *>(reinterpret_cast<const float *>(sb + S::c_off) + w * HY2 + 2 * l);
+    };
+    // Row cz = 0 kept for the epilogue, and the face modes.
+    auto take_face = [&](const float (&raw)[2][3][3], float (&Uk)[9], float2 (&F)[HF]) {
+#pragma unroll
+        for (int n = 0; n < 3; ++n)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) Uk[3 * n + d] = raw[0][n][d];
+        face_h2(raw, F);
+    };
+    double dsum = 0.0, dsum2 = 0.0;
+    // Corner partial pairs P of node plane p -> the row-w sums of node
+    // columns 2l, 2l + 1 (q), and the row-(w + 1) partials into the z
+    // exchange buffer (read by warp w + 1 after the next barrier).
+    auto reduce_y = [&](int p, const float2 (&P)[HF], float (&q)[6]) {
+        float *z = zb + (p & 1) * (WZ * ZROW2 * 3);
+        float zp[6];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const float a0 = __shfl_up_sync(0xffffffffu, P[8 + d].y, 1);
+            const float a1 = __shfl_up_sync(0xffffffffu, P[12 + d].y, 1);
+            q[d] = P[d].x + (l > 0 ? a0 : 0.f);
+            q[3 + d] = P[d].y + P[8 + d].x;
+            zp[d] = P[4 + d].x + (l > 0 ? a1 : 0.f);
+            zp[3 + d] = P[4 + d].y + P[12 + d].x;
+        }
+        float2 *zr = reinterpret_cast<float2 *>(z + (w * ZROW2 + 2 * l) * 3);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) zr[i] = make_float2(zp[2 * i], zp[2 * i + 1]);
+        if (l == 31)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) z[(w * ZROW2 + HY2) * 3 + d] = P[12 + d].y;
+    };
+    // Finish node plane p with the epilogue tiles of ring stage s.
+    auto emit = [&](int p, int s, const float2 (&P)[HF], const float (&q)[6], const float (&Uu)[9], const Epi2 &e) {
+        if (!zok) return;
+        const unsigned char *sb = smem + (s % HRING) * S::slot;
+        const float *ef = reinterpret_cast<const float *>(sb + S::ef_off) + w * HUW2;
+        const float *ed = reinterpret_cast<const float *>(sb + S::ed_off) + w * HUW2;
+        const double *er = reinterpret_cast<const double *>(sb + S::er_off) + w * HUW2;
+        const float *ez = reinterpret_cast<const float *>(sb + S::ez_off) + w * HUW2;
+        const uint8_t *em = sb + S::m_off + w * HM2;
+        const float *z = zb + (p & 1) * (WZ * ZROW2 * 3);
+        const int k = kc0 + w, at = ((p - P0) * WZ + w) * 3;
+        float zv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (w > 0) lds6(z + ((w - 1) * ZROW2 + 2 * l) * 3, zv);
+        float R[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) R[i] = q[i] + zv[i];
+        if (seam) {   // node column jc0: finished after the cluster barrier
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                s_own[at + d] = q[d];
+                s_ownz[at + d] = zv[d];
+            }
+        }
+        if (in0) h_store2<MODE>(L.at(p, j0, k), in1, !seam, e, R, Uu, out, omega, dsum, dsum2);
+        if (l == 31) {   // this CTA's part of node column jc0 + HY2
+            float Sq[3], Sz[3], Sd[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                Sq[d] = P[8 + d].y;
+                Sz[d] = w > 0 ? z[((w - 1) * ZROW2 + HY2) * 3 + d] : 0.f;
+                Sd[d] = Sq[d] + Sz[d];
+            }
+            if (r + 1 < CY) {
+                float *rem = cluster.map_shared_rank(s_recv, r + 1);
+                float *remz = cluster.map_shared_rank(s_recvz, r + 1);
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    rem[at + d] = Sq[d];
+                    remz[at + d] = Sz[d];
+                }
+            } else if (tail_owner) {
+                const float uu[3] = {Uu[6], Uu[7], Uu[8]};
+                h_store<float, MODE>(L.at(p, g.ny, k), em[HY2], Sd, uu, ef + 3 * HY2, ed + 3 * HY2, out, omega,
+                                     dsum, er + 3 * HY2, ez + 3 * HY2, dsum2);
+            }
+        }
+    };
+
+    int cur = 0;
+    bool fail = false;
+    // Step t: the element pair between faces t - 1 (Fc) and t (from raw,
+    // waited for and read in step t - 1); then, before the barrier, the face
+    // of stage t + 1 and the epilogue operands of node plane p = E0 + t - 1
+    // (both in ring slots already waited for), so that their shared-memory
+    // latency overlaps the barrier.
+    float raw[2][3][3];
+    float2 cxn = make_float2(0.f, 0.f);
+    auto step = [&](int t, float (&Uc)[9], float2 (&Fc)[HF], float2 (&Ac)[HF], float (&Un)[9], float2 (&Fn)[HF],
+                    float2 (&An)[HF]) {
+        cur = t;
+        wait_stage(t);
+        load_face(t, raw, cxn);
+        take_face(raw, Un, Fn);
+        element_h2(Fc, Fn, cxn, hc, Ac, An);
+        const int p = E0 + t - 1;   // node plane finished by this element pair
+        const bool out_plane = p >= P0;
+        float q[6];
+        Epi2 e;
+        if (out_plane) {
+            face_h(Ac);   // node partials of plane p
+            reduce_y(p, Ac, q);
+        }
+        fail = __syncthreads_or(bad);   // z partners visible; ring slot t - 1 free
+        if (!fail && tid == 0 && t - 1 + HRING < nst) issue(t - 1 + HRING);
+        if (!fail && out_plane) {
+            load_epi2<MODE>(smem + (t % HRING) * S::slot, w, l, e);
+            emit(p, t, Ac, q, Uc, e);
+        }
+    };
+    auto finish_last = [&](float (&Uc)[9], float2 (&Ac)[HF]) {   // plane nx: only elements nx - 1 touch it
+        cur = nE + 1;
+        wait_stage(nE + 1);
+        float q[6];
+        Epi2 e;
+        face_h(Ac);
+        reduce_y(E1, Ac, q);
+        load_epi2<MODE>(smem + ((nE + 1) % HRING) * S::slot, w, l, e);
+        fail = __syncthreads_or(bad);
+        if (!fail) emit(E1, nE + 1, Ac, q, Uc, e);
+    };
+
+    float U0[9], U1[9];
+    float2 F0[HF], A0[HF], F1[HF], A1[HF];
+    wait_stage(0);
+    load_face(0, raw, cxn);
+    take_face(raw, U0, F0);
+#pragma unroll
+    for (int q = 0; q < HF; ++q) A0[q] = make_float2(0.f, 0.f);
+    fail = __syncthreads_or(bad);
+    {
+        int t = 1;
+        for (; !fail && t + 1 <= nE; t += 2) {
+            step(t, U0, F0, A0, U1, F1, A1);
+            if (!fail) step(t + 1, U1, F1, A1, U0, F0, A0);
+        }
+        if (!fail && t <= nE) {   // odd count: one more step, the state ends in set 1
+            step(t, U0, F0, A0, U1, F1, A1);
+            if (!fail && last_plane) finish_last(U1, A1);
+        } else if (!fail && last_plane) {
+            finish_last(U0, A0);
+        }
+    }
+    if (fail && tid == 0) {
+        for (int s = cur; s < issued; ++s)
+            if (s != skip_stage) (void)mbar_wait_for(&bar[s % HRING], (uint32_t)((s / HRING) & 1), kHDrainNs);
+        if (err) atomicExch(err, GPUTO_ERR_TIMEOUT);
+    }
+    cluster.sync();   // seam partials from the left neighbour have arrived
+    if (!fail && r > 0) {   // node column jc0, from both sides of the seam
+        const int np = P1 - P0;
+        for (int idx = tid; idx < np * WZ; idx += NT) {
+            const int pp = idx / WZ, ww = idx - pp * WZ;
+            const int k = kc0 + ww, p = P0 + pp, at = idx * 3;
+            if (!((ww >= 1 || zt == 0) && k <= g.nz)) continue;
+            const long long base = L.at(p, jc0, k);
+            float v[3], uu[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                v[d] = (s_own[at + d] + s_recv[at + d]) + (s_ownz[at + d] + s_recvz[at + d]);
+                if (N::PRE)
+                    uu[d] = hmul(hmul(prerelax, f[base + d]), rdiag[base + d]);
+                else
+                    uu[d] = (MODE == MODE_APPLY || N::D) ? ug[base + d] : 0.f;
+            }
+            h_store<float, MODE>(base, mask[g.node(p, jc0, k)], v, uu, f + base, rdiag + base, out, omega, dsum,
+                                 Rd + base, zo + base, dsum2);
+        }
+    }
+    if ((MODE == MODE_APPLY || MODE == MODE_JACOBI_DOT) && dot_partial) {
+        constexpr bool PAIR = MODE == MODE_JACOBI_DOT;
+        double *red = reinterpret_cast<double *>(smem + S::red_off);
+        for (int o = 16; o > 0; o >>= 1) {
+            dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
+            if (PAIR) dsum2 += __shfl_xor_sync(0xffffffffu, dsum2, o);
+        }
+        if (l == 0) {
+            red[w] = dsum;
+            red[WZ + w] = dsum2;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double v = 0.0, v2 = 0.0;
+            for (int qq = 0; qq < WZ; ++qq) {
+                v += red[qq];
+                v2 += red[WZ + qq];
+            }
+            const long long cta = blockIdx.x + gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
+            if (MODE == MODE_APPLY) {
+                dot_partial[cta] = v;
+            } else {
+                dot_partial[2 * cta] = v;
+                dot_partial[2 * cta + 1] = v2;
+            }
+        }
+    }
+}
+
 template <typename T> constexpr int hwz() { return 8; }
 
 // Row pitch of the padded mask copy: TMA needs 16-byte row strides.
 long long hmask_pitch(const Grid &g) { return ((long long)g.ny + 1 + 15) & ~15LL; }
 
-template <typename T>
-int hztiles(const Grid &g)
+// z tiles of WZ element rows, overlapping by one row
+int hztiles_wz(const Grid &g, int WZ)
 {
-    constexpr int WZ = hwz<T>();
     const int rest = g.nz + 1 - WZ;
     return 1 + (rest > 0 ? (rest + WZ - 2) / (WZ - 1) : 0);
 }
+template <typename T> int hztiles(const Grid &g) { return hztiles_wz(g, hwz<T>()); }
 
 // Test hook for the bounded waits (gputo_debug_set_sweep_fault): the ring
 // stage whose copies a launch leaves unissued (-1: none) and how long each
@@ -645,8 +1169,9 @@ SweepFaultHook sweep_fault_hook()
 }
 
 struct HState {
-    bool init = false, ok = false;
+    bool init = false, ok = false, ok2 = false;
     int resident[2][7][HMAXCY + 1] = {};   // [FP64?][mode][cluster size]: clusters resident on the device
+    int resident2[7][HMAXCY + 1] = {};     // the same for the paired FP32 kernel (hsweep2_kernel)
 };
 
 HState &hstate(int dev)
@@ -658,14 +1183,15 @@ HState &hstate(int dev)
 // Node planes per x chunk: whole rounds of resident clusters, few overlapping
 // elements, and a fixed cost per CTA of about four planes.
 template <typename T>
-int hchunk(const Grid &g, int mode)
+int hchunk(const Grid &g, int mode, bool pairs = false)
 {
     int dev = 0;
     cudaGetDevice(&dev);
-    const int cy = (g.ny + HY - 1) / HY;
-    const int res = cy <= HMAXCY ? hstate(dev).resident[sizeof(T) == 8][mode][cy] : 0;
+    const int cy = (g.ny + (pairs ? HY2 : HY) - 1) / (pairs ? HY2 : HY);
+    const HState &hs = hstate(dev);
+    const int res = cy <= HMAXCY ? (pairs ? hs.resident2[mode][cy] : hs.resident[sizeof(T) == 8][mode][cy]) : 0;
     if (res <= 0 || g.nx <= HTX) return g.nx <= HTX ? (g.nx > 0 ? g.nx : 1) : HTX;
-    const long long nzt = hztiles<T>(g);
+    const long long nzt = pairs ? hztiles_wz(g, HWZ2) : hztiles<T>(g);
     long long best = -1;
     int bh = HTX;
     for (int ncx = (g.nx + HTX - 1) / HTX; ncx <= g.nx; ++ncx) {
@@ -685,19 +1211,19 @@ int hchunk(const Grid &g, int mode)
 // The x chunk of a launch: the caller's choice (an autotuned option, clamped
 // to 1 .. HTX planes) or the heuristic above.
 template <typename T>
-int hsweep_chunk(const Grid &g, int mode, int xchunk)
+int hsweep_chunk(const Grid &g, int mode, int xchunk, bool pairs = false)
 {
-    if (xchunk <= 0) return hchunk<T>(g, mode);
+    if (xchunk <= 0) return hchunk<T>(g, mode, pairs);
     int c = xchunk < HTX ? xchunk : HTX;
     return c < g.nx ? c : (g.nx > 0 ? g.nx : 1);
 }
 
 template <typename T>
-dim3 hgrid(const Grid &g, int htx)
+dim3 hgrid(const Grid &g, int htx, bool pairs = false)
 {
-    const int cy = (g.ny + HY - 1) / HY;
+    const int cy = (g.ny + (pairs ? HY2 : HY) - 1) / (pairs ? HY2 : HY);
     const int ncx = g.nx > htx ? (g.nx + htx - 1) / htx : 1;
-    return dim3((unsigned)cy, (unsigned)hztiles<T>(g), (unsigned)ncx);
+    return dim3((unsigned)cy, (unsigned)(pairs ? hztiles_wz(g, HWZ2) : hztiles<T>(g)), (unsigned)ncx);
 }
 
 template <typename T, int MODE>
@@ -764,9 +1290,94 @@ int hlaunch(const Lay &L, const ELay &E, const HadamardKe &hk, const T *CX, cons
     const SweepFaultHook hook = sweep_fault_hook();
     GPUTO_CUDA(cudaLaunchKernelEx(&cfg, hsweep_kernel<T, MODE, WZ>, mu, md, mf, mc, mm, mr, mz, L, hc, htx, f, rdiag, mask,
                                   out, omega, prerelax, dot_partial, done, err, Rd, zo, hook.wait_ns, hook.skip_stage,
-                                  ce, dcv, dsK, uc, Lc ? *Lc : L));
+                                  ce, dcv, dsK, uc, Lc ? *Lc : L, u));
     count_launches(1);
     return GPUTO_OK;
+}
+
+// The paired FP32 sweep (hsweep2_kernel): the same maps with boxes of HY2
+// element columns.
+template <int MODE>
+int hlaunch2(const Lay &L, const ELay &E, const HadamardKe &hk, const float *CX, const float *u, const float *f,
+             const float *rdiag, const uint8_t *maskp, const uint8_t *mask, float *out, float omega, float prerelax,
+             double *dot_partial, const int *done, int *err, cudaStream_t st, const double *Rd, const float *zo,
+             int xchunk)
+{
+    constexpr int WZ = HWZ2;
+    using N = HNeeds<MODE>;
+    using S = HSmem2<MODE>;
+    const Grid &g = L.g;
+    const uint64_t es = sizeof(float);
+    auto node_map = [&](CUtensorMap *m, const float *base) {
+        return make_tmap_3d(m, base, (int)es, (uint64_t)L.pitch, (uint64_t)g.nz + 1, (uint64_t)g.nx + 1,
+                            L.pitch * es, L.pitch * es * (g.nz + 1), HUW2, WZ + 1, 1);
+    };
+    CUtensorMap mu, md, mf, mc, mm, mr, mz;
+    int s = node_map(&mu, N::PRE ? f : u);
+    if (!s && N::DOT) {
+        s = make_tmap_3d(&mr, Rd, 8, (uint64_t)L.pitch, (uint64_t)g.nz + 1, (uint64_t)g.nx + 1, L.pitch * 8,
+                         L.pitch * 8 * (g.nz + 1), HUW2, WZ + 1, 1);
+        if (!s) s = node_map(&mz, zo);
+    }
+    if (!s && N::D) s = node_map(&md, rdiag);
+    if (!s && N::F) s = node_map(&mf, f);
+    if (!s)
+        s = make_tmap_3d(&mc, CX, (int)es, (uint64_t)E.pitch, (uint64_t)E.g.nz, (uint64_t)E.g.nx, E.pitch * es,
+                         E.pitch * es * E.g.nz, HY2, WZ, 1);
+    const uint64_t mp = hmask_pitch(g);
+    if (!s)
+        s = make_tmap_3d(&mm, maskp, 1, mp, (uint64_t)g.nz + 1, (uint64_t)g.nx + 1, mp, mp * (g.nz + 1), HM2, WZ, 1);
+    if (s) return s;
+    if (!N::D) md = mu;
+    if (!N::F) mf = mu;
+    if (!N::DOT) mr = mz = mu;
+    const HC<float2> hc = pair_hc(make_hc<float>(hk));
+    const int htx = hsweep_chunk<float>(g, MODE, xchunk, true);
+    const dim3 grid = hgrid<float>(g, htx, true);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(32 * WZ);
+    cfg.dynamicSmemBytes = S::bytes;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = grid.x;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const SweepFaultHook hook = sweep_fault_hook();
+    GPUTO_CUDA(cudaLaunchKernelEx(&cfg, hsweep2_kernel<MODE>, mu, md, mf, mc, mm, mr, mz, L, hc, htx, f, rdiag, mask,
+                                  out, omega, prerelax, dot_partial, done, err, Rd, zo, hook.wait_ns,
+                                  hook.skip_stage, u));
+    count_launches(1);
+    return GPUTO_OK;
+}
+
+template <int MODE>
+cudaError_t h2set_attr()
+{
+    return cudaFuncSetAttribute(hsweep2_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)HSmem2<MODE>::bytes);
+}
+
+template <int MODE>
+int h2resident(int cy)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)cy, 1, 1);
+    cfg.blockDim = dim3(32 * HWZ2);
+    cfg.dynamicSmemBytes = HSmem2<MODE>::bytes;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)cy;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, hsweep2_kernel<MODE>, &cfg) != cudaSuccess) return 0;
+    return n;
 }
 
 template <typename T, int MODE>
@@ -927,6 +1538,19 @@ int init_hsweep_kernels()
     }
     cudaGetLastError();
     s.ok = true;
+    if (h2set_attr<MODE_APPLY>() == cudaSuccess && h2set_attr<MODE_DEFECT>() == cudaSuccess &&
+        h2set_attr<MODE_JACOBI>() == cudaSuccess && h2set_attr<MODE_JACOBI_PRE>() == cudaSuccess &&
+        h2set_attr<MODE_JACOBI_DOT>() == cudaSuccess) {
+        for (int cy = 1; cy <= HMAXCY; ++cy) {
+            s.resident2[MODE_APPLY][cy] = h2resident<MODE_APPLY>(cy);
+            s.resident2[MODE_DEFECT][cy] = h2resident<MODE_DEFECT>(cy);
+            s.resident2[MODE_JACOBI][cy] = h2resident<MODE_JACOBI>(cy);
+            s.resident2[MODE_JACOBI_PRE][cy] = h2resident<MODE_JACOBI_PRE>(cy);
+            s.resident2[MODE_JACOBI_DOT][cy] = h2resident<MODE_JACOBI_DOT>(cy);
+        }
+        s.ok2 = true;
+    }
+    cudaGetLastError();   // without the paired kernel, hsweep_kernel serves the FP32 sweeps
     return GPUTO_OK;
 }
 
@@ -944,10 +1568,23 @@ bool hsweep_fits(const Grid &g)
     return true;
 }
 
-template <typename T>
-int hsweep_blocks(const Grid &g, int mode, int xchunk)
+bool hsweep_pairs_fit(const Grid &g)
 {
-    const dim3 gr = hgrid<T>(g, hsweep_chunk<T>(g, mode, xchunk));
+    int dev = 0;
+    if (!hsweep_fits<float>(g) || cudaGetDevice(&dev) != cudaSuccess) return false;
+    const HState &s = hstate(dev);
+    const int cy = (g.ny + HY2 - 1) / HY2;
+    if (!s.ok2 || cy > HMAXCY) return false;
+    for (int m = 0; m < 5; ++m)
+        if (s.resident2[m][cy] <= 0) return false;
+    return true;
+}
+
+template <typename T>
+int hsweep_blocks(const Grid &g, int mode, int xchunk, bool pairs)
+{
+    pairs = pairs && sizeof(T) == 4 && mode != MODE_ENERGY && mode != MODE_JACOBI_PRO && hsweep_pairs_fit(g);
+    const dim3 gr = hgrid<T>(g, hsweep_chunk<T>(g, mode, xchunk, pairs), pairs);
     return (int)(gr.x * gr.y * gr.z);
 }
 
@@ -1027,8 +1664,33 @@ template <typename T>
 int launch_hsweep(int mode, const Lay &L, const ELay &E, const HadamardKe &hk, const T *CX, const T *u, const T *f,
                   const T *rdiag, const uint8_t *mask, const uint8_t *maskp, T *out, T omega, T prerelax,
                   double *dot_partial, const int *done, int *err, cudaStream_t st, const double *Rd, const T *zo,
-                  const T *uc, const Lay *Lc, int xchunk)
+                  const T *uc, const Lay *Lc, int xchunk, bool pairs)
 {
+    if constexpr (sizeof(T) == 4) {
+        if (pairs && mode != MODE_JACOBI_PRO && hsweep_pairs_fit(L.g)) {
+            switch (mode) {
+            case MODE_JACOBI_DOT:
+                if (!Rd || !zo || !dot_partial) {
+                    set_error("a Jacobi sweep with dots needs the residual, z_old and the partials");
+                    return GPUTO_ERR_ARG;
+                }
+                return hlaunch2<MODE_JACOBI_DOT>(L, E, hk, CX, u, f, rdiag, maskp, mask, out, omega, prerelax,
+                                                 dot_partial, done, err, st, Rd, zo, xchunk);
+            case MODE_APPLY:
+                return hlaunch2<MODE_APPLY>(L, E, hk, CX, u, f, rdiag, maskp, mask, out, omega, prerelax, dot_partial,
+                                            done, err, st, nullptr, nullptr, xchunk);
+            case MODE_DEFECT:
+                return hlaunch2<MODE_DEFECT>(L, E, hk, CX, u, f, rdiag, maskp, mask, out, omega, prerelax, nullptr,
+                                             done, err, st, nullptr, nullptr, xchunk);
+            case MODE_JACOBI:
+                return hlaunch2<MODE_JACOBI>(L, E, hk, CX, u, f, rdiag, maskp, mask, out, omega, prerelax, nullptr,
+                                             done, err, st, nullptr, nullptr, xchunk);
+            default:
+                return hlaunch2<MODE_JACOBI_PRE>(L, E, hk, CX, u, f, rdiag, maskp, mask, out, omega, prerelax,
+                                                 nullptr, done, err, st, nullptr, nullptr, xchunk);
+            }
+        }
+    }
     switch (mode) {
     case MODE_JACOBI_PRO:
         if (!uc || !Lc || Lc->g.nx * 2 != L.g.nx || Lc->g.ny * 2 != L.g.ny || Lc->g.nz * 2 != L.g.nz) {
@@ -1067,15 +1729,16 @@ int launch_hsweep(int mode, const Lay &L, const ELay &E, const HadamardKe &hk, c
 
 template bool hsweep_fits<float>(const Grid &);
 template bool hsweep_fits<double>(const Grid &);
-template int hsweep_blocks<float>(const Grid &, int, int);
-template int hsweep_blocks<double>(const Grid &, int, int);
+template int hsweep_blocks<float>(const Grid &, int, int, bool);
+template int hsweep_blocks<double>(const Grid &, int, int, bool);
 template int launch_hsweep<float>(int, const Lay &, const ELay &, const HadamardKe &, const float *, const float *,
                                   const float *, const float *, const uint8_t *, const uint8_t *, float *, float,
                                   float, double *, const int *, int *, cudaStream_t, const double *, const float *,
-                                  const float *, const Lay *, int);
+                                  const float *, const Lay *, int, bool);
 template int launch_hsweep<double>(int, const Lay &, const ELay &, const HadamardKe &, const double *,
                                    const double *, const double *, const double *, const uint8_t *,
                                    const uint8_t *, double *, double, double, double *, const int *, int *,
-                                   cudaStream_t, const double *, const double *, const double *, const Lay *, int);
+                                   cudaStream_t, const double *, const double *, const double *, const Lay *, int,
+                                   bool);
 
 }  // namespace gputo

@@ -108,6 +108,7 @@ int Solver::create(int nelx, int nely, int nelz, int nl_, const gputo_options *o
     }
     if (opt.nswp < 0 || opt.nswp_fine < 0 || opt.check_every < 1 || !(opt.omega > 0) || opt.tc_parts < 0 ||
         (opt.sweep_xchunk != 0 && (opt.sweep_xchunk < 8 || opt.sweep_xchunk > 32)) ||
+        opt.sweep_pairs < 0 || opt.sweep_pairs > 1 ||
         opt.tc_parts > 2 ||
         opt.tc_xchunk < 0 || (opt.coarse != GPUTO_COARSE_GALERKIN && opt.coarse != GPUTO_COARSE_REDISCRETIZED) ||
         (opt.precision != GPUTO_PREC_FP64 && opt.precision != GPUTO_PREC_MIXED)) {
@@ -182,6 +183,9 @@ int Solver::create(int nelx, int nely, int nelz, int nl_, const gputo_options *o
     // the smallest x chunk an option may ask for gives the most CTAs
     partial_cap = std::max({fine_sweep_blocks(g[0]), hsweep_blocks<double>(g[0], MODE_APPLY, 8),
                             2 * hsweep_blocks<float>(g[0], MODE_JACOBI_DOT, 8),
+                            2 * hsweep_blocks<float>(g[0], MODE_JACOBI_DOT, 0),
+                            2 * hsweep_blocks<float>(g[0], MODE_JACOBI_DOT, 8, true),
+                            2 * hsweep_blocks<float>(g[0], MODE_JACOBI_DOT, 0, true),
                             2 * hsweep_blocks<double>(g[0], MODE_ENERGY), 1 << 12});
     ALLOC(partial, partial_cap);
     ALLOC(ticket, 4);
@@ -547,7 +551,8 @@ void Solver::iteration(cudaStream_t st)
         launch_pcg_update(nv, Uw, R, P, Q, partial, ticket, sc, st, Lf[0].f);
         if (fused_dot()) {
             vcycle_impl<float>(Lf, CXpf, Lf[0].f, Lf[0].u1, done, st, R, Zold32, partial);
-            launch_finish_dot2(hsweep_blocks<float>(g[0], MODE_JACOBI_DOT, opt.sweep_xchunk), partial, sc, st);
+            launch_finish_dot2(hsweep_blocks<float>(g[0], MODE_JACOBI_DOT, opt.sweep_xchunk, opt.sweep_pairs != 0),
+                               partial, sc, st);
         } else {
             vcycle_impl<float>(Lf, CXpf, Lf[0].f, Lf[0].u1, done, st);
             launch_dot2<float>(nv, R, Lf[0].u1, Zold32, partial, ticket, sc, done, st);
@@ -700,6 +705,7 @@ int Solver::set_tunables(const gputo_options &o)
 {
     if (o.nswp < 0 || o.nswp_fine < 0 || o.check_every < 1 || !(o.omega > 0) || o.tc_parts < 0 || o.tc_parts > 2 ||
         (o.sweep_xchunk != 0 && (o.sweep_xchunk < 8 || o.sweep_xchunk > 32)) ||
+        o.sweep_pairs < 0 || o.sweep_pairs > 1 ||
         o.tc_xchunk < 0 ||
         o.fine_op < 0 || o.fine_op > 1 ||
         (o.tc_parts > 0 && opt.precision != GPUTO_PREC_MIXED)) {
@@ -710,6 +716,7 @@ int Solver::set_tunables(const gputo_options &o)
     opt.nswp_fine = o.nswp_fine;
     opt.fuse_prolong = o.fuse_prolong;
     opt.sweep_xchunk = o.sweep_xchunk;
+    opt.sweep_pairs = o.sweep_pairs;
     opt.omega = o.omega;
     opt.prerelax = o.prerelax;
     opt.check_every = o.check_every;

@@ -106,7 +106,8 @@ struct Solver {
     {
         if (use_hsweep<T>(Lo.g) && B.rdiag)
             return launch_hsweep<T>(mode, Lo, E, hk, CXl, u, f, B.rdiag, mask[l], maskp[l], out, omega, pr,
-                                    dot_partial, done, err, st, Rd, zo, uc, Lc, l == 0 ? opt.sweep_xchunk : 0);
+                                    dot_partial, done, err, st, Rd, zo, uc, Lc, l == 0 ? opt.sweep_xchunk : 0,
+                                    l == 0 && opt.sweep_pairs != 0);
         return launch_fine_sweep<T>(mode, Lo, E, CXl, u, f, B.diag, mask[l], out, omega, pr, dot_partial, done, err,
                                     st);
     }

@@ -102,6 +102,10 @@ typedef struct {
                             fine sweeps: 0 = chosen from the device's resident
                             clusters, else 8 .. 32 (the autotuner's tile
                             choice)                                               */
+    int sweep_pairs;     /* 1 (default): the FP32 fine sweeps of the mixed
+                            V-cycle give each lane two element columns
+                            (paired FP32 arithmetic, nely <= 512; same results
+                            bit for bit); 0: one column per lane              */
 } gputo_options;
 
 void gputo_default_options(gputo_options *opt);
