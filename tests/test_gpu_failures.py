@@ -104,13 +104,14 @@ def test_nan_stiffness_is_caught_by_the_coarsest_factor(oracle, gputo):
     assert nit == nito and np.linalg.norm(U2 - Uo) <= 1e-9 * np.linalg.norm(Uo)
 
 
-@pytest.mark.parametrize("prec", ["fp64", "fp32"])
-def test_bounded_wait_runs_out_and_the_context_stays_usable(oracle, gputo, torch, prec):
+@pytest.mark.parametrize("prec,pairs", [("fp64", 0), ("fp32", 0), ("fp32", 1)])
+def test_bounded_wait_runs_out_and_the_context_stays_usable(oracle, gputo, torch, prec, pairs):
+    """pairs: the FP32 sweep variant (one or two element columns per lane)."""
     p, CX = _case(oracle, (32, 16, 16), seed=5)
     f64 = dict(dtype=torch.float64, device="cuda")
     mixed = prec == "fp32"
     s = gputo.Solver(32, 16, 16, 4, gputo.default_options(
-        precision=gputo.PREC_MIXED if mixed else gputo.PREC_FP64))
+        precision=gputo.PREC_MIXED if mixed else gputo.PREC_FP64, sweep_pairs=pairs))
     s.set_problem(p.Ke0, p.fixed)
     s.setup(torch.as_tensor(CX, **f64))
     u = torch.as_tensor(np.random.default_rng(6).standard_normal(p.ndof), **f64)
