@@ -652,18 +652,19 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
 // the index arithmetic, the seam branches) are shared by two elements.  The
 // node pairs of the epilogue move as 8-byte words (f, 1/diag, the z
 // partners, the output).  About 40 % fewer instructions per element than
-// hsweep_kernel.  Twice the state per thread (about 200 registers): CTAs of
-// four warps, two per SM.  The per-step CTA barrier holds all of a CTA's
-// warps in the same phase (element arithmetic, then shuffles and shared
-// memory, then stores); a second CTA on the SM issues during the first one's
-// barrier and latency phases.
+// hsweep_kernel.  Twice the state per thread (165-200 registers): CTAs of
+// four warps, two or three per SM.  The per-step CTA barrier holds all of a
+// CTA's warps in the same phase (element arithmetic, then shuffles and shared
+// memory, then stores); the other CTAs on the SM issue during one CTA's
+// barrier, latency and ring-filling phases.  (Eight warps per CTA, with the
+// barrier or with the warps synchronised point to point by mbarriers, and
+// loading the next face before the barrier, all measured slower.)
 constexpr int HY2 = 64;     // element columns per CTA along y (two per lane)
 constexpr int HUW2 = 196;   // u box width: 3 (HY2 + 1) = 195 values, rounded to 16 bytes
 constexpr int HM2 = 80;     // mask box width in bytes: HY2 + 1 = 65 nodes, rounded to 16
 constexpr int ZROW2 = 66;   // z exchange row: 65 node columns, even so node pairs are 8-byte aligned
-constexpr int HWZ2 = 4;     // warps (element rows along z) per CTA: two CTAs share an SM, so one CTA's
-                            // barrier leaves the other issuing (measured 79 us against 84 us for one
-                            // CTA of eight warps, despite the extra overlapping row)
+constexpr int HWZ2 = 4;     // warps (element rows along z) per CTA (measured 79 us against 84 us for one
+                            // CTA of eight warps per SM, despite the extra overlapping row in four)
 
 template <int MODE>
 struct HSmem2 {
@@ -830,8 +831,16 @@ __device__ __forceinline__ void h_store2(long long base, bool in1, bool count0, 
     }
 }
 
+// CTAs per SM the compiler budgets registers for: three where three fit in
+// shared memory (168 registers, no spills; the Jacobi sweep measured 73.7
+// against 78.2 us at two), else two.
+template <int MODE> struct HMinBlocks2 {
+    static constexpr int value = (MODE == MODE_APPLY || MODE == MODE_DEFECT || MODE == MODE_JACOBI) ? 3 : 2;
+};
+static_assert(3 * (HSmem2<MODE_JACOBI>::bytes + 1024) <= 228 * 1024, "three Jacobi CTAs must share an SM");
+
 template <int MODE>
-__global__ void __launch_bounds__(32 * HWZ2, 2)
+__global__ void __launch_bounds__(32 * HWZ2, HMinBlocks2<MODE>::value)
 hsweep2_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ CUtensorMap tm_d,
                const __grid_constant__ CUtensorMap tm_f, const __grid_constant__ CUtensorMap tm_c,
                const __grid_constant__ CUtensorMap tm_m, const __grid_constant__ CUtensorMap tm_r,
