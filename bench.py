@@ -637,6 +637,8 @@ def run_one_step(args):
     F, fixed = gputo.cantilever(NELX, NELY, NELZ)
     opts = gputo.default_options(precision=prec, nswp_fine=args.nswp_fine,
                                  check_every=8 if args.nswp_fine else 1, sweep_pairs=args.sweep_pairs)
+    if args.nswp:
+        opts.nswp = args.nswp
     dl = gputo.DesignLoop(NELX, NELY, NELZ, NL, F, fixed, gputo.hex8_stiffness(), volfrac=VOLFRAC,
                           penal=PENAL, rmin=RMIN, move=MOVE, tol=TOL, maxit=MAXIT,
                           options=opts, x0=bench_design())
@@ -850,6 +852,7 @@ def main():
     ap.add_argument("--sweep-pairs", type=int, default=1, choices=[0, 1],
                     help="profiling aid: FP32 fine sweeps with two element columns per lane (1) or one (0)")
     ap.add_argument("--one-step", choices=["mixed", "fp64"], help="profiling aid: one design iteration")
+    ap.add_argument("--nswp", type=int, default=0, help="profiling aid: V-cycle sweeps for --one-step (0: 3)")
     ap.add_argument("--nswp-fine", type=int, default=0,
                     help="with --one-step: Jacobi sweeps on the finest level (the autotuner's choice)")
     ap.add_argument("--workload", default="cantilever", choices=["cantilever", "batch", "bridge", "homog"],

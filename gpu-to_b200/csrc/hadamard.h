@@ -28,10 +28,14 @@ __device__ __forceinline__ float2 hfma(float2 a, float2 b, float2 c) { return __
 __device__ __forceinline__ float2 operator+(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 operator-(float2 a, float2 b) { return __ffma2_rn(make_float2(-1.f, -1.f), b, a); }
 __device__ __forceinline__ float2 operator*(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 operator-(float2 a) { return make_float2(-a.x, -a.y); }
 __device__ __forceinline__ float hmul(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ double hmul(double a, double b) { return __dmul_rn(a, b); }
 template <typename T> __device__ __forceinline__ T hzero() { return T(0); }
 template <> __device__ __forceinline__ float2 hzero<float2>() { return make_float2(0.f, 0.f); }
+// A constant in the arithmetic type (both halves of a pair).
+template <typename T> __device__ __forceinline__ T hconst(double v) { return (T)v; }
+template <> __device__ __forceinline__ float2 hconst<float2>(double v) { return make_float2((float)v, (float)v); }
 inline HC<float2> pair_hc(const HC<float> &k)
 {
     auto p = [](float v) { return make_float2(v, v); };

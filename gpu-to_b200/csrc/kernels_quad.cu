@@ -19,8 +19,10 @@
 // axis, so the gradients at all 8 Gauss points cost 72 operations; the
 // adjoint sum_g B_g^T sigma_g comes back as y = (1/8) T W, W built from sums
 // of the stress over the Gauss points.  About 530 operations per element
-// instead of 1250 FMAs for the strain-displacement products.
+// instead of 1250 FMAs for the strain-displacement products.  In FP32 a
+// thread takes two elements adjacent along y on float2 pairs.
 #include "gputo_internal.h"
+#include "hadamard.h"
 
 namespace gputo {
 
@@ -53,6 +55,95 @@ __device__ __forceinline__ void h22(const T (&P)[2][2], T (&H)[4])
     H[3] = q1 - q0;
 }
 
+// Pass 1 of one element from its 24 corner values ue (corner a, component
+// d at 3 a + d) and its 8 Gauss-point densities cg[ix][iz][iy] to its 24
+// outputs.  V is the arithmetic type: float or double for one element, float2
+// for two elements in one instruction stream (paired FP32 instructions).
+template <typename V>
+__device__ __forceinline__ void quad_body(const V (&ue)[24], const V (&cg)[2][2][2], V lam, V mu, V (&ye)[24])
+{
+    // corner a -> index c = 4 x + 2 y + z; modes p use the same bits
+    V Vm[3][8];
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) Vm[d][4 * local_x(a) + 2 * local_y(a) + local_z(a)] = ue[3 * a + d];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) fwht8(Vm[d]);
+    const V s = hconst<V>(0.57735026918962576451);   // Gauss coordinate 1/sqrt(3)
+    // 8 x displacement gradient: Gx[d][iy][iz] = 8 du_d/dx at Gauss points
+    // (., iy, iz), Gy[d][ix][iz], Gz[d][ix][iy] likewise
+    V Gx[3][2][2], Gy[3][2][2], Gz[3][2][2];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const V si = i ? s : -s;
+            const V ax = hfma(si, Vm[d][6], -Vm[d][4]), bx = hfma(-si, Vm[d][7], Vm[d][5]);
+            const V ay = hfma(si, Vm[d][6], -Vm[d][2]), by = hfma(-si, Vm[d][7], Vm[d][3]);
+            const V az = hfma(si, Vm[d][5], -Vm[d][1]), bz = hfma(-si, Vm[d][7], Vm[d][3]);
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const V sj = j ? s : -s;
+                Gx[d][i][j] = hfma(sj, bx, ax);
+                Gy[d][i][j] = hfma(sj, by, ay);
+                Gz[d][i][j] = hfma(sj, bz, az);
+            }
+        }
+    // stress at each Gauss point, summed over the axis its column does not
+    // depend on: Px[d][iy][iz] = sum_ix sigma[d][x], Py[d][ix][iz], Pz[d][ix][iy]
+    V Px[3][2][2], Py[3][2][2], Pz[3][2][2];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) Px[d][i][j] = Py[d][i][j] = Pz[d][i][j] = hzero<V>();
+#pragma unroll
+    for (int ix = 0; ix < 2; ++ix)
+#pragma unroll
+        for (int iz = 0; iz < 2; ++iz)
+#pragma unroll
+            for (int iy = 0; iy < 2; ++iy) {
+                const V c = cg[ix][iz][iy];
+                const V cl = c * lam, cm = c * mu, cm2 = cm + cm;   // lam, mu carry 1/64
+                const V g00 = Gx[0][iy][iz], g01 = Gy[0][ix][iz], g02 = Gz[0][ix][iy];
+                const V g10 = Gx[1][iy][iz], g11 = Gy[1][ix][iz], g12 = Gz[1][ix][iy];
+                const V g20 = Gx[2][iy][iz], g21 = Gy[2][ix][iz], g22 = Gz[2][ix][iy];
+                const V tr = g00 + g11 + g22;
+                const V s00 = hfma(cl, tr, cm2 * g00), s11 = hfma(cl, tr, cm2 * g11), s22 = hfma(cl, tr, cm2 * g22);
+                const V s01 = cm * (g01 + g10), s02 = cm * (g02 + g20), s12 = cm * (g12 + g21);
+                Px[0][iy][iz] = Px[0][iy][iz] + s00;
+                Px[1][iy][iz] = Px[1][iy][iz] + s01;
+                Px[2][iy][iz] = Px[2][iy][iz] + s02;
+                Py[0][ix][iz] = Py[0][ix][iz] + s01;
+                Py[1][ix][iz] = Py[1][ix][iz] + s11;
+                Py[2][ix][iz] = Py[2][ix][iz] + s12;
+                Pz[0][ix][iy] = Pz[0][ix][iy] + s02;
+                Pz[1][ix][iy] = Pz[1][ix][iy] + s12;
+                Pz[2][ix][iy] = Pz[2][ix][iy] + s22;
+            }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        V X[4], Y[4], Z[4];   // [00, 10, 01, 11]: sums weighted by the signs of the two Gauss coordinates
+        h22(Px[d], X);
+        h22(Py[d], Y);
+        h22(Pz[d], Z);
+        V W[8];
+        W[0] = hzero<V>();
+        W[1] = -Z[0];
+        W[2] = -Y[0];
+        W[3] = s * (Y[2] + Z[2]);
+        W[4] = -X[0];
+        W[5] = s * (X[2] + Z[1]);
+        W[6] = s * (X[1] + Y[1]);
+        W[7] = -(s * s) * (X[3] + Y[3] + Z[3]);
+        fwht8(W);
+#pragma unroll
+        for (int a = 0; a < 8; ++a) ye[3 * a + d] = W[4 * local_x(a) + 2 * local_y(a) + local_z(a)];
+    }
+}
+
 template <typename T, bool PRE>
 __global__ void __launch_bounds__(128)
 quad_element_kernel(Lay L, const T *__restrict__ CXp, ELay Ef,
@@ -82,89 +173,68 @@ quad_element_kernel(Lay L, const T *__restrict__ CXp, ELay Ef,
             }
         }
     }
-    // corner a -> index c = 4 x + 2 y + z; modes p use the same bits
-    T V[3][8];
+    T cg[2][2][2];
 #pragma unroll
-    for (int a = 0; a < 8; ++a)
+    for (int ix = 0; ix < 2; ++ix)
 #pragma unroll
-        for (int d = 0; d < 3; ++d) V[d][4 * local_x(a) + 2 * local_y(a) + local_z(a)] = ue[3 * a + d];
+        for (int iz = 0; iz < 2; ++iz)
 #pragma unroll
-    for (int d = 0; d < 3; ++d) fwht8(V[d]);
-    const T s = T(0.57735026918962576451);   // Gauss coordinate 1/sqrt(3)
-    // 8 x displacement gradient: Gx[d][iy][iz] = 8 du_d/dx at Gauss points
-    // (., iy, iz), Gy[d][ix][iz], Gz[d][ix][iy] likewise
-    T Gx[3][2][2], Gy[3][2][2], Gz[3][2][2];
+            for (int iy = 0; iy < 2; ++iy) cg[ix][iz][iy] = CXp[Ef.at(2 * i + ix, 2 * j + iy, 2 * k + iz)];
+    T ye[24];
+    quad_body<T>(ue, cg, lam, mu, ye);
 #pragma unroll
-    for (int d = 0; d < 3; ++d)
+    for (int m = 0; m < 24; ++m) y[(long long)m * nel + e] = ye[m];
+}
+
+// FP32 pass 1 on element pairs (j, j + 1), j even (the level-1 ny is even):
+// the shared node column j + 1 is loaded once, the arithmetic runs on float2
+// (about half the instructions), and each output pair is one 8-byte store.
+template <bool PRE>
+__global__ void __launch_bounds__(128)
+quad_element2_kernel(Lay L, const float *__restrict__ CXp, ELay Ef, const float *__restrict__ u,
+                     const float *__restrict__ f, const float *__restrict__ rdiag, float prerelax, float lam,
+                     float mu, float *__restrict__ y, const int *__restrict__ done)
+{
+    pdl_wait();
+    if (done && *done) return;
+    const Grid &g = L.g;
+    const long long nel = g.nel();
+    const long long e = 2 * ((long long)blockIdx.x * blockDim.x + threadIdx.x);
+    if (e >= nel) return;
+    const long long t = e / g.ny;
+    const int j = (int)(e - t * g.ny);
+    const int i = (int)(t / g.nz);
+    const int k = (int)(t - (long long)i * g.nz);
+    float2 ue[24];
 #pragma unroll
-        for (int i = 0; i < 2; ++i) {
-            const T si = i ? s : -s;
-            const T ax = fma(si, V[d][6], -V[d][4]), bx = fma(-si, V[d][7], V[d][5]);
-            const T ay = fma(si, V[d][6], -V[d][2]), by = fma(-si, V[d][7], V[d][3]);
-            const T az = fma(si, V[d][5], -V[d][1]), bz = fma(-si, V[d][7], V[d][3]);
+    for (int x = 0; x < 2; ++x)
 #pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                const T sj = j ? s : -s;
-                Gx[d][i][j] = fma(sj, bx, ax);
-                Gy[d][i][j] = fma(sj, by, ay);
-                Gz[d][i][j] = fma(sj, bz, az);
+        for (int z = 0; z < 2; ++z) {
+            const long long nb = L.at(i + x, j, k + z);   // node columns j, j + 1, j + 2
+            float v[9];
+#pragma unroll
+            for (int q = 0; q < 9; ++q) v[q] = PRE ? hmul(hmul(prerelax, f[nb + q]), rdiag[nb + q]) : u[nb + q];
+#pragma unroll
+            for (int yy = 0; yy < 2; ++yy) {
+                const int a = local_index(x, yy, z);
+#pragma unroll
+                for (int d = 0; d < 3; ++d) ue[3 * a + d] = make_float2(v[3 * yy + d], v[3 * yy + 3 + d]);
             }
         }
-    // stress at each Gauss point, summed over the axis its column does not
-    // depend on: Px[d][iy][iz] = sum_ix sigma[d][x], Py[d][ix][iz], Pz[d][ix][iy]
-    T Px[3][2][2], Py[3][2][2], Pz[3][2][2];
-#pragma unroll
-    for (int d = 0; d < 3; ++d)
-#pragma unroll
-        for (int i = 0; i < 2; ++i)
-#pragma unroll
-            for (int j = 0; j < 2; ++j) Px[d][i][j] = Py[d][i][j] = Pz[d][i][j] = T(0);
+    float2 cg[2][2][2];
 #pragma unroll
     for (int ix = 0; ix < 2; ++ix)
 #pragma unroll
         for (int iz = 0; iz < 2; ++iz)
 #pragma unroll
             for (int iy = 0; iy < 2; ++iy) {
-                const T c = CXp[Ef.at(2 * i + ix, 2 * j + iy, 2 * k + iz)];
-                const T cl = c * lam, cm = c * mu, cm2 = cm + cm;   // lam, mu carry 1/64
-                const T g00 = Gx[0][iy][iz], g01 = Gy[0][ix][iz], g02 = Gz[0][ix][iy];
-                const T g10 = Gx[1][iy][iz], g11 = Gy[1][ix][iz], g12 = Gz[1][ix][iy];
-                const T g20 = Gx[2][iy][iz], g21 = Gy[2][ix][iz], g22 = Gz[2][ix][iy];
-                const T tr = g00 + g11 + g22;
-                const T s00 = fma(cl, tr, cm2 * g00), s11 = fma(cl, tr, cm2 * g11), s22 = fma(cl, tr, cm2 * g22);
-                const T s01 = cm * (g01 + g10), s02 = cm * (g02 + g20), s12 = cm * (g12 + g21);
-                Px[0][iy][iz] += s00;
-                Px[1][iy][iz] += s01;
-                Px[2][iy][iz] += s02;
-                Py[0][ix][iz] += s01;
-                Py[1][ix][iz] += s11;
-                Py[2][ix][iz] += s12;
-                Pz[0][ix][iy] += s02;
-                Pz[1][ix][iy] += s12;
-                Pz[2][ix][iy] += s22;
+                const long long c0 = Ef.at(2 * i + ix, 2 * j + iy, 2 * k + iz);
+                cg[ix][iz][iy] = make_float2(CXp[c0], CXp[c0 + 2]);
             }
-    T ye[24];
+    float2 ye[24];
+    quad_body<float2>(ue, cg, make_float2(lam, lam), make_float2(mu, mu), ye);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        T X[4], Y[4], Z[4];   // [00, 10, 01, 11]: sums weighted by the signs of the two Gauss coordinates
-        h22(Px[d], X);
-        h22(Py[d], Y);
-        h22(Pz[d], Z);
-        T W[8];
-        W[0] = T(0);
-        W[1] = -Z[0];
-        W[2] = -Y[0];
-        W[3] = s * (Y[2] + Z[2]);
-        W[4] = -X[0];
-        W[5] = s * (X[2] + Z[1]);
-        W[6] = s * (X[1] + Y[1]);
-        W[7] = -(s * s) * (X[3] + Y[3] + Z[3]);
-        fwht8(W);
-#pragma unroll
-        for (int a = 0; a < 8; ++a) ye[3 * a + d] = W[4 * local_x(a) + 2 * local_y(a) + local_z(a)];
-    }
-#pragma unroll
-    for (int m = 0; m < 24; ++m) y[(long long)m * nel + e] = ye[m];
+    for (int m = 0; m < 24; ++m) *reinterpret_cast<float2 *>(y + (long long)m * nel + e) = ye[m];
 }
 
 template <typename T, int MODE>
@@ -240,12 +310,27 @@ int launch_quad_sweep(int mode, const Lay &L, const ELay &Ef, const T *CX, const
     const int bs = 128;
     const unsigned eb = (unsigned)((L.g.nel() + bs - 1) / bs);
     const dim3 nb = plane_grid(L.g, bs);   // quad_node_kernel: one row of CTAs per node plane
-    if (mode == MODE_JACOBI_PRE)
-        launch_pdl(quad_element_kernel<T, true>, dim3(eb), dim3(bs), 0, st, L, CX, Ef, u, f, rdiag, prerelax, lam, mu,
-                                                        yscratch, done);
-    else
-        launch_pdl(quad_element_kernel<T, false>, dim3(eb), dim3(bs), 0, st, L, CX, Ef, u, f, rdiag, prerelax, lam, mu,
-                                                         yscratch, done);
+    bool paired = false;
+    if constexpr (sizeof(T) == 4) {
+        if (L.g.ny % 2 == 0) {   // element pairs
+            paired = true;
+            const unsigned eb2 = (unsigned)((L.g.nel() / 2 + bs - 1) / bs);
+            if (mode == MODE_JACOBI_PRE)
+                launch_pdl(quad_element2_kernel<true>, dim3(eb2), dim3(bs), 0, st, L, CX, Ef, u, f, rdiag, prerelax,
+                           lam, mu, yscratch, done);
+            else
+                launch_pdl(quad_element2_kernel<false>, dim3(eb2), dim3(bs), 0, st, L, CX, Ef, u, f, rdiag, prerelax,
+                           lam, mu, yscratch, done);
+        }
+    }
+    if (!paired) {
+        if (mode == MODE_JACOBI_PRE)
+            launch_pdl(quad_element_kernel<T, true>, dim3(eb), dim3(bs), 0, st, L, CX, Ef, u, f, rdiag, prerelax, lam,
+                       mu, yscratch, done);
+        else
+            launch_pdl(quad_element_kernel<T, false>, dim3(eb), dim3(bs), 0, st, L, CX, Ef, u, f, rdiag, prerelax, lam,
+                       mu, yscratch, done);
+    }
     switch (mode) {
     case MODE_APPLY:
         launch_pdl(quad_node_kernel<T, MODE_APPLY>, dim3(nb), dim3(bs), 0, st, L, yscratch, u, f, rdiag, mask, out, omega, prerelax, done);
