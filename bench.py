@@ -49,9 +49,10 @@ METRIC = "s/design-iter @12.7M DOF, tol 1e-6: mixed+learned vs FP64 MGCG, same B
 # iteration for iteration on smaller grids).  The CPU arm extrapolates its
 # bounded sample to this count.
 FP64_NIT_ON_BENCH_DESIGN = 71
-# dram__bytes_read.sum + dram__bytes_write.sum of one FP32 Jacobi sweep launch at
-# 256x128x128 (184.3 MB + 36.7 MB), from an ncu capture of bench.py --micro jacobi32.
-HSWEEP32_DRAM_BYTES = 221.0e6
+# dram__bytes_read.sum + dram__bytes_write.sum of one FP32 Jacobi sweep launch
+# (hsweep2_kernel) at 256x128x128 (188.7 MB + 37.1 MB), from an ncu capture of
+# bench.py --micro jacobi32.
+HSWEEP32_DRAM_BYTES = 225.8e6
 
 
 def bench_design(nelx=NELX, nely=NELY, nelz=NELZ):
@@ -389,11 +390,11 @@ def run_ours(args):
     # (the largest share of an ncu launch list of one step); its DRAM traffic per
     # launch is read + write from one ncu capture of this workload.
     dom = kernels["fine_jacobi_fp32"]
-    roofline = {"bound": "hbm", "kernel": "hsweep_kernel<float, MODE_JACOBI> (damped Jacobi sweep, FP32)",
+    roofline = {"bound": "hbm", "kernel": "hsweep2_kernel<MODE_JACOBI> (damped Jacobi sweep, FP32, element pairs)",
                 "achieved": round(dom["gbs"], 1), "peak": hbm_peak, "unit": "GB/s",
                 "frac": round(dom["gbs"] / hbm_peak, 4), "peak_source": peak_src,
                 "traffic": HSWEEP32_DRAM_BYTES,
-                "note": "issue-bound, not HBM-bound: ~380 instructions per element at 57% issue activity"}
+                "note": "issue-bound, not HBM-bound: 39.1M warp instructions per launch at 51% issue activity"}
 
     result = {
         "metric": METRIC, "value": round(s_mixed, 5), "unit": "s/design-iter",
