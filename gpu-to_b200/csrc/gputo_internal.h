@@ -87,6 +87,7 @@ struct PcgScalars {
     int nit;         // reference's return value
     int status;      // gputo_status raised on the device (breakdown)
     int flexible;
+    int x_pending;   // 1 between a residual update and the U update of the same iteration
 };
 
 // Per-level storage of the multigrid hierarchy.
@@ -293,11 +294,14 @@ int reduce_partials_capacity();
 void launch_dot(long long n, const double *a, const double *b, double *partial, unsigned *ticket,
                 PcgScalars *sc, int which, const int *done, cudaStream_t st);
 // R32 (optional): also write float(R) there.
-void launch_pcg_update(long long n, double *U, double *R, const double *P, const double *Q,
-                       double *partial, unsigned *ticket, PcgScalars *sc, cudaStream_t st, float *R32 = nullptr);
-// Z: double, or float for the FP32 V-cycle output read directly.
+void launch_pcg_update(long long n, double *R, const double *Q, double *partial, unsigned *ticket, PcgScalars *sc,
+                       cudaStream_t st, float *R32 = nullptr);
+// Z: double, or float for the FP32 V-cycle output read directly.  Also
+// applies the pending U += alpha P.
 template <typename Z>
-void launch_p_update(long long n, const Z *z, double *P, Z *Zold, const PcgScalars *sc, cudaStream_t st);
+void launch_p_update(long long n, const Z *z, double *P, Z *Zold, double *U, PcgScalars *sc, cudaStream_t st);
+// U += alpha P when a solve stopped with that update pending.
+void launch_flush_x(long long n, double *U, const double *P, const PcgScalars *sc, cudaStream_t st);
 template <typename Z>
 void launch_dot2(long long n, const double *r, const Z *z, const Z *zold, double *partial, unsigned *ticket,
                  PcgScalars *sc, const int *done, cudaStream_t st);

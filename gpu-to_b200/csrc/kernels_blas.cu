@@ -192,29 +192,30 @@ template void launch_dot2<double>(long long, const double *, const double *, con
 template void launch_dot2<float>(long long, const double *, const float *, const float *, double *, unsigned *,
                                  PcgScalars *, const int *, cudaStream_t);
 
-// U += alpha P, R -= alpha Q, and r'r (mgcg1.cu:258-259,269); R32, when
-// given, receives float(R) for the mixed-precision V-cycle.
+// R -= alpha Q and r'r (mgcg1.cu:259,269); R32, when given, receives
+// float(R) for the mixed-precision V-cycle.  The solution's update U += alpha
+// P (mgcg1.cu:258) is left pending: p_update_kernel applies it, as it reads P
+// anyway, and a solve that stops before the direction update applies it in
+// launch_flush_x.  Same values as updating U here (P does not change in
+// between), 16 bytes per dof less traffic.
 __global__ void __launch_bounds__(kRedThreads)
-pcg_update_kernel(long long n, double *__restrict__ U, double *__restrict__ R,
-                  const double *__restrict__ P, const double *__restrict__ Q,
+pcg_update_kernel(long long n, double *__restrict__ R, const double *__restrict__ Q,
                   double *__restrict__ partial, unsigned *ticket, PcgScalars *sc, float *__restrict__ R32)
 {
     pdl_wait();
     if (sc->done) return;
     __shared__ double red[kRedThreads / 32];
     const double alpha = sc->alpha;
+    if (blockIdx.x == 0 && threadIdx.x == 0) sc->x_pending = 1;
     double v = 0.0;
     // two neighbouring entries per trip (16-byte loads and stores)
     const long long n2 = n >> 1;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n2;
          i += (long long)gridDim.x * blockDim.x) {
-        const double2 p = reinterpret_cast<const double2 *>(P)[i], q = reinterpret_cast<const double2 *>(Q)[i];
-        double2 u = reinterpret_cast<double2 *>(U)[i], r = reinterpret_cast<double2 *>(R)[i];
-        u.x = fma(alpha, p.x, u.x);
-        u.y = fma(alpha, p.y, u.y);
+        const double2 q = reinterpret_cast<const double2 *>(Q)[i];
+        double2 r = reinterpret_cast<double2 *>(R)[i];
         r.x = fma(-alpha, q.x, r.x);
         r.y = fma(-alpha, q.y, r.y);
-        reinterpret_cast<double2 *>(U)[i] = u;
         reinterpret_cast<double2 *>(R)[i] = r;
         if (R32) reinterpret_cast<float2 *>(R32)[i] = make_float2((float)r.x, (float)r.y);
         v = fma(r.x, r.x, v);
@@ -222,7 +223,6 @@ pcg_update_kernel(long long n, double *__restrict__ U, double *__restrict__ R,
     }
     if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
         const long long i = n - 1;
-        U[i] = fma(alpha, P[i], U[i]);
         const double r = fma(-alpha, Q[i], R[i]);
         R[i] = r;
         if (R32) R32[i] = (float)r;
@@ -239,27 +239,33 @@ pcg_update_kernel(long long n, double *__restrict__ U, double *__restrict__ R,
     }
 }
 
-void launch_pcg_update(long long n, double *U, double *R, const double *P, const double *Q,
-                       double *partial, unsigned *ticket, PcgScalars *sc, cudaStream_t st, float *R32)
+void launch_pcg_update(long long n, double *R, const double *Q, double *partial, unsigned *ticket, PcgScalars *sc,
+                       cudaStream_t st, float *R32)
 {
-    launch_pdl(pcg_update_kernel, dim3(red_blocks(n)), dim3(kRedThreads), 0, st, n, U, R, P, Q, partial, ticket, sc,
-               R32);
+    launch_pdl(pcg_update_kernel, dim3(red_blocks(n)), dim3(kRedThreads), 0, st, n, R, Q, partial, ticket, sc, R32);
     count_launches(1);
 }
 
-// P = Z + beta P (mgcg1.cu:265); the flexible variant also keeps Z as Z_old.
+// U += alpha P (the update pcg_update_kernel left pending, with the old P),
+// then P = Z + beta P (mgcg1.cu:258,265); the flexible variant also keeps Z as
+// Z_old.
 template <typename Z>
 __global__ void p_update_kernel(long long n, const Z *__restrict__ z_in, double *__restrict__ P,
-                                Z *__restrict__ Zold, const PcgScalars *sc)
+                                Z *__restrict__ Zold, double *__restrict__ U, PcgScalars *sc)
 {
     pdl_wait();
     if (sc->done) return;
-    const double beta = sc->beta;
+    const double beta = sc->beta, alpha = sc->alpha;
+    // read only by launch_flush_x, after this kernel in stream order
+    if (blockIdx.x == 0 && threadIdx.x == 0) sc->x_pending = 0;
     const long long n2 = n >> 1;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n2;
          i += (long long)gridDim.x * blockDim.x) {
         const Z z0 = z_in[2 * i], z1 = z_in[2 * i + 1];
-        double2 p = reinterpret_cast<double2 *>(P)[i];
+        double2 p = reinterpret_cast<double2 *>(P)[i], u = reinterpret_cast<double2 *>(U)[i];
+        u.x = fma(alpha, p.x, u.x);
+        u.y = fma(alpha, p.y, u.y);
+        reinterpret_cast<double2 *>(U)[i] = u;
         p.x = fma(beta, p.x, (double)z0);
         p.y = fma(beta, p.y, (double)z1);
         reinterpret_cast<double2 *>(P)[i] = p;
@@ -270,21 +276,40 @@ __global__ void p_update_kernel(long long n, const Z *__restrict__ z_in, double 
     }
     if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
         const Z z = z_in[n - 1];
+        U[n - 1] = fma(alpha, P[n - 1], U[n - 1]);
         P[n - 1] = fma(beta, P[n - 1], (double)z);
         if (Zold) Zold[n - 1] = z;
     }
 }
 
 template <typename Z>
-void launch_p_update(long long n, const Z *z, double *P, Z *Zold, const PcgScalars *sc, cudaStream_t st)
+void launch_p_update(long long n, const Z *z, double *P, Z *Zold, double *U, PcgScalars *sc, cudaStream_t st)
 {
-    launch_pdl(p_update_kernel<Z>, dim3(red_blocks(n)), dim3(kRedThreads), 0, st, n, z, P, Zold, sc);
+    launch_pdl(p_update_kernel<Z>, dim3(red_blocks(n)), dim3(kRedThreads), 0, st, n, z, P, Zold, U, sc);
     count_launches(1);
 }
-template void launch_p_update<double>(long long, const double *, double *, double *, const PcgScalars *,
+template void launch_p_update<double>(long long, const double *, double *, double *, double *, PcgScalars *,
                                       cudaStream_t);
-template void launch_p_update<float>(long long, const float *, double *, float *, const PcgScalars *,
+template void launch_p_update<float>(long long, const float *, double *, float *, double *, PcgScalars *,
                                      cudaStream_t);
+
+// The solution update still pending when a solve stopped after its residual
+// update (converged, maxit, or a breakdown found by the dot at the end of the
+// iteration): U += alpha P.
+__global__ void flush_x_kernel(long long n, double *__restrict__ U, const double *__restrict__ P,
+                               const PcgScalars *sc)
+{
+    if (!sc->x_pending) return;
+    const double alpha = sc->alpha;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        U[i] = fma(alpha, P[i], U[i]);
+}
+
+void launch_flush_x(long long n, double *U, const double *P, const PcgScalars *sc, cudaStream_t st)
+{
+    flush_x_kernel<<<red_blocks(n), kRedThreads, 0, st>>>(n, U, P, sc);
+    count_launches(1);
+}
 
 // U = 0, R = F, res0 = ||F|| and the scalar state (mgcg1.cu:235-238).
 __global__ void __launch_bounds__(kRedThreads)

@@ -548,7 +548,7 @@ void Solver::iteration(cudaStream_t st)
     if (opt.precision == GPUTO_PREC_MIXED && !net_on) {
         // float(r) comes from the residual update and z stays the FP32
         // V-cycle output: no precision-conversion passes
-        launch_pcg_update(nv, Uw, R, P, Q, partial, ticket, sc, st, Lf[0].f);
+        launch_pcg_update(nv, R, Q, partial, ticket, sc, st, Lf[0].f);
         if (fused_dot()) {
             vcycle_impl<float>(Lf, CXpf, Lf[0].f, Lf[0].u1, done, st, R, Zold32, partial);
             launch_finish_dot2(hsweep_blocks<float>(g[0], MODE_JACOBI_DOT, opt.sweep_xchunk, opt.sweep_pairs != 0),
@@ -557,17 +557,17 @@ void Solver::iteration(cudaStream_t st)
             vcycle_impl<float>(Lf, CXpf, Lf[0].f, Lf[0].u1, done, st);
             launch_dot2<float>(nv, R, Lf[0].u1, Zold32, partial, ticket, sc, done, st);
         }
-        launch_p_update<float>(nv, Lf[0].u1, P, Zold32, sc, st);
+        launch_p_update<float>(nv, Lf[0].u1, P, Zold32, Uw, sc, st);
         return;
     }
-    launch_pcg_update(nv, Uw, R, P, Q, partial, ticket, sc, st);
+    launch_pcg_update(nv, R, Q, partial, ticket, sc, st);
     vcycle(R, Z, done, st);
     if (Zold) {
         launch_dot2<double>(nv, R, Z, Zold, partial, ticket, sc, done, st);
-        launch_p_update<double>(nv, Z, P, Zold, sc, st);
+        launch_p_update<double>(nv, Z, P, Zold, Uw, sc, st);
     } else {
         launch_dot(nv, R, Z, partial, ticket, sc, 2 /*DOT_RZ*/, done, st);
-        launch_p_update<double>(nv, Z, P, nullptr, sc, st);
+        launch_p_update<double>(nv, Z, P, nullptr, Uw, sc, st);
     }
 }
 
@@ -620,6 +620,7 @@ int Solver::solve_poll(cudaStream_t st, bool *finished)
 
 int Solver::solve_end(double *Up, double *relres, int *nit, cudaStream_t st)
 {
+    launch_flush_x(lay[0].size(), Uw, P, sc, st);   // the last iteration's U update, if still pending
     GPUTO_CUDA(cudaGetLastError());
     if (Up != Uw)
         GPUTO_CUDA(cudaMemcpyAsync(Up, Uw, sizeof(double) * lay[0].size(), cudaMemcpyDeviceToDevice, st));
