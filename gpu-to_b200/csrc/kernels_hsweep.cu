@@ -245,12 +245,11 @@ __device__ __forceinline__ void h_store(long long base, unsigned m, const T (&ku
 // z = x chunk (node planes [c htx, (c + 1) htx), the last one up to nx;
 // htx <= HTX).  The Dirichlet bits come by TMA from a copy with rows padded
 // to 16 bytes (tm_m); rdiag = 1/diag.
-// CTAs per SM the compiler budgets registers for: 2 where two fit in shared
-// memory (FP64 apply and defect measured 10 % faster at 2, with a few spills,
-// than at 1); the FP64 Jacobi instances hold 129 and 158 KB, so only one fits.
+// CTAs per SM the compiler budgets registers for: 2, and 3 for the FP64
+// energy apply (128 registers: 135.6 us against 153.7 us at 2; the FP64 apply
+// measured no faster at 3 or 4).
 template <typename T, int MODE> struct HMinBlocks {
-    static constexpr int value =
-        (sizeof(T) == 4 || MODE == MODE_APPLY || MODE == MODE_DEFECT || MODE == MODE_ENERGY) ? 2 : 1;
+    static constexpr int value = (sizeof(T) == 8 && MODE == MODE_ENERGY) ? 3 : 2;
 };
 
 template <typename T, int MODE, int WZ>
@@ -1148,7 +1147,9 @@ hsweep2_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__
     }
 }
 
-template <typename T> constexpr int hwz() { return 8; }
+// Warps (element rows along z) per CTA: FP32 8; FP64 4, so that more CTAs share an SM (the FP64 apply
+// measured 126.8 against 132.0 us with 8, despite the extra overlapping row in four)
+template <typename T> constexpr int hwz() { return sizeof(T) == 8 ? 4 : 8; }
 
 // Row pitch of the padded mask copy: TMA needs 16-byte row strides.
 long long hmask_pitch(const Grid &g) { return ((long long)g.ny + 1 + 15) & ~15LL; }
