@@ -180,7 +180,7 @@ int gputo_autotune_dev(gputo_solver *h, const double *F, double *U, double tol, 
     }
     const gputo_options base = s.opt;
     std::vector<gputo_options> cand;
-    for (int nswp : {2, 3, 4}) {
+    for (int nswp : {1, 2, 3, 4}) {
         gputo_options o = base;
         o.nswp = nswp;
         o.nswp_fine = 0;
