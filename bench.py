@@ -567,7 +567,7 @@ def run_reference(args):
     print(json.dumps(out))
 
 
-KERNELS = {"apply64": 0, "jacobi32": 1, "level1_32": 2, "level1_64": 3, "jacobi_tc": 4, "energy_fused": 5,
+KERNELS = {"apply64": 0, "jacobi32": 1, "level1_32": 2, "level1_64": 3, "jacobi_tc": 4, "energy_fused": 5, "level2_32": 6,
            "energy64": -1, "energy_tc": -2, "filter": -3}
 
 
@@ -582,7 +582,7 @@ def run_micro(args):
     F, fixed = gputo.cantilever(nelx, nely, nelz)
     x0 = bench_design(nelx, nely, nelz)
     kinds = list(KERNELS) if args.micro == "all" else [args.micro]
-    mixed = any(k in ("jacobi32", "level1_32", "jacobi_tc") for k in kinds)
+    mixed = any(k in ("jacobi32", "level1_32", "jacobi_tc", "level2_32") for k in kinds)
     opts = gputo.default_options(precision=gputo.PREC_MIXED if mixed else gputo.PREC_FP64,
                                  tc_parts=2 if "jacobi_tc" in kinds else 0, sweep_pairs=args.sweep_pairs)
     s = gputo.Solver(nelx, nely, nelz, nl, opts)

@@ -450,11 +450,13 @@ int gputo_debug_set_sweep_fault(int skip_stage, unsigned wait_us)
 
 int gputo_solver_time_kernel(gputo_solver *h, int which, int reps, double *ms, void *stream)
 {
-    if (!h || !ms || reps < 1 || which < 0 || which > 5) return GPUTO_ERR_ARG;
+    if (!h || !ms || reps < 1 || which < 0 || which > 6) return GPUTO_ERR_ARG;
     Solver &s = h->s;
     if (!s.ready) return GPUTO_ERR_ARG;
     if (which == 5 && !(s.use_hsweep<double>(s.g[0]) && gputo::hsweep_energy_fits(s.g[0]))) return GPUTO_ERR_ARG;
-    if ((which == 1 || which == 2 || which == 4) && s.opt.precision != GPUTO_PREC_MIXED) return GPUTO_ERR_ARG;
+    if ((which == 1 || which == 2 || which == 4 || which == 6) && s.opt.precision != GPUTO_PREC_MIXED)
+        return GPUTO_ERR_ARG;
+    if (which == 6 && (s.nl < 4 || s.redisc())) return GPUTO_ERR_ARG;
     if ((which == 2 || which == 3) && s.nl < 2) return GPUTO_ERR_ARG;
     cudaStream_t st = s.stream(stream);
     cudaEvent_t e0, e1;
@@ -480,6 +482,16 @@ int gputo_solver_time_kernel(gputo_solver *h, int which, int reps, double *ms, v
             r = gputo::launch_tc_sweep(s.opt.tc_parts > 0 ? s.opt.tc_parts : 1, gputo::MODE_JACOBI, s.lay[0],
                                        s.elay, s.CXpf, s.Lf[0].u0, s.Lf[0].f, s.Lf[0].diag, s.mask[0],
                                        s.Lf[0].u1, 0.48f, 0.7f, s.opt.tc_xchunk, nullptr, s.err, st);
+            break;
+        case 6:   // level 2, FP32 (stored Galerkin element matrices)
+            if (s.Lf[2].yq)
+                gputo::launch_packed_sweep_ec<float>(gputo::MODE_JACOBI, s.lay[2], s.Lf[2].Apk, s.Lf[2].u0,
+                                                     s.Lf[2].f, s.Lf[2].rdiag, s.mask[2], s.Lf[2].u1, 0.48f, 0.7f,
+                                                     s.Lf[2].yq, nullptr, st);
+            else
+                gputo::launch_packed_sweep<float>(gputo::MODE_JACOBI, s.lay[2], s.Lf[2].Apk, s.Lf[2].u0,
+                                                  s.Lf[2].f, s.Lf[2].rdiag, s.mask[2], s.Lf[2].u1, 0.48f, 0.7f,
+                                                  nullptr, st);
             break;
         case 2:
             if (s.quad_level1())

@@ -249,8 +249,9 @@ long long gputo_solver_launch_count(const gputo_solver *s);
  * Jacobi sweep, 2 level-1 FP32 sweep, 3 level-1 FP64 sweep, 4 fine-level
  * tensor-core Jacobi sweep (tc_parts of the options, 1 if 0), 5 the FP64
  * apply with the element energies (gputo_solver_energy_dev's pass; Hadamard-
- * basis grids only).  Inputs are the solver's own work vectors; results are
- * discarded.  Needs setup first. */
+ * basis grids only), 6 level-2 FP32 sweep (Galerkin element matrices; nl >=
+ * 4).  Inputs are the solver's own work vectors; results are discarded.
+ * Needs setup first. */
 int gputo_solver_time_kernel(gputo_solver *s, int which, int reps, double *ms_per_launch,
                              void *stream);
 
