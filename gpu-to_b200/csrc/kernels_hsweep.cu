@@ -368,7 +368,7 @@ hsweep_kernel(const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ 
     // ring stage s (node plane p = E0 + s) in place, from the coarse tiles
     // that came by TMA with the stage (plane p / 2 in slot s, for odd p plane
     // (p - 1) / 2 in slot s - 1 or, at s = 0, the extra tile), with the same
-    // taps in the same order as prolong_node, the fixed dofs zeroed from the
+    // taps in the same order as prolong_cell_kernel, the fixed dofs zeroed from the
     // stage's own Dirichlet tile.  Tile t + 1 is corrected during step t,
     // before the barrier that ends it, so no barrier of its own is needed
     // (tile 0 before the first one).
