@@ -860,6 +860,41 @@ int gputo_density_filter_dev(const double *in, const double *divisor, double *ou
     return GPUTO_OK;
 }
 
+int gputo_time_filter_dev(const double *const *in, double *const *out, int n, int nelx, int nely, int nelz,
+                          double rmin, int reps, double *ms, void *stream)
+{
+    if (!in || !out || n < 1 || n > 64 || reps < 1 || !ms || !grid_ok(nelx, nely, nelz) || !(rmin > 0))
+        return GPUTO_ERR_ARG;
+    for (int q = 0; q < n; ++q)
+        if (!in[q] || !out[q]) return GPUTO_ERR_ARG;
+    int st = gputo::check_device();
+    if (st) return st;
+    const int R = (int)std::ceil(rmin) - 1;
+    if (nelx <= R || nely <= R || nelz <= R) {
+        gputo::set_error("filter radius exceeds the grid");
+        return GPUTO_ERR_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const Grid g{nelx, nely, nelz};
+    for (int q = 0; q < n; ++q)
+        if ((st = gputo::launch_filter(g, in[q], nullptr, out[q], rmin, 1, s))) return st;
+    cudaEvent_t e0, e1;
+    GPUTO_CUDA(cudaEventCreate(&e0));
+    GPUTO_CUDA(cudaEventCreate(&e1));
+    GPUTO_CUDA(cudaEventRecord(e0, s));
+    for (int r = 0; r < reps && !st; ++r) st = gputo::launch_filter(g, in[r % n], nullptr, out[r % n], rmin, 1, s);
+    GPUTO_CUDA(cudaEventRecord(e1, s));
+    GPUTO_CUDA(cudaEventSynchronize(e1));
+    float t = 0.f;
+    GPUTO_CUDA(cudaEventElapsedTime(&t, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st) return st;
+    GPUTO_CUDA(cudaGetLastError());
+    *ms = (double)t / reps;
+    return GPUTO_OK;
+}
+
 int gputo_density_filter(const double *in, const double *divisor, double *out, int nelx,
                          int nely, int nelz, double rmin, int normalize)
 {

@@ -272,6 +272,20 @@ filter_kernel(Grid g, const double *__restrict__ in, const double *__restrict__ 
 // memory once (two slots, one barrier per plane) and costs (2R + 1)^2 shared
 // loads per output instead of (2R + 1)^3.  Output i sums P_R(i - R), ...,
 // P_0(i), ..., P_R(i + R) in plane order.
+// Planes arrive by cp.async into a ring of kFPS shared-memory slots (input,
+// and the divisor when given), kFPS - 1 planes ahead of the one in use, one
+// barrier per plane (two planes ahead in registers reached 0.40 of HBM).
+constexpr int kFPS = 4;
+
+__device__ __forceinline__ void cp_async8(void *dst, const void *src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 template <int R>
 __global__ void __launch_bounds__(256)
 filter_plane_kernel(Grid g, const double *__restrict__ in, const double *__restrict__ div,
@@ -279,7 +293,8 @@ filter_plane_kernel(Grid g, const double *__restrict__ in, const double *__restr
 {
     using FT = FiltTile<R>;
     constexpr int W = FT::W;
-    extern __shared__ double fs[];   // [2][PLANE]
+    extern __shared__ double fs[];   // [kFPS][PLANE] input planes, then (with a divisor) [kFPS][PLANE] divisor planes
+    double *fd = fs + kFPS * FT::PLANE;
     const int tid = threadIdx.x, ly = tid & 31, lz = tid >> 5;
     const int j0 = blockIdx.x * kFTY, k0 = blockIdx.y * kFTZ;
     const int x0 = blockIdx.z * xc, x1 = min(x0 + xc, g.nx);
@@ -294,14 +309,20 @@ filter_plane_kernel(Grid g, const double *__restrict__ in, const double *__restr
             off[q] = (long long)mirror_index(k0 + zz - R, g.nz) * g.ny + mirror_index(j0 + yy - R, g.ny);
         }
     }
-    auto fetch = [&](int px, double (&v)[FT::NPOS]) {
-        const long long base = (long long)mirror_index(px, g.nx) * ps;
+    const int T = x1 - x0 + 2 * R;   // planes x0 - R .. x1 + R - 1
+    // plane t (t < T) into slot t mod kFPS; one commit group per plane, empty past the end
+    auto fetch = [&](int t) {
+        if (t < T) {
+            const long long base = (long long)mirror_index(x0 - R + t, g.nx) * ps;
+            const int sl = (t % kFPS) * FT::PLANE;
 #pragma unroll
-        for (int q = 0; q < FT::NPOS; ++q)
-            if (off[q] >= 0) {
-                const long long s = base + off[q];
-                v[q] = div ? in[s] / div[s] : in[s];
-            }
+            for (int q = 0; q < FT::NPOS; ++q)
+                if (off[q] >= 0) {
+                    cp_async8(fs + sl + tid + 256 * q, in + base + off[q]);
+                    if (div) cp_async8(fd + sl + tid + 256 * q, div + base + off[q]);
+                }
+        }
+        cp_async_commit();
     };
     const int j = j0 + ly, k = k0 + lz;
     const bool mine = j < g.ny && k < g.nz;
@@ -309,34 +330,51 @@ filter_plane_kernel(Grid g, const double *__restrict__ in, const double *__restr
     double acc[W];
 #pragma unroll
     for (int s = 0; s < W; ++s) acc[s] = 0.0;
-    const int T = x1 - x0 + 2 * R;   // planes x0 - R .. x1 + R - 1
-    double pre[2][FT::NPOS];
-    fetch(x0 - R, pre[0]);
-    if (T > 1) fetch(x0 - R + 1, pre[1]);
+#pragma unroll
+    for (int t = 0; t < kFPS - 1; ++t) fetch(t);
     for (int t0 = 0; t0 < T; t0 += 2 * W)
 #pragma unroll
     for (int u = 0; u < 2 * W; ++u) {
         const int t = t0 + u;
         if (t >= T) break;                 // the same for the whole CTA
         const int q = x0 - R + t;          // this plane
-        double *P = fs + (u & 1) * FT::PLANE;
+        cp_async_wait<kFPS - 2>();         // this thread's copies of plane t have landed
+        __syncthreads();                   // everyone's have; slot (t - 1) mod kFPS is free
+        fetch(t + kFPS - 1);
+        double *P = fs + (t % kFPS) * FT::PLANE;
+        if (div) {   // in / divisor, in place, once per plane
+            const double *D = fd + (t % kFPS) * FT::PLANE;
 #pragma unroll
-        for (int v = 0; v < FT::NPOS; ++v)
-            if (off[v] >= 0) P[tid + 256 * v] = pre[u & 1][v];
-        __syncthreads();
-        if (t + 2 < T) fetch(q + 2, pre[u & 1]);   // in flight while this plane is used
+            for (int v = 0; v < FT::NPOS; ++v)
+                if (off[v] >= 0) P[tid + 256 * v] = P[tid + 256 * v] / D[tid + 256 * v];
+            __syncthreads();
+        }
+        auto val = [&](int zz, int yy) { return P[zz * FT::TYH + yy]; };
         double pa[R + 1];
+        if constexpr (R == 1) {
+            // radius 1: the weight of a tap depends only on how many of its
+            // offsets are non-zero (centre, face, edge, corner), so each plane
+            // needs the centre, the sum of its 4 edge neighbours and the sum
+            // of its 4 corners
+            const int zc = lz + 1, yc = ly + 1;
+            const double s0 = val(zc, yc);
+            const double s1 = (val(zc, yc - 1) + val(zc, yc + 1)) + (val(zc - 1, yc) + val(zc + 1, yc));
+            const double s2 = (val(zc - 1, yc - 1) + val(zc - 1, yc + 1)) + (val(zc + 1, yc - 1) + val(zc + 1, yc + 1));
+            const double w0 = cFilterH[13], w1 = cFilterH[12], w2 = cFilterH[9], w3 = cFilterH[0];
+            pa[0] = fma(w2, s2, fma(w1, s1, w0 * s0));
+            pa[1] = fma(w3, s2, fma(w2, s1, w1 * s0));
+        } else {
 #pragma unroll
-        for (int a = 0; a <= R; ++a) pa[a] = 0.0;
+            for (int a = 0; a <= R; ++a) pa[a] = 0.0;
 #pragma unroll
-        for (int c = -R; c <= R; ++c) {
-            const double *row = P + (lz + R + c) * FT::TYH + ly + R;
+            for (int c = -R; c <= R; ++c)
 #pragma unroll
-            for (int b = -R; b <= R; ++b) {
-                const double x = row[b];
+                for (int b = -R; b <= R; ++b) {
+                    const double x = val(lz + R + c, ly + R + b);
 #pragma unroll
-                for (int a = 0; a <= R; ++a) pa[a] = fma(cFilterH[((a + R) * W + (b + R)) * W + (c + R)], x, pa[a]);
-            }
+                    for (int a = 0; a <= R; ++a)
+                        pa[a] = fma(cFilterH[((a + R) * W + (b + R)) * W + (c + R)], x, pa[a]);
+                }
         }
         // output q + a (a = -R..R) sits in slot (t + a + R) mod W
 #pragma unroll
@@ -349,6 +387,105 @@ filter_plane_kernel(Grid g, const double *__restrict__ in, const double *__restr
         if (i >= x0 && mine) out[(long long)i * ps + obase] = acc[sl] * scale;
         acc[sl] = 0.0;
     }
+    cp_async_wait<0>();   // the empty trailing groups
+}
+
+// Radius 1 with four output rows along z per thread, tiles of 32 (y) x 32 (z)
+// outputs: a thread reads its 6 x 3 window of each plane once for its four
+// outputs, 4.5 shared loads per output instead of 9 (the 32 x 8 tiles above
+// are bound by shared-memory bandwidth in FP64).  The same ring and the same
+// arithmetic per output as filter_plane_kernel<1>.
+constexpr int kF1Y = 32, kF1Z = 32;
+
+template <bool DIV>
+__global__ void __launch_bounds__(256)
+filter_r1_kernel(Grid g, const double *__restrict__ in, const double *__restrict__ div,
+                 double *__restrict__ out, double scale, int xc)
+{
+    constexpr int TYH = kF1Y + 2, TZH = kF1Z + 2, PLANE = TYH * TZH, NPOS = (PLANE + 255) / 256;
+    extern __shared__ double fs[];   // [kFPS][PLANE] input planes, then (DIV) [kFPS][PLANE] divisor planes
+    double *fd = fs + kFPS * PLANE;
+    const int tid = threadIdx.x, ly = tid & 31, lg = tid >> 5;
+    const int j0 = blockIdx.x * kF1Y, k0 = blockIdx.y * kF1Z;
+    const int x0 = blockIdx.z * xc, x1 = min(x0 + xc, g.nx);
+    const long long ps = (long long)g.ny * g.nz;
+    long long off[NPOS];
+#pragma unroll
+    for (int q = 0; q < NPOS; ++q) {
+        const int p = tid + 256 * q;
+        off[q] = -1;
+        if (p < PLANE) {
+            const int zz = p / TYH, yy = p - zz * TYH;
+            off[q] = (long long)mirror_index(k0 + zz - 1, g.nz) * g.ny + mirror_index(j0 + yy - 1, g.ny);
+        }
+    }
+    const int T = x1 - x0 + 2;   // planes x0 - 1 .. x1
+    auto fetch = [&](int t) {
+        if (t < T) {
+            const long long base = (long long)mirror_index(x0 - 1 + t, g.nx) * ps;
+            const int sl = (t % kFPS) * PLANE;
+#pragma unroll
+            for (int q = 0; q < NPOS; ++q)
+                if (off[q] >= 0) {
+                    cp_async8(fs + sl + tid + 256 * q, in + base + off[q]);
+                    if (DIV) cp_async8(fd + sl + tid + 256 * q, div + base + off[q]);
+                }
+        }
+        cp_async_commit();
+    };
+    const int j = j0 + ly, kr = k0 + 4 * lg;   // output column; first of the thread's four rows
+    const bool jok = j < g.ny;
+    const double w0 = cFilterH[13], w1 = cFilterH[12], w2 = cFilterH[9], w3 = cFilterH[0];
+    double acc[3][4];
+#pragma unroll
+    for (int s = 0; s < 3; ++s)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) acc[s][r] = 0.0;
+#pragma unroll
+    for (int t = 0; t < kFPS - 1; ++t) fetch(t);
+    for (int t0 = 0; t0 < T; t0 += 6)
+#pragma unroll
+    for (int u = 0; u < 6; ++u) {
+        const int t = t0 + u;
+        if (t >= T) break;   // the same for the whole CTA
+        const int q = x0 - 1 + t;
+        cp_async_wait<kFPS - 2>();
+        __syncthreads();
+        fetch(t + kFPS - 1);
+        double *P = fs + (t % kFPS) * PLANE;
+        if (DIV) {   // in / divisor, in place, once per plane
+            const double *D = fd + (t % kFPS) * PLANE;
+#pragma unroll
+            for (int v = 0; v < NPOS; ++v)
+                if (off[v] >= 0) P[tid + 256 * v] = P[tid + 256 * v] / D[tid + 256 * v];
+            __syncthreads();
+        }
+        double v[6][3];
+#pragma unroll
+        for (int r = 0; r < 6; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) v[r][c] = P[(4 * lg + r) * TYH + ly + c];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const double s0 = v[r + 1][1];
+            const double s1 = (v[r + 1][0] + v[r + 1][2]) + (v[r][1] + v[r + 2][1]);
+            const double s2 = (v[r][0] + v[r][2]) + (v[r + 2][0] + v[r + 2][2]);
+            const double p0 = fma(w2, s2, fma(w1, s1, w0 * s0));
+            const double p1 = fma(w3, s2, fma(w2, s1, w1 * s0));
+            // output q + a (a = -1, 0, 1) sits in slot (u + a + 1) mod 3
+            acc[u % 3][r] += p1;
+            acc[(u + 1) % 3][r] += p0;
+            acc[(u + 2) % 3][r] += p1;
+        }
+        // output q - 1 is complete
+        const int i = q - 1, sl = u % 3;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            if (i >= x0 && jok && kr + r < g.nz) out[(long long)i * ps + (long long)(kr + r) * g.ny + j] = acc[sl][r] * scale;
+            acc[sl][r] = 0.0;
+        }
+    }
+    cp_async_wait<0>();   // the empty trailing groups
 }
 
 template <int R>
@@ -367,6 +504,34 @@ int filter_launch(const Grid &g, const double *in, const double *div, double *ou
         });
         GPUTO_CUDA(e);
     }
+    if constexpr (R == 1) {
+        // tiles of 32 x 32 outputs; x chunks for about 592 CTAs (4 per SM, one wave), at least 6 planes each
+        constexpr size_t plane = sizeof(double) * (kF1Y + 2) * (kF1Z + 2);
+        const size_t smem = (div ? 2 : 1) * kFPS * plane;
+        if (div) {
+            static std::once_flag once[64];
+            int dev = 0;
+            GPUTO_CUDA(cudaGetDevice(&dev));
+            cudaError_t e = cudaSuccess;
+            std::call_once(once[dev < 64 ? dev : 63], [&]() {
+                e = cudaFuncSetAttribute(filter_r1_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(2 * kFPS * plane));
+            });
+            GPUTO_CUDA(e);
+        }
+        const unsigned ty = (unsigned)((g.ny + kF1Y - 1) / kF1Y), tz = (unsigned)((g.nz + kF1Z - 1) / kF1Z);
+        const long long tiles = (long long)ty * tz;
+        const long long want = std::max(1LL, (592 + tiles - 1) / tiles);
+        int xc = (int)std::max(6LL, ((long long)g.nx + want - 1) / want);
+        if (xc > g.nx) xc = g.nx;
+        const unsigned tx = (unsigned)((g.nx + xc - 1) / xc);
+        if (div)
+            filter_r1_kernel<true><<<dim3(ty, tz, tx), 256, smem, st>>>(g, in, div, out, scale, xc);
+        else
+            filter_r1_kernel<false><<<dim3(ty, tz, tx), 256, smem, st>>>(g, in, div, out, scale, xc);
+        count_launches(1);
+        return GPUTO_OK;
+    }
     const unsigned ty = (unsigned)((g.ny + kFTY - 1) / kFTY), tz = (unsigned)((g.nz + kFTZ - 1) / kFTZ);
     // x chunks: about 1184 CTAs (8 per SM) in all, at least 16 planes each
     const long long tiles = (long long)ty * tz;
@@ -375,8 +540,8 @@ int filter_launch(const Grid &g, const double *in, const double *div, double *ou
     if (xc > g.nx) xc = g.nx;
     const unsigned tx = (unsigned)((g.nx + xc - 1) / xc);
     if constexpr (R >= 1 && R <= 3)
-        filter_plane_kernel<R><<<dim3(ty, tz, tx), 256, sizeof(double) * 2 * FT::PLANE, st>>>(g, in, div, out, scale,
-                                                                                              xc);
+        filter_plane_kernel<R><<<dim3(ty, tz, tx), 256, sizeof(double) * (div ? 2 : 1) * kFPS * FT::PLANE, st>>>(
+            g, in, div, out, scale, xc);
     else
         filter_kernel<R><<<dim3(ty, tz, tx), 256, FT::bytes, st>>>(g, in, div, out, scale, xc);
     count_launches(1);

@@ -113,6 +113,7 @@ SIGNATURES = {
     "gputo_compliance_sens_tc_dev": (_i, [_dp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _dp, _vp]),
     "gputo_compliance_sens_noalloc_dev": (_i, [_dp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _dp, _vp]),
     "gputo_density_filter_dev": (_i, [_vp, _vp, _vp, _i, _i, _i, _d, _i, _vp]),
+    "gputo_time_filter_dev": (_i, [_vp, _vp, _i, _i, _i, _i, _d, _i, _dp, _vp]),
     "gputo_density_filter": (_i, [_dp, _dp, _dp, _i, _i, _i, _d, _i]),
     "gputo_simp_dev": (_i, [_vp, ctypes.c_longlong, _d, _d, _d, _vp, _vp, _vp]),
     "gputo_simp": (_i, [_dp, ctypes.c_longlong, _d, _d, _d, _dp, _dp]),
@@ -683,6 +684,18 @@ def density_filter(x, nelx, nely, nelz, rmin, divisor=None, normalize=True):
     _check(_lib.gputo_density_filter(_p(x), None if dv is None else _p(dv), _p(out), nelx, nely,
                                      nelz, float(rmin), int(bool(normalize))), "gputo_density_filter")
     return out
+
+
+def time_filter_dev(inputs, outputs, nelx, nely, nelz, rmin, reps=20, stream=None):
+    """Profiling aid: mean ms of one normalised filter launch, launches back to
+    back cycling through the (input, output) device-array pairs."""
+    n = len(inputs)
+    ins = (ctypes.c_void_p * n)(*[_ptr(x) for x in inputs])
+    outs = (ctypes.c_void_p * n)(*[_ptr(x) for x in outputs])
+    ms = ctypes.c_double(0.0)
+    _check(_lib.gputo_time_filter_dev(ins, outs, n, nelx, nely, nelz, float(rmin), int(reps), ctypes.byref(ms),
+                                      _ptr_stream(stream)), "gputo_time_filter_dev")
+    return ms.value
 
 
 def density_filter_dev(x, out, nelx, nely, nelz, rmin, divisor=None, normalize=True, stream=None):

@@ -459,6 +459,13 @@ int gputo_density_filter_dev(const double *in, const double *divisor, double *ou
                              int nely, int nelz, double rmin, int normalize, void *stream);
 int gputo_density_filter(const double *in, const double *divisor, double *out, int nelx,
                          int nely, int nelz, double rmin, int normalize);
+/* Profiling aid (no counterpart in the reference): the mean time of one
+ * normalised density-filter launch (no divisor), 'reps' launches back to back
+ * on 'stream' cycling through the n input/output pairs (device arrays of nel
+ * doubles), CUDA events on that stream, after one warm-up launch per pair.
+ * Unlike gputo_density_filter_dev, no synchronisation between launches. */
+int gputo_time_filter_dev(const double *const *in, double *const *out, int n, int nelx, int nely, int nelz,
+                          double rmin, int reps, double *ms_per_launch, void *stream);
 
 /* SIMP interpolation (top3D125modCuda.m:124,130) on device arrays of n:
  *   CX = Emin + xPhys^penal (E0 - Emin),  dsK = -penal (E0 - Emin) xPhys^(penal-1)
