@@ -122,6 +122,7 @@ void gputo_default_options(gputo_options *o)
     o->fuse_prolong = 0;
     o->sweep_xchunk = 0;
     o->sweep_pairs = 1;
+    o->nswp_coarse = 0;
 }
 
 int gputo_fine_op_constants(const double *Ke, double *c8)

@@ -139,7 +139,12 @@ struct Solver {
     // (MODE_JACOBI_DOT) when that sweep is the Hadamard-basis kernel.
     bool fused_dot() const { return use_hsweep<float>(g[0]) && Lf[0].rdiag && opt.tc_parts == 0 && sweeps(0) > 0; }
     // Jacobi sweeps per smoothing step on level l
-    int sweeps(int l) const { return (l == 0 && opt.nswp_fine > 0) ? opt.nswp_fine : opt.nswp; }
+    int sweeps(int l) const
+    {
+        if (l == 0 && opt.nswp_fine > 0) return opt.nswp_fine;
+        if (l >= 2 && opt.nswp_coarse > 0) return opt.nswp_coarse;
+        return opt.nswp;
+    }
     int run_graph(int batch, cudaStream_t st);
     void note(int s)
     {

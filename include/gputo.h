@@ -104,8 +104,11 @@ typedef struct {
                             choice)                                               */
     int sweep_pairs;     /* 1 (default): the FP32 fine sweeps of the mixed
                             V-cycle give each lane two element columns
-                            (paired FP32 arithmetic, nely <= 512; same results
+                            (paired FP32 arithmetic, nely <= 256; same results
                             bit for bit); 0: one column per lane              */
+    int nswp_coarse;     /* Jacobi sweeps per smoothing step on levels 2 and
+                            below (0 = nswp; level 1 keeps nswp): an
+                            autotuner choice                                      */
 } gputo_options;
 
 void gputo_default_options(gputo_options *opt);
@@ -314,13 +317,15 @@ void gputo_batch_destroy(gputo_batch *b);
 int gputo_batch_solve_dev(gputo_batch *b, const double *const *F, double *const *U, double tol, int maxit,
                           int check_every, double *relres, int *nit);
 
-/* Change the options that need no new hierarchy (nswp, omega, prerelax,
- * check_every, use_graph, tc_parts, tc_xchunk) on an existing solver, e.g. to
+/* Change the options that need no new hierarchy (nswp, nswp_fine,
+ * nswp_coarse, omega, prerelax, check_every, use_graph, tc_parts, tc_xchunk,
+ * sweep_xchunk, sweep_pairs) on an existing solver, e.g. to
  * reuse what gputo_autotune_dev chose for another solver of the same shape. */
 int gputo_solver_set_options(gputo_solver *s, const gputo_options *opt);
 
 /* Choose the options that change neither the hierarchy nor its buffers
- * (Jacobi sweeps per smoothing step; for GPUTO_PREC_MIXED also the CUDA-core
+ * (Jacobi sweeps per smoothing step, on all levels, the finest level and
+ * levels 2 and below; for GPUTO_PREC_MIXED also the CUDA-core
  * or tensor-core fine smoother and its x-chunk; host check interval) by
  * timing complete solves of this solver's problem (F, U: device vectors as
  * for gputo_solver_solve_dev) with CUDA events.  The fastest candidate that
