@@ -188,7 +188,7 @@ def time_design_loop(gputo, torch, precision, x0, F, fixed, Ke0, steps, warmup, 
         if tune and w == 0:
             torch.cuda.synchronize()
             best, bms, _ = gputo.autotune(dl.solver, dl.F, torch.zeros_like(dl.U), TOL, MAXIT)
-            dl.tuned = {"nswp": best.nswp, "nswp_fine": best.nswp_fine, "nswp_coarse": best.nswp_coarse, "sweep_xchunk": best.sweep_xchunk,
+            dl.tuned = {"nswp": best.nswp, "nswp_fine": best.nswp_fine, "nswp_coarse": best.nswp_coarse, "coarse_from": best.coarse_from, "sweep_xchunk": best.sweep_xchunk,
                         "tc_parts": best.tc_parts,
                         "check_every": best.check_every, "solve_ms": round(bms, 2)}
     torch.cuda.synchronize()
@@ -706,7 +706,7 @@ def run_batch(args):
             "dtype": "f64 outer / f32 V-cycle", "data": "synthetic",
             "config": {"workload": "uneven multi-design batch", "designs": [list(m[2]) for m in members],
                        "total_dofs": dofs, "nit": nits,
-                       "tuned": {"x".join(map(str, k)): {"nswp": v.nswp, "nswp_fine": v.nswp_fine, "nswp_coarse": v.nswp_coarse, "sweep_xchunk": v.sweep_xchunk,
+                       "tuned": {"x".join(map(str, k)): {"nswp": v.nswp, "nswp_fine": v.nswp_fine, "nswp_coarse": v.nswp_coarse, "coarse_from": v.coarse_from, "sweep_xchunk": v.sweep_xchunk,
                                                          "tc_parts": v.tc_parts,
                                                          "tc_xchunk": v.tc_xchunk} for k, v in tuned.items()}}}
     print(json.dumps(line))

@@ -185,6 +185,7 @@ int gputo_autotune_dev(gputo_solver *h, const double *F, double *U, double tol, 
         o.nswp = nswp;
         o.nswp_fine = 0;
         o.nswp_coarse = 0;
+        o.coarse_from = 0;
         o.use_graph = 1;
         o.check_every = 8;
         o.tc_parts = 0;
@@ -194,15 +195,18 @@ int gputo_autotune_dev(gputo_solver *h, const double *F, double *U, double tol, 
             o.nswp_fine = nf;
             cand.push_back(o);
         }
-        if (nswp <= 3)   // levels 2 and below apart from level 1, where a sweep costs least
-            for (int nf : {1, 2})
-                for (int nc : {2, 3, 4, 5, 6, 8}) {
-                    if (nc == nswp || nf > nswp) continue;
-                    o.nswp_fine = nf;
-                    o.nswp_coarse = nc;
-                    cand.push_back(o);
-                }
+        if (nswp <= 3)   // the coarser levels apart, where a sweep costs least
+            for (int from : {2, 3})
+                for (int nf : {1, 2})
+                    for (int nc : {2, 3, 4, 5, 6, 8}) {
+                        if (nc == nswp || nf > nswp || (from == 3 && s.nl < 5)) continue;
+                        o.nswp_fine = nf;
+                        o.nswp_coarse = nc;
+                        o.coarse_from = from;
+                        cand.push_back(o);
+                    }
         o.nswp_coarse = 0;
+        o.coarse_from = 0;
         if (nswp == 3)   // the fine sweeps' tile: node planes per CTA along x
             for (int nf : {0, 1})
                 for (int xc : {16, 24}) {

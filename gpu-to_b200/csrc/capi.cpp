@@ -123,6 +123,7 @@ void gputo_default_options(gputo_options *o)
     o->sweep_xchunk = 0;
     o->sweep_pairs = 1;
     o->nswp_coarse = 0;
+    o->coarse_from = 0;
 }
 
 int gputo_fine_op_constants(const double *Ke, double *c8)

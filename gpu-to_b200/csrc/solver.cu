@@ -106,7 +106,8 @@ int Solver::create(int nelx, int nely, int nelz, int nl_, const gputo_options *o
         set_error("nelx, nely, nelz must be divisible by 2^(nl-1)");
         return GPUTO_ERR_ARG;
     }
-    if (opt.nswp < 0 || opt.nswp_fine < 0 || opt.nswp_coarse < 0 || opt.check_every < 1 || !(opt.omega > 0) ||
+    if (opt.nswp < 0 || opt.nswp_fine < 0 || opt.nswp_coarse < 0 || opt.coarse_from < 0 || opt.coarse_from == 1 ||
+        opt.check_every < 1 || !(opt.omega > 0) ||
         opt.tc_parts < 0 ||
         (opt.sweep_xchunk != 0 && (opt.sweep_xchunk < 8 || opt.sweep_xchunk > 32)) ||
         opt.sweep_pairs < 0 || opt.sweep_pairs > 1 ||
@@ -705,7 +706,8 @@ int Solver::energy(const double *dsK, double *ce, double *dc, double *out2, cuda
 // Options that change neither the hierarchy nor its buffers.
 int Solver::set_tunables(const gputo_options &o)
 {
-    if (o.nswp < 0 || o.nswp_fine < 0 || o.nswp_coarse < 0 || o.check_every < 1 || !(o.omega > 0) || o.tc_parts < 0 ||
+    if (o.nswp < 0 || o.nswp_fine < 0 || o.nswp_coarse < 0 || o.coarse_from < 0 || o.coarse_from == 1 ||
+        o.check_every < 1 || !(o.omega > 0) || o.tc_parts < 0 ||
         o.tc_parts > 2 ||
         (o.sweep_xchunk != 0 && (o.sweep_xchunk < 8 || o.sweep_xchunk > 32)) ||
         o.sweep_pairs < 0 || o.sweep_pairs > 1 ||
@@ -718,6 +720,7 @@ int Solver::set_tunables(const gputo_options &o)
     opt.nswp = o.nswp;
     opt.nswp_fine = o.nswp_fine;
     opt.nswp_coarse = o.nswp_coarse;
+    opt.coarse_from = o.coarse_from;
     opt.fuse_prolong = o.fuse_prolong;
     opt.sweep_xchunk = o.sweep_xchunk;
     opt.sweep_pairs = o.sweep_pairs;

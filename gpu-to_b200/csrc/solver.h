@@ -142,7 +142,7 @@ struct Solver {
     int sweeps(int l) const
     {
         if (l == 0 && opt.nswp_fine > 0) return opt.nswp_fine;
-        if (l >= 2 && opt.nswp_coarse > 0) return opt.nswp_coarse;
+        if (l >= (opt.coarse_from > 0 ? opt.coarse_from : 2) && opt.nswp_coarse > 0) return opt.nswp_coarse;
         return opt.nswp;
     }
     int run_graph(int batch, cudaStream_t st);

@@ -53,7 +53,8 @@ class Options(ctypes.Structure):
     _fields_ = [("precision", _i), ("nswp", _i), ("omega", _d), ("prerelax", _d), ("nu", _d),
                 ("check_every", _i), ("use_graph", _i), ("max_coarse_dofs", _i), ("tc_parts", _i),
                 ("tc_xchunk", _i), ("coarse", _i), ("fine_op", _i), ("nswp_fine", _i),
-                ("fuse_prolong", _i), ("sweep_xchunk", _i), ("sweep_pairs", _i), ("nswp_coarse", _i)]
+                ("fuse_prolong", _i), ("sweep_xchunk", _i), ("sweep_pairs", _i), ("nswp_coarse", _i),
+                ("coarse_from", _i)]
 
 
 SIGNATURES = {

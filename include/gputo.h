@@ -106,9 +106,10 @@ typedef struct {
                             V-cycle give each lane two element columns
                             (paired FP32 arithmetic, nely <= 256; same results
                             bit for bit); 0: one column per lane              */
-    int nswp_coarse;     /* Jacobi sweeps per smoothing step on levels 2 and
-                            below (0 = nswp; level 1 keeps nswp): an
-                            autotuner choice                                      */
+    int nswp_coarse;     /* Jacobi sweeps per smoothing step on levels
+                            coarse_from and below (0 = nswp; the levels above
+                            keep nswp): an autotuner choice                       */
+    int coarse_from;     /* first level of nswp_coarse, >= 2 (0 = 2)             */
 } gputo_options;
 
 void gputo_default_options(gputo_options *opt);
