@@ -196,10 +196,10 @@ int gputo_autotune_dev(gputo_solver *h, const double *F, double *U, double tol, 
             cand.push_back(o);
         }
         if (nswp <= 3)   // the coarser levels apart, where a sweep costs least
-            for (int from : {2, 3})
+            for (int from : {2, 3, 4})
                 for (int nf : {1, 2})
-                    for (int nc : {2, 3, 4, 5, 6, 8}) {
-                        if (nc == nswp || nf > nswp || (from == 3 && s.nl < 5)) continue;
+                    for (int nc : {2, 3, 4, 6, 8, 12}) {
+                        if (nc == nswp || nf > nswp || from > s.nl - 2) continue;
                         o.nswp_fine = nf;
                         o.nswp_coarse = nc;
                         o.coarse_from = from;

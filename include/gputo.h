@@ -109,7 +109,8 @@ typedef struct {
     int nswp_coarse;     /* Jacobi sweeps per smoothing step on levels
                             coarse_from and below (0 = nswp; the levels above
                             keep nswp): an autotuner choice                       */
-    int coarse_from;     /* first level of nswp_coarse, >= 2 (0 = 2)             */
+    int coarse_from;     /* first level of nswp_coarse, >= 2 (0 = 2): the
+                            autotuner tries 2, 3 and 4                           */
 } gputo_options;
 
 void gputo_default_options(gputo_options *opt);
