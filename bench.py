@@ -625,6 +625,8 @@ def run_one_step(args):
                                  check_every=8 if args.nswp_fine else 1, sweep_pairs=args.sweep_pairs)
     if args.nswp:
         opts.nswp = args.nswp
+    opts.nswp_coarse = args.nswp_coarse
+    opts.coarse_from = args.coarse_from
     dl = gputo.DesignLoop(NELX, NELY, NELZ, NL, F, fixed, gputo.hex8_stiffness(), volfrac=VOLFRAC,
                           penal=PENAL, rmin=RMIN, move=MOVE, tol=TOL, maxit=MAXIT,
                           options=opts, x0=bench_design())
@@ -839,6 +841,8 @@ def main():
                     help="profiling aid: FP32 fine sweeps with two element columns per lane (1) or one (0)")
     ap.add_argument("--one-step", choices=["mixed", "fp64"], help="profiling aid: one design iteration")
     ap.add_argument("--nswp", type=int, default=0, help="profiling aid: V-cycle sweeps for --one-step (0: 3)")
+    ap.add_argument("--nswp-coarse", type=int, default=0, help="with --one-step: sweeps from level --coarse-from on")
+    ap.add_argument("--coarse-from", type=int, default=0, help="with --one-step: first level of --nswp-coarse (0: 2)")
     ap.add_argument("--nswp-fine", type=int, default=0,
                     help="with --one-step: Jacobi sweeps on the finest level (the autotuner's choice)")
     ap.add_argument("--workload", default="cantilever", choices=["cantilever", "batch", "bridge", "homog"],

@@ -355,6 +355,9 @@ void count_launches(long long n);
 // unaffected.
 #if defined(__CUDACC__)
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// Lets the next kernel in the stream launch before this one has finished (its
+// pdl_wait() still waits for this kernel's completion).
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 // Grid of thread-per-node kernels, one row of CTAs per x node plane
 // (blockIdx.y = i), so a thread finds (j, k) with one 32-bit division.

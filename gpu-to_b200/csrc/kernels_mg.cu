@@ -217,28 +217,50 @@ packed_sweep_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u,
 // A[row, col] reads 32 neighbouring elements (the [300][nel] layout is
 // element-fastest): four 32-byte sectors per warp instead of 32.  The eight
 // slot partials are summed in a fixed order through shared memory.
-// One CTA of the slot sweep (CTA index vb): 32 nodes, warp w = element slot
-// (ex, ez, ey) of the 8 around each node.  Shared by the kernel below and the
-// persistent coarse-level kernel; ends with a barrier so 'part' can be reused.
+// Warp w takes element slot (ex, ez, ey) = bits of w of the 8 around each
+// node.  The element matrices do not change during a solve, so a thread
+// loads its slot's 72 entries first, then lets the next kernel in the stream
+// launch (griddepcontrol.launch_dependents: its entry loads overlap this
+// kernel's tail), and only then waits for its predecessor before it reads u,
+// f or 1/diag.  Kernels before a sweep that write the matrices (the setup)
+// never release their successors early, so they have completed by then.
 template <typename T, int MODE>
-__device__ __forceinline__ void slot_sweep_block(const Lay &L, const T *__restrict__ A, const T *__restrict__ u,
-                                                 const T *__restrict__ f, const T *__restrict__ rdiag,
-                                                 const uint8_t *__restrict__ mask, T *__restrict__ out, T omega,
-                                                 T prerelax, long long vb, T (&part)[8][32][3])
+__global__ void __launch_bounds__(256)
+packed_sweep_slot_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u, const T *__restrict__ f,
+                         const T *__restrict__ rdiag, const uint8_t *__restrict__ mask, T *__restrict__ out,
+                         T omega, T prerelax, const int *__restrict__ done)
 {
+    __shared__ T part[8][32][3];
     const Grid &g = L.g;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const long long n = vb * 32 + lane;
+    const long long n = (long long)blockIdx.x * 32 + lane;
     const bool have = n < g.nnod();
     int i = 0, j = 0, k = 0;
     if (have) node_ijk(g, n, i, j, k);
     const int ex = (w >> 2) & 1, ez = (w >> 1) & 1, ey = w & 1;
     const int ei = i - 1 + ex, ej = j - 1 + ey, ek = k - 1 + ez;
+    const bool slot = have && ei >= 0 && ei < g.nx && ej >= 0 && ej < g.ny && ek >= 0 && ek < g.nz;
+    const long long nel = g.nel();
+    const long long e = slot ? g.elem(ei, ej, ek) : 0;
+    const int a = local_index(1 - ex, 1 - ey, 1 - ez);
+    // FP32: all 72 entries in registers before the wait; FP64 loads them after
+    // it (144 registers of entries would halve the CTAs per SM)
+    constexpr bool EARLY = sizeof(T) == 4;
+    T am[3][24];   // rows 3 a + d of the slot's element matrix
+    auto load_entries = [&]() {
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+#pragma unroll
+            for (int col = 0; col < 24; ++col)
+                am[d][col] = slot ? A[(long long)packed_index(3 * a + d, col) * nel + e] : T(0);
+    };
+    if (EARLY) load_entries();
+    pdl_trigger();
+    pdl_wait();
+    if (done && *done) return;
+    if (!EARLY) load_entries();
     T acc[3] = {T(0), T(0), T(0)};
-    if (have && ei >= 0 && ei < g.nx && ej >= 0 && ej < g.ny && ek >= 0 && ek < g.nz) {
-        const long long nel = g.nel();
-        const long long e = g.elem(ei, ej, ek);
-        const int a = local_index(1 - ex, 1 - ey, 1 - ez);
+    if (slot) {
         T ub[24];
 #pragma unroll
         for (int b = 0; b < 8; ++b) {
@@ -255,8 +277,7 @@ __device__ __forceinline__ void slot_sweep_block(const Lay &L, const T *__restri
 #pragma unroll
         for (int d = 0; d < 3; ++d)
 #pragma unroll
-            for (int col = 0; col < 24; ++col)
-                acc[d] = fma(A[(long long)packed_index(3 * a + d, col) * nel + e], ub[col], acc[d]);
+            for (int col = 0; col < 24; ++col) acc[d] = fma(am[d][col], ub[col], acc[d]);
     }
 #pragma unroll
     for (int d = 0; d < 3; ++d) part[w][lane][d] = acc[d];
@@ -291,19 +312,6 @@ __device__ __forceinline__ void slot_sweep_block(const Lay &L, const T *__restri
             }
         }
     }
-    __syncthreads();
-}
-
-template <typename T, int MODE>
-__global__ void __launch_bounds__(256)
-packed_sweep_slot_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u, const T *__restrict__ f,
-                         const T *__restrict__ rdiag, const uint8_t *__restrict__ mask, T *__restrict__ out,
-                         T omega, T prerelax, const int *__restrict__ done)
-{
-    pdl_wait();
-    if (done && *done) return;
-    __shared__ T part[8][32][3];
-    slot_sweep_block<T, MODE>(L, A, u, f, rdiag, mask, out, omega, prerelax, blockIdx.x, part);
 }
 
 template <typename T>
