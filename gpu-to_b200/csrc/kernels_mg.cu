@@ -411,6 +411,7 @@ __global__ void restrict_kernel(Lay Lc, Lay Lf, const T *__restrict__ rf,
                                 const int *__restrict__ done)
 {
     pdl_wait();
+    pdl_trigger();   // the next kernel (a coarse sweep) may start loading its matrix
     if (done && *done) return;
     int i, j, k;
     if (!plane_ijk(Lc.g, i, j, k)) return;
@@ -446,6 +447,7 @@ __global__ void prolong_cell_kernel(Lay Lf, Lay Lc, const T *__restrict__ uc, co
                                     T *__restrict__ uf, const int *__restrict__ done)
 {
     pdl_wait();
+    pdl_trigger();
     if (done && *done) return;
     int I, J, K;
     if (!plane_ijk(Lc.g, I, J, K)) return;
@@ -1061,31 +1063,43 @@ __device__ __forceinline__ long long padded_pos(const Lay &L, long long r)
 // y = M x for a dense row-major n x n triangular matrix, one warp per row,
 // FP64 accumulation.  in_padded / out_padded: x / y live in the level's padded
 // layout (otherwise dense vectors of n).
-template <typename Tin, typename Tout>
-__device__ __forceinline__ void gemv_row(const Lay &L, const double *__restrict__ M, const Tin *__restrict__ x,
-                                         Tout *__restrict__ y, int lower, int in_padded, int out_padded, int row,
-                                         int lane)
-{
-    const int n = (int)L.g.ndof();
-    const int lo = lower ? 0 : row, hi = lower ? row + 1 : n;
-    const double *mr = M + (long long)row * n;
-    double s = 0.0;
-    for (int c = lo + lane; c < hi; c += 32)
-        s = fma(mr[c], (double)x[in_padded ? padded_pos(L, c) : c], s);
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) y[out_padded ? padded_pos(L, row) : row] = (Tout)s;
-}
+// The inverse factor does not change during a solve: a lane loads its first
+// kGemvPre entries of the row before waiting on the previous kernel (the
+// rest, for n > 32 kGemvPre, after it), and lets the next kernel launch.  A
+// warp per row: lane l sums columns l, l + 32, ... in order, then the lanes
+// are summed by shuffles.
+constexpr int kGemvPre = 24;
 
 template <typename Tin, typename Tout>
 __global__ void gemv_warp_kernel(Lay L, const double *__restrict__ M, const Tin *__restrict__ x,
                                  Tout *__restrict__ y, int lower, int in_padded, int out_padded,
                                  const int *__restrict__ done)
 {
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const int n = (int)L.g.ndof();
+    const bool live = row < n;
+    const int lo = lower ? 0 : row, hi = !live ? 0 : (lower ? row + 1 : n);
+    const double *mr = M + (long long)(live ? row : 0) * n;
+    double pre[kGemvPre];
+#pragma unroll
+    for (int q = 0; q < kGemvPre; ++q) {
+        const int c = lo + lane + 32 * q;
+        pre[q] = c < hi ? mr[c] : 0.0;
+    }
+    pdl_trigger();
     pdl_wait();
     if (done && *done) return;
-    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (row >= (int)L.g.ndof()) return;
-    gemv_row<Tin, Tout>(L, M, x, y, lower, in_padded, out_padded, row, threadIdx.x & 31);
+    if (!live) return;
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < kGemvPre; ++q) {
+        const int c = lo + lane + 32 * q;
+        if (c < hi) s = fma(pre[q], (double)x[in_padded ? padded_pos(L, c) : c], s);
+    }
+    for (int c = lo + lane + 32 * kGemvPre; c < hi; c += 32)
+        s = fma(mr[c], (double)x[in_padded ? padded_pos(L, c) : c], s);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) y[out_padded ? padded_pos(L, row) : row] = (Tout)s;
 }
 
 // Coarsest solve x = A^-1 b = Linv^T (Linv b) with the explicit inverse of the
