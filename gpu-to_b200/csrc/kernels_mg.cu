@@ -854,107 +854,127 @@ void launch_dense_fix(const Grid &g, const uint8_t *mask, double *AQ, cudaStream
     count_launches(1);
 }
 
-// Blocked left-looking Cholesky A = L L^T of the dense coarsest matrix, in
+// Blocked right-looking Cholesky A = L L^T of the dense coarsest matrix, in
 // place in the lower triangle, 32-column panels (textbook algorithm; the
-// reference launches one kernel per row, mgcg1.cu:2099-2142):
-//   for each panel [c0, c0+w):
-//     update:  A[r][c0+j] -= sum_{k<c0} L[r][k] L[c0+j][k]   for r >= c0+j
-//              (a tiled FP64 GEMM over all rows below the panel, many CTAs)
-//     factor:  the w x w diagonal block in shared memory, then each row below
-//              solves L[r][panel] D^T = A[r][panel] (one CTA)
-// info = 1-based index of the first non-positive pivot, 0 on success; once
-// set, every later kernel returns at once.
+// reference factors row by row, one kernel launch per row,
+// mgcg1.cu:2099-2142).  For each panel [c0, c0 + w):
+//   chol_diag_kernel   the w x w diagonal block, factored in shared memory
+//                      (one CTA, a thread per entry);
+//   chol_panel_kernel  each row r below it solves L[r][panel] D^T = A[r][panel]
+//                      (a thread per row, many CTAs);
+//   chol_trail_kernel  the trailing lower triangle loses the panel's rank-w
+//                      product, A[r][c] -= sum_k L[r][c0 + k] L[c][c0 + k]
+//                      (a CTA per 32 x 32 tile on or below the diagonal).
+// Each step is a short latency-bound kernel (675 unknowns on the
+// 256 x 128 x 128 grid), so all of them, and the inverse below, run back to
+// back under programmatic dependent launch: a kernel lets the next one launch
+// at its start and waits for its predecessor before it reads anything.
+// info = 1-based index of the first non-positive (or NaN) pivot, 0 on
+// success; once set, every later factor kernel returns at once.
 constexpr int kCholB = 32;
 
-__global__ void __launch_bounds__(256) chol_update_kernel(int n, int c0, int w, double *__restrict__ A,
-                                                          const int *__restrict__ info)
+__global__ void __launch_bounds__(1024) chol_diag_kernel(int n, int c0, int w, double *__restrict__ A,
+                                                         int *__restrict__ info)
 {
-    if (*info) return;
-    __shared__ double Ar[kCholB][kCholB + 1];
-    __shared__ double Ac[kCholB][kCholB + 1];
-    const int r0 = c0 + blockIdx.x * kCholB;   // row block (rows >= c0)
-    const int ty = threadIdx.x >> 3, tx = threadIdx.x & 7;   // 32 rows x 8 threads, 4 cols each
-    double acc[4] = {0, 0, 0, 0};
-    for (int kk = 0; kk < c0; kk += kCholB) {
-        for (int idx = threadIdx.x; idx < kCholB * kCholB; idx += 256) {
-            const int rr = idx / kCholB, k = idx - rr * kCholB;
-            const int gr = r0 + rr, gc = c0 + rr, gk = kk + k;
-            Ar[rr][k] = (gr < n && gk < c0) ? A[(long long)gr * n + gk] : 0.0;
-            Ac[rr][k] = (rr < w && gk < c0) ? A[(long long)gc * n + gk] : 0.0;
-        }
-        __syncthreads();
-#pragma unroll 8
-        for (int k = 0; k < kCholB; ++k) {
-            const double a = Ar[ty][k];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) acc[q] = fma(a, Ac[tx * 4 + q][k], acc[q]);
-        }
-        __syncthreads();
-    }
-    const int r = r0 + ty;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int j = tx * 4 + q, col = c0 + j;
-        if (r < n && j < w && r >= col) A[(long long)r * n + col] -= acc[q];
-    }
-}
-
-__global__ void __launch_bounds__(512) chol_factor_kernel(int n, int c0, int w, double *__restrict__ A,
-                                                          int *__restrict__ info)
-{
+    pdl_wait();
+    pdl_trigger();
     if (*info) return;
     __shared__ double D[kCholB][kCholB + 1];
     __shared__ int bad;
-    const int tid = threadIdx.x, nt = blockDim.x;
+    const int tid = threadIdx.x, r = tid >> 5, c = tid & 31;
     if (tid == 0) bad = 0;
-    for (int idx = tid; idx < kCholB * kCholB; idx += nt) {
-        const int r = idx / kCholB, c = idx - r * kCholB;
-        D[r][c] = (r < w && c <= r) ? A[(long long)(c0 + r) * n + c0 + c] : 0.0;
-    }
+    D[r][c] = (r < w && c <= r) ? A[(long long)(c0 + r) * n + c0 + c] : 0.0;
     __syncthreads();
-    for (int c = 0; c < w; ++c) {
+    for (int j = 0; j < w; ++j) {
         if (tid == 0) {
-            const double s = D[c][c];
+            const double s = D[j][j];
             if (!(s > 0.0)) {
-                bad = c0 + c + 1;
-                D[c][c] = 1.0;
+                bad = c0 + j + 1;
+                D[j][j] = 1.0;
             } else {
-                D[c][c] = sqrt(s);
+                D[j][j] = sqrt(s);
             }
         }
         __syncthreads();
         if (bad) break;
-        if (tid > c && tid < w) D[tid][c] /= D[c][c];
+        if (tid > j && tid < w) D[tid][j] /= D[j][j];
         __syncthreads();
-        // trailing update inside the block: D[r][cc] -= D[r][c] D[cc][c], c < cc <= r < w
-        for (int idx = tid; idx < kCholB * kCholB; idx += nt) {
-            const int r = idx / kCholB, cc = idx - r * kCholB;
-            if (cc > c && cc <= r && r < w) D[r][cc] = fma(-D[r][c], D[cc][c], D[r][cc]);
-        }
+        // trailing update inside the block: D[r][c] -= D[r][j] D[c][j], j < c <= r < w
+        if (c > j && c <= r && r < w) D[r][c] = fma(-D[r][j], D[c][j], D[r][c]);
         __syncthreads();
     }
     if (bad) {
         if (tid == 0) atomicCAS(info, 0, bad);
         return;
     }
-    for (int idx = tid; idx < kCholB * kCholB; idx += nt) {
+    if (r < w && c <= r) A[(long long)(c0 + r) * n + c0 + c] = D[r][c];
+}
+
+constexpr int kCholPanelRows = 128;
+
+__global__ void __launch_bounds__(kCholPanelRows) chol_panel_kernel(int n, int c0, int w, double *__restrict__ A,
+                                                                    const int *__restrict__ info)
+{
+    pdl_wait();
+    pdl_trigger();
+    if (*info) return;
+    __shared__ double D[kCholB][kCholB + 1];
+    for (int idx = threadIdx.x; idx < kCholB * kCholB; idx += kCholPanelRows) {
         const int r = idx / kCholB, c = idx - r * kCholB;
-        if (r < w && c <= r) A[(long long)(c0 + r) * n + c0 + c] = D[r][c];
+        D[r][c] = (r < w && c <= r) ? A[(long long)(c0 + r) * n + c0 + c] : 0.0;
     }
-    // rows below the block: x D^T = a  (forward substitution, one row per thread)
-    for (int r = c0 + w + tid; r < n; r += nt) {
-        double x[kCholB];
-        double *row = A + (long long)r * n + c0;
+    __syncthreads();
+    const int r = c0 + w + blockIdx.x * kCholPanelRows + threadIdx.x;
+    if (r >= n) return;
+    // x D^T = a, forward substitution along the row
+    double *row = A + (long long)r * n + c0;
+    double x[kCholB];
 #pragma unroll
-        for (int c = 0; c < kCholB; ++c) {
-            if (c < w) {
-                double s = row[c];
+    for (int c = 0; c < kCholB; ++c) x[c] = c < w ? row[c] : 0.0;
 #pragma unroll
-                for (int k = 0; k < c; ++k) s = fma(-x[k], D[c][k], s);
-                x[c] = s / D[c][c];
-                row[c] = x[c];
-            }
+    for (int c = 0; c < kCholB; ++c) {
+        if (c < w) {
+            double s = x[c];
+#pragma unroll
+            for (int k = 0; k < c; ++k) s = fma(-x[k], D[c][k], s);
+            x[c] = s / D[c][c];
         }
+    }
+#pragma unroll
+    for (int c = 0; c < kCholB; ++c)
+        if (c < w) row[c] = x[c];
+}
+
+// grid (t, t) over the trailing 32 x 32 tiles; tiles above the diagonal return
+__global__ void __launch_bounds__(256) chol_trail_kernel(int n, int c0, int w, double *__restrict__ A,
+                                                         const int *__restrict__ info)
+{
+    pdl_wait();
+    pdl_trigger();
+    if (blockIdx.y > blockIdx.x || *info) return;
+    __shared__ double Ar[kCholB][kCholB + 1];
+    __shared__ double Ac[kCholB][kCholB + 1];
+    const int t0 = c0 + w;
+    const int r0 = t0 + blockIdx.x * kCholB, q0 = t0 + blockIdx.y * kCholB;
+    for (int idx = threadIdx.x; idx < kCholB * kCholB; idx += 256) {
+        const int rr = idx / kCholB, k = idx - rr * kCholB;
+        Ar[rr][k] = (r0 + rr < n && k < w) ? A[(long long)(r0 + rr) * n + c0 + k] : 0.0;
+        Ac[rr][k] = (q0 + rr < n && k < w) ? A[(long long)(q0 + rr) * n + c0 + k] : 0.0;
+    }
+    __syncthreads();
+    const int ty = threadIdx.x >> 3, tx = threadIdx.x & 7;   // 32 rows x 8 threads, 4 columns each
+    double acc[4] = {0, 0, 0, 0};
+#pragma unroll 8
+    for (int k = 0; k < kCholB; ++k) {
+        const double a = Ar[ty][k];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[q] = fma(a, Ac[tx * 4 + q][k], acc[q]);
+    }
+    const int r = r0 + ty;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int col = q0 + tx * 4 + q;
+        if (r < n && col <= r) A[(long long)r * n + col] -= acc[q];
     }
 }
 
@@ -963,91 +983,149 @@ void launch_cholesky(int n, double *A, int *info, cudaStream_t st)
     cudaMemsetAsync(info, 0, sizeof(int), st);
     for (int c0 = 0; c0 < n; c0 += kCholB) {
         const int w = (n - c0) < kCholB ? (n - c0) : kCholB;
-        if (c0 > 0) {
-            const unsigned blocks = (unsigned)((n - c0 + kCholB - 1) / kCholB);
-            chol_update_kernel<<<blocks, 256, 0, st>>>(n, c0, w, A, info);
-            count_launches(1);
-        }
-        chol_factor_kernel<<<1, 512, 0, st>>>(n, c0, w, A, info);
+        const int m = n - c0 - w;   // rows below the panel
+        launch_pdl(chol_diag_kernel, dim3(1), dim3(kCholB * kCholB), 0, st, n, c0, w, A, info);
         count_launches(1);
-    }
-}
-
-// Explicit inverse of the lower Cholesky factor, one warp per column
-// (forward substitution against e_c); writes Linv (row-major, lower) and its
-// transpose.  Used so that each coarse solve is two dense triangular
-// matrix-vector products instead of 2n dependent steps.
-__global__ void tri_inverse_kernel(int n, const double *__restrict__ L, double *__restrict__ Linv,
-                                   double *__restrict__ LinvT)
-{
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    const int c = warp;
-    if (c >= n) return;
-    for (int r = lane; r < c; r += 32) {
-        Linv[(long long)r * n + c] = 0.0;
-        LinvT[(long long)c * n + r] = 0.0;
-    }
-    for (int r = c; r < n; ++r) {
-        // x_r = (delta_rc - sum_{c<=kk<r} L[r][kk] x_kk) / L[r][r]
-        double s = 0.0;
-        for (int kk = c + lane; kk < r; kk += 32) s += L[(long long)r * n + kk] * Linv[(long long)kk * n + c];
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        const double x = ((r == c ? 1.0 : 0.0) - s) / L[(long long)r * n + r];
-        if (lane == 0) {
-            Linv[(long long)r * n + c] = x;
-            LinvT[(long long)c * n + r] = x;
+        if (m > 0) {
+            const int *cinfo = info;
+            launch_pdl(chol_panel_kernel, dim3((unsigned)((m + kCholPanelRows - 1) / kCholPanelRows)),
+                       dim3(kCholPanelRows), 0, st, n, c0, w, A, cinfo);
+            const unsigned t = (unsigned)((m + kCholB - 1) / kCholB);
+            launch_pdl(chol_trail_kernel, dim3(t, t), dim3(256), 0, st, n, c0, w, A, cinfo);
+            count_launches(2);
         }
-        __syncwarp();
     }
 }
 
-// The same with the column being built kept in shared memory: each step of a
-// column's forward substitution reads its earlier entries from there instead
-// of from global memory (stride n), which shortens the serial chain per row.
-// One warp (CTA) per column; x_r for r >= c lives at xs[r - c].
-__global__ void __launch_bounds__(32) tri_inverse_col_kernel(int n, const double *__restrict__ L,
-                                                             double *__restrict__ Linv, double *__restrict__ LinvT)
+// Explicit inverse of the lower Cholesky factor, so that each coarse solve is
+// two dense triangular matrix-vector products instead of 2n dependent steps.
+// Blocked by recursive doubling with the block formula
+//   [A 0; B C]^-1 = [A^-1 0; -C^-1 B A^-1  C^-1]:
+//   tri_diag_inverse_kernel  the inverse of every 32 x 32 diagonal block (a
+//                            thread per column, forward substitution in
+//                            shared memory; zeros above its diagonal);
+//   for s = 32, 64, 128, ... < n, blocks [o, o + s) and [o + s, o + 2s)
+//   (o = 2 s p, the second clipped at n) are paired:
+//     tri_double_kernel<1>   T = B A^-1 into LinvT (scratch until the end);
+//     tri_double_kernel<2>   the pair's lower-left block X = -C^-1 T;
+//   tri_transpose_kernel     LinvT = Linv^T, zeros in Linv's strict upper
+//                            triangle.
+// Both products skip the 32 x 32 blocks that are zero by triangularity, so
+// only blocks on or below the diagonal are read, and every one of them was
+// written at an earlier level.  2 log2(n / 32) + 2 launches (12 for n = 675)
+// instead of a serial chain of n steps per column.
+__global__ void __launch_bounds__(kCholB) tri_diag_inverse_kernel(int n, const double *__restrict__ L,
+                                                                  double *__restrict__ Linv)
 {
-    extern __shared__ double xs[];
-    const int c = blockIdx.x, lane = threadIdx.x;
-    for (int r = lane; r < c; r += 32) {
-        Linv[(long long)r * n + c] = 0.0;
-        LinvT[(long long)c * n + r] = 0.0;
-    }
-    for (int r = c; r < n; ++r) {
-        const double *Lr = L + (long long)r * n;
-        double s = 0.0;
-        for (int kk = c + lane; kk < r; kk += 32) s = fma(Lr[kk], xs[kk - c], s);
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        const double x = ((r == c ? 1.0 : 0.0) - s) / Lr[r];
-        if (lane == 0) {
-            xs[r - c] = x;
-            Linv[(long long)r * n + c] = x;
-            LinvT[(long long)c * n + r] = x;
+    pdl_wait();
+    pdl_trigger();
+    __shared__ double Ls[kCholB][kCholB + 1];
+    __shared__ double X[kCholB][kCholB + 1];   // X[i][j]: row i of column j of the block's inverse
+    const int b0 = blockIdx.x * kCholB, w = min(kCholB, n - b0), j = threadIdx.x;
+    for (int i = 0; i < w; ++i) Ls[i][j] = (j <= i) ? L[(long long)(b0 + i) * n + b0 + j] : 0.0;
+    __syncwarp();
+    if (j < w) {
+        X[j][j] = 1.0 / Ls[j][j];
+        for (int i = j + 1; i < w; ++i) {
+            double s = 0.0;
+            for (int k = j; k < i; ++k) s = fma(Ls[i][k], X[k][j], s);
+            X[i][j] = -s / Ls[i][i];
         }
-        __syncwarp();
+    }
+    __syncwarp();
+    if (j < w)
+        for (int i = 0; i < w; ++i) Linv[(long long)(b0 + i) * n + b0 + j] = (j <= i) ? X[i][j] : 0.0;
+}
+
+// grid (s / 32 column tiles, s / 32 row tiles, pairs); 32 x 32 output tile per CTA
+template <int STEP>
+__global__ void __launch_bounds__(256) tri_double_kernel(int n, int s, const double *__restrict__ L,
+                                                         double *__restrict__ Linv, double *__restrict__ Tb)
+{
+    pdl_wait();
+    pdl_trigger();
+    const int o = 2 * s * (int)blockIdx.z, rows0 = o + s;
+    const int sc = min(s, n - rows0);   // rows of C (> 0 for every pair the grid holds)
+    const int i0 = blockIdx.y * kCholB, j0 = blockIdx.x * kCholB;
+    if (i0 >= sc) return;
+    __shared__ double P[kCholB][kCholB + 1];
+    __shared__ double Q[kCholB][kCholB + 1];
+    const int ty = threadIdx.x >> 3, tx = threadIdx.x & 7;
+    double acc[4] = {0, 0, 0, 0};
+    // STEP 1: T[i][j] = sum_{k >= j} B[i][k] Ainv[k][j]  (k chunks from j0's on)
+    // STEP 2: X[i][j] = -sum_{k <= i} Cinv[i][k] T[k][j] (k chunks up to i0's)
+    const int kbeg = STEP == 1 ? j0 : 0;
+    const int kend = STEP == 1 ? s : min(i0 + kCholB, sc);
+    for (int k0 = kbeg; k0 < kend; k0 += kCholB) {
+        for (int idx = threadIdx.x; idx < kCholB * kCholB; idx += 256) {
+            const int a = idx / kCholB, b = idx - a * kCholB;
+            const bool pin = i0 + a < sc && k0 + b < kend;   // P[a][b]: row i0 + a, column k0 + b
+            const bool qin = k0 + a < kend;                   // Q[a][b]: row k0 + a, column j0 + b
+            if (STEP == 1) {
+                P[a][b] = pin ? L[(long long)(rows0 + i0 + a) * n + o + k0 + b] : 0.0;
+                Q[a][b] = qin ? Linv[(long long)(o + k0 + a) * n + o + j0 + b] : 0.0;
+            } else {
+                P[a][b] = pin ? Linv[(long long)(rows0 + i0 + a) * n + rows0 + k0 + b] : 0.0;
+                Q[a][b] = qin ? Tb[(long long)(rows0 + k0 + a) * n + o + j0 + b] : 0.0;
+            }
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int k = 0; k < kCholB; ++k) {
+            const double a = P[ty][k];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[q] = fma(a, Q[k][tx * 4 + q], acc[q]);
+        }
+        __syncthreads();
+    }
+    const int i = i0 + ty;
+    if (i >= sc) return;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const long long at = (long long)(rows0 + i) * n + o + j0 + tx * 4 + q;
+        if (STEP == 1) Tb[at] = acc[q];
+        else Linv[at] = -acc[q];
     }
 }
 
-constexpr int kTriInvMaxSmem = 200 * 1024;
+// The last kernel of the setup's factor chain: it does not release its
+// successor early, because the coarse-solve GEMVs read the inverse before
+// they wait on their predecessor.
+__global__ void __launch_bounds__(256) tri_transpose_kernel(int n, double *__restrict__ Linv,
+                                                            double *__restrict__ LinvT)
+{
+    pdl_wait();
+    __shared__ double t[kCholB][kCholB + 1];
+    const int bx = blockIdx.x * kCholB, by = blockIdx.y * kCholB;   // Linv tile: rows by.., columns bx..
+    for (int a = threadIdx.y; a < kCholB; a += 8) {
+        const int r = by + a, c = bx + threadIdx.x;
+        double v = 0.0;
+        if (r < n && c < n) {
+            if (c <= r) v = Linv[(long long)r * n + c];
+            else Linv[(long long)r * n + c] = 0.0;
+        }
+        t[a][threadIdx.x] = v;
+    }
+    __syncthreads();
+    for (int a = threadIdx.y; a < kCholB; a += 8) {
+        const int r = bx + a, c = by + threadIdx.x;   // LinvT[r][c] = Linv[c][r]
+        if (r < n && c < n) LinvT[(long long)r * n + c] = t[threadIdx.x][a];
+    }
+}
 
 void launch_tri_inverse(int n, const double *L, double *Linv, double *LinvT, cudaStream_t st)
 {
-    const size_t smem = sizeof(double) * (size_t)n;
-    static bool attr_set[64] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (smem <= (size_t)kTriInvMaxSmem && dev < 64) {
-        if (!attr_set[dev]) {   // setup runs outside stream capture
-            cudaFuncSetAttribute(tri_inverse_col_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTriInvMaxSmem);
-            attr_set[dev] = true;
-        }
-        tri_inverse_col_kernel<<<(unsigned)n, 32, smem, st>>>(n, L, Linv, LinvT);
-    } else {
-        const int bs = 128;  // 4 columns per CTA
-        tri_inverse_kernel<<<(unsigned)((n * 32 + bs - 1) / bs), bs, 0, st>>>(n, L, Linv, LinvT);
+    const unsigned nb = (unsigned)((n + kCholB - 1) / kCholB);
+    launch_pdl(tri_diag_inverse_kernel, dim3(nb), dim3(kCholB), 0, st, n, L, Linv);
+    count_launches(1);
+    for (int s = kCholB; s < n; s *= 2) {
+        const unsigned pairs = (unsigned)((n - s + 2 * s - 1) / (2 * s));
+        const dim3 grid((unsigned)(s / kCholB), (unsigned)(s / kCholB), pairs);
+        launch_pdl(tri_double_kernel<1>, grid, dim3(256), 0, st, n, s, L, Linv, LinvT);
+        launch_pdl(tri_double_kernel<2>, grid, dim3(256), 0, st, n, s, L, Linv, LinvT);
+        count_launches(2);
     }
+    launch_pdl(tri_transpose_kernel, dim3(nb, nb), dim3(kCholB, 8), 0, st, n, Linv, LinvT);
     count_launches(1);
 }
 
