@@ -657,7 +657,10 @@ void launch_build_level1(const Grid &gc, const double *CXfine, double *Apk, cuda
 // Levels >= 2: Galerkin P^T A P over the 8 children of each coarse element
 // (mgcg1.cu:1678-1743 coarseAe3c), computed child by child as
 // A_E = sum_c Pc^T A_c Pc with the 8x8 node weights Pc.  One CTA of 576
-// threads per coarse element; thread t owns entry (t/24, t%24).
+// threads per coarse element; thread t owns entry (t/24, t%24).  The eight
+// children's packed matrices (2,400 values) are staged in shared memory by
+// one round of independent loads (a plane's eight children side by side, so
+// the two y-neighbours share a sector) before the products.
 __global__ void __launch_bounds__(576) build_galerkin_kernel(Grid gc, const double *__restrict__ Af,
                                                              double *__restrict__ A)
 {
@@ -669,21 +672,23 @@ __global__ void __launch_bounds__(576) build_galerkin_kernel(Grid gc, const doub
     const int k = (int)(t - (long long)i * gc.nz);
     const Grid gf{2 * gc.nx, 2 * gc.ny, 2 * gc.nz};
     const long long nelf = gf.nel();
-    __shared__ double S[576];
+    __shared__ double Sp[8][300];   // child c's packed matrix
     __shared__ double Tm[576];
     const int tid = threadIdx.x;
+    for (int idx = tid; idx < 8 * 300; idx += 576) {
+        const int c = idx & 7, pk = idx >> 3;
+        Sp[c][pk] = Af[(long long)pk * nelf + gf.elem(2 * i + local_x(c), 2 * j + local_y(c), 2 * k + local_z(c))];
+    }
+    __syncthreads();
     const int m = tid / 24, n = tid - 24 * (tid / 24);
     const int am = m / 3, p = m - 3 * am;   // row: coarse local node, component
     const int an = n / 3, q = n - 3 * an;   // column
     double acc = 0.0;
     for (int c = 0; c < 8; ++c) {
-        const int ci = 2 * i + local_x(c), cj = 2 * j + local_y(c), ck = 2 * k + local_z(c);
-        S[tid] = Af[(long long)packed_index(m, n) * nelf + gf.elem(ci, cj, ck)];
-        __syncthreads();
         // Tm[(b,p)][(an,q)] = sum_b' S[(b,p)][(b',q)] Pc[b'][an]   (here m = (b,p))
         double tv = 0.0;
 #pragma unroll
-        for (int b2 = 0; b2 < 8; ++b2) tv = fma(S[m * 24 + 3 * b2 + q], cPc[(c * 8 + b2) * 8 + an], tv);
+        for (int b2 = 0; b2 < 8; ++b2) tv = fma(Sp[c][packed_index(m, 3 * b2 + q)], cPc[(c * 8 + b2) * 8 + an], tv);
         Tm[tid] = tv;
         __syncthreads();
         // acc[(am,p)][n] += sum_b Pc[b][am] Tm[(b,p)][n]
@@ -700,40 +705,64 @@ void launch_build_galerkin(const Grid &gc, const double *Afine, double *Apk, cud
     count_launches(1);
 }
 
-// Level 2 from the fine CX: A_E[p] = sum_{f<64} CX_f Mq[f][p], one CTA per
-// level-2 element, one thread per packed entry.
-__global__ void __launch_bounds__(320) build_level2_quad_kernel(Grid g2, const double *__restrict__ CXf,
-                                                                const double *__restrict__ Mq,
-                                                                double *__restrict__ A)
+// Level 2 from the fine CX: A_E[p] = sum_{f<64} CX_f Mq[f][p].  A CTA takes
+// 32 consecutive level-2 elements: their 64 fine CX values each go to shared
+// memory, then warp w computes packed entries [38 w, 38 w + 38) two at a time
+// with lane = element, so each Mq entry is one broadcast load per warp and
+// each store of an entry plane is 32 consecutive elements.
+constexpr int kL2qElems = 32;
+constexpr int kL2qWarps = 8;
+constexpr int kL2qPer = 38;   // packed entries per warp (8 x 38 >= 300, even)
+
+__global__ void __launch_bounds__(kL2qWarps * 32) build_level2_quad_kernel(Grid g2, const double *__restrict__ CXf,
+                                                                          const double *__restrict__ Mq,
+                                                                          double *__restrict__ A)
 {
-    const long long E = blockIdx.x;
     const long long nel = g2.nel();
-    const long long t = E / g2.ny;
-    const int j = (int)(E - t * g2.ny);
-    const int i = (int)(t / g2.nz);
-    const int k = (int)(t - (long long)i * g2.nz);
+    const long long E0 = (long long)blockIdx.x * kL2qElems;
     const Grid gff{4 * g2.nx, 4 * g2.ny, 4 * g2.nz};
-    __shared__ double cx[64];
-    const int tid = threadIdx.x;
-    if (tid < 64) {
-        const int c = tid >> 3, gq = tid & 7;
-        const int ix = gq >> 2, iz = (gq >> 1) & 1, iy = gq & 1;   // gq = 4 ix + 2 iz + iy
-        cx[tid] = CXf[gff.elem(2 * (2 * i + local_x(c)) + ix, 2 * (2 * j + local_y(c)) + iy,
-                               2 * (2 * k + local_z(c)) + iz)];
+    __shared__ double cx[kL2qElems][65];
+    for (int idx = threadIdx.x; idx < kL2qElems * 64; idx += kL2qWarps * 32) {
+        const int el = idx >> 6, f = idx & 63;
+        const long long E = E0 + el;
+        double v = 0.0;
+        if (E < nel) {
+            const long long t = E / g2.ny;
+            const int j = (int)(E - t * g2.ny);
+            const int i = (int)(t / g2.nz);
+            const int k = (int)(t - (long long)i * g2.nz);
+            const int c = f >> 3, gq = f & 7;
+            const int ix = gq >> 2, iz = (gq >> 1) & 1, iy = gq & 1;   // gq = 4 ix + 2 iz + iy
+            v = CXf[gff.elem(2 * (2 * i + local_x(c)) + ix, 2 * (2 * j + local_y(c)) + iy,
+                             2 * (2 * k + local_z(c)) + iz)];
+        }
+        cx[el][f] = v;
     }
     __syncthreads();
-    if (tid >= 300) return;
-    double acc = 0.0;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const long long E = E0 + lane;
+    const int p0 = w * kL2qPer, p1 = min(300, p0 + kL2qPer);
+    for (int pp = p0; pp < p1; pp += 2) {
+        double a0 = 0.0, a1 = 0.0;
 #pragma unroll 8
-    for (int f = 0; f < 64; ++f) acc = fma(cx[f], Mq[f * 300 + tid], acc);
-    A[(long long)tid * nel + E] = acc;
+        for (int f = 0; f < 64; ++f) {
+            const double v = cx[lane][f];
+            a0 = fma(v, __ldg(Mq + f * 300 + pp), a0);
+            a1 = fma(v, __ldg(Mq + f * 300 + pp + 1), a1);
+        }
+        if (E < nel) {
+            A[(long long)pp * nel + E] = a0;
+            A[(long long)(pp + 1) * nel + E] = a1;
+        }
+    }
 }
 
 void launch_build_galerkin_from_quad(const Grid &g2, const double *CXfine, double *Apk, cudaStream_t st)
 {
     int dev = 0;
     cudaGetDevice(&dev);
-    build_level2_quad_kernel<<<(unsigned)g2.nel(), 320, 0, st>>>(g2, CXfine, quad_galerkin_blocks(dev), Apk);
+    build_level2_quad_kernel<<<(unsigned)((g2.nel() + kL2qElems - 1) / kL2qElems), kL2qWarps * 32, 0, st>>>(
+        g2, CXfine, quad_galerkin_blocks(dev), Apk);
     count_launches(1);
 }
 
