@@ -340,8 +340,13 @@ def run_ours(args):
     s_fp64 = replica_seconds(t_d, max(1, args.steps // 2), ws)
     s_mixed_ref = replica_seconds(t_u, max(1, args.steps // 2), ws)
 
-    # e2e: host buffers through the drop-in C ABI
+    # e2e: host buffers through the drop-in C ABI, with the options the
+    # autotuner chose for the device-resident measurement (passed in the
+    # mgcg1 call's options, as a caller would)
     opts = gputo.default_options(precision=gputo.PREC_MIXED)
+    if tuned:
+        for k in ("nswp", "nswp_fine", "nswp_coarse", "coarse_from", "sweep_xchunk", "tc_parts", "check_every"):
+            setattr(opts, k, tuned[k])
     xhost = x0.copy()
     e2e_state = {}
     for _ in range(1):
@@ -417,7 +422,8 @@ def run_ours(args):
         "dof_iters_per_s": round(ndof * np.mean([i["nit"] for i in inf_m]) / s_mixed, 1),   # all replicas
         "e2e": {"value": round(t_e2e, 5), "unit": "s/design-iter", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "timing": "host wall clock around synchronous "
-                                                          "host-buffer C-ABI calls"},
+                                                          "host-buffer C-ABI calls",
+                "options": "the autotuned solver options of value" if tuned else "defaults"},
         "gpu_launches": int(launches),
         "roofline": roofline,
         "kernels": {k: {kk: (round(vv, 4) if isinstance(vv, float) else vv) for kk, vv in v.items()}

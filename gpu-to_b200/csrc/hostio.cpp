@@ -28,7 +28,7 @@ namespace gputo {
 namespace {
 
 constexpr size_t kChunk = size_t(8) << 20;   // bytes per pinned chunk
-constexpr int kCopyThreads = 8;              // default host threads per chunk copy
+constexpr int kCopyThreads = 4;              // default host threads per chunk copy
 constexpr size_t kMinSplit = size_t(1) << 20;
 
 // Runs job(i) for i in [0, parts) on a few persistent threads plus the caller.
