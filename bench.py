@@ -259,24 +259,28 @@ def mixed_parity(gputo, torch, dl, fixed, Ke0, stream):
 
 
 def e2e_design_iteration(gputo, x, F, fixed, Ke0, opts, state):
-    """One design iteration through the host-buffer C ABI, as a MATLAB caller
-    would run it with these drop-ins (top3D125modCuda.m:105-152; like the
+    """One design iteration through the host-buffer C ABI, as a C caller
+    would run it with these drop-ins (top3D125modCuda.m:105-152).  Like the
     driver, dV and the U array are made once before the loop and kept in
-    'state').  Returns (xnew, info, h2d, d2h)."""
+    'state', and so are the host output arrays each C-ABI call writes into
+    (a fresh output page costs a first-touch fault per call otherwise).
+    Returns (xnew, info, h2d, d2h)."""
     nel = x.size
     nd = F.size
     if "U" not in state:
         state["U"] = np.zeros(nd)
         state["dV"] = np.full(nel, 1.0 / nel / VOLFRAC)
+        for k in ("xPhys", "CX", "dsK", "ce", "dc", "dcf", "dV0", "xnew"):
+            state[k] = np.zeros(nel)
     U, dV = state["U"], state["dV"]
-    xPhys = gputo.density_filter(x, NELX, NELY, NELZ, RMIN)
-    CX, dsK = gputo.simp(xPhys, PENAL, 1.0, 1e-9)
+    xPhys = gputo.density_filter(x, NELX, NELY, NELZ, RMIN, out=state["xPhys"])
+    CX, dsK = gputo.simp(xPhys, PENAL, 1.0, 1e-9, out=(state["CX"], state["dsK"]))
     rr, nit = gputo.mgcg1(Ke0, F, U, CX, fixed, fixed.size, NELX, NELY, NELZ, NL, TOL, MAXIT,
                           printLev=0, options=opts)
-    ce, dc, c = gputo.compliance_sens(Ke0, U, CX, dsK, NELX, NELY, NELZ)
-    dcf = gputo.density_filter(dc, NELX, NELY, NELZ, RMIN)
-    dV0 = gputo.density_filter(dV, NELX, NELY, NELZ, RMIN)
-    xnew, lmid = gputo.oc_update(x, dcf, dV0, VOLFRAC, MOVE)
+    ce, dc, c = gputo.compliance_sens(Ke0, U, CX, dsK, NELX, NELY, NELZ, out=(state["ce"], state["dc"]))
+    dcf = gputo.density_filter(dc, NELX, NELY, NELZ, RMIN, out=state["dcf"])
+    dV0 = gputo.density_filter(dV, NELX, NELY, NELZ, RMIN, out=state["dV0"])
+    xnew, lmid = gputo.oc_update(x, dcf, dV0, VOLFRAC, MOVE, out=state["xnew"])
     # bytes crossing PCIe, counted from the arrays each call copies
     h2d = 8 * (nel                       # filter(x)
                + nel                     # simp: xPhys

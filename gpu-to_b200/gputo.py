@@ -642,15 +642,27 @@ def launch_count() -> int:
     return int(_lib.gputo_solver_launch_count(None))
 
 
-def compliance_sens(Ke0, U, CX, dsK, nelx, nely, nelz):
-    """Host-buffer form (U in the MATLAB frame): returns (ce, dc, compliance)."""
+def _host_out(a, n, name):
+    """A caller's output array: float64, C-contiguous, writeable, n values."""
+    if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous and a.flags.writeable
+            and a.size == n):
+        raise ValueError(f"{name} must be a writeable C-contiguous float64 array of {n} values")
+    return a
+
+
+def compliance_sens(Ke0, U, CX, dsK, nelx, nely, nelz, out=None):
+    """Host-buffer form (U in the MATLAB frame): returns (ce, dc, compliance).
+    out: optional (ce, dc) arrays to write into (a loop that keeps them skips
+    the first-touch cost of fresh output pages)."""
     Ke0 = np.ascontiguousarray(Ke0, dtype=np.float64).reshape(-1)
     U = np.ascontiguousarray(U, dtype=np.float64)
     CX = np.ascontiguousarray(CX, dtype=np.float64)
     dsK = np.ascontiguousarray(dsK, dtype=np.float64)
     ne = nelx * nely * nelz
-    ce = np.zeros(ne)
-    dc = np.zeros(ne)
+    if out is None:
+        ce, dc = np.zeros(ne), np.zeros(ne)
+    else:
+        ce, dc = _host_out(out[0], ne, "ce"), _host_out(out[1], ne, "dc")
     c = ctypes.c_double(0.0)
     _check(_lib.gputo_compliance_sens(_p(Ke0), _p(U), _p(CX), _p(dsK), nelx, nely, nelz, _p(ce),
                                       _p(dc), ctypes.byref(c)), "gputo_compliance_sens")
@@ -677,10 +689,11 @@ def compliance_sens_tc_dev(Ke0, U, CX, dsK, nelx, nely, nelz, ce=None, dc=None, 
     return c.value
 
 
-def density_filter(x, nelx, nely, nelz, rmin, divisor=None, normalize=True):
-    """Host-buffer form of the driver's imfilter calls."""
+def density_filter(x, nelx, nely, nelz, rmin, divisor=None, normalize=True, out=None):
+    """Host-buffer form of the driver's imfilter calls (out: optional array
+    to write into; it may be x, which is copied to the device first)."""
     x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
-    out = np.zeros_like(x)
+    out = np.zeros_like(x) if out is None else _host_out(out, x.size, "out")
     dv = None if divisor is None else np.ascontiguousarray(divisor, dtype=np.float64).reshape(-1)
     _check(_lib.gputo_density_filter(_p(x), None if dv is None else _p(dv), _p(out), nelx, nely,
                                      nelz, float(rmin), int(bool(normalize))), "gputo_density_filter")
@@ -710,10 +723,14 @@ def simp_dev(xphys, CX, dsK=None, penal=3.0, E0=1.0, Emin=1e-9, stream=None):
                                _ptr(CX), _ptr(dsK), _ptr_stream(stream)), "gputo_simp_dev")
 
 
-def simp(xphys, penal=3.0, E0=1.0, Emin=1e-9):
-    """Host-array SIMP (top3D125modCuda.m:124,130): returns (CX, dsK)."""
+def simp(xphys, penal=3.0, E0=1.0, Emin=1e-9, out=None):
+    """Host-array SIMP (top3D125modCuda.m:124,130): returns (CX, dsK)
+    (out: optional (CX, dsK) arrays to write into)."""
     xphys = np.ascontiguousarray(xphys, dtype=np.float64).reshape(-1)
-    CX, dsK = np.empty_like(xphys), np.empty_like(xphys)
+    if out is None:
+        CX, dsK = np.empty_like(xphys), np.empty_like(xphys)
+    else:
+        CX, dsK = _host_out(out[0], xphys.size, "CX"), _host_out(out[1], xphys.size, "dsK")
     _check(_lib.gputo_simp(_p(xphys), xphys.size, float(penal), float(E0), float(Emin), _p(CX), _p(dsK)),
            "gputo_simp")
     return CX, dsK
@@ -727,12 +744,12 @@ def oc_update_dev(x, dc, dv0, xnew, volfrac, move, stream=None):
     return lm.value
 
 
-def oc_update(x, dc, dv0, volfrac, move):
-    """Host-buffer form: returns (xnew, lmid)."""
+def oc_update(x, dc, dv0, volfrac, move, out=None):
+    """Host-buffer form: returns (xnew, lmid) (out: optional array for xnew)."""
     x = np.ascontiguousarray(x, dtype=np.float64)
     dc = np.ascontiguousarray(dc, dtype=np.float64)
     dv0 = np.ascontiguousarray(dv0, dtype=np.float64)
-    xn = np.zeros_like(x)
+    xn = np.zeros_like(x) if out is None else _host_out(out, x.size, "out")
     lm = ctypes.c_double(0.0)
     _check(_lib.gputo_oc_update(_p(x), _p(dc), _p(dv0), x.size, float(volfrac), float(move),
                                 _p(xn), ctypes.byref(lm)), "gputo_oc_update")

@@ -132,3 +132,21 @@ def test_mgcg9_gateway_exports_mexfunction_and_rejects_bad_calls(gputo):
     res, it = call_mex(mex, [np.zeros(576), np.zeros(10), np.zeros(10), np.zeros(3), np.ones(1),
                              1, 2, 2, 2, 2, 1e-8, 10, 2, 0, 0.3, 1.0, 1.0, 1.0])
     assert it == -1.0
+
+
+def test_host_output_arrays_are_checked_before_any_device_work(gputo):
+    """out= of the host-array calls must be writeable C-contiguous float64
+    arrays of the element count; anything else is a ValueError, raised before
+    the library is called."""
+    x = np.full(64, 0.5)
+    for bad in (np.zeros(63), np.zeros(64, dtype=np.float32), np.zeros((64, 2))[:, 0]):
+        with pytest.raises(ValueError):
+            gputo.density_filter(x, 4, 4, 4, 1.5, out=bad)
+        with pytest.raises(ValueError):
+            gputo.oc_update(x, -x, x, 0.3, 0.2, out=bad)
+        with pytest.raises(ValueError):
+            gputo.simp(x, out=(bad, np.zeros(64)))
+    ro = np.zeros(64)
+    ro.flags.writeable = False
+    with pytest.raises(ValueError):
+        gputo.density_filter(x, 4, 4, 4, 1.5, out=ro)

@@ -337,6 +337,35 @@ def test_host_calls_reuse_their_workspace(oracle, gputo):
         assert abs(lm - lr) <= 1e-12 * abs(lr) and np.abs(xn - xr).max() <= 1e-12
 
 
+def test_host_calls_write_into_caller_arrays(oracle, gputo):
+    """out= (arrays a design loop allocates once): the same values as the
+    allocating forms, bit for bit, also when the output is the input array
+    (inputs reach the device before any output is written)."""
+    rng = np.random.default_rng(13)
+    nelx, nely, nelz = 64, 32, 32
+    nel = nelx * nely * nelz
+    p = oracle.cantilever(nelx, nely, nelz)
+    x = rng.uniform(0.05, 1.0, nel)
+    U = rng.standard_normal(p.ndof)
+    outs = {k: np.full(nel, np.nan) for k in ("f", "CX", "dsK", "ce", "dc", "xn")}
+    f = gputo.density_filter(x, nelx, nely, nelz, 3 ** 0.5)
+    assert gputo.density_filter(x, nelx, nely, nelz, 3 ** 0.5, out=outs["f"]) is outs["f"]
+    assert np.array_equal(outs["f"], f)
+    CX, dsK = gputo.simp(f, 3.0, 1.0, 1e-9)
+    gputo.simp(f, 3.0, 1.0, 1e-9, out=(outs["CX"], outs["dsK"]))
+    assert np.array_equal(outs["CX"], CX) and np.array_equal(outs["dsK"], dsK)
+    ce, dc, c = gputo.compliance_sens(p.Ke0, U, CX, dsK, nelx, nely, nelz)
+    _, _, c2 = gputo.compliance_sens(p.Ke0, U, CX, dsK, nelx, nely, nelz, out=(outs["ce"], outs["dc"]))
+    assert np.array_equal(outs["ce"], ce) and np.array_equal(outs["dc"], dc) and c2 == c
+    dv = np.full(nel, 1.0 / nel)
+    xn, lm = gputo.oc_update(x, -np.abs(dc), dv, 0.3, 0.2)
+    _, lm2 = gputo.oc_update(x, -np.abs(dc), dv, 0.3, 0.2, out=outs["xn"])
+    assert np.array_equal(outs["xn"], xn) and lm2 == lm
+    xa = x.copy()
+    gputo.density_filter(xa, nelx, nely, nelz, 3 ** 0.5, out=xa)   # in place
+    assert np.array_equal(xa, f)
+
+
 def test_host_simp_matches_oracle(oracle, gputo):
     x = np.random.default_rng(12).uniform(0.0, 1.0, 3 * 10 ** 6 + 7)   # several staging chunks
     CX, dsK = gputo.simp(x, 3.0, 1.0, 1e-9)
