@@ -660,7 +660,9 @@ void launch_build_level1(const Grid &gc, const double *CXfine, double *Apk, cuda
 // threads per coarse element; thread t owns entry (t/24, t%24).  The eight
 // children's packed matrices (2,400 values) are staged in shared memory by
 // one round of independent loads (a plane's eight children side by side, so
-// the two y-neighbours share a sector) before the products.
+// the two y-neighbours share a sector) before the products, and so are the
+// 512 node weights (a warp reads up to 8 different weights at once, which
+// constant memory would serialise).
 __global__ void __launch_bounds__(576) build_galerkin_kernel(Grid gc, const double *__restrict__ Af,
                                                              double *__restrict__ A)
 {
@@ -674,7 +676,9 @@ __global__ void __launch_bounds__(576) build_galerkin_kernel(Grid gc, const doub
     const long long nelf = gf.nel();
     __shared__ double Sp[8][300];   // child c's packed matrix
     __shared__ double Tm[576];
+    __shared__ double Pw[512];      // cPc
     const int tid = threadIdx.x;
+    if (tid < 512) Pw[tid] = cPc[tid];
     for (int idx = tid; idx < 8 * 300; idx += 576) {
         const int c = idx & 7, pk = idx >> 3;
         Sp[c][pk] = Af[(long long)pk * nelf + gf.elem(2 * i + local_x(c), 2 * j + local_y(c), 2 * k + local_z(c))];
@@ -688,12 +692,12 @@ __global__ void __launch_bounds__(576) build_galerkin_kernel(Grid gc, const doub
         // Tm[(b,p)][(an,q)] = sum_b' S[(b,p)][(b',q)] Pc[b'][an]   (here m = (b,p))
         double tv = 0.0;
 #pragma unroll
-        for (int b2 = 0; b2 < 8; ++b2) tv = fma(Sp[c][packed_index(m, 3 * b2 + q)], cPc[(c * 8 + b2) * 8 + an], tv);
+        for (int b2 = 0; b2 < 8; ++b2) tv = fma(Sp[c][packed_index(m, 3 * b2 + q)], Pw[(c * 8 + b2) * 8 + an], tv);
         Tm[tid] = tv;
         __syncthreads();
         // acc[(am,p)][n] += sum_b Pc[b][am] Tm[(b,p)][n]
 #pragma unroll
-        for (int b = 0; b < 8; ++b) acc = fma(cPc[(c * 8 + b) * 8 + am], Tm[(3 * b + p) * 24 + n], acc);
+        for (int b = 0; b < 8; ++b) acc = fma(Pw[(c * 8 + b) * 8 + am], Tm[(3 * b + p) * 24 + n], acc);
         __syncthreads();
     }
     if (n <= m) A[(long long)packed_index(m, n) * nel + E] = acc;
@@ -705,54 +709,67 @@ void launch_build_galerkin(const Grid &gc, const double *Afine, double *Apk, cud
     count_launches(1);
 }
 
-// Level 2 from the fine CX: A_E[p] = sum_{f<64} CX_f Mq[f][p].  A CTA takes
-// 32 consecutive level-2 elements: their 64 fine CX values each go to shared
-// memory, then warp w computes packed entries [38 w, 38 w + 38) two at a time
-// with lane = element, so each Mq entry is one broadcast load per warp and
-// each store of an entry plane is 32 consecutive elements.
+// Level 2 from the fine CX: A_E[p] = sum_{f<64} CX_f Mq[f][p].  Persistent
+// CTAs (one per SM) stage the whole 64 x 300 Mq (153.6 KB) in shared memory
+// once, then take blocks of 32 consecutive level-2 elements: the block's 64
+// fine CX values per element go to shared memory, warp w computes packed
+// entries [30 w, 30 w + 30) three at a time with lane = element (each Mq
+// value a broadcast read), and each store of an entry plane is 32
+// consecutive elements.  The sum over f runs in order, as before.
 constexpr int kL2qElems = 32;
-constexpr int kL2qWarps = 8;
-constexpr int kL2qPer = 38;   // packed entries per warp (8 x 38 >= 300, even)
+constexpr int kL2qWarps = 10;
+constexpr int kL2qPer = 30;   // packed entries per warp (10 x 30 = 300)
+constexpr size_t kL2qSmem = sizeof(double) * (64 * 300 + kL2qElems * 65);
 
 __global__ void __launch_bounds__(kL2qWarps * 32) build_level2_quad_kernel(Grid g2, const double *__restrict__ CXf,
                                                                           const double *__restrict__ Mq,
                                                                           double *__restrict__ A)
 {
+    extern __shared__ double l2q_smem[];
+    double *Ms = l2q_smem;              // [64][300]
+    double *cx = l2q_smem + 64 * 300;   // [32][65]
     const long long nel = g2.nel();
-    const long long E0 = (long long)blockIdx.x * kL2qElems;
+    const long long nblk = (nel + kL2qElems - 1) / kL2qElems;
     const Grid gff{4 * g2.nx, 4 * g2.ny, 4 * g2.nz};
-    __shared__ double cx[kL2qElems][65];
-    for (int idx = threadIdx.x; idx < kL2qElems * 64; idx += kL2qWarps * 32) {
-        const int el = idx >> 6, f = idx & 63;
-        const long long E = E0 + el;
-        double v = 0.0;
-        if (E < nel) {
-            const long long t = E / g2.ny;
-            const int j = (int)(E - t * g2.ny);
-            const int i = (int)(t / g2.nz);
-            const int k = (int)(t - (long long)i * g2.nz);
-            const int c = f >> 3, gq = f & 7;
-            const int ix = gq >> 2, iz = (gq >> 1) & 1, iy = gq & 1;   // gq = 4 ix + 2 iz + iy
-            v = CXf[gff.elem(2 * (2 * i + local_x(c)) + ix, 2 * (2 * j + local_y(c)) + iy,
-                             2 * (2 * k + local_z(c)) + iz)];
-        }
-        cx[el][f] = v;
-    }
-    __syncthreads();
+    for (int idx = threadIdx.x; idx < 64 * 300; idx += kL2qWarps * 32) Ms[idx] = Mq[idx];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const long long E = E0 + lane;
-    const int p0 = w * kL2qPer, p1 = min(300, p0 + kL2qPer);
-    for (int pp = p0; pp < p1; pp += 2) {
-        double a0 = 0.0, a1 = 0.0;
-#pragma unroll 8
-        for (int f = 0; f < 64; ++f) {
-            const double v = cx[lane][f];
-            a0 = fma(v, __ldg(Mq + f * 300 + pp), a0);
-            a1 = fma(v, __ldg(Mq + f * 300 + pp + 1), a1);
+    const int p0 = w * kL2qPer;
+    for (long long blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+        const long long E0 = blk * kL2qElems;
+        __syncthreads();   // Ms staged (first block); the previous block's cx reads done
+        for (int idx = threadIdx.x; idx < kL2qElems * 64; idx += kL2qWarps * 32) {
+            const int el = idx >> 6, f = idx & 63;
+            const long long E = E0 + el;
+            double v = 0.0;
+            if (E < nel) {
+                const long long t = E / g2.ny;
+                const int j = (int)(E - t * g2.ny);
+                const int i = (int)(t / g2.nz);
+                const int k = (int)(t - (long long)i * g2.nz);
+                const int c = f >> 3, gq = f & 7;
+                const int ix = gq >> 2, iz = (gq >> 1) & 1, iy = gq & 1;   // gq = 4 ix + 2 iz + iy
+                v = CXf[gff.elem(2 * (2 * i + local_x(c)) + ix, 2 * (2 * j + local_y(c)) + iy,
+                                 2 * (2 * k + local_z(c)) + iz)];
+            }
+            cx[el * 65 + f] = v;
         }
-        if (E < nel) {
-            A[(long long)pp * nel + E] = a0;
-            A[(long long)(pp + 1) * nel + E] = a1;
+        __syncthreads();
+        const long long E = E0 + lane;
+        for (int pp = p0; pp < p0 + kL2qPer; pp += 3) {
+            double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+#pragma unroll 8
+            for (int f = 0; f < 64; ++f) {
+                const double v = cx[lane * 65 + f];
+                const double *mf = Ms + f * 300 + pp;
+                a0 = fma(v, mf[0], a0);
+                a1 = fma(v, mf[1], a1);
+                a2 = fma(v, mf[2], a2);
+            }
+            if (E < nel) {
+                A[(long long)pp * nel + E] = a0;
+                A[(long long)(pp + 1) * nel + E] = a1;
+                A[(long long)(pp + 2) * nel + E] = a2;
+            }
         }
     }
 }
@@ -761,8 +778,17 @@ void launch_build_galerkin_from_quad(const Grid &g2, const double *CXfine, doubl
 {
     int dev = 0;
     cudaGetDevice(&dev);
-    build_level2_quad_kernel<<<(unsigned)((g2.nel() + kL2qElems - 1) / kL2qElems), kL2qWarps * 32, 0, st>>>(
-        g2, CXfine, quad_galerkin_blocks(dev), Apk);
+    static bool attr_set[64] = {};
+    static int sms[64] = {};
+    if (dev < 64 && !attr_set[dev]) {   // setup runs outside stream capture
+        cudaFuncSetAttribute(build_level2_quad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kL2qSmem);
+        cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
+        attr_set[dev] = true;
+    }
+    const long long nblk = (g2.nel() + kL2qElems - 1) / kL2qElems;
+    const int sm = (dev < 64 && sms[dev] > 0) ? sms[dev] : 148;
+    const unsigned grid = (unsigned)(nblk < sm ? nblk : sm);
+    build_level2_quad_kernel<<<grid, kL2qWarps * 32, kL2qSmem, st>>>(g2, CXfine, quad_galerkin_blocks(dev), Apk);
     count_launches(1);
 }
 
