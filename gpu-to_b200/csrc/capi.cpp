@@ -645,15 +645,18 @@ static int mex_solve(const char *log_name, int cg_lines, const double *Ke0, cons
     const long long nd = s.g[0].ndof(), ne = s.g[0].nel();
     std::unique_lock<std::mutex> io(gputo::host_io_mutex());
     GPUTO_CUDA(cudaStreamSynchronize(strm));   // set_problem's uploads have landed before Dn is reused
-    st = gputo::host_to_device(s.Dn, F, sizeof(double) * nd);
+    // CX first: the hierarchy's setup kernels run on strm while F is staged
+    // in (the setup reads neither Dn nor Fw)
+    st = gputo::host_to_device(s.CX, CX, sizeof(double) * ne);
+    if (!st) st = s.setup_enqueue(s.CX, strm);
+    if (!st) st = gputo::host_to_device(s.Dn, F, sizeof(double) * nd);
     if (!st) gputo::launch_pack(s.lay[0], s.Dn, s.Fw, 0, strm);
-    if (!st) st = gputo::host_to_device(s.CX, CX, sizeof(double) * ne);
     io.unlock();
+    if (!st) st = s.setup_finish(strm);
     if (st) {
         if (log) std::fclose(log);
         return st;
     }
-    st = s.setup(s.CX, strm);
     if (!st) st = s.solve(s.Fw, s.Uw, tol, maxit, relres, nit, strm, printLev >= cg_lines ? log : nullptr);
     if (!st || st == GPUTO_ERR_BREAKDOWN) {
         // solver frame -> MATLAB frame: y components negated (mgcg1.cu:282-283)

@@ -276,6 +276,12 @@ int Solver::check_error_flags(cudaStream_t st)
 
 int Solver::setup(const double *CX_in, cudaStream_t st)
 {
+    const int s = setup_enqueue(CX_in, st);
+    return s ? s : setup_finish(st);
+}
+
+int Solver::setup_enqueue(const double *CX_in, cudaStream_t st)
+{
     if (!have_problem) {
         set_error("gputo_solver_set_problem must come before setup");
         return GPUTO_ERR_ARG;
@@ -327,6 +333,12 @@ int Solver::setup(const double *CX_in, cudaStream_t st)
     }
     for (int l = 0; l < nl; ++l)
         if (L[l].rdiag) launch_recip<double>(lay[l].size(), L[l].diag, L[l].rdiag, st);
+    GPUTO_CUDA(cudaGetLastError());
+    return GPUTO_OK;
+}
+
+int Solver::setup_finish(cudaStream_t st)
+{
     int h_info = 0;
     GPUTO_CUDA(cudaMemcpyAsync(&h_info, info, sizeof(int), cudaMemcpyDeviceToHost, st));
     GPUTO_CUDA(cudaStreamSynchronize(st));

@@ -77,6 +77,11 @@ struct Solver {
     int set_problem(const double *Ke0, const double *fixed1b, int nfd, cudaStream_t st);
     // CX in natural element order (device).
     int setup(const double *CX_dev, cudaStream_t st);
+    // setup() in two parts: the hierarchy's kernels enqueued on st, then the
+    // wait for them and the coarsest factor's pivot check (host work such as
+    // a right-hand side's upload can run in between)
+    int setup_enqueue(const double *CX_dev, cudaStream_t st);
+    int setup_finish(cudaStream_t st);
     // F, U in the padded layout (solver-owned or compatible buffers).
     int solve(const double *Fp, double *Up, double tol, int maxit, double *relres, int *nit,
               cudaStream_t st, FILE *log);
