@@ -928,6 +928,10 @@ void launch_dense_fix(const Grid &g, const uint8_t *mask, double *AQ, cudaStream
 // success; once set, every later factor kernel returns at once.
 constexpr int kCholB = 32;
 
+// Column step j: every thread forms the pivot sqrt(D[j][j]) and the scaled
+// entries it needs itself (the same operations on the same values, so the
+// same bits as one thread forming them), the scaled column goes to Lc, and the
+// trailing update writes only columns > j: one barrier per column.
 __global__ void __launch_bounds__(1024) chol_diag_kernel(int n, int c0, int w, double *__restrict__ A,
                                                          int *__restrict__ info)
 {
@@ -935,69 +939,60 @@ __global__ void __launch_bounds__(1024) chol_diag_kernel(int n, int c0, int w, d
     pdl_trigger();
     if (*info) return;
     __shared__ double D[kCholB][kCholB + 1];
-    __shared__ int bad;
+    __shared__ double Lc[kCholB][kCholB + 1];
     const int tid = threadIdx.x, r = tid >> 5, c = tid & 31;
-    if (tid == 0) bad = 0;
     D[r][c] = (r < w && c <= r) ? A[(long long)(c0 + r) * n + c0 + c] : 0.0;
+    Lc[r][c] = 0.0;
     __syncthreads();
     for (int j = 0; j < w; ++j) {
-        if (tid == 0) {
-            const double s = D[j][j];
-            if (!(s > 0.0)) {
-                bad = c0 + j + 1;
-                D[j][j] = 1.0;
-            } else {
-                D[j][j] = sqrt(s);
-            }
+        const double s = D[j][j];
+        if (!(s > 0.0)) {   // the same value in every thread
+            if (tid == 0) atomicCAS(info, 0, c0 + j + 1);
+            return;
+        }
+        const double d = sqrt(s);
+        if (r < w && r >= j) {
+            const double lrj = r == j ? d : D[r][j] / d;
+            if (c == j) Lc[r][j] = lrj;
+            // trailing update inside the block: D[r][c] -= L[r][j] L[c][j], j < c <= r < w
+            if (c > j && c <= r) D[r][c] = fma(-lrj, D[c][j] / d, D[r][c]);
         }
         __syncthreads();
-        if (bad) break;
-        if (tid > j && tid < w) D[tid][j] /= D[j][j];
-        __syncthreads();
-        // trailing update inside the block: D[r][c] -= D[r][j] D[c][j], j < c <= r < w
-        if (c > j && c <= r && r < w) D[r][c] = fma(-D[r][j], D[c][j], D[r][c]);
-        __syncthreads();
     }
-    if (bad) {
-        if (tid == 0) atomicCAS(info, 0, bad);
-        return;
-    }
-    if (r < w && c <= r) A[(long long)(c0 + r) * n + c0 + c] = D[r][c];
+    if (r < w && c <= r) A[(long long)(c0 + r) * n + c0 + c] = Lc[r][c];
 }
 
-constexpr int kCholPanelRows = 128;
+// A warp per row below the panel: x D^T = a by forward substitution, lane c
+// holding entry c; step k finishes x_k on lane k and broadcasts it, and the
+// later lanes subtract x_k D[c][k] (each lane's updates in order of k, as a
+// thread-per-row substitution applies them).
+constexpr int kCholPanelWarps = 8;
 
-__global__ void __launch_bounds__(kCholPanelRows) chol_panel_kernel(int n, int c0, int w, double *__restrict__ A,
-                                                                    const int *__restrict__ info)
+__global__ void __launch_bounds__(kCholPanelWarps * 32) chol_panel_kernel(int n, int c0, int w,
+                                                                         double *__restrict__ A,
+                                                                         const int *__restrict__ info)
 {
     pdl_wait();
     pdl_trigger();
     if (*info) return;
     __shared__ double D[kCholB][kCholB + 1];
-    for (int idx = threadIdx.x; idx < kCholB * kCholB; idx += kCholPanelRows) {
+    for (int idx = threadIdx.x; idx < kCholB * kCholB; idx += kCholPanelWarps * 32) {
         const int r = idx / kCholB, c = idx - r * kCholB;
         D[r][c] = (r < w && c <= r) ? A[(long long)(c0 + r) * n + c0 + c] : 0.0;
     }
     __syncthreads();
-    const int r = c0 + w + blockIdx.x * kCholPanelRows + threadIdx.x;
-    if (r >= n) return;
-    // x D^T = a, forward substitution along the row
+    const int lane = threadIdx.x & 31;
+    const int r = c0 + w + blockIdx.x * kCholPanelWarps + (threadIdx.x >> 5);
+    if (r >= n) return;   // the same for the whole warp
     double *row = A + (long long)r * n + c0;
-    double x[kCholB];
-#pragma unroll
-    for (int c = 0; c < kCholB; ++c) x[c] = c < w ? row[c] : 0.0;
-#pragma unroll
-    for (int c = 0; c < kCholB; ++c) {
-        if (c < w) {
-            double s = x[c];
-#pragma unroll
-            for (int k = 0; k < c; ++k) s = fma(-x[k], D[c][k], s);
-            x[c] = s / D[c][c];
-        }
+    double s = lane < w ? row[lane] : 0.0;
+    for (int k = 0; k < w; ++k) {
+        double xk = lane == k ? s / D[k][k] : 0.0;
+        xk = __shfl_sync(0xffffffffu, xk, k);
+        if (lane == k) s = xk;
+        else if (lane > k) s = fma(-xk, D[lane][k], s);
     }
-#pragma unroll
-    for (int c = 0; c < kCholB; ++c)
-        if (c < w) row[c] = x[c];
+    if (lane < w) row[lane] = s;
 }
 
 // grid (t, t) over the trailing 32 x 32 tiles; tiles above the diagonal return
@@ -1043,8 +1038,8 @@ void launch_cholesky(int n, double *A, int *info, cudaStream_t st)
         count_launches(1);
         if (m > 0) {
             const int *cinfo = info;
-            launch_pdl(chol_panel_kernel, dim3((unsigned)((m + kCholPanelRows - 1) / kCholPanelRows)),
-                       dim3(kCholPanelRows), 0, st, n, c0, w, A, cinfo);
+            launch_pdl(chol_panel_kernel, dim3((unsigned)((m + kCholPanelWarps - 1) / kCholPanelWarps)),
+                       dim3(kCholPanelWarps * 32), 0, st, n, c0, w, A, cinfo);
             const unsigned t = (unsigned)((m + kCholB - 1) / kCholB);
             launch_pdl(chol_trail_kernel, dim3(t, t), dim3(256), 0, st, n, c0, w, A, cinfo);
             count_launches(2);
