@@ -259,6 +259,20 @@ packed_sweep_slot_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u
     pdl_wait();
     if (done && *done) return;
     if (!EARLY) load_entries();
+    // warp 0's epilogue operands, loaded together with the products' inputs
+    // instead of after the slot sum
+    T fe[3] = {T(0), T(0), T(0)}, re[3] = {T(0), T(0), T(0)}, ue[3] = {T(0), T(0), T(0)};
+    unsigned me = 0;
+    if (w == 0 && have) {
+        const long long base = L.at(i, j, k);
+        me = mask[n];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            if (MODE != MODE_APPLY) fe[d] = f[base + d];
+            if (MODE == MODE_JACOBI || MODE == MODE_JACOBI_PRE) re[d] = rdiag[base + d];
+            if (MODE == MODE_JACOBI) ue[d] = u[base + d];
+        }
+    }
     T acc[3] = {T(0), T(0), T(0)};
     if (slot) {
         T ub[24];
@@ -290,25 +304,24 @@ packed_sweep_slot_kernel(Lay L, const T *__restrict__ A, const T *__restrict__ u
 #pragma unroll
             for (int q = 1; q < 8; ++q) s[d] += part[q][lane][d];
         }
-        const unsigned m = mask[n];
         const long long base = L.at(i, j, k);
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             const long long dof = base + d;
-            const bool fixed = (m >> d) & 1u;
+            const bool fixed = (me >> d) & 1u;
             if (MODE == MODE_APPLY) {
                 out[dof] = fixed ? T(0) : s[d];
             } else if (MODE == MODE_DEFECT) {
-                out[dof] = fixed ? T(0) : f[dof] - s[d];
+                out[dof] = fixed ? T(0) : fe[d] - s[d];
             } else {
-                const T r = fixed ? T(0) : f[dof] - s[d];
+                const T r = fixed ? T(0) : fe[d] - s[d];
                 T us;
                 if (MODE == MODE_JACOBI_PRE) {
-                    us = prerelax * f[dof] * rdiag[dof];
+                    us = prerelax * fe[d] * re[d];
                 } else {
-                    us = u[dof];
+                    us = ue[d];
                 }
-                out[dof] = us + omega * r * rdiag[dof];
+                out[dof] = us + omega * r * re[d];
             }
         }
     }
