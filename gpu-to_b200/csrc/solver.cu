@@ -56,7 +56,7 @@ Solver::~Solver()
 {
     if (own_stream) cudaStreamSynchronize(own_stream);
     for (void *p : owned) cudaFree(p);
-    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    drop_graphs();
     if (h_sc) cudaFreeHost(h_sc);
     if (own_stream) cudaStreamDestroy(own_stream);
 }
@@ -228,10 +228,8 @@ int Solver::set_problem(const double *Ke0, const double *fixed1b, int nfd, cudaS
     if (s1) return s1;
     HadamardKe nhk;
     hadamard_ke(Ke, &nhk);
-    if (graph_exec && (nhk.ok != hk.ok || std::memcmp(nhk.c, hk.c, sizeof(hk.c)) != 0)) {
-        cudaGraphExecDestroy(graph_exec);   // the captured sweeps carry the constants
-        graph_exec = nullptr;
-    }
+    if (nhk.ok != hk.ok || std::memcmp(nhk.c, hk.c, sizeof(hk.c)) != 0)
+        drop_graphs();   // the captured sweeps carry the constants
     hk = nhk;
     s1 = upload_quadrature_parts(opt.nu, st);
     if (s1) return s1;
@@ -539,10 +537,7 @@ int Solver::attach_net(Net *n, int mode)
     ref_plain_nit = ref_net_nit = -1;
     net_solves = 0;
     const bool want = net_mode == 1;
-    if (want != net_on && graph_exec) {
-        cudaGraphExecDestroy(graph_exec);
-        graph_exec = nullptr;
-    }
+    if (want != net_on) drop_graphs();
     net_on = want;
     return GPUTO_OK;
 }
@@ -606,10 +601,7 @@ int Solver::solve_begin(const double *Fp, double tol, int maxit, cudaStream_t st
             want = ref_net_nit < ref_plain_nit;
             if (net_solves % 8 == 7) want = !want;
         }
-        if (want != net_on && graph_exec) {
-            cudaGraphExecDestroy(graph_exec);
-            graph_exec = nullptr;
-        }
+        if (want != net_on) drop_graphs();
         net_on = want;
     }
     const long long nv = lay[0].size();
@@ -743,35 +735,60 @@ int Solver::set_tunables(const gputo_options &o)
     opt.tc_parts = o.tc_parts;
     opt.tc_xchunk = o.tc_xchunk;
     opt.fine_op = o.fine_op;
-    if (graph_exec) {
-        cudaGraphExecDestroy(graph_exec);
-        graph_exec = nullptr;
-    }
+    drop_graphs();
     return GPUTO_OK;
 }
 
-// The PCG iteration captured once into a CUDA graph (all pointers are
-// solver-owned, all scalars device-resident), replayed 'batch' times.
+void Solver::drop_graphs()
+{
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph_exec_n) cudaGraphExecDestroy(graph_exec_n);
+    graph_exec = graph_exec_n = nullptr;
+    graph_n = 0;
+}
+
+// 'iters' PCG iterations captured back to back into one executable graph
+// (all pointers are solver-owned, all scalars device-resident; iteration()
+// keeps no host state, so the capture equals 'iters' replays of one).
+int Solver::capture_iterations(int iters, cudaStream_t st, cudaGraphExec_t *exec)
+{
+    cudaGraph_t gr;
+    launch_status = GPUTO_OK;
+    GPUTO_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    for (int b = 0; b < iters; ++b) iteration(st);
+    GPUTO_CUDA(cudaStreamEndCapture(st, &gr));
+    if (launch_status) {
+        cudaGraphDestroy(gr);
+        return launch_status;
+    }
+    cudaError_t e = cudaGraphInstantiate(exec, gr, 0);
+    cudaGraphDestroy(gr);
+    GPUTO_CUDA(e);
+    return GPUTO_OK;
+}
+
+// 'batch' iterations between host checks: one launch of a graph that holds
+// them all (no graph boundary between iterations); a shorter last batch
+// replays the one-iteration graph.
 int Solver::run_graph(int batch, cudaStream_t st)
 {
-    if (!graph_exec || graph_stream != st) {
-        if (graph_exec) {
-            cudaGraphExecDestroy(graph_exec);
-            graph_exec = nullptr;
+    if (graph_stream != st) drop_graphs();
+    graph_stream = st;
+    if (batch > 1 && batch == opt.check_every) {
+        if (!graph_exec_n || graph_n != batch) {
+            if (graph_exec_n) cudaGraphExecDestroy(graph_exec_n);
+            graph_exec_n = nullptr;
+            graph_n = 0;
+            const int s = capture_iterations(batch, st, &graph_exec_n);
+            if (s) return s;
+            graph_n = batch;
         }
-        cudaGraph_t gr;
-        launch_status = GPUTO_OK;
-        GPUTO_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        iteration(st);
-        GPUTO_CUDA(cudaStreamEndCapture(st, &gr));
-        if (launch_status) {
-            cudaGraphDestroy(gr);
-            return launch_status;
-        }
-        cudaError_t e = cudaGraphInstantiate(&graph_exec, gr, 0);
-        cudaGraphDestroy(gr);
-        GPUTO_CUDA(e);
-        graph_stream = st;
+        GPUTO_CUDA(cudaGraphLaunch(graph_exec_n, st));
+        return GPUTO_OK;
+    }
+    if (!graph_exec) {
+        const int s = capture_iterations(1, st, &graph_exec);
+        if (s) return s;
     }
     for (int b = 0; b < batch; ++b) GPUTO_CUDA(cudaGraphLaunch(graph_exec, st));
     return GPUTO_OK;

@@ -51,7 +51,11 @@ struct Solver {
     double *e2 = nullptr;         // (|F - K U|^2, compliance) of energy()
     int launch_status = GPUTO_OK;   // first failure seen while enqueuing kernels
 
-    cudaGraphExec_t graph_exec = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;     // one PCG iteration
+    cudaGraphExec_t graph_exec_n = nullptr;   // graph_n iterations back to back (a host-check interval)
+    int graph_n = 0;
+    void drop_graphs();
+    int capture_iterations(int iters, cudaStream_t st, cudaGraphExec_t *exec);
     cudaStream_t graph_stream = nullptr;
 
     // learned coarse-grid correction (mixed precision, nl >= 3): z += P P net(R R r)
