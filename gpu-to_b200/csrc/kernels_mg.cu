@@ -672,7 +672,7 @@ void launch_build_level1(const Grid &gc, const double *CXfine, double *Apk, cuda
 // A_E = sum_c Pc^T A_c Pc with the 8x8 node weights Pc.  One CTA of 576
 // threads per coarse element; thread t owns entry (t/24, t%24).  The eight
 // children's packed matrices (2,400 values) are staged in shared memory by
-// one round of independent loads (a plane's eight children side by side, so
+// one batch of independent loads (a plane's eight children side by side, so
 // the two y-neighbours share a sector) before the products, and so are the
 // 512 node weights (a warp reads up to 8 different weights at once, which
 // constant memory would serialise).
